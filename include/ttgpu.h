@@ -1,0 +1,174 @@
+/* libttgpu: B200-native TT rounding and AMEn inner loop behind a C ABI.
+ *
+ * Plain pointers and sizes only.  Column-major FP64 arrays throughout, in the
+ * layouts of TT-Toolbox (paths relative to the TT-Toolbox source tree):
+ *   TT tensor core k : [r_k, n_k, r_{k+1}]        (@tt_tensor/core2cell.m:9-11)
+ *   TT matrix core k : [r_k, n_k, m_k, r_{k+1}]   (@tt_matrix/core2cell.m:9-11)
+ *   flat core vector : cores concatenated, offsets ps (@tt_tensor/tt_tensor.m:33-41)
+ *
+ * Conventions
+ *   - Every function returns TTG_OK (0) or an error code; ttg_last_error()
+ *     gives a message for the calling thread.  Nothing aborts the process.
+ *   - Handles (ttg_context, ttg_tt) are owned by the library; host buffers are
+ *     borrowed for the duration of the call; *_download copies out.
+ *   - One context = one device and one CUDA stream.  Calls are synchronous at
+ *     the ABI.  A context must not be used by two threads at once.
+ *   - Kernel-level entries (ttg_local_matvec, ttg_next_phi, ttg_local_solve)
+ *     take DEVICE pointers of the context's device.
+ */
+#ifndef TTGPU_H
+#define TTGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TTG_OK = 0,
+  TTG_ERR_INVALID = 1,     /* bad argument / inconsistent shapes            */
+  TTG_ERR_CUDA = 2,        /* CUDA runtime error                            */
+  TTG_ERR_SOLVER = 3,      /* cuSOLVER error or LAPACK info != 0            */
+  TTG_ERR_NOCONV = 4,      /* iteration cap reached without convergence     */
+  TTG_ERR_ALLOC = 5,       /* device allocation failed                      */
+  TTG_ERR_TIMEOUT = 6,     /* a bounded device-side wait gave up            */
+  TTG_ERR_UNSUPPORTED = 7  /* option value not implemented                  */
+};
+
+/* Arithmetic of the contractions.  TTG_FP64: everything in FP64 (parity mode).
+ * TTG_MIXED: local matvecs / Phi contractions on BF16 tensor cores with FP32
+ * accumulation inside the Krylov solver, FP64 residuals and refinement,
+ * FP64 QR/SVD. */
+enum { TTG_FP64 = 0, TTG_MIXED = 1 };
+
+typedef struct ttg_context_s* ttg_context;
+typedef struct ttg_tt_s* ttg_tt;
+
+/* ---- library / context --------------------------------------------------- */
+const char* ttg_last_error(void);
+int ttg_version(void);
+int ttg_context_create(int device, ttg_context* out);
+int ttg_context_destroy(ttg_context ctx);
+int ttg_context_sync(ttg_context ctx);
+
+/* Device memory helpers for callers without an allocator of their own. */
+int ttg_malloc(ttg_context ctx, size_t bytes, void** out);
+int ttg_free(ttg_context ctx, void* p);
+int ttg_memcpy_h2d(ttg_context ctx, void* dst_dev, const void* src_host, size_t bytes);
+int ttg_memcpy_d2h(ttg_context ctx, void* dst_host, const void* src_dev, size_t bytes);
+
+/* ---- device-resident TT tensors / matrices -------------------------------
+ * Replaces the MATLAB objects built by @tt_tensor/tt_tensor.m:33-41 and
+ * @tt_matrix/tt_matrix.m:33-40.  m == NULL makes a TT tensor, otherwise a TT
+ * matrix with row sizes n and column sizes m.  r has d+1 entries.  The flat
+ * core is copied from host memory. */
+int ttg_tt_upload(ttg_context ctx, int64_t d, const int64_t* n, const int64_t* m,
+                  const int64_t* r, const double* core_host, ttg_tt* out);
+/* Any output pointer may be NULL.  n, m: d entries; r: d+1 entries. */
+int ttg_tt_shape(ttg_tt t, int64_t* d, int64_t* n, int64_t* m, int64_t* r,
+                 int64_t* numel);
+int ttg_tt_download(ttg_tt t, double* core_host);
+int ttg_tt_free(ttg_tt t);
+
+/* ---- TT rounding ----------------------------------------------------------
+ * Replaces tt = round(tt, eps[, rmax])  (@tt_tensor/round.m:1, algorithm
+ * round.m:20-108 with my_chop2, core/my_chop2.m:18-35): left-to-right QR
+ * sweep, right-to-left truncated SVD sweep with threshold
+ * eps/sqrt(d-1)*||s||, then norm balancing.  rmax: NULL (no cap), one value
+ * (nrmax == 1) or d+1 values.  *out is a new handle. */
+typedef struct {
+  double ms_total;     /* device time of the whole rounding            */
+  double ms_qr_sweep;  /* left-to-right QR sweep                       */
+  double ms_svd_sweep; /* right-to-left SVD sweep                      */
+  int64_t max_rank;    /* max rank of the result                       */
+} ttg_round_stats;
+
+int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax,
+              int32_t precision, ttg_tt* out, ttg_round_stats* stats);
+
+/* ---- AMEn solve -----------------------------------------------------------
+ * Replaces [x,testdata,z] = amen_solve2(A, y, tol, 'name', value, ...)
+ * (solve/amen_solve2.m:1, options :75-107,161-203) on the default path:
+ * kicktype 'als', trunc_norm 'residual', local GMRES per fmex/solve3d_2.c
+ * (Householder Arnoldi, fmex/solve3d.c:339-518).  Also the whole-solve seam of
+ * fmex/fort_amen_solve_mex.F90:20-21.
+ * x0 / z0 may be NULL: then a right-orthogonal random TT of rank 2 / kickrank
+ * is drawn on the device (the reference's tt_rand(n,d,2,-1),
+ * amen_solve2.m:222-224,250-252; the random stream differs from MATLAB's). */
+typedef struct {
+  int64_t nswp;          /* 50   */
+  int64_t rmax;          /* 1000 */
+  int64_t max_full_size; /* 50   */
+  int64_t local_restart; /* 40   */
+  int64_t local_iters;   /* 2    */
+  int64_t kickrank;      /* 4    */
+  double resid_damp;     /* 2    */
+  double tol_exit;       /* <= 0: tol                       */
+  int32_t trunc_norm;    /* 1 = 'residual' (only value supported) */
+  int32_t local_prec;    /* 0 = '' (only value supported)   */
+  int32_t precision;     /* TTG_FP64 or TTG_MIXED           */
+  int32_t verb;          /* 0 silent, 1 per-sweep line on stderr */
+  uint64_t seed;         /* seed for device-drawn x0/z0     */
+} ttg_amen_opts;
+
+#define TTG_MAX_SWEEPS_RECORDED 64
+typedef struct {
+  int64_t sweeps;
+  int64_t matvecs;        /* local matvecs in the working precision      */
+  int64_t matvecs_fp64;   /* FP64 local matvecs (residual checks)        */
+  int64_t local_solves;
+  int64_t gmres_iters;
+  int64_t max_rank;
+  double max_res[TTG_MAX_SWEEPS_RECORDED]; /* per sweep, amen_solve2.m:521 */
+  double max_dx[TTG_MAX_SWEEPS_RECORDED];
+  double ms_total;
+  double ms_matvec;       /* device time inside local matvecs (if timed)  */
+  double matvec_gflop;    /* algorithmic FLOPs of all local matvecs / 1e9 */
+} ttg_amen_stats;
+
+void ttg_amen_opts_default(ttg_amen_opts* opts);
+int ttg_amen_solve(ttg_tt A, ttg_tt y, double tol, const ttg_amen_opts* opts,
+                   ttg_tt x0, ttg_tt z0, ttg_tt* x_out, ttg_amen_stats* stats);
+
+/* ---- kernel-level entries (device pointers) --------------------------------
+ * Local matvec y = (Phi1 x A x Phi2) x, the reference's bfun3
+ * (solve/amen_solve2.m:924-951; twin fmex/solve3d.c:141-195).
+ * Phi1 [rx1, rx1, ra1], A [ra1, n, n, ra2], Phi2 [rx2, ra2, rx2],
+ * x, y [rx1, n, rx2].  x and y must not overlap. */
+int ttg_local_matvec(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2,
+                     int64_t ra1, int64_t ra2, const double* Phi1,
+                     const double* A, const double* Phi2, const double* x,
+                     double* y, int32_t precision);
+
+/* Interface update, the reference's compute_next_Phi
+ * (solve/amen_solve2.m:834-920).  dir 0 = 'lr': Phi_prev [rx1, ry1, ra1] ->
+ * Phi_out [rx2, ry2, ra2];  dir 1 = 'rl': Phi_prev [ry2, ra2, rx2] ->
+ * Phi_out [ry1, ra1, rx1].  x [rx1, n, rx2], y [ry1, n, ry2],
+ * A [ra1, n, n, ra2] or NULL (then ra1 = ra2 = 1, the X'Y variant).
+ * If nrm_out != NULL the result is divided by its Frobenius norm, which is
+ * returned in *nrm_out (host), as with nargout > 1 (:907-914). */
+int ttg_next_phi(ttg_context ctx, int32_t dir, int64_t rx1, int64_t n,
+                 int64_t rx2, int64_t ry1, int64_t ry2, int64_t ra1,
+                 int64_t ra2, const double* Phi_prev, const double* x,
+                 const double* A, const double* y, double* Phi_out,
+                 double* nrm_out);
+
+/* Local solve with the signature of the MEX gateway
+ * sol = solve3d_2(Phi1, A, Phi2, rhs, tol, trunc_norm, sol_prev, prec,
+ *                 nrestart, niters, verb)       (fmex/solve3d_2.c:121-122)
+ * Residual branch (trunc_norm = 1) only; prec must be 0.  tol is relative to
+ * ||rhs|| as in the MEX (fmex/solve3d_2.c:263-267).  nrestart is clamped to
+ * rx1*n*rx2 (:184).  *iters_out (nullable) receives the Krylov iterations. */
+int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2,
+                    int64_t ra1, int64_t ra2, const double* Phi1,
+                    const double* A, const double* Phi2, const double* rhs,
+                    double tol, int32_t trunc_norm, const double* sol_prev,
+                    int32_t prec, int64_t nrestart, int64_t niters,
+                    double* sol_out, int32_t precision, int64_t* iters_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TTGPU_H */

@@ -1,0 +1,212 @@
+"""GPU parity of the FP64 path against the oracle, through the C ABI.
+
+Tolerances (FP64 mode): kernel-level results within 1e-12 relative; whole
+solves/roundings within 1e-10 relative (gauge-invariant: compared as full
+tensors or through TT differences), ranks identical.
+"""
+import numpy as np
+import pytest
+
+import ttgpu
+from oracle import amen as oamen
+from oracle.builders import aniso_config, kron_sum_operator, lap1d, laplace_config, round_config
+from oracle.round import tt_round
+from golden_io import load_fixture
+from oracle.tt import TT, TTMatrix, tt_norm, tt_rand, tt_randn, true_residual
+
+pytestmark = pytest.mark.gpu
+
+KERNEL_TOL = 1e-12
+SOLVE_TOL = 1e-10
+
+
+def host_tt(t):
+    return ttgpu.TensorTrain(t.n, t.r, t.flat())
+
+
+def host_mat(A):
+    return ttgpu.TTMatrix(A.n, A.m, A.r, A.flat())
+
+
+def back(t):
+    return TT.from_flat(t.n, t.r, t.core)
+
+
+def rel(a, b):
+    return np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300)
+
+
+def tt_rel(x, ref):
+    return tt_norm(x - ref) / tt_norm(ref)
+
+
+SHAPES = [(1, 4, 2, 1, 2), (3, 5, 7, 2, 3), (33, 17, 65, 3, 2), (70, 9, 64, 2, 3),
+          (64, 64, 64, 3, 3), (128, 32, 128, 2, 2)]
+
+
+@pytest.mark.parametrize("rx1,n,rx2,ra1,ra2", SHAPES)
+def test_local_matvec_parity(ctx, rx1, n, rx2, ra1, ra2):
+    rng = np.random.default_rng(rx1 * 1000 + n)
+    Phi1 = rng.standard_normal((rx1, rx1, ra1))
+    A = rng.standard_normal((ra1, n, n, ra2))
+    Phi2 = rng.standard_normal((rx2, ra2, rx2))
+    x = rng.standard_normal(rx1 * n * rx2)
+    y = ttgpu.bfun3(Phi1, A, Phi2, x, ctx=ctx)
+    assert rel(y, oamen.bfun3(Phi1, A, Phi2, x)) < KERNEL_TOL
+
+
+@pytest.mark.parametrize("direction", ["lr", "rl"])
+@pytest.mark.parametrize("withA", [True, False])
+@pytest.mark.parametrize("rx1,n,rx2,ry1,ry2,ra1,ra2",
+                         [(3, 4, 5, 2, 3, 2, 3), (40, 16, 33, 4, 4, 3, 3), (64, 32, 64, 64, 64, 2, 2)])
+def test_next_phi_parity(ctx, direction, withA, rx1, n, rx2, ry1, ry2, ra1, ra2):
+    rng = np.random.default_rng(rx1 + 7 * ry1 + (1 if withA else 0))
+    x = rng.standard_normal((rx1, n, rx2))
+    y = rng.standard_normal((ry1, n, ry2))
+    A = rng.standard_normal((ra1, n, n, ra2)) if withA else None
+    if direction == "lr":
+        P = rng.standard_normal((rx1, ry1, ra1) if withA else (rx1, ry1))
+    else:
+        P = rng.standard_normal((ry2, ra2, rx2) if withA else (ry2, rx2))
+    ref, _ = oamen.compute_next_Phi(P, x, A, y, direction)
+    got = ttgpu.compute_next_Phi(P, x, A, y, direction, ctx=ctx)
+    assert got.shape == ref.shape
+    assert rel(got, ref) < KERNEL_TOL
+    refn, nrm_ref = oamen.compute_next_Phi(P, x, A, y, direction, want_norm=True)
+    gotn, nrm = ttgpu.compute_next_Phi(P, x, A, y, direction, want_norm=True, ctx=ctx)
+    assert nrm == pytest.approx(nrm_ref, rel=1e-12)
+    assert rel(gotn, refn) < KERNEL_TOL
+
+
+def _local_system(rng, rx1, n, rx2, shift=10.0):
+    """A well-posed local system: Laplacian core between SPD-ish interfaces."""
+    A = kron_sum_operator([lap1d(n) / (n + 1) ** 2] * 3).cores[1]
+    Phi1 = rng.standard_normal((rx1, rx1, 2)) * 0.1
+    Phi1 = Phi1 + np.transpose(Phi1, (1, 0, 2))
+    Phi1[:, :, 1] += shift * np.eye(rx1)
+    Phi2 = rng.standard_normal((rx2, 2, rx2)) * 0.1
+    Phi2 = Phi2 + np.transpose(Phi2, (2, 1, 0))
+    Phi2[:, 0, :] += shift * np.eye(rx2)
+    return Phi1, A, Phi2
+
+
+@pytest.mark.parametrize("rx1,n,rx2,tol,nrestart,niters",
+                         [(4, 8, 5, 1e-10, 40, 2), (16, 16, 12, 1e-6, 20, 3), (30, 32, 30, 1e-12, 40, 2)])
+def test_local_solve_parity(ctx, rx1, n, rx2, tol, nrestart, niters):
+    rng = np.random.default_rng(11 + rx1)
+    Phi1, A, Phi2 = _local_system(rng, rx1, n, rx2)
+    sz = rx1 * n * rx2
+    rhs = rng.standard_normal(sz)
+    sol_prev = rng.standard_normal(sz) * 0.01
+    st = {}
+    ref = oamen.solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, nrestart, niters, st)
+    info = {}
+    got = ttgpu.solve3d_2(Phi1, A, Phi2, rhs, tol, 1, sol_prev, 0, nrestart, niters, 0, ctx=ctx,
+                          info=info)
+    assert rel(got, ref) < 1e-10
+    assert info["iters"] >= 1
+
+
+def test_local_solve_rejects_bad_shapes(ctx):
+    with pytest.raises(ttgpu.TTGError, match="ra1 in Phi1 and A"):
+        ttgpu.solve3d_2(np.zeros((2, 2, 2)), np.zeros((3, 4, 4, 1)), np.zeros((2, 1, 2)),
+                        np.zeros(16), 1e-6, 1, np.zeros(16), ctx=ctx)
+    with pytest.raises(ttgpu.TTGError) as e:
+        ttgpu.solve3d_2(np.ones((2, 2, 1)), np.ones((1, 4, 4, 1)), np.ones((2, 1, 2)),
+                        np.ones(16), 1e-6, 0, np.ones(16), ctx=ctx)
+    assert e.value.code == 1
+
+
+@pytest.mark.parametrize("cfg", [dict(d=6, n=4, r=3, terms=3, seed=7, eps=1e-12),
+                                 dict(d=8, n=6, r=8, terms=2, seed=9, eps=1e-10),
+                                 dict(d=5, n=16, r=24, terms=4, seed=4, eps=1e-8)])
+def test_round_parity(ctx, cfg):
+    x = round_config(d=cfg["d"], n=cfg["n"], r=cfg["r"], terms=cfg["terms"], seed=cfg["seed"])
+    ref, info = tt_round(x, cfg["eps"])
+    got = back(ttgpu.round(host_tt(x), cfg["eps"], ctx=ctx))
+    assert list(got.r) == list(ref.r)
+    assert tt_rel(got, ref) < SOLVE_TOL
+    assert tt_rel(got, x) <= max(cfg["eps"], 1e-13)
+
+
+def test_round_rmax_and_full_tensor(ctx):
+    x = round_config(d=5, n=3, r=4, terms=2, seed=5)
+    ref, _ = tt_round(x, 1e-14, 3)
+    got = back(ttgpu.round(host_tt(x), 1e-14, rmax=3, ctx=ctx))
+    assert list(got.r) == list(ref.r)
+    assert rel(got.full(), ref.full()) < SOLVE_TOL
+    # d+1 rmax values
+    rm = [1, 2, 3, 3, 2, 1]
+    ref2, _ = tt_round(x, 1e-14, rm)
+    got2 = back(ttgpu.round(host_tt(x), 1e-14, rmax=rm, ctx=ctx))
+    assert list(got2.r) == list(ref2.r)
+
+
+def _amen_pair(ctx, A, y, x0, z0, tol, **opts):
+    ref, info = oamen.amen_solve2(A, y, tol, x0, z0, **opts)
+    st = {}
+    got = ttgpu.amen_solve2(host_mat(A), host_tt(y), tol, x0=host_tt(x0), z0=host_tt(z0),
+                            ctx=ctx, stats=st, **opts)
+    return ref, info, back(got), st
+
+
+def test_amen_parity_laplace_small(ctx):
+    A, y, x0, z0 = laplace_config(d=4, n=8)
+    ref, info, got, st = _amen_pair(ctx, A, y, x0, z0, 1e-8, rmax=20, nswp=8)
+    assert st["sweeps"] == info["sweeps"]
+    assert list(got.r) == list(ref.r)
+    assert tt_rel(got, ref) < SOLVE_TOL
+
+
+def test_amen_parity_dense_branch(ctx):
+    """n=4: the local systems are below max_full_size, exercising B \\ rhs."""
+    A, y, x0, z0 = laplace_config(d=5, n=4)
+    ref, info, got, st = _amen_pair(ctx, A, y, x0, z0, 1e-9, nswp=6)
+    assert list(got.r) == list(ref.r)
+    assert tt_rel(got, ref) < SOLVE_TOL
+
+
+def test_amen_parity_config1(ctx):
+    """The reference's CPU-runnable workload: d=8, n=32 Laplacian, tol 1e-6, rmax 20."""
+    A, y, x0, z0 = laplace_config(d=8, n=32)
+    ref, info, got, st = _amen_pair(ctx, A, y, x0, z0, 1e-6, rmax=20)
+    assert st["sweeps"] == info["sweeps"]
+    assert list(got.r) == list(ref.r)
+    assert tt_rel(got, ref) < SOLVE_TOL
+    assert true_residual(A, got, y) < 1e-5
+    np.testing.assert_allclose(st["max_res"], info["max_res"], rtol=1e-6)
+
+
+def test_amen_parity_aniso_rank3(ctx):
+    A, y, x0, z0 = aniso_config(d=5, n=16)
+    ref, info, got, st = _amen_pair(ctx, A, y, x0, z0, 1e-8, rmax=24, nswp=6)
+    assert list(got.r) == list(ref.r)
+    assert tt_rel(got, ref) < SOLVE_TOL
+
+
+def test_amen_device_drawn_initial_guess(ctx):
+    A, y, x0, z0 = laplace_config(d=6, n=16)
+    st = {}
+    got = back(ttgpu.amen_solve2(host_mat(A), host_tt(y), 1e-6, rmax=20, ctx=ctx, stats=st))
+    assert st["max_res"][-1] < 1e-6
+    assert true_residual(A, got, y) < 1e-5
+
+
+def test_amen_fixture_refinement(ctx):
+    """From the reference's stored solution of its ex2 system, two AMEn sweeps
+    keep the published residual (tests/tt-solve/README:15-16)."""
+    A, rhs, xs, stored = load_fixture("ex2")
+    got = back(ttgpu.amen_solve2(host_mat(A), host_tt(rhs), 1e-6, x0=host_tt(xs),
+                                 z0=host_tt(tt_rand(A.n, A.d, 4, np.random.default_rng(0), -1)),
+                                 nswp=2, ctx=ctx))
+    assert true_residual(A, got, rhs) < stored
+
+
+def test_amen_errors(ctx):
+    A, y, x0, z0 = laplace_config(d=3, n=4)
+    Ar = TTMatrix([c[:, :, :3, :] for c in A.cores])
+    with pytest.raises(ttgpu.TTGError, match="rectangular"):
+        ttgpu.amen_solve2(host_mat(Ar), host_tt(y), 1e-6, ctx=ctx)
+    with pytest.raises(ttgpu.TTGError) as e:
+        ttgpu.amen_solve2(host_mat(A), host_tt(y), 1e-6, kicktype="svd", ctx=ctx)
+    assert e.value.code == 7

@@ -1,0 +1,550 @@
+// AMEn solver on the device: restates solve/amen_solve2.m:67-831 on its
+// default option path (kicktype 'als', trunc_norm 'residual', no local
+// preconditioner, MEX local solver).  All cores, interfaces (Phi) and local
+// vectors live on the device; the host keeps ranks, the norm bookkeeping
+// scalars (nrmsa/nrmsy/nrmsx/nrmsc) and the truncation decisions.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "amen.h"
+#include "linalg.h"
+#include "mixed.h"
+#include "round.h"
+
+namespace ttg {
+
+LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, const double* A,
+                             const double* Phi2, const double* rhs, double tol,
+                             const double* sol_prev, int64_t nrestart, int64_t niters,
+                             double* sol, int precision) {
+  if (precision == TTG_MIXED)
+    return local_solve_mixed(c, d, Phi1, A, Phi2, rhs, tol, sol_prev, nrestart, niters, sol);
+  LocalSolveResult out;
+  const int64_t sz = d.in_size();
+  if (nrestart > sz) nrestart = sz;                                   // solve3d_2.c:184
+  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size()), dres(c, sz);
+  auto mv = [&](const double* x, double* y) {
+    local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
+  };
+  mv(sol_prev, dres.p());                                             // solve3d_2.c:257
+  out.matvecs_fp64++;
+  axpby_f64(c, sz, 1.0, rhs, -1.0, dres.p());                         // :259-262
+  DBuf<double> s2(c, 2);
+  dot_f64(c, sz, dres.p(), nullptr, s2.p(), true);
+  dot_f64(c, sz, rhs, nullptr, s2.p() + 1, true);
+  double h[2];
+  read_scalars(c, s2.p(), h, 2);
+  double tol_prev = h[0] / h[1];                                      // :263
+  if (tol_prev < tol) tol_prev = tol;                                 // :264
+  GmresResult g = gmres_hh_f64(c, mv, dres.p(), sz, nrestart, tol / tol_prev, niters, sol);  // :267
+  axpby_f64(c, sz, 1.0, sol_prev, 1.0, sol);                          // :277-278
+  out.iters = g.iters;
+  out.matvecs_fp64 += g.matvecs;
+  return out;
+}
+
+namespace {
+
+struct Core {
+  DBuf<double> buf;
+  double* p() const { return buf.p(); }
+};
+
+// ||B x - rhs|| / nrhs with the FP64 local matvec (res into host).
+double local_residual(Context* c, const MvDims& d, const double* Phi1, const double* A,
+                      const double* Phi2, const double* x, const double* rhs, double nrhs,
+                      double* tmp, double* t1, double* t2) {
+  local_matvec_f64(c, d, Phi1, A, Phi2, x, tmp, t1, t2);
+  DBuf<double> s(c, 1);
+  diffnrm_f64(c, d.out_size(), tmp, rhs, s.p(), true);
+  double h;
+  read_scalars(c, s.p(), &h, 1);
+  return h / nrhs;
+}
+
+double dense_residual(Context* c, int64_t N, const double* B, const double* x, const double* rhs,
+                      double nrhs, double* tmp) {
+  gemm_f64(c, false, false, N, 1, N, 1.0, B, N, 0, x, N, 0, 0.0, tmp, N, 0, 1);
+  DBuf<double> s(c, 1);
+  diffnrm_f64(c, N, tmp, rhs, s.p(), true);
+  double h;
+  read_scalars(c, s.p(), &h, 1);
+  return h / nrhs;
+}
+
+double host_norm(Context* c, int64_t n, const double* x) { return nrm2_host(c, n, x); }
+
+// Normalise in place by the Frobenius norm; returns the norm (1 if zero),
+// as compute_next_Phi with nargout > 1 (amen_solve2.m:907-914).
+double normalize(Context* c, int64_t n, double* x) {
+  double nrm = host_norm(c, n, x);
+  if (nrm > 0) {
+    axpby_f64(c, n, 1.0 / nrm, x, 0.0, x);
+  } else {
+    nrm = 1.0;
+  }
+  return nrm;
+}
+
+}  // namespace
+
+ttg_tt_s* tt_rand_device(Context* c, const std::vector<int64_t>& n, int64_t r, uint64_t seed) {
+  const int64_t d = int64_t(n.size());
+  std::vector<int64_t> rr(d + 1, r);
+  rr[0] = 1;
+  rr[d] = 1;
+  std::vector<DBuf<double>> cores(d);
+  uint64_t off = 0;
+  for (int64_t i = d - 1; i >= 0; --i) {           // tt_rand.m:52-57 (RL)
+    const int64_t m = n[i] * rr[i + 1], k0 = rr[i];
+    DBuf<double> G(c, m * k0);
+    randn_f64(c, m * k0, seed, off, G.p());
+    off += uint64_t(m * k0);
+    const int64_t k = std::min(m, k0);
+    DBuf<double> Q(c, m * k), R(c, k * k0);
+    qr_f64(c, m, k0, G.p(), Q.p(), R.p());
+    rr[i] = k;
+    cores[i].reset(c, k * m);
+    transpose_f64(c, m, k, Q.p(), m, cores[i].p(), k);
+  }
+  auto* t = new ttg_tt_s();
+  t->ctx = c;
+  t->d = d;
+  t->is_matrix = false;
+  t->n = n;
+  t->r = rr;
+  t->ps.assign(d + 1, 0);
+  for (int64_t k = 0; k < d; ++k) t->ps[k + 1] = t->ps[k] + rr[k] * n[k] * rr[k + 1];
+  t->numel = t->ps[d];
+  t->core = static_cast<double*>(c->alloc->get(sizeof(double) * t->numel));
+  for (int64_t k = 0; k < d; ++k) copy_f64(c, t->ps[k + 1] - t->ps[k], cores[k].p(), t->core + t->ps[k]);
+  sync(c);
+  return t;
+}
+
+ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts& o,
+                     ttg_tt_s* x0h, ttg_tt_s* z0h, ttg_amen_stats* stats) {
+  Context* c = Ah->ctx;
+  TTG_REQUIRE(Ah->is_matrix, "A must be a TT matrix");
+  TTG_REQUIRE(!yh->is_matrix, "y must be a TT tensor");
+  TTG_REQUIRE(yh->ctx == c, "A and y belong to different contexts");
+  TTG_REQUIRE(Ah->d == yh->d, "A.d != y.d");
+  const int64_t d = yh->d;
+  TTG_REQUIRE(d >= 2, "amen_solve needs d >= 2");
+  for (int64_t k = 0; k < d; ++k) {
+    TTG_REQUIRE(Ah->n[k] == Ah->m[k],
+                "AMEn does not know how to solve rectangular systems (core %lld)", (long long)k);  // :216-218
+    TTG_REQUIRE(Ah->n[k] == yh->n[k], "mode size mismatch at core %lld", (long long)k);
+  }
+  TTG_REQUIRE(Ah->r[0] == 1 && Ah->r[d] == 1 && yh->r[0] == 1 && yh->r[d] == 1,
+              "border ranks must be 1");
+  TTG_REQUIRE(o.trunc_norm == 1, "only trunc_norm 'residual' is implemented");
+  TTG_REQUIRE(o.local_prec == 0, "local preconditioners are not implemented");
+  TTG_REQUIRE(o.precision == TTG_FP64 || o.precision == TTG_MIXED, "unknown precision %d",
+              o.precision);
+  TTG_REQUIRE(o.nswp >= 1 && o.local_restart >= 1 && o.local_iters >= 1 && o.rmax >= 1 &&
+                  o.kickrank >= 0,
+              "invalid options");
+  const std::vector<int64_t> n = yh->n;
+  const int64_t nswp = o.nswp, rmax = o.rmax, max_full_size = o.max_full_size;
+  const int64_t kickrank = o.kickrank;
+  const double resid_damp = o.resid_damp;
+  const double tol_exit = o.tol_exit > 0 ? o.tol_exit : tol;            // :156-158
+  const bool use_z = kickrank > 0;                                      // :246
+
+  cudaEvent_t e0, e1;
+  TTG_CUDA(cudaEventCreate(&e0));
+  TTG_CUDA(cudaEventCreate(&e1));
+  TTG_CUDA(cudaEventRecord(e0, c->stream));
+  const int64_t mv0 = c->matvecs, fl0 = c->matvec_flops;
+
+  // Initial guesses (:222-224, :250-252).
+  ttg_tt_s* x0own = nullptr;
+  ttg_tt_s* z0own = nullptr;
+  if (!x0h) x0h = x0own = tt_rand_device(c, n, 2, o.seed);
+  if (use_z && !z0h) z0h = z0own = tt_rand_device(c, n, kickrank, o.seed ^ 0x5bd1e995ull);
+  TTG_REQUIRE(x0h->d == d && !x0h->is_matrix, "x0 shape mismatch");
+  for (int64_t k = 0; k < d; ++k) TTG_REQUIRE(x0h->n[k] == n[k], "x0 mode size mismatch");
+  if (use_z) {
+    TTG_REQUIRE(z0h->d == d && !z0h->is_matrix, "z0 shape mismatch");
+    for (int64_t k = 0; k < d; ++k) TTG_REQUIRE(z0h->n[k] == n[k], "z0 mode size mismatch");
+  }
+
+  std::vector<int64_t> rx = x0h->r, ry = yh->r, ra = Ah->r, rz;
+  std::vector<Core> crx(d), crz(d);
+  for (int64_t k = 0; k < d; ++k) {
+    const int64_t sz = x0h->ps[k + 1] - x0h->ps[k];
+    crx[k].buf.reset(c, sz);
+    copy_f64(c, sz, x0h->core + x0h->ps[k], crx[k].p());
+  }
+  if (use_z) {
+    rz = z0h->r;
+    for (int64_t k = 0; k < d; ++k) {
+      const int64_t sz = z0h->ps[k + 1] - z0h->ps[k];
+      crz[k].buf.reset(c, sz);
+      copy_f64(c, sz, z0h->core + z0h->ps[k], crz[k].p());
+    }
+  }
+  if (x0own) ttg_tt_free(x0own);
+  if (z0own) ttg_tt_free(z0own);
+  auto cry = [&](int64_t k) { return yh->core + yh->ps[k]; };
+  auto crA = [&](int64_t k) { return Ah->core + Ah->ps[k]; };
+
+  std::vector<Core> phia(d + 1), phiy(d + 1), phiza(d + 1), phizy(d + 1);
+  for (int64_t k : {int64_t(0), d}) {                                   // :243-249
+    for (auto* v : {&phia, &phiy, &phiza, &phizy}) {
+      (*v)[k].buf.reset(c, 1);
+      fill_f64(c, 1, 1.0, (*v)[k].p());
+    }
+  }
+  std::vector<double> nrmsa(d - 1, 1.0), nrmsy(d - 1, 1.0), nrmsx(d - 1, 1.0);  // :277-279
+  double nrmsc = 1.0;                                                   // :282
+  bool last_sweep = false;
+  int64_t local_solves = 0, gmres_iters = 0, mv_fp64 = 0;
+  int64_t swp_done = 0;
+  std::vector<double> hs;
+
+  for (int64_t swp = 1; swp <= nswp; ++swp) {                           // :296
+    // ------------- right-to-left orthogonalisation (:299-438)
+    int64_t rznew = 0;
+    for (int64_t i = d - 1; i >= 1; --i) {
+      if (use_z && !last_sweep) {                                       // :301-324
+        DBuf<double> zt;  // (n*rz_{i+1}) x k, to be orthogonalised
+        int64_t kz = 0;
+        const int64_t ncols = n[i] * rz[i + 1];
+        if (swp > 1) {
+          MvDims zd{rz[i], rx[i], ra[i], n[i], n[i], rx[i + 1], ra[i + 1], rz[i + 1]};
+          DBuf<double> crzAt(c, zd.out_size());
+          local_matvec_f64(c, zd, phiza[i].p(), crA(i), phiza[i + 1].p(), crx[i].p(), crzAt.p());
+          mv_fp64++;
+          DBuf<double> t(c, rz[i] * n[i] * ry[i + 1]), crzy(c, rz[i] * n[i] * rz[i + 1]);
+          gemm_f64(c, false, false, rz[i], n[i] * ry[i + 1], ry[i], 1.0, phizy[i].p(), rz[i], 0,
+                   cry(i), ry[i], 0, 0.0, t.p(), rz[i], 0, 1);
+          gemm_f64(c, false, false, rz[i] * n[i], rz[i + 1], ry[i + 1], 1.0, t.p(), rz[i] * n[i], 0,
+                   phizy[i + 1].p(), ry[i + 1], 0, 0.0, crzy.p(), rz[i] * n[i], 0, 1);
+          axpby_f64(c, zd.out_size(), -1.0, crzAt.p(), nrmsc, crzy.p());  // crzy*nrmsc - crzAt
+          const int64_t K = std::min(rz[i], ncols);
+          DBuf<double> U(c, rz[i] * K), S(c, K), VT(c, K * ncols);
+          svd_f64(c, rz[i], ncols, crzy.p(), U.p(), S.p(), VT.p());       // :311
+          kz = std::min(kickrank, K);                                     // :312
+          zt.reset(c, ncols * kz);
+          transpose_f64(c, kz, ncols, VT.p(), K, zt.p(), ncols);
+        } else {
+          kz = rz[i];
+          zt.reset(c, ncols * kz);
+          transpose_f64(c, rz[i], ncols, crz[i].p(), rz[i], zt.p(), ncols);  // :317
+        }
+        const int64_t kq = std::min(ncols, kz);
+        DBuf<double> Q(c, ncols * kq), R(c, kq * kz);
+        qr_f64(c, ncols, kz, zt.p(), Q.p(), R.p());                      // :320
+        rznew = kq;
+        crz[i].buf.reset(c, kq * ncols);
+        transpose_f64(c, ncols, kq, Q.p(), ncols, crz[i].p(), kq);       // :322-323
+      }
+      if (swp > 1) nrmsc = nrmsc / (nrmsy[i - 1] / (nrmsa[i - 1] * nrmsx[i - 1]));  // :325-328
+      // QR of x_i^T (:331-342)
+      const int64_t ncols = n[i] * rx[i + 1];
+      DBuf<double> crT(c, ncols * rx[i]);
+      transpose_f64(c, rx[i], ncols, crx[i].p(), rx[i], crT.p(), ncols);
+      const int64_t kq = std::min(ncols, rx[i]);
+      DBuf<double> Q(c, ncols * kq), rv(c, kq * rx[i]);
+      qr_f64(c, ncols, rx[i], crT.p(), Q.p(), rv.p());
+      // cr2 = x_{i-1} * rv^T (:347-349)
+      const int64_t m2 = rx[i - 1] * n[i - 1];
+      DBuf<double> cr2(c, m2 * kq);
+      gemm_f64(c, false, true, m2, kq, rx[i], 1.0, crx[i - 1].p(), m2, 0, rv.p(), kq, 0, 0.0,
+               cr2.p(), m2, 0, 1);
+      double curnorm = host_norm(c, m2 * kq, cr2.p());                   // :351-357
+      if (curnorm > 0)
+        axpby_f64(c, m2 * kq, 1.0 / curnorm, cr2.p(), 0.0, cr2.p());
+      else
+        curnorm = 1.0;
+      nrmsx[i - 1] *= curnorm;
+      rx[i] = kq;                                                         // :359
+      crx[i].buf.reset(c, kq * ncols);
+      transpose_f64(c, ncols, kq, Q.p(), ncols, crx[i].p(), kq);          // :360-362
+      crx[i - 1].buf = std::move(cr2);
+      // Interfaces (:364-365)
+      phia[i].buf.reset(c, rx[i] * ra[i] * rx[i]);
+      next_phi_f64(c, 1, rx[i], n[i], rx[i + 1], rx[i], rx[i + 1], ra[i], ra[i + 1],
+                   phia[i + 1].p(), crx[i].p(), crA(i), crx[i].p(), phia[i].p());
+      nrmsa[i - 1] = normalize(c, rx[i] * ra[i] * rx[i], phia[i].p());
+      phiy[i].buf.reset(c, ry[i] * rx[i]);
+      next_phi_f64(c, 1, rx[i], n[i], rx[i + 1], ry[i], ry[i + 1], 1, 1, phiy[i + 1].p(),
+                   crx[i].p(), nullptr, cry(i), phiy[i].p());
+      nrmsy[i - 1] = normalize(c, ry[i] * rx[i], phiy[i].p());
+      nrmsc = nrmsc * (nrmsy[i - 1] / (nrmsa[i - 1] * nrmsx[i - 1]));    // :372
+      if (use_z && !last_sweep) {                                         // :432-436
+        rz[i] = rznew;
+        phiza[i].buf.reset(c, rx[i] * ra[i] * rz[i]);
+        next_phi_f64(c, 1, rz[i], n[i], rz[i + 1], rx[i], rx[i + 1], ra[i], ra[i + 1],
+                     phiza[i + 1].p(), crz[i].p(), crA(i), crx[i].p(), phiza[i].p());
+        axpby_f64(c, rx[i] * ra[i] * rz[i], 1.0 / nrmsa[i - 1], phiza[i].p(), 0.0, phiza[i].p());
+        phizy[i].buf.reset(c, ry[i] * rz[i]);
+        next_phi_f64(c, 1, rz[i], n[i], rz[i + 1], ry[i], ry[i + 1], 1, 1, phizy[i + 1].p(),
+                     crz[i].p(), nullptr, cry(i), phizy[i].p());
+        axpby_f64(c, ry[i] * rz[i], 1.0 / nrmsy[i - 1], phizy[i].p(), 0.0, phizy[i].p());
+      }
+    }
+
+    // ------------- left-to-right solve sweep (:444-791)
+    double max_res = 0.0, max_dx = 0.0;
+    for (int64_t i = 0; i < d; ++i) {
+      const double* Phi1 = phia[i].p();
+      const double* Phi2 = phia[i + 1].p();
+      const double* A1 = crA(i);
+      MvDims md{rx[i], rx[i], ra[i], n[i], n[i], rx[i + 1], ra[i + 1], rx[i + 1]};
+      const int64_t N = md.in_size();
+      const double* sol_prev = crx[i].p();
+      // y1 = y_i * nrmsc (:453); rhs = phiy_i * y1 * phiy_{i+1} (:456-461)
+      const int64_t ysz = ry[i] * n[i] * ry[i + 1];
+      DBuf<double> y1(c, ysz);
+      axpby_f64(c, ysz, nrmsc, cry(i), 0.0, y1.p());
+      DBuf<double> t(c, rx[i] * n[i] * ry[i + 1]), rhs(c, N);
+      gemm_f64(c, false, false, rx[i], n[i] * ry[i + 1], ry[i], 1.0, phiy[i].p(), rx[i], 0,
+               y1.p(), ry[i], 0, 0.0, t.p(), rx[i], 0, 1);
+      gemm_f64(c, false, false, rx[i] * n[i], rx[i + 1], ry[i + 1], 1.0, t.p(), rx[i] * n[i], 0,
+               phiy[i + 1].p(), ry[i + 1], 0, 0.0, rhs.p(), rx[i] * n[i], 0, 1);
+      const double norm_rhs = host_norm(c, N, rhs.p());                  // :462
+      const double real_tol = (tol / std::sqrt(double(d))) / resid_damp; // :466
+      const bool full = N < max_full_size;                                // :468
+      DBuf<double> sol(c, N), tmp(c, N), B, t1(c, md.t1_size()), t2(c, md.t2_size());
+      double res_prev = 0.0, res_new = 0.0;
+      if (full) {
+        B.reset(c, N * N);
+        assemble_local_f64(c, rx[i], n[i], rx[i + 1], ra[i], ra[i + 1], Phi1, A1, Phi2, B.p());
+        res_prev = dense_residual(c, N, B.p(), sol_prev, rhs.p(), norm_rhs, tmp.p());  // :482
+        copy_f64(c, N, rhs.p(), sol.p());
+        lu_solve_f64(c, N, B.p(), sol.p(), 1);                            // :486
+        res_new = dense_residual(c, N, B.p(), sol.p(), rhs.p(), norm_rhs, tmp.p());    // :487
+      } else {
+        res_prev = local_residual(c, md, Phi1, A1, Phi2, sol_prev, rhs.p(), norm_rhs, tmp.p(),
+                                  t1.p(), t2.p());                        // :495
+        mv_fp64++;
+        if (norm_rhs > 0) {                                               // :497
+          LocalSolveResult lr = local_solve(c, md, Phi1, A1, Phi2, rhs.p(), real_tol, sol_prev,
+                                            o.local_restart, o.local_iters, sol.p(),
+                                            o.precision);                 // :501
+          local_solves++;
+          gmres_iters += lr.iters;
+          mv_fp64 += lr.matvecs_fp64;
+          res_new = local_residual(c, md, Phi1, A1, Phi2, sol.p(), rhs.p(), norm_rhs, tmp.p(),
+                                   t1.p(), t2.p());                       // :504
+          mv_fp64++;
+        } else {
+          fill_f64(c, N, 0.0, sol.p());
+          res_new = 0.0;
+        }
+      }
+      {
+        DBuf<double> s(c, 2);
+        diffnrm_f64(c, N, sol.p(), sol_prev, s.p(), true);
+        dot_f64(c, N, sol.p(), nullptr, s.p() + 1, true);
+        double h[2];
+        read_scalars(c, s.p(), h, 2);
+        const double dx = h[1] > 0 ? h[0] / h[1] : 0.0;                    // :519
+        max_dx = std::max(max_dx, dx);
+        max_res = std::max(max_res, res_prev);                            // :521
+      }
+      // Truncation (:530-601)
+      const int64_t M = rx[i] * n[i], r2 = rx[i + 1];
+      DBuf<double> u, v;  // u: M x r ; v: r2 x r
+      int64_t r = 0;
+      if (kickrank >= 0 && i < d - 1) {
+        const int64_t K = std::min(M, r2);
+        DBuf<double> U(c, M * K), S(c, K), VT(c, K * r2);
+        svd_f64(c, M, r2, sol.p(), U.p(), S.p(), VT.p());                // :533
+        hs.resize(K);
+        TTG_CUDA(cudaMemcpyAsync(hs.data(), S.p(), sizeof(double) * K, cudaMemcpyDeviceToHost,
+                                 c->stream));
+        sync(c);
+        const double thr = std::max(real_tol * resid_damp, res_new);
+        int64_t rr = 0;
+        bool any = false;
+        DBuf<double> us(c, M * K), cursol(c, M * r2);
+        for (rr = K - 1; rr >= 1; --rr) {                                 // :539-550
+          any = true;
+          copy2d_f64(c, M, rr, U.p(), M, us.p(), M, S.p());
+          gemm_f64(c, false, false, M, r2, rr, 1.0, us.p(), M, 0, VT.p(), K, 0, 0.0, cursol.p(),
+                   M, 0, 1);
+          double res;
+          if (full) {
+            res = dense_residual(c, N, B.p(), cursol.p(), rhs.p(), norm_rhs, tmp.p());
+          } else {
+            res = local_residual(c, md, Phi1, A1, Phi2, cursol.p(), rhs.p(), norm_rhs, tmp.p(),
+                                 t1.p(), t2.p());
+            mv_fp64++;
+          }
+          if (res > thr) break;
+        }
+        if (any && rr < 1) rr = 1;  // MATLAB leaves the loop variable at 1
+        r = (any ? rr : K - 1) + 1;                                       // :551
+        r = std::min(r, K);                                               // :593
+        r = std::min(r, rmax);                                            // :594
+        u.reset(c, M * r);
+        copy_f64(c, M * r, U.p(), u.p());                                 // :603
+        v.reset(c, r2 * r);                                               // :604 v = V(:,1:r)*diag(s)
+        DBuf<double> vtmp(c, r2 * r);
+        transpose_f64(c, r, r2, VT.p(), K, vtmp.p(), r2);
+        copy2d_f64(c, r2, r, vtmp.p(), r2, v.p(), r2, S.p());
+      } else {                                                             // :596-601
+        const int64_t K = std::min(M, r2);
+        DBuf<double> Q(c, M * K), R(c, K * r2);
+        qr_f64(c, M, r2, sol.p(), Q.p(), R.p());
+        r = K;
+        u = std::move(Q);
+        v.reset(c, r2 * K);
+        transpose_f64(c, K, r2, R.p(), K, v.p(), r2);
+      }
+
+      DBuf<double> uv;
+      if ((use_z && !last_sweep) || (i < d - 1 && kickrank > 0 && !last_sweep)) {
+        uv.reset(c, M * r2);
+        gemm_f64(c, false, true, M, r2, r, 1.0, u.p(), M, 0, v.p(), r2, 0, 0.0, uv.p(), M, 0, 1);
+      }
+      if (use_z && !last_sweep) {                                          // :605-623
+        MvDims zd{rz[i], rx[i], ra[i], n[i], n[i], rx[i + 1], ra[i + 1], rz[i + 1]};
+        DBuf<double> crzAt(c, zd.out_size());
+        local_matvec_f64(c, zd, phiza[i].p(), A1, phiza[i + 1].p(), uv.p(), crzAt.p());
+        mv_fp64++;
+        DBuf<double> tz(c, rz[i] * n[i] * ry[i + 1]), crzy(c, rz[i] * n[i] * rz[i + 1]);
+        gemm_f64(c, false, false, rz[i], n[i] * ry[i + 1], ry[i], 1.0, phizy[i].p(), rz[i], 0,
+                 y1.p(), ry[i], 0, 0.0, tz.p(), rz[i], 0, 1);
+        gemm_f64(c, false, false, rz[i] * n[i], rz[i + 1], ry[i + 1], 1.0, tz.p(), rz[i] * n[i], 0,
+                 phizy[i + 1].p(), ry[i + 1], 0, 0.0, crzy.p(), rz[i] * n[i], 0, 1);
+        axpby_f64(c, zd.out_size(), -1.0, crzAt.p(), 1.0, crzy.p());       // :612
+        const int64_t mz = rz[i] * n[i];
+        const int64_t K = std::min(mz, rz[i + 1]);
+        DBuf<double> U(c, mz * K), S(c, K), VT(c, K * rz[i + 1]);
+        svd_f64(c, mz, rz[i + 1], crzy.p(), U.p(), S.p(), VT.p());       // :613
+        const int64_t kz = std::min(kickrank, K);                          // :614
+        const int64_t kq = std::min(mz, kz);
+        DBuf<double> Q(c, mz * kq), R(c, kq * kz);
+        qr_f64(c, mz, kz, U.p(), Q.p(), R.p());                            // :619
+        rznew = kq;
+        crz[i].buf = std::move(Q);                                         // :621-622
+      }
+
+      if (i < d - 1) {                                                     // :625
+        if (kickrank > 0 && !last_sweep) {                                 // :626
+          MvDims ld{rx[i], rx[i], ra[i], n[i], n[i], rx[i + 1], ra[i + 1], rz[i + 1]};
+          DBuf<double> leftresid(c, ld.out_size());
+          local_matvec_f64(c, ld, Phi1, A1, phiza[i + 1].p(), uv.p(), leftresid.p());  // :702
+          mv_fp64++;
+          DBuf<double> ty(c, rx[i] * n[i] * ry[i + 1]), uk(c, M * rz[i + 1]);
+          gemm_f64(c, false, false, rx[i], n[i] * ry[i + 1], ry[i], 1.0, phiy[i].p(), rx[i], 0,
+                   y1.p(), ry[i], 0, 0.0, ty.p(), rx[i], 0, 1);            // :704
+          gemm_f64(c, false, false, M, rz[i + 1], ry[i + 1], 1.0, ty.p(), M, 0, phizy[i + 1].p(),
+                   ry[i + 1], 0, 0.0, uk.p(), M, 0, 1);                     // :706
+          axpby_f64(c, M * rz[i + 1], -1.0, leftresid.p(), 1.0, uk.p());   // :707
+          // [u, rv] = qr([u, uk]) ; v = [v, 0] * rv.'  (:713-716)
+          const int64_t radd = rz[i + 1], wcols = r + radd;
+          DBuf<double> uu(c, M * wcols);
+          copy_f64(c, M * r, u.p(), uu.p());
+          copy_f64(c, M * radd, uk.p(), uu.p() + M * r);
+          const int64_t kq = std::min(M, wcols);
+          DBuf<double> Q(c, M * kq), rv(c, kq * wcols);
+          qr_f64(c, M, wcols, uu.p(), Q.p(), rv.p());
+          // v_new (r2 x kq) = v (r2 x r) * rv(:, 1:r)^T  (the zero block drops out)
+          DBuf<double> vn(c, r2 * kq);
+          gemm_f64(c, false, true, r2, kq, r, 1.0, v.p(), r2, 0, rv.p(), kq, 0, 0.0, vn.p(), r2, 0,
+                   1);
+          u = std::move(Q);
+          v = std::move(vn);
+          r = kq;
+        }
+        // v = v.' * x_{i+1}  (:732-734)
+        const int64_t nc = n[i + 1] * rx[i + 2];
+        DBuf<double> vx(c, r * nc);
+        gemm_f64(c, true, false, r, nc, r2, 1.0, v.p(), r2, 0, crx[i + 1].p(), r2, 0, 0.0, vx.p(),
+                 r, 0, 1);
+        nrmsc = nrmsc / (nrmsy[i] / (nrmsa[i] * nrmsx[i]));               // :737
+        double curnorm = host_norm(c, r * nc, vx.p());                     // :739-745
+        if (curnorm > 0)
+          axpby_f64(c, r * nc, 1.0 / curnorm, vx.p(), 0.0, vx.p());
+        else
+          curnorm = 1.0;
+        nrmsx[i] *= curnorm;
+        // Interfaces (:751-752)
+        phia[i + 1].buf.reset(c, r * r * ra[i + 1]);
+        next_phi_f64(c, 0, rx[i], n[i], r, rx[i], r, ra[i], ra[i + 1], phia[i].p(), u.p(), A1,
+                     u.p(), phia[i + 1].p());
+        nrmsa[i] = normalize(c, r * r * ra[i + 1], phia[i + 1].p());
+        phiy[i + 1].buf.reset(c, r * ry[i + 1]);
+        next_phi_f64(c, 0, rx[i], n[i], r, ry[i], ry[i + 1], 1, 1, phiy[i].p(), u.p(), nullptr,
+                     cry(i), phiy[i + 1].p());
+        nrmsy[i] = normalize(c, r * ry[i + 1], phiy[i + 1].p());
+        nrmsc = nrmsc * (nrmsy[i] / (nrmsa[i] * nrmsx[i]));               // :754
+        rx[i + 1] = r;                                                     // :765-767
+        crx[i].buf = std::move(u);
+        crx[i + 1].buf = std::move(vx);
+        if (use_z && !last_sweep) {                                        // :770-774
+          rz[i + 1] = rznew;
+          phiza[i + 1].buf.reset(c, rz[i + 1] * rx[i + 1] * ra[i + 1]);
+          next_phi_f64(c, 0, rz[i], n[i], rz[i + 1], rx[i], rx[i + 1], ra[i], ra[i + 1],
+                       phiza[i].p(), crz[i].p(), A1, crx[i].p(), phiza[i + 1].p());
+          axpby_f64(c, rz[i + 1] * rx[i + 1] * ra[i + 1], 1.0 / nrmsa[i], phiza[i + 1].p(), 0.0,
+                    phiza[i + 1].p());
+          phizy[i + 1].buf.reset(c, rz[i + 1] * ry[i + 1]);
+          next_phi_f64(c, 0, rz[i], n[i], rz[i + 1], ry[i], ry[i + 1], 1, 1, phizy[i].p(),
+                       crz[i].p(), nullptr, cry(i), phizy[i + 1].p());
+          axpby_f64(c, rz[i + 1] * ry[i + 1], 1.0 / nrmsy[i], phizy[i + 1].p(), 0.0,
+                    phizy[i + 1].p());
+        }
+      } else {
+        crx[i].buf = std::move(sol);                                       // :778-779
+      }
+    }
+    swp_done = swp;
+    int64_t maxr = 0;
+    for (auto v : rx) maxr = std::max(maxr, v);
+    if (stats && swp <= TTG_MAX_SWEEPS_RECORDED) {
+      stats->max_res[swp - 1] = max_res;
+      stats->max_dx[swp - 1] = max_dx;
+    }
+    if (o.verb > 0)
+      fprintf(stderr, "=amen_solve= sweep %lld, max_dx: %3.3e, max_res: %3.3e, max_rank: %lld\n",
+              (long long)swp, max_dx, max_res, (long long)maxr);            // :793-795
+    if (last_sweep) break;                                                 // :797-799
+    if (max_res < tol_exit) last_sweep = true;                             // :806-808
+  }
+
+  // Distribute the norms (:816-820) and assemble the output.
+  double lsum = 0.0;
+  for (double v : nrmsx) lsum += std::log(v);
+  const double nx = std::exp(lsum / double(d));
+  auto* out = new ttg_tt_s();
+  out->ctx = c;
+  out->d = d;
+  out->is_matrix = false;
+  out->n = n;
+  out->r = rx;
+  out->ps.assign(d + 1, 0);
+  for (int64_t k = 0; k < d; ++k) out->ps[k + 1] = out->ps[k] + rx[k] * n[k] * rx[k + 1];
+  out->numel = out->ps[d];
+  out->core = static_cast<double*>(c->alloc->get(sizeof(double) * out->numel));
+  for (int64_t k = 0; k < d; ++k)
+    axpby_f64(c, out->ps[k + 1] - out->ps[k], nx, crx[k].p(), 0.0, out->core + out->ps[k]);
+  TTG_CUDA(cudaEventRecord(e1, c->stream));
+  TTG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (stats) {
+    stats->sweeps = swp_done;
+    stats->matvecs = c->matvecs - mv0;
+    stats->matvecs_fp64 = mv_fp64;
+    stats->local_solves = local_solves;
+    stats->gmres_iters = gmres_iters;
+    int64_t mr = 0;
+    for (auto v : rx) mr = std::max(mr, v);
+    stats->max_rank = mr;
+    stats->ms_total = ms;
+    stats->matvec_gflop = double(c->matvec_flops - fl0) * 1e-9;
+  }
+  return out;
+}
+
+}  // namespace ttg

@@ -1,0 +1,28 @@
+#pragma once
+#include "gmres.h"
+
+namespace ttg {
+
+// Local solve with the semantics of the MEX gateway solve3d_2, residual branch
+// (fmex/solve3d_2.c:254-279): dres = rhs - B sol_prev, GMRES on dres with
+// tolerance tol / max(||dres||/||rhs||, tol), sol = sol_prev + dsol.
+// precision TTG_FP64 runs dgmresr_hh on FP64 matvecs; TTG_MIXED runs the
+// low-precision Krylov solver inside an FP64 refinement loop.
+struct LocalSolveResult {
+  int64_t iters = 0;
+  int64_t matvecs = 0;
+  int64_t matvecs_fp64 = 0;
+};
+LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, const double* A,
+                             const double* Phi2, const double* rhs, double tol,
+                             const double* sol_prev, int64_t nrestart, int64_t niters,
+                             double* sol, int precision);
+
+ttg_tt_s* amen_solve(ttg_tt_s* A, ttg_tt_s* y, double tol, const ttg_amen_opts& o,
+                     ttg_tt_s* x0, ttg_tt_s* z0, ttg_amen_stats* stats);
+
+// Right-orthogonal random TT of rank r (tt_rand(n,d,r,-1), core/tt_rand.m:40-62)
+// with entries from the device hash generator.
+ttg_tt_s* tt_rand_device(Context* c, const std::vector<int64_t>& n, int64_t r, uint64_t seed);
+
+}  // namespace ttg

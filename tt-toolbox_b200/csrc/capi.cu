@@ -1,0 +1,126 @@
+// extern "C" entry points of the hot path (include/ttgpu.h).
+#include <cmath>
+
+#include "amen.h"
+#include "linalg.h"
+#include "round.h"
+
+using namespace ttg;
+
+extern "C" {
+
+void ttg_amen_opts_default(ttg_amen_opts* o) {
+  if (!o) return;
+  o->nswp = 50;            // amen_solve2.m:79
+  o->rmax = 1000;          // :87
+  o->max_full_size = 50;   // :75
+  o->local_restart = 40;   // :80
+  o->local_iters = 2;      // :81
+  o->kickrank = 4;         // :102
+  o->resid_damp = 2.0;     // :77
+  o->tol_exit = 0.0;       // :92, :156-158
+  o->trunc_norm = 1;       // :88-89
+  o->local_prec = 0;       // :83-84
+  o->precision = TTG_FP64;
+  o->verb = 0;
+  o->seed = 0x243F6A8885A308D3ull;
+}
+
+int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax, int32_t precision,
+              ttg_tt* out, ttg_round_stats* stats) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(in && out, "NULL argument");
+  TTG_REQUIRE(std::isfinite(eps) && eps >= 0, "eps must be finite and >= 0");
+  TTG_REQUIRE(rmax == nullptr || nrmax == 1 || nrmax == in->d + 1,
+              "rmax must have 1 or d+1 entries");
+  TTG_CUDA(cudaSetDevice(in->ctx->device));
+  std::vector<int64_t> rm;
+  if (rmax) {
+    rm.assign(rmax, rmax + nrmax);
+    for (auto v : rm) TTG_REQUIRE(v >= 1, "rmax entries must be >= 1");
+  }
+  *out = round_tt(in, eps, rm, precision, stats);
+  TTG_API_END
+}
+
+int ttg_amen_solve(ttg_tt A, ttg_tt y, double tol, const ttg_amen_opts* opts, ttg_tt x0,
+                   ttg_tt z0, ttg_tt* x_out, ttg_amen_stats* stats) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(A && y && x_out, "NULL argument");
+  TTG_REQUIRE(std::isfinite(tol) && tol > 0, "tol must be > 0");
+  ttg_amen_opts o;
+  if (opts)
+    o = *opts;
+  else
+    ttg_amen_opts_default(&o);
+  if (stats) *stats = ttg_amen_stats{};
+  TTG_CUDA(cudaSetDevice(A->ctx->device));
+  if (x0) TTG_REQUIRE(x0->ctx == A->ctx, "x0 belongs to another context");
+  if (z0) TTG_REQUIRE(z0->ctx == A->ctx, "z0 belongs to another context");
+  *x_out = amen_solve(A, y, tol, o, x0, z0, stats);
+  TTG_API_END
+}
+
+int ttg_local_matvec(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
+                     int64_t ra2, const double* Phi1, const double* A, const double* Phi2,
+                     const double* x, double* y, int32_t precision) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && Phi1 && A && Phi2 && x && y, "NULL argument");
+  TTG_REQUIRE(rx1 >= 1 && n >= 1 && rx2 >= 1 && ra1 >= 1 && ra2 >= 1, "sizes must be >= 1");
+  TTG_REQUIRE(precision == TTG_FP64, "ttg_local_matvec: precision %d not available",
+              precision);
+  Context* c = &ctx->c;
+  TTG_CUDA(cudaSetDevice(c->device));
+  MvDims d{rx1, rx1, ra1, n, n, rx2, ra2, rx2};
+  local_matvec_f64(c, d, Phi1, A, Phi2, x, y);
+  sync(c);
+  TTG_API_END
+}
+
+int ttg_next_phi(ttg_context ctx, int32_t dir, int64_t rx1, int64_t n, int64_t rx2, int64_t ry1,
+                 int64_t ry2, int64_t ra1, int64_t ra2, const double* Phi_prev, const double* x,
+                 const double* A, const double* y, double* Phi_out, double* nrm_out) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && Phi_prev && x && y && Phi_out, "NULL argument");
+  TTG_REQUIRE(dir == 0 || dir == 1, "dir must be 0 ('lr') or 1 ('rl')");
+  TTG_REQUIRE(rx1 >= 1 && n >= 1 && rx2 >= 1 && ry1 >= 1 && ry2 >= 1, "sizes must be >= 1");
+  if (A) TTG_REQUIRE(ra1 >= 1 && ra2 >= 1, "ra sizes must be >= 1");
+  Context* c = &ctx->c;
+  TTG_CUDA(cudaSetDevice(c->device));
+  const int64_t cnt =
+      next_phi_f64(c, dir, rx1, n, rx2, ry1, ry2, ra1, ra2, Phi_prev, x, A, y, Phi_out);
+  if (nrm_out) {
+    double nrm = nrm2_host(c, cnt, Phi_out);
+    if (nrm > 0)
+      axpby_f64(c, cnt, 1.0 / nrm, Phi_out, 0.0, Phi_out);
+    else
+      nrm = 1.0;
+    *nrm_out = nrm;
+  }
+  sync(c);
+  TTG_API_END
+}
+
+int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
+                    int64_t ra2, const double* Phi1, const double* A, const double* Phi2,
+                    const double* rhs, double tol, int32_t trunc_norm, const double* sol_prev,
+                    int32_t prec, int64_t nrestart, int64_t niters, double* sol_out,
+                    int32_t precision, int64_t* iters_out) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && Phi1 && A && Phi2 && rhs && sol_prev && sol_out, "NULL argument");
+  TTG_REQUIRE(rx1 >= 1 && n >= 1 && rx2 >= 1 && ra1 >= 1 && ra2 >= 1, "sizes must be >= 1");
+  TTG_REQUIRE(trunc_norm == 1, "only the residual branch (trunc_norm = 1) is implemented");
+  TTG_REQUIRE(prec == 0, "local preconditioners are not implemented");
+  TTG_REQUIRE(nrestart >= 1 && niters >= 1, "nrestart and niters must be >= 1");
+  TTG_REQUIRE(std::isfinite(tol) && tol > 0, "tol must be > 0");
+  Context* c = &ctx->c;
+  TTG_CUDA(cudaSetDevice(c->device));
+  MvDims d{rx1, rx1, ra1, n, n, rx2, ra2, rx2};
+  LocalSolveResult r =
+      local_solve(c, d, Phi1, A, Phi2, rhs, tol, sol_prev, nrestart, niters, sol_out, precision);
+  sync(c);
+  if (iters_out) *iters_out = r.iters;
+  TTG_API_END
+}
+
+}  // extern "C"

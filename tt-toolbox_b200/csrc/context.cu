@@ -1,0 +1,278 @@
+// Context, caching allocator, error reporting and TT handles of libttgpu.
+#include <cstdarg>
+#include <cstring>
+
+#include "internal.h"
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+namespace ttg {
+
+void fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw Error{code, std::string(buf)};
+}
+
+Allocator::~Allocator() {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device_);
+  for (auto& kv : free_)
+    for (void* p : kv.second) cudaFree(p);
+  for (auto& kv : live_) cudaFree(kv.first);
+  cudaSetDevice(prev);
+}
+
+size_t Allocator::size_class(size_t bytes) {
+  // 256-byte granularity below 1 MiB, then 1/8-octave classes.
+  if (bytes < 256) return 256;
+  if (bytes <= (1u << 20)) return (bytes + 255) & ~size_t(255);
+  size_t p = 1;
+  while (p < bytes) p <<= 1;
+  size_t step = p >> 3;
+  return ((bytes + step - 1) / step) * step;
+}
+
+void* Allocator::get(size_t bytes) {
+  size_t cls = size_class(bytes);
+  auto it = free_.find(cls);
+  void* p = nullptr;
+  if (it != free_.end() && !it->second.empty()) {
+    p = it->second.back();
+    it->second.pop_back();
+    cached_ -= cls;
+  } else {
+    cudaError_t e = cudaMalloc(&p, cls);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      // Give cached blocks back and retry once.
+      for (auto& kv : free_) {
+        for (void* q : kv.second) cudaFree(q);
+        kv.second.clear();
+      }
+      cached_ = 0;
+      e = cudaMalloc(&p, cls);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(TTG_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", cls, cudaGetErrorString(e));
+      }
+    }
+  }
+  live_[p] = cls;
+  in_use_ += cls;
+  return p;
+}
+
+void Allocator::put(void* p) {
+  auto it = live_.find(p);
+  if (it == live_.end()) return;
+  size_t cls = it->second;
+  live_.erase(it);
+  in_use_ -= cls;
+  free_[cls].push_back(p);
+  cached_ += cls;
+}
+
+void set_last_error(const char* msg) { g_last_error = msg; }
+
+void sync(Context* c) { TTG_CUDA(cudaStreamSynchronize(c->stream)); }
+
+void read_scalars(Context* c, const double* d, double* h, int count) {
+  TTG_CUDA(cudaMemcpyAsync(c->h_scal, d, sizeof(double) * count, cudaMemcpyDeviceToHost,
+                           c->stream));
+  TTG_CUDA(cudaStreamSynchronize(c->stream));
+  memcpy(h, c->h_scal, sizeof(double) * count);
+}
+
+}  // namespace ttg
+
+using namespace ttg;
+
+// ---------------------------------------------------------------------------
+// C ABI: library, context, memory
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+const char* ttg_last_error(void) { return g_last_error.c_str(); }
+
+int ttg_version(void) { return 10000; }
+
+int ttg_context_create(int device, ttg_context* out) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(out != nullptr, "out is NULL");
+  int ndev = 0;
+  TTG_CUDA(cudaGetDeviceCount(&ndev));
+  TTG_REQUIRE(device >= 0 && device < ndev, "device %d out of range (%d devices)", device, ndev);
+  TTG_CUDA(cudaSetDevice(device));
+  auto* h = new ttg_context_s();
+  Context& c = h->c;
+  c.device = device;
+  TTG_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
+  TTG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  TTG_SOLVER(cusolverDnCreate(&c.solver));
+  TTG_SOLVER(cusolverDnSetStream(c.solver, c.stream));
+  c.alloc = new Allocator(device);
+  TTG_CUDA(cudaMallocHost(&c.h_scal, 4096 * sizeof(double)));
+  TTG_CUDA(cudaMalloc(&c.d_err, 64 * sizeof(int)));
+  TTG_CUDA(cudaMemset(c.d_err, 0, 64 * sizeof(int)));
+  TTG_CUDA(cudaEventCreate(&c.ev0));
+  TTG_CUDA(cudaEventCreate(&c.ev1));
+  *out = h;
+  TTG_API_END
+}
+
+int ttg_context_destroy(ttg_context ctx) {
+  TTG_API_BEGIN
+  if (!ctx) return TTG_OK;
+  Context& c = ctx->c;
+  cudaSetDevice(c.device);
+  cudaStreamSynchronize(c.stream);
+  delete c.alloc;
+  if (c.solver) cusolverDnDestroy(c.solver);
+  if (c.h_scal) cudaFreeHost(c.h_scal);
+  if (c.d_err) cudaFree(c.d_err);
+  if (c.ev0) cudaEventDestroy(c.ev0);
+  if (c.ev1) cudaEventDestroy(c.ev1);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  delete ctx;
+  TTG_API_END
+}
+
+int ttg_context_sync(ttg_context ctx) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx, "ctx is NULL");
+  TTG_CUDA(cudaSetDevice(ctx->c.device));
+  sync(&ctx->c);
+  TTG_API_END
+}
+
+int ttg_malloc(ttg_context ctx, size_t bytes, void** out) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && out, "NULL argument");
+  TTG_CUDA(cudaSetDevice(ctx->c.device));
+  *out = nullptr;
+  if (bytes) {
+    cudaError_t e = cudaMalloc(out, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      fail(TTG_ERR_ALLOC, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+  }
+  TTG_API_END
+}
+
+int ttg_free(ttg_context ctx, void* p) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx, "ctx is NULL");
+  TTG_CUDA(cudaSetDevice(ctx->c.device));
+  if (p) {
+    sync(&ctx->c);
+    TTG_CUDA(cudaFree(p));
+  }
+  TTG_API_END
+}
+
+int ttg_memcpy_h2d(ttg_context ctx, void* dst, const void* src, size_t bytes) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx, "ctx is NULL");
+  TTG_REQUIRE(bytes == 0 || (dst && src), "NULL pointer");
+  TTG_CUDA(cudaSetDevice(ctx->c.device));
+  if (bytes) {
+    TTG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->c.stream));
+    sync(&ctx->c);
+  }
+  TTG_API_END
+}
+
+int ttg_memcpy_d2h(ttg_context ctx, void* dst, const void* src, size_t bytes) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx, "ctx is NULL");
+  TTG_REQUIRE(bytes == 0 || (dst && src), "NULL pointer");
+  TTG_CUDA(cudaSetDevice(ctx->c.device));
+  if (bytes) {
+    TTG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->c.stream));
+    sync(&ctx->c);
+  }
+  TTG_API_END
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: TT handles
+// ---------------------------------------------------------------------------
+
+int ttg_tt_upload(ttg_context ctx, int64_t d, const int64_t* n, const int64_t* m,
+                  const int64_t* r, const double* core, ttg_tt* out) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && n && r && core && out, "NULL argument");
+  TTG_REQUIRE(d >= 1 && d <= 4096, "d = %lld out of range", (long long)d);
+  Context* c = &ctx->c;
+  TTG_CUDA(cudaSetDevice(c->device));
+  auto* t = new ttg_tt_s();
+  t->ctx = c;
+  t->d = d;
+  t->is_matrix = (m != nullptr);
+  t->n.assign(n, n + d);
+  if (m) t->m.assign(m, m + d);
+  t->r.assign(r, r + d + 1);
+  t->ps.assign(d + 1, 0);
+  for (int64_t k = 0; k < d; ++k) {
+    if (n[k] < 1 || (m && m[k] < 1) || r[k] < 1 || r[k + 1] < 1) {
+      delete t;
+      fail(TTG_ERR_INVALID, "non-positive size at core %lld", (long long)k);
+    }
+    int64_t sz = r[k] * n[k] * (m ? m[k] : 1) * r[k + 1];
+    t->ps[k + 1] = t->ps[k] + sz;
+  }
+  t->numel = t->ps[d];
+  t->core = static_cast<double*>(c->alloc->get(sizeof(double) * t->numel));
+  TTG_CUDA(cudaMemcpyAsync(t->core, core, sizeof(double) * t->numel, cudaMemcpyHostToDevice,
+                           c->stream));
+  sync(c);
+  *out = t;
+  TTG_API_END
+}
+
+int ttg_tt_shape(ttg_tt t, int64_t* d, int64_t* n, int64_t* m, int64_t* r, int64_t* numel) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(t, "NULL handle");
+  if (d) *d = t->d;
+  if (n) memcpy(n, t->n.data(), sizeof(int64_t) * t->d);
+  if (m) {
+    if (t->is_matrix)
+      memcpy(m, t->m.data(), sizeof(int64_t) * t->d);
+    else
+      memcpy(m, t->n.data(), sizeof(int64_t) * t->d);
+  }
+  if (r) memcpy(r, t->r.data(), sizeof(int64_t) * (t->d + 1));
+  if (numel) *numel = t->numel;
+  TTG_API_END
+}
+
+int ttg_tt_download(ttg_tt t, double* core) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(t && core, "NULL argument");
+  TTG_CUDA(cudaSetDevice(t->ctx->device));
+  TTG_CUDA(cudaMemcpyAsync(core, t->core, sizeof(double) * t->numel, cudaMemcpyDeviceToHost,
+                           t->ctx->stream));
+  sync(t->ctx);
+  TTG_API_END
+}
+
+int ttg_tt_free(ttg_tt t) {
+  TTG_API_BEGIN
+  if (!t) return TTG_OK;
+  cudaSetDevice(t->ctx->device);
+  cudaStreamSynchronize(t->ctx->stream);
+  t->ctx->alloc->put(t->core);
+  delete t;
+  TTG_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,357 @@
+// Device GMRES with Householder orthogonalisation (FP64).
+//
+// Restates dgmresr_hh (fmex/solve3d.c:339-518).  The Arnoldi work outside
+// the matvec is done by three cooperative kernels, each one launch covering
+// a whole sequence of reflector applications:
+//   hh_build  : v_j = P_0 ... P_{j-1} (P_j e_j), normalised       (:396-406)
+//   hh_tail   : w = P_j ... P_0 (B v_j), next reflector, Givens     (:421-473)
+//   hh_correct: upper-triangular solve and the correction x += Q y  (:487-507)
+// plus hh_init for the restart vector (:376-392).  Each reflector needs a
+// global dot product before its update, so the blocks meet at a grid barrier
+// per reflector; the partial sums are reduced in a fixed order, so results
+// are deterministic run to run.  Every barrier wait is bounded: on timeout
+// the kernel raises the context error flag and runs to completion, and the
+// host returns TTG_ERR_TIMEOUT.
+#include <cmath>
+
+#include "gmres.h"
+
+namespace ttg {
+
+namespace {
+
+constexpr int HH_THREADS = 256;
+constexpr long long BAR_SPIN_LIMIT = 1LL << 24;
+
+struct HhArgs {
+  int64_t sz;
+  int64_t nrestart;
+  double* U;  // sz x (nrestart+1)
+  double* w;
+  double* w2;
+  double* sol;
+  const double* rhs;
+  double* tau;   // nrestart+1
+  double* J;     // 2 x nrestart
+  double* R;     // nrestart x nrestart
+  double* scal;  // [0] nrmrhs [1] curres [2] nrmr [3] exact-flag
+  double* part;  // 2 * gridDim.x
+  unsigned* bar; // [0] count [1] generation [2] reduction parity
+  int* err;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum, result broadcast to every thread.
+__device__ double block_sum_all(double v) {
+  __shared__ double sh[33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double r = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+    r = warp_sum(r);
+    if (threadIdx.x == 0) sh[32] = r;
+  }
+  __syncthreads();
+  return sh[32];
+}
+
+__device__ void grid_barrier(unsigned* bar, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = bar + 1;
+    volatile int* verr = err;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == gen) {
+        if (*verr) break;
+        if (++spins > BAR_SPIN_LIMIT) {
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Grid-wide deterministic sum; every thread of every block gets the result.
+// Partial buffers alternate so one barrier per reduction suffices.
+__device__ double grid_sum(double v, const HhArgs& a, unsigned& parity) {
+  v = block_sum_all(v);
+  double* part = a.part + (parity & 1u) * gridDim.x;
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+  grid_barrier(a.bar, a.err);
+  double s = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(part + i);
+  s = block_sum_all(s);
+  parity ^= 1u;
+  return s;
+}
+
+#define GRID_LOOP(idx, n)                                                           \
+  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < (n);    \
+       idx += int64_t(gridDim.x) * blockDim.x)
+
+// w = rhs - w2 ; U_0 = Householder vector of w ; tau_0 = -beta  (:376-392)
+__global__ void __launch_bounds__(HH_THREADS) k_hh_init(HhArgs a, int it) {
+  unsigned parity = 0;
+  const int64_t sz = a.sz;
+  double s = 0.0;
+  GRID_LOOP(i, sz) {
+    const double v = a.rhs[i] - a.w2[i];
+    a.w[i] = v;
+    s += v * v;
+  }
+  const double nrmr = sqrt(grid_sum(s, a, parity));
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (it == 0) a.scal[0] = nrmr;
+    a.scal[2] = nrmr;
+    a.scal[3] = (nrmr == 0.0) ? 1.0 : 0.0;
+  }
+  if (nrmr == 0.0) return;
+  const double w0 = __ldcg(a.w);
+  const double beta = (w0 < 0.0) ? -nrmr : nrmr;
+  const double nu = sqrt(2.0 * nrmr * nrmr + 2.0 * beta * w0);
+  GRID_LOOP(i, sz) {
+    const double v = (i == 0) ? (a.w[i] + beta) : a.w[i];
+    a.U[i] = v / nu;
+  }
+  if (blockIdx.x == 0) {
+    for (int64_t k = threadIdx.x; k <= a.nrestart; k += blockDim.x) a.tau[k] = 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) a.tau[0] = -beta;
+  }
+}
+
+// v_j = P_0 ... P_{j-1} (P_j e_j), normalised, into w  (:396-406)
+__global__ void __launch_bounds__(HH_THREADS) k_hh_build(HhArgs a, int64_t j) {
+  unsigned parity = 0;
+  const int64_t sz = a.sz;
+  const double* Uj = a.U + j * sz;
+  const double ujj = __ldcg(Uj + j);
+  GRID_LOOP(i, sz) { a.w[i] = -2.0 * ujj * Uj[i] + (i == j ? 1.0 : 0.0); }
+  for (int64_t r = j - 1; r >= 0; --r) {
+    const double* Ur = a.U + r * sz;
+    double s = 0.0;
+    GRID_LOOP(i, sz) s += Ur[i] * a.w[i];
+    const double dot = grid_sum(s, a, parity);
+    GRID_LOOP(i, sz) a.w[i] -= 2.0 * dot * Ur[i];
+  }
+  double s = 0.0;
+  GRID_LOOP(i, sz) s += a.w[i] * a.w[i];
+  const double inv = 1.0 / sqrt(grid_sum(s, a, parity));
+  GRID_LOOP(i, sz) a.w[i] *= inv;
+}
+
+// w2 = P_j ... P_0 w2 ; new reflector U_{j+1} ; Givens ; R(:,j) ; residual (:421-473)
+__global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
+  unsigned parity = 0;
+  const int64_t sz = a.sz;
+  double* w = a.w2;
+  for (int64_t r = 0; r <= j; ++r) {
+    const double* Ur = a.U + r * sz;
+    double s = 0.0;
+    GRID_LOOP(i, sz) s += Ur[i] * w[i];
+    const double dot = grid_sum(s, a, parity);
+    GRID_LOOP(i, sz) w[i] -= 2.0 * dot * Ur[i];
+  }
+  if (j < sz - 1) {
+    double s = 0.0;
+    GRID_LOOP(i, sz) if (i > j) s += w[i] * w[i];
+    double alpha = sqrt(grid_sum(s, a, parity));
+    const double wj1 = __ldcg(w + j + 1);
+    double* Un = a.U + (j + 1) * sz;
+    if (alpha != 0.0) {
+      if (wj1 < 0.0) alpha = -alpha;
+      const double nu = sqrt(2.0 * alpha * alpha + 2.0 * alpha * wj1);
+      GRID_LOOP(i, sz) {
+        double u;
+        if (i <= j)
+          u = 0.0;
+        else if (i == j + 1)
+          u = (w[i] + alpha) / nu;
+        else
+          u = w[i] / nu;
+        Un[i] = u;
+        if (i == j + 1)
+          w[i] = -alpha;
+        else if (i > j + 1)
+          w[i] = 0.0;
+      }
+    } else {
+      GRID_LOOP(i, sz) Un[i] = (i <= j) ? 0.0 : w[i];
+    }
+  }
+  grid_barrier(a.bar, a.err);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // Givens rotations to the top of w (:445-449)
+    for (int64_t i = 0; i < j; ++i) {
+      const double b = __ldcg(w + i), b1 = __ldcg(w + i + 1);
+      const double c0 = a.J[2 * i], c1 = a.J[2 * i + 1];
+      w[i] = c0 * b + c1 * b1;
+      w[i + 1] = -c1 * b + c0 * b1;
+    }
+    if (j < sz - 1) {  // new rotator (:454-465)
+      const double wj = __ldcg(w + j), wj1 = __ldcg(w + j + 1);
+      const double rho = sqrt(wj * wj + wj1 * wj1);
+      const double c0 = wj / rho, c1 = wj1 / rho;
+      a.J[2 * j] = c0;
+      a.J[2 * j + 1] = c1;
+      a.tau[j + 1] = -c1 * a.tau[j];
+      a.tau[j] = c0 * a.tau[j];
+      w[j] = rho;
+      w[j + 1] = 0.0;
+    }
+    for (int64_t k = 0; k < a.nrestart; ++k) a.R[k + j * a.nrestart] = (k < sz) ? __ldcg(w + k) : 0.0;
+    a.scal[1] = fabs(a.tau[j + 1]) / a.scal[0];
+  }
+}
+
+// Triangular solve + correction sol += P_0..P_j (sum y_i e_i)  (:487-507)
+__global__ void __launch_bounds__(HH_THREADS) k_hh_correct(HhArgs a, int64_t j, int64_t ni) {
+  extern __shared__ double y[];
+  unsigned parity = 0;
+  const int64_t sz = a.sz;
+  if (threadIdx.x == 0) {
+    for (int64_t row = ni - 1; row >= 0; --row) {
+      double v = a.tau[row];
+      for (int64_t col = row + 1; col < ni; ++col) v -= a.R[row + col * a.nrestart] * y[col];
+      y[row] = v / a.R[row + row * a.nrestart];
+    }
+  }
+  __syncthreads();
+  const double* Uj = a.U + j * sz;
+  const double ujj = __ldcg(Uj + j);
+  const double yj = y[j];
+  GRID_LOOP(i, sz) a.w[i] = -2.0 * ujj * yj * Uj[i] + (i == j ? yj : 0.0);
+  for (int64_t r = j - 1; r >= 0; --r) {
+    const double* Ur = a.U + r * sz;
+    double s = 0.0;
+    GRID_LOOP(i, sz) {
+      if (i == r) a.w[i] += y[r];
+      s += Ur[i] * a.w[i];
+    }
+    const double dot = grid_sum(s, a, parity);
+    GRID_LOOP(i, sz) a.w[i] -= 2.0 * dot * Ur[i];
+  }
+  GRID_LOOP(i, sz) a.sol[i] += a.w[i];
+}
+
+int coop_blocks(Context* c, const void* kernel, size_t smem, int64_t sz) {
+  int occ = 0;
+  TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, HH_THREADS, smem));
+  if (occ < 1) occ = 1;
+  int64_t want = (sz + HH_THREADS * 4 - 1) / (HH_THREADS * 4);
+  int64_t cap = int64_t(c->num_sms) * std::min(occ, 2);
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  return int(want);
+}
+
+void launch_coop(Context* c, const void* kernel, int blocks, size_t smem, void** args) {
+  TTG_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(HH_THREADS), args, smem,
+                                       c->stream));
+  c->launches += 1;
+}
+
+}  // namespace
+
+GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, int64_t sz,
+                         int64_t nrestart, double tol, int64_t niters, double* sol) {
+  GmresResult res;
+  TTG_REQUIRE(nrestart >= 1 && nrestart <= 4096, "nrestart %lld out of range",
+              (long long)nrestart);
+  DBuf<double> U(c, size_t(sz) * (nrestart + 1)), w(c, sz), w2(c, sz);
+  DBuf<double> small(c, (nrestart + 1) + 2 * nrestart + nrestart * nrestart + 8);
+  const int blocks = std::min(
+      std::min(coop_blocks(c, (const void*)k_hh_init, 0, sz), coop_blocks(c, (const void*)k_hh_build, 0, sz)),
+      std::min(coop_blocks(c, (const void*)k_hh_tail, 0, sz),
+               coop_blocks(c, (const void*)k_hh_correct, sizeof(double) * nrestart, sz)));
+  DBuf<double> part(c, 2 * blocks);
+  DBuf<unsigned> bar(c, 4);
+  TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 4 * sizeof(unsigned), c->stream));
+  TTG_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+
+  HhArgs a;
+  a.sz = sz;
+  a.nrestart = nrestart;
+  a.U = U.p();
+  a.w = w.p();
+  a.w2 = w2.p();
+  a.sol = sol;
+  a.rhs = rhs;
+  a.tau = small.p();
+  a.J = a.tau + (nrestart + 1);
+  a.R = a.J + 2 * nrestart;
+  a.scal = a.R + nrestart * nrestart;
+  a.part = part.p();
+  a.bar = bar.p();
+  a.err = c->d_err;
+  fill_f64(c, sz, 0.0, sol);
+
+  double curres = INFINITY;
+  for (int64_t it = 0; it < niters; ++it) {
+    apply(sol, w2.p());
+    res.matvecs++;
+    int itv = int(it);
+    void* args_init[] = {&a, &itv};
+    launch_coop(c, (const void*)k_hh_init, blocks, 0, args_init);
+    double hs[4];
+    read_scalars(c, a.scal, hs, 4);
+    if (hs[3] != 0.0) {  // exact solution: nothing to correct
+      curres = 0.0;
+      break;
+    }
+    bool broke = false;
+    int64_t j = 0;
+    for (j = 0; j < nrestart; ++j) {
+      void* args_b[] = {&a, &j};
+      launch_coop(c, (const void*)k_hh_build, blocks, 0, args_b);
+      apply(w.p(), w2.p());
+      res.matvecs++;
+      void* args_t[] = {&a, &j};
+      launch_coop(c, (const void*)k_hh_tail, blocks, 0, args_t);
+      res.iters++;
+      read_scalars(c, a.scal + 1, &curres, 1);
+      if (curres < tol) {
+        broke = true;
+        break;
+      }
+    }
+    int64_t ni;
+    if (!broke) {
+      j = nrestart - 1;
+      ni = nrestart;
+    } else {
+      ni = j + 1;
+    }
+    void* args_c[] = {&a, &j, &ni};
+    launch_coop(c, (const void*)k_hh_correct, blocks, sizeof(double) * nrestart, args_c);
+    if (curres < tol) break;
+  }
+  int herr = 0;
+  TTG_CUDA(cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  if (herr) fail(TTG_ERR_TIMEOUT, "GMRES grid barrier timed out");
+  res.relres = curres;
+  return res;
+}
+
+}  // namespace ttg

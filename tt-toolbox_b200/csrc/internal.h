@@ -1,0 +1,177 @@
+// Internal declarations of libttgpu (not part of the C-ABI).
+//
+// One context = one device, one stream, one cuSOLVER handle and one caching
+// device allocator.  All kernels of a context run on its stream.  Host code
+// reports failures by throwing ttg::Error; every extern "C" entry point
+// catches and converts to a status code + message (include/ttgpu.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/ttgpu.h"
+
+namespace ttg {
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int code, const char* fmt, ...);
+
+#define TTG_CUDA(call)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      ::ttg::fail(TTG_ERR_CUDA, "%s:%d: %s: %s", __FILE__, __LINE__, #call,         \
+                  cudaGetErrorString(e_));                                          \
+  } while (0)
+
+#define TTG_SOLVER(call)                                                            \
+  do {                                                                              \
+    cusolverStatus_t s_ = (call);                                                   \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                              \
+      ::ttg::fail(TTG_ERR_SOLVER, "%s:%d: %s: cusolver status %d", __FILE__,        \
+                  __LINE__, #call, (int)s_);                                        \
+  } while (0)
+
+#define TTG_CHECK_LAUNCH() TTG_CUDA(cudaGetLastError())
+
+#define TTG_REQUIRE(cond, ...)                                                      \
+  do {                                                                              \
+    if (!(cond)) ::ttg::fail(TTG_ERR_INVALID, __VA_ARGS__);                         \
+  } while (0)
+
+// Caching device allocator: blocks are rounded up to a size class and kept
+// on per-class free lists, so a solve that reaches steady state performs no
+// cudaMalloc.  Not thread-safe (a context is single-threaded by contract).
+class Allocator {
+ public:
+  explicit Allocator(int device) : device_(device) {}
+  ~Allocator();
+  void* get(size_t bytes);
+  void put(void* p);
+  size_t bytes_in_use() const { return in_use_; }
+  size_t bytes_cached() const { return cached_; }
+
+ private:
+  static size_t size_class(size_t bytes);
+  int device_;
+  std::map<size_t, std::vector<void*>> free_;
+  std::map<void*, size_t> live_;
+  size_t in_use_ = 0, cached_ = 0;
+};
+
+struct Context;
+
+// RAII device buffer drawn from a context's allocator.
+template <typename T>
+class DBuf {
+ public:
+  DBuf() = default;
+  DBuf(Context* c, size_t n);
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept { swap(o); }
+  DBuf& operator=(DBuf&& o) noexcept {
+    release();
+    swap(o);
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void reset(Context* c, size_t n);  // reallocate if capacity too small
+  T* p() const { return p_; }
+  size_t size() const { return n_; }
+  void release();
+
+ private:
+  void swap(DBuf& o) {
+    std::swap(c_, o.c_);
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+  }
+  Context* c_ = nullptr;
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+struct Context {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  Allocator* alloc = nullptr;
+  // Small pinned host buffer for scalar read-back.
+  double* h_scal = nullptr;
+  int* d_err = nullptr;  // device error flag (bounded waits)
+  // Counters (reset by the caller through ttg_stats).
+  int64_t launches = 0;
+  int64_t matvecs = 0;
+  int64_t matvec_flops = 0;
+  float ms_matvec = 0.f;
+  // Event timing of the local matvec (optional).
+  bool time_matvec = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+template <typename T>
+DBuf<T>::DBuf(Context* c, size_t n) {
+  reset(c, n);
+}
+template <typename T>
+void DBuf<T>::reset(Context* c, size_t n) {
+  if (c_ == c && n <= n_ && p_) return;
+  release();
+  c_ = c;
+  n_ = n;
+  p_ = n ? static_cast<T*>(c->alloc->get(n * sizeof(T))) : nullptr;
+}
+template <typename T>
+void DBuf<T>::release() {
+  if (p_ && c_) c_->alloc->put(p_);
+  p_ = nullptr;
+  n_ = 0;
+}
+
+void set_last_error(const char* msg);
+
+#define TTG_API_BEGIN try {
+#define TTG_API_END                                    \
+  }                                                    \
+  catch (const ::ttg::Error& e) {                      \
+    ::ttg::set_last_error(e.msg.c_str());              \
+    return e.code;                                     \
+  }                                                    \
+  catch (const std::exception& e) {                    \
+    ::ttg::set_last_error(e.what());                   \
+    return TTG_ERR_INVALID;                            \
+  }                                                    \
+  ::ttg::set_last_error("");                           \
+  return TTG_OK;
+
+// Copy a device scalar (or a few) to the host; synchronises the stream.
+void read_scalars(Context* c, const double* d, double* h, int count);
+void sync(Context* c);
+
+}  // namespace ttg
+
+// TT handle: cores stay resident on the device of the owning context.
+struct ttg_tt_s {
+  ttg::Context* ctx;
+  int64_t d;
+  bool is_matrix;
+  std::vector<int64_t> n, m, r, ps;  // ps: 0-based offsets (d+1)
+  double* core;                      // device, numel doubles
+  int64_t numel;
+};
+
+struct ttg_context_s {
+  ttg::Context c;
+};

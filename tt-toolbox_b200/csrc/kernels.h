@@ -1,0 +1,45 @@
+// Launchers of the device kernels used by the host drivers.
+#pragma once
+#include "internal.h"
+
+namespace ttg {
+
+// C[b] = alpha * op(A[b]) * op(B[b]) + beta * C[b], column-major, FP64.
+//   op(A) is M x K: tA=false -> A(m,k) = A[m + k*lda];  tA=true -> A[k + m*lda]
+//   op(B) is K x N: tB=false -> B(k,n) = B[k + n*ldb];  tB=true -> B[n + k*ldb]
+// Batch b uses A + b*sA, B + b*sB, C + b*sC.  FP64 tensor-core (DMMA) tiles.
+void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, double alpha,
+              const double* A, int64_t lda, int64_t sA, const double* B, int64_t ldb,
+              int64_t sB, double beta, double* C, int64_t ldc, int64_t sC, int64_t batch = 1);
+
+// out = sum(x.*y) (or sum(x.^2) when y == nullptr) into a device scalar;
+// deterministic two-stage reduction.  If do_sqrt, stores sqrt of the sum.
+void dot_f64(Context* c, int64_t n, const double* x, const double* y, double* out,
+             bool do_sqrt = false);
+// Frobenius norm to host (synchronises).
+double nrm2_host(Context* c, int64_t n, const double* x);
+// Squared distance ||x - y||^2 into device scalar (sqrt if requested).
+void diffnrm_f64(Context* c, int64_t n, const double* x, const double* y, double* out,
+                 bool do_sqrt = true);
+
+// y = a*x + b*y ; with a, b host scalars.
+void axpby_f64(Context* c, int64_t n, double a, const double* x, double b, double* y);
+// y = x * s[0] / s[1] style scaling with device scalars: y = x * (num ? *num : 1) / (den ? *den : 1)
+void scale_dev_f64(Context* c, int64_t n, const double* x, double* y, const double* num,
+                   const double* den);
+void fill_f64(Context* c, int64_t n, double v, double* y);
+void copy_f64(Context* c, int64_t n, const double* x, double* y);
+
+// out (cols x rows) = in(rows x cols)^T, column-major, batched with strides.
+void transpose_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_t ldi,
+                   double* out, int64_t ldo, int64_t batch = 1, int64_t si = 0, int64_t so = 0);
+
+// Copy a sub-matrix: out[i + j*ldo] = in[i + j*ldi] * (scale_col ? scale_col[j] : 1)
+void copy2d_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_t ldi,
+                double* out, int64_t ldo, const double* scale_col = nullptr);
+
+// Right-orthogonal random core generator input: N(0,1) entries from a
+// counter-based hash (seed, offset).
+void randn_f64(Context* c, int64_t n, uint64_t seed, uint64_t offset, double* y);
+
+}  // namespace ttg

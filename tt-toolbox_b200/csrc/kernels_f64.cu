@@ -1,0 +1,416 @@
+// FP64 kernels: DMMA-tiled batched GEMM, deterministic reductions,
+// transposes and elementwise helpers.
+//
+// The GEMM is the contraction engine of the FP64 (parity) path: every local
+// matvec (bfun3) and every interface update (compute_next_Phi) is written as
+// three batched column-major GEMMs whose operand layouts need no explicit
+// permutations (see local_ops.cu).  Tiles: 64x64x16 per CTA, 4 warps of
+// 32x32, each warp issuing mma.sync.m8n8k4 f64 (the FP64 tensor path; tcgen05
+// has no FP64 kind).  Global->shared staging with cp.async (8-byte granules so
+// any leading dimension works), double buffered.
+#include "kernels.h"
+
+namespace ttg {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, PADS = 8;
+
+struct GemmP {
+  int64_t M, N, K;
+  const double* A;
+  int64_t lda, sA;
+  const double* B;
+  int64_t ldb, sB;
+  double* C;
+  int64_t ldc, sC;
+  double alpha, beta;
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  int bytes = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
+  __shared__ double As[2][BK][BM + PADS];
+  __shared__ double Bs[2][BK][BN + PADS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t bz = blockIdx.z;
+  const double* __restrict__ A = p.A + bz * p.sA;
+  const double* __restrict__ B = p.B + bz * p.sB;
+  double* __restrict__ C = p.C + bz * p.sC;
+  const int64_t m0 = int64_t(blockIdx.x) * BM, n0 = int64_t(blockIdx.y) * BN;
+  const int64_t M = p.M, N = p.N, K = p.K;
+
+  auto load_tile = [&](int64_t k0, int buf) {
+    if (!TA) {  // m contiguous
+      const int m = tid & 63, kb = tid >> 6;
+      const int64_t gm = m0 + m;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int k = kb + 2 * i;
+        const int64_t gk = k0 + k;
+        const bool ok = gm < M && gk < K;
+        cp_async8(&As[buf][k][m], ok ? A + gm + gk * p.lda : A, ok);
+      }
+    } else {  // k contiguous: A(m,k) = A[k + m*lda]
+      const int k = tid & 15, mb = tid >> 4;
+      const int64_t gk = k0 + k;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int m = mb + 8 * i;
+        const int64_t gm = m0 + m;
+        const bool ok = gm < M && gk < K;
+        cp_async8(&As[buf][k][m], ok ? A + gk + gm * p.lda : A, ok);
+      }
+    }
+    if (!TB) {  // k contiguous: B(k,n) = B[k + n*ldb]
+      const int k = tid & 15, nb = tid >> 4;
+      const int64_t gk = k0 + k;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int n = nb + 8 * i;
+        const int64_t gn = n0 + n;
+        const bool ok = gn < N && gk < K;
+        cp_async8(&Bs[buf][k][n], ok ? B + gk + gn * p.ldb : B, ok);
+      }
+    } else {  // n contiguous: B(k,n) = B[n + k*ldb]
+      const int n = tid & 63, kb = tid >> 6;
+      const int64_t gn = n0 + n;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int k = kb + 2 * i;
+        const int64_t gk = k0 + k;
+        const bool ok = gn < N && gk < K;
+        cp_async8(&Bs[buf][k][n], ok ? B + gn + gk * p.ldb : B, ok);
+      }
+    }
+    cp_async_commit();
+  };
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  const int64_t ktiles = (K + BK - 1) / BK;
+  if (ktiles > 0) load_tile(0, 0);
+  for (int64_t kt = 0; kt < ktiles; ++kt) {
+    const int buf = int(kt & 1);
+    if (kt + 1 < ktiles) {
+      load_tile((kt + 1) * BK, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK / 4; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk * 4 + t][wm + i * 8 + g];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk * 4 + t][wn + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t row = m0 + wm + i * 8 + g;
+    if (row >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int64_t col = n0 + wn + j * 8 + 2 * t + e;
+        if (col < N) {
+          double* dst = C + row + col * p.ldc;
+          double v = p.alpha * acc[i][j][e];
+          if (p.beta != 0.0) v += p.beta * *dst;
+          *dst = v;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
+
+constexpr int RED_THREADS = 256;
+constexpr int RED_MAX_BLOCKS = 1024;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;  // valid in thread 0
+}
+
+// mode 0: sum x*y ; mode 1: sum x^2 ; mode 2: sum (x-y)^2
+__global__ void k_reduce_partial(int64_t n, const double* __restrict__ x,
+                                 const double* __restrict__ y, int mode,
+                                 double* __restrict__ part) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const double a = x[i];
+    if (mode == 0)
+      s += a * y[i];
+    else if (mode == 1)
+      s += a * a;
+    else {
+      const double dlt = a - y[i];
+      s += dlt * dlt;
+    }
+  }
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_reduce_final(int nparts, const double* __restrict__ part, double* out,
+                               int do_sqrt) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) *out = do_sqrt ? sqrt(s) : s;
+}
+
+void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int mode,
+                   double* out, bool do_sqrt) {
+  int nb = int(std::min<int64_t>((n + RED_THREADS * 4 - 1) / (RED_THREADS * 4), RED_MAX_BLOCKS));
+  if (nb < 1) nb = 1;
+  DBuf<double> part(c, nb);
+  k_reduce_partial<<<nb, RED_THREADS, 0, c->stream>>>(n, x, y, mode, part.p());
+  k_reduce_final<<<1, RED_THREADS, 0, c->stream>>>(nb, part.p(), out, do_sqrt ? 1 : 0);
+  c->launches += 2;
+  TTG_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise
+// ---------------------------------------------------------------------------
+
+__global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b,
+                        double* __restrict__ y) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = (b == 0.0 ? 0.0 : b * y[i]) + a * x[i];
+}
+
+__global__ void k_scale_dev(int64_t n, const double* __restrict__ x, double* __restrict__ y,
+                            const double* num, const double* den) {
+  const double s = (num ? *num : 1.0) / (den ? *den : 1.0);
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = x[i] * s;
+}
+
+__global__ void k_fill(int64_t n, double v, double* y) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = v;
+}
+
+__global__ void k_transpose(int64_t rows, int64_t cols, const double* __restrict__ in,
+                            int64_t ldi, int64_t si, double* __restrict__ out, int64_t ldo,
+                            int64_t so) {
+  __shared__ double tile[32][33];
+  const int64_t b = blockIdx.z;
+  in += b * si;
+  out += b * so;
+  const int64_t r0 = int64_t(blockIdx.x) * 32, c0 = int64_t(blockIdx.y) * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int64_t r = r0 + threadIdx.x, cc = c0 + j;
+    if (r < rows && cc < cols) tile[j][threadIdx.x] = in[r + cc * ldi];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int64_t cc = c0 + threadIdx.x, r = r0 + j;
+    if (r < rows && cc < cols) out[cc + r * ldo] = tile[threadIdx.x][j];
+  }
+}
+
+__global__ void k_copy2d(int64_t rows, int64_t cols, const double* __restrict__ in, int64_t ldi,
+                         double* __restrict__ out, int64_t ldo, const double* scale_col) {
+  const int64_t total = rows * cols;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = i % rows, cidx = i / rows;
+    double v = in[r + cidx * ldi];
+    if (scale_col) v *= scale_col[cidx];
+    out[r + cidx * ldo] = v;
+  }
+}
+
+// splitmix64-based counter hash -> two uniforms -> Box-Muller normal.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_randn(int64_t n, uint64_t seed, uint64_t offset, double* y) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const uint64_t h1 = mix64(seed ^ mix64(2 * (offset + i)));
+    const uint64_t h2 = mix64(seed ^ mix64(2 * (offset + i) + 1));
+    const double u1 = (double((h1 >> 11) + 1)) * (1.0 / 9007199254740993.0);
+    const double u2 = double(h2 >> 11) * (1.0 / 9007199254740992.0);
+    y[i] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  }
+}
+
+int grid_for(Context* c, int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  int64_t cap = int64_t(c->num_sms) * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return int(b);
+}
+
+}  // namespace
+
+void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, double alpha,
+              const double* A, int64_t lda, int64_t sA, const double* B, int64_t ldb, int64_t sB,
+              double beta, double* C, int64_t ldc, int64_t sC, int64_t batch) {
+  if (M <= 0 || N <= 0 || batch <= 0) return;
+  if (K <= 0) {
+    // C = beta*C
+    for (int64_t b = 0; b < batch; ++b) {
+      if (beta == 0.0) {
+        for (int64_t j = 0; j < N; ++j) fill_f64(c, M, 0.0, C + b * sC + j * ldc);
+      } else if (beta != 1.0) {
+        for (int64_t j = 0; j < N; ++j) axpby_f64(c, M, 0.0, C + b * sC + j * ldc, beta, C + b * sC + j * ldc);
+      }
+    }
+    return;
+  }
+  TTG_REQUIRE(batch <= 65535, "gemm batch %lld too large", (long long)batch);
+  const int64_t gx = (M + BM - 1) / BM, gy = (N + BN - 1) / BN;
+  TTG_REQUIRE(gy <= 65535 && gx <= 0x7fffffff, "gemm too large");
+  GemmP p{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta};
+  dim3 grid{unsigned(gx), unsigned(gy), unsigned(batch)};
+  if (!tA && !tB)
+    k_gemm_f64<false, false><<<grid, 128, 0, c->stream>>>(p);
+  else if (!tA && tB)
+    k_gemm_f64<false, true><<<grid, 128, 0, c->stream>>>(p);
+  else if (tA && !tB)
+    k_gemm_f64<true, false><<<grid, 128, 0, c->stream>>>(p);
+  else
+    k_gemm_f64<true, true><<<grid, 128, 0, c->stream>>>(p);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void dot_f64(Context* c, int64_t n, const double* x, const double* y, double* out, bool do_sqrt) {
+  reduce_launch(c, n, x, y, y ? 0 : 1, out, do_sqrt);
+}
+
+void diffnrm_f64(Context* c, int64_t n, const double* x, const double* y, double* out,
+                 bool do_sqrt) {
+  reduce_launch(c, n, x, y, 2, out, do_sqrt);
+}
+
+double nrm2_host(Context* c, int64_t n, const double* x) {
+  DBuf<double> s(c, 1);
+  dot_f64(c, n, x, nullptr, s.p(), true);
+  double h = 0.0;
+  read_scalars(c, s.p(), &h, 1);
+  return h;
+}
+
+void axpby_f64(Context* c, int64_t n, double a, const double* x, double b, double* y) {
+  if (n <= 0) return;
+  k_axpby<<<grid_for(c, n), 256, 0, c->stream>>>(n, a, x, b, y);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void scale_dev_f64(Context* c, int64_t n, const double* x, double* y, const double* num,
+                   const double* den) {
+  if (n <= 0) return;
+  k_scale_dev<<<grid_for(c, n), 256, 0, c->stream>>>(n, x, y, num, den);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void fill_f64(Context* c, int64_t n, double v, double* y) {
+  if (n <= 0) return;
+  k_fill<<<grid_for(c, n), 256, 0, c->stream>>>(n, v, y);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void copy_f64(Context* c, int64_t n, const double* x, double* y) {
+  if (n <= 0 || x == y) return;
+  TTG_CUDA(cudaMemcpyAsync(y, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+}
+
+void transpose_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_t ldi,
+                   double* out, int64_t ldo, int64_t batch, int64_t si, int64_t so) {
+  if (rows <= 0 || cols <= 0 || batch <= 0) return;
+  TTG_REQUIRE((cols + 31) / 32 <= 65535 && batch <= 65535, "transpose too large");
+  dim3 grid{unsigned((rows + 31) / 32), unsigned((cols + 31) / 32), unsigned(batch)};
+  k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(rows, cols, in, ldi, si, out, ldo, so);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void copy2d_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_t ldi,
+                double* out, int64_t ldo, const double* scale_col) {
+  if (rows <= 0 || cols <= 0) return;
+  k_copy2d<<<grid_for(c, rows * cols), 256, 0, c->stream>>>(rows, cols, in, ldi, out, ldo,
+                                                            scale_col);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void randn_f64(Context* c, int64_t n, uint64_t seed, uint64_t offset, double* y) {
+  if (n <= 0) return;
+  k_randn<<<grid_for(c, n), 256, 0, c->stream>>>(n, seed, offset, y);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+}  // namespace ttg

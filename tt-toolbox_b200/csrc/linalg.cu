@@ -1,0 +1,123 @@
+// FP64 QR / SVD / LU on the device through cuSOLVER (library factorizations;
+// the contractions around them are this library's own kernels).
+#include "linalg.h"
+
+namespace ttg {
+
+namespace {
+
+__global__ void k_triu(int64_t k, int64_t n, const double* __restrict__ A, int64_t lda,
+                       double* __restrict__ R) {
+  const int64_t total = k * n;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e % k, j = e / k;
+    R[e] = (i <= j) ? A[i + j * lda] : 0.0;
+  }
+}
+
+void check_info(Context* c, const int* dinfo, const char* what) {
+  int info = 0;
+  TTG_CUDA(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  if (info != 0) fail(TTG_ERR_SOLVER, "%s returned info = %d", what, info);
+}
+
+int as_int(int64_t v, const char* what) {
+  TTG_REQUIRE(v >= 0 && v <= 0x7fffffff, "%s = %lld exceeds the 32-bit solver range", what,
+              (long long)v);
+  return int(v);
+}
+
+}  // namespace
+
+void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t lda, double* R) {
+  if (k <= 0 || n <= 0) return;
+  int64_t blocks = (k * n + 255) / 256;
+  if (blocks > int64_t(c->num_sms) * 8) blocks = int64_t(c->num_sms) * 8;
+  k_triu<<<unsigned(blocks), 256, 0, c->stream>>>(k, n, A, lda, R);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R) {
+  const int64_t k = std::min(m, n);
+  const int mi = as_int(m, "m"), ni = as_int(n, "n"), ki = as_int(k, "k");
+  DBuf<double> work(c, m * n), tau(c, k > 0 ? k : 1);
+  DBuf<int> info(c, 1);
+  copy_f64(c, m * n, A, work.p());
+  int lw1 = 0, lw2 = 0;
+  TTG_SOLVER(cusolverDnDgeqrf_bufferSize(c->solver, mi, ni, work.p(), mi, &lw1));
+  TTG_SOLVER(cusolverDnDorgqr_bufferSize(c->solver, mi, ki, ki, work.p(), mi, tau.p(), &lw2));
+  DBuf<double> ws(c, std::max(std::max(lw1, lw2), 1));
+  TTG_SOLVER(cusolverDnDgeqrf(c->solver, mi, ni, work.p(), mi, tau.p(), ws.p(), lw1, info.p()));
+  extract_triu_f64(c, k, n, work.p(), m, R);
+  TTG_SOLVER(cusolverDnDorgqr(c->solver, mi, ki, ki, work.p(), mi, tau.p(), ws.p(), lw2, info.p()));
+  copy_f64(c, m * k, work.p(), Q);
+  check_info(c, info.p(), "geqrf/orgqr");
+  return k;
+}
+
+namespace {
+// gesvd on m >= n, econ; A is overwritten.
+void gesvd_tall(Context* c, int64_t m, int64_t n, double* A, double* U, double* S, double* VT) {
+  const int mi = as_int(m, "m"), ni = as_int(n, "n");
+  int lwork = 0;
+  TTG_SOLVER(cusolverDnDgesvd_bufferSize(c->solver, mi, ni, &lwork));
+  DBuf<double> ws(c, std::max(lwork, 1)), rwork(c, std::max<int64_t>(n, 1));
+  DBuf<int> info(c, 1);
+  signed char jobu = 'S', jobvt = 'S';
+  TTG_SOLVER(cusolverDnDgesvd(c->solver, jobu, jobvt, mi, ni, A, mi, S, U, mi, VT, ni, ws.p(),
+                              lwork, rwork.p(), info.p()));
+  check_info(c, info.p(), "gesvd");
+}
+}  // namespace
+
+int64_t svd_f64(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
+                double* VT) {
+  const int64_t k = std::min(m, n);
+  if (k <= 0) return 0;
+  if (m >= n) {
+    if (m >= 2 * n && n > 1) {
+      // A = Q R ; R = Ur S VT ; U = Q Ur
+      DBuf<double> Q(c, m * n), R(c, n * n), Ur(c, n * n);
+      qr_f64(c, m, n, A, Q.p(), R.p());
+      gesvd_tall(c, n, n, R.p(), Ur.p(), S, VT);
+      gemm_f64(c, false, false, m, n, n, 1.0, Q.p(), m, 0, Ur.p(), n, 0, 0.0, U, m, 0, 1);
+    } else {
+      DBuf<double> W(c, m * n);
+      copy_f64(c, m * n, A, W.p());
+      gesvd_tall(c, m, n, W.p(), U, S, VT);
+    }
+  } else {
+    // A^T (n x m) = U' S V'^T  ->  A = V' S U'^T : U = V' = (VT')^T, VT = U'^T
+    DBuf<double> At(c, n * m), Up(c, n * m), VTp(c, m * m);
+    transpose_f64(c, m, n, A, m, At.p(), n);
+    if (n >= 2 * m && m > 1) {
+      DBuf<double> Q(c, n * m), R(c, m * m), Ur(c, m * m);
+      qr_f64(c, n, m, At.p(), Q.p(), R.p());
+      gesvd_tall(c, m, m, R.p(), Ur.p(), S, VTp.p());
+      gemm_f64(c, false, false, n, m, m, 1.0, Q.p(), n, 0, Ur.p(), m, 0, 0.0, Up.p(), n, 0, 1);
+    } else {
+      gesvd_tall(c, n, m, At.p(), Up.p(), S, VTp.p());
+    }
+    transpose_f64(c, m, m, VTp.p(), m, U, m);     // U (m x m) = VT'^T
+    transpose_f64(c, n, m, Up.p(), n, VT, m);     // VT (m x n) = U'^T
+  }
+  return k;
+}
+
+void lu_solve_f64(Context* c, int64_t N, const double* B, double* rhs, int64_t nrhs) {
+  const int Ni = as_int(N, "N"), nr = as_int(nrhs, "nrhs");
+  DBuf<double> W(c, N * N);
+  DBuf<int> piv(c, std::max<int64_t>(N, 1)), info(c, 1);
+  copy_f64(c, N * N, B, W.p());
+  int lwork = 0;
+  TTG_SOLVER(cusolverDnDgetrf_bufferSize(c->solver, Ni, Ni, W.p(), Ni, &lwork));
+  DBuf<double> ws(c, std::max(lwork, 1));
+  TTG_SOLVER(cusolverDnDgetrf(c->solver, Ni, Ni, W.p(), Ni, ws.p(), piv.p(), info.p()));
+  TTG_SOLVER(cusolverDnDgetrs(c->solver, CUBLAS_OP_N, Ni, nr, W.p(), Ni, piv.p(), rhs, Ni, info.p()));
+  check_info(c, info.p(), "getrf/getrs");
+}
+
+}  // namespace ttg

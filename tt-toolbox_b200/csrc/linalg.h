@@ -1,0 +1,26 @@
+// FP64 dense factorizations on the device (QR, SVD, LU solve).
+#pragma once
+#include "kernels.h"
+
+namespace ttg {
+
+// Thin QR of the m x n column-major A (lda = m): Q (m x k, ld m) and
+// R (k x n, ld k), k = min(m, n).  A is not modified.  Householder QR with
+// LAPACK's sign convention (geqrf/orgqr), as MATLAB's qr(A,0).
+int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R);
+
+// Economy SVD A = U diag(S) VT of the m x n column-major A:
+// U (m x k, ld m), S (k) on the device, VT (k x n, ld k), k = min(m, n).
+// A is not modified.  Returns k.  Tall inputs (m >= 2n) are reduced by a QR
+// first; wide inputs are transposed.
+int64_t svd_f64(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
+                double* VT);
+
+// Solve the square N x N system B X = RHS (nrhs columns) by LU with partial
+// pivoting; RHS is overwritten by X.  B is not modified.
+void lu_solve_f64(Context* c, int64_t N, const double* B, double* rhs, int64_t nrhs = 1);
+
+// R = triu(A(0:k, 0:n)) (k x n, ld k) from a geqrf output (ld lda).
+void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t lda, double* R);
+
+}  // namespace ttg

@@ -1,0 +1,13 @@
+// Mixed-precision local solve: low-precision Krylov solver inside an FP64
+// iterative-refinement loop on the local residual.
+#pragma once
+#include "amen.h"
+
+namespace ttg {
+
+LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Phi1,
+                                   const double* A, const double* Phi2, const double* rhs,
+                                   double tol, const double* sol_prev, int64_t nrestart,
+                                   int64_t niters, double* sol);
+
+}  // namespace ttg

@@ -1,0 +1,531 @@
+"""Python host side of libttgpu (ctypes over the C ABI in include/ttgpu.h).
+
+Mirrors the reference's MATLAB interface for the hot path, with the same
+argument meaning and error behaviour:
+
+* ``round(tt, eps, rmax=None)``            -- ``@tt_tensor/round.m:1``
+* ``amen_solve2(A, y, tol, **opts)``       -- ``solve/amen_solve2.m:1`` (options :161-203)
+* ``solve3d_2(Phi1, A, Phi2, rhs, tol, trunc_norm, sol_prev, prec, nrestart, niters, verb)``
+                                            -- MEX gateway ``fmex/solve3d_2.c:121-122``
+* ``bfun3(Phi1, A, Phi2, x)``              -- ``solve/amen_solve2.m:924-951``
+* ``compute_next_Phi(Phi_prev, x, A, y, direction, extnrm=None)``
+                                            -- ``solve/amen_solve2.m:834-920``
+
+Host arrays are numpy FP64 in column-major reference layouts.  There is no
+CPU fallback: loading fails loudly when ``libttgpu.so`` (or a GPU) is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libttgpu.so")
+
+TTG_FP64, TTG_MIXED = 0, 1
+_PREC = {"fp64": TTG_FP64, "mixed": TTG_MIXED, TTG_FP64: TTG_FP64, TTG_MIXED: TTG_MIXED}
+
+_i64 = C.c_int64
+_p64 = C.POINTER(C.c_int64)
+_pd = C.POINTER(C.c_double)
+_vp = C.c_void_p
+
+
+class TTGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("libttgpu error %d: %s" % (code, msg))
+        self.code = code
+
+
+class AmenOpts(C.Structure):
+    _fields_ = [("nswp", _i64), ("rmax", _i64), ("max_full_size", _i64),
+                ("local_restart", _i64), ("local_iters", _i64), ("kickrank", _i64),
+                ("resid_damp", C.c_double), ("tol_exit", C.c_double),
+                ("trunc_norm", C.c_int32), ("local_prec", C.c_int32),
+                ("precision", C.c_int32), ("verb", C.c_int32), ("seed", C.c_uint64)]
+
+
+MAX_SWEEPS = 64
+
+
+class AmenStats(C.Structure):
+    _fields_ = [("sweeps", _i64), ("matvecs", _i64), ("matvecs_fp64", _i64),
+                ("local_solves", _i64), ("gmres_iters", _i64), ("max_rank", _i64),
+                ("max_res", C.c_double * MAX_SWEEPS), ("max_dx", C.c_double * MAX_SWEEPS),
+                ("ms_total", C.c_double), ("ms_matvec", C.c_double),
+                ("matvec_gflop", C.c_double)]
+
+    def to_dict(self):
+        s = int(self.sweeps)
+        k = min(s, MAX_SWEEPS)
+        return dict(sweeps=s, matvecs=int(self.matvecs), matvecs_fp64=int(self.matvecs_fp64),
+                    local_solves=int(self.local_solves), gmres_iters=int(self.gmres_iters),
+                    max_rank=int(self.max_rank), max_res=list(self.max_res[:k]),
+                    max_dx=list(self.max_dx[:k]), ms_total=float(self.ms_total),
+                    matvec_gflop=float(self.matvec_gflop))
+
+
+class RoundStats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_qr_sweep", C.c_double),
+                ("ms_svd_sweep", C.c_double), ("max_rank", _i64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libttgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libttgpu.so not found at %s; run `python -m ttgpu.build` in "
+                          "tt-toolbox_b200/" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    L.ttg_last_error.restype = C.c_char_p
+    L.ttg_version.restype = C.c_int
+    sigs = {
+        "ttg_context_create": [C.c_int, C.POINTER(_vp)],
+        "ttg_context_destroy": [_vp],
+        "ttg_context_sync": [_vp],
+        "ttg_malloc": [_vp, C.c_size_t, C.POINTER(_vp)],
+        "ttg_free": [_vp, _vp],
+        "ttg_memcpy_h2d": [_vp, _vp, _vp, C.c_size_t],
+        "ttg_memcpy_d2h": [_vp, _vp, _vp, C.c_size_t],
+        "ttg_tt_upload": [_vp, _i64, _p64, _p64, _p64, _pd, C.POINTER(_vp)],
+        "ttg_tt_shape": [_vp, _p64, _p64, _p64, _p64, _p64],
+        "ttg_tt_download": [_vp, _pd],
+        "ttg_tt_free": [_vp],
+        "ttg_round": [_vp, C.c_double, _p64, _i64, C.c_int32, C.POINTER(_vp),
+                      C.POINTER(RoundStats)],
+        "ttg_amen_solve": [_vp, _vp, C.c_double, C.POINTER(AmenOpts), _vp, _vp,
+                           C.POINTER(_vp), C.POINTER(AmenStats)],
+        "ttg_local_matvec": [_vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp,
+                             C.c_int32],
+        "ttg_next_phi": [_vp, C.c_int32, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _vp, _vp,
+                         _vp, _vp, _vp, _pd],
+        "ttg_local_solve": [_vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp, C.c_double,
+                            C.c_int32, _vp, C.c_int32, _i64, _i64, _vp, C.c_int32, _p64],
+    }
+    for name, args in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.ttg_amen_opts_default.argtypes = [C.POINTER(AmenOpts)]
+    L.ttg_amen_opts_default.restype = None
+    _lib = L
+    return L
+
+
+def _check(code):
+    if code != 0:
+        raise TTGError(code, lib().ttg_last_error().decode(errors="replace"))
+
+
+def _i64arr(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.int64))
+
+
+def _ptr64(a):
+    return a.ctypes.data_as(_p64)
+
+
+def _ptrd(a):
+    return a.ctypes.data_as(_pd)
+
+
+# ---------------------------------------------------------------------------
+# Host containers (flat-core layout of @tt_tensor/tt_tensor.m:33-41)
+# ---------------------------------------------------------------------------
+
+class TensorTrain:
+    """Host TT tensor: mode sizes ``n[d]``, ranks ``r[d+1]``, flat column-major ``core``."""
+
+    def __init__(self, n, r, core):
+        self.n = _i64arr(n)
+        self.r = _i64arr(r)
+        self.core = np.ascontiguousarray(np.asarray(core, dtype=np.float64).ravel())
+        need = int(np.sum(self.n * self.r[:-1] * self.r[1:]))
+        if self.core.size != need or self.r.size != self.n.size + 1:
+            raise ValueError("inconsistent TT sizes")
+
+    @property
+    def d(self):
+        return int(self.n.size)
+
+    @classmethod
+    def from_cores(cls, cores):
+        n = [c.shape[1] for c in cores]
+        r = [cores[0].shape[0]] + [c.shape[2] for c in cores]
+        return cls(n, r, np.concatenate([np.asarray(c).ravel(order="F") for c in cores]))
+
+    def cores(self):
+        out, pos = [], 0
+        for k in range(self.d):
+            sz = int(self.r[k] * self.n[k] * self.r[k + 1])
+            out.append(self.core[pos:pos + sz].reshape(
+                (int(self.r[k]), int(self.n[k]), int(self.r[k + 1])), order="F"))
+            pos += sz
+        return out
+
+
+class TTMatrix:
+    """Host TT matrix: row sizes ``n``, column sizes ``m``, ranks ``r``, flat core
+    with cores ``[r_k, n_k, m_k, r_{k+1}]`` (``@tt_matrix/tt_matrix.m:33-40``)."""
+
+    def __init__(self, n, m, r, core):
+        self.n = _i64arr(n)
+        self.m = _i64arr(m)
+        self.r = _i64arr(r)
+        self.core = np.ascontiguousarray(np.asarray(core, dtype=np.float64).ravel())
+        need = int(np.sum(self.n * self.m * self.r[:-1] * self.r[1:]))
+        if self.core.size != need:
+            raise ValueError("inconsistent TT-matrix sizes")
+
+    @property
+    def d(self):
+        return int(self.n.size)
+
+    @classmethod
+    def from_cores(cls, cores):
+        n = [c.shape[1] for c in cores]
+        m = [c.shape[2] for c in cores]
+        r = [cores[0].shape[0]] + [c.shape[3] for c in cores]
+        return cls(n, m, r, np.concatenate([np.asarray(c).ravel(order="F") for c in cores]))
+
+
+# ---------------------------------------------------------------------------
+# Device context / handles
+# ---------------------------------------------------------------------------
+
+class Context:
+    """One device + one CUDA stream (``ttg_context``)."""
+
+    def __init__(self, device=0):
+        h = _vp()
+        _check(lib().ttg_context_create(int(device), C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().ttg_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        _check(lib().ttg_context_sync(self.h))
+
+    # device memory helpers
+    def to_device(self, a):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F")
+                                 if np.asarray(a).ndim > 1 else np.asarray(a, dtype=np.float64))
+        return DeviceArray(self, a)
+
+    def empty(self, n):
+        return DeviceArray(self, None, n)
+
+
+class DeviceArray:
+    """Flat FP64 device buffer owned by a context."""
+
+    def __init__(self, ctx, host=None, n=None):
+        self.ctx = ctx
+        self.n = int(host.size if host is not None else n)
+        p = _vp()
+        _check(lib().ttg_malloc(ctx.h, max(self.n, 1) * 8, C.byref(p)))
+        self.p = p
+        if host is not None and self.n:
+            _check(lib().ttg_memcpy_h2d(ctx.h, self.p, host.ctypes.data_as(_vp), self.n * 8))
+
+    def get(self):
+        out = np.empty(self.n, dtype=np.float64)
+        if self.n:
+            _check(lib().ttg_memcpy_d2h(self.ctx.h, out.ctypes.data_as(_vp), self.p, self.n * 8))
+        return out
+
+    def free(self):
+        if self.p:
+            lib().ttg_free(self.ctx.h, self.p)
+            self.p = None
+
+    def __del__(self):
+        try:
+            if self.ctx.h:
+                self.free()
+        except Exception:
+            pass
+
+
+class DeviceTT:
+    """Device-resident TT tensor or matrix (``ttg_tt``)."""
+
+    def __init__(self, ctx, h):
+        self.ctx = ctx
+        self.h = h
+
+    @classmethod
+    def upload(cls, ctx, t):
+        h = _vp()
+        n = _i64arr(t.n)
+        r = _i64arr(t.r)
+        core = np.ascontiguousarray(t.core, dtype=np.float64)
+        if isinstance(t, TTMatrix):
+            m = _i64arr(t.m)
+            _check(lib().ttg_tt_upload(ctx.h, t.d, _ptr64(n), _ptr64(m), _ptr64(r), _ptrd(core),
+                                       C.byref(h)))
+        else:
+            _check(lib().ttg_tt_upload(ctx.h, t.d, _ptr64(n), None, _ptr64(r), _ptrd(core),
+                                       C.byref(h)))
+        return cls(ctx, h)
+
+    def shape(self):
+        d = _i64()
+        _check(lib().ttg_tt_shape(self.h, C.byref(d), None, None, None, None))
+        d = d.value
+        n = np.zeros(d, np.int64)
+        m = np.zeros(d, np.int64)
+        r = np.zeros(d + 1, np.int64)
+        numel = _i64()
+        _check(lib().ttg_tt_shape(self.h, None, _ptr64(n), _ptr64(m), _ptr64(r), C.byref(numel)))
+        return n, m, r, numel.value
+
+    def download(self):
+        n, m, r, numel = self.shape()
+        core = np.empty(numel, np.float64)
+        _check(lib().ttg_tt_download(self.h, _ptrd(core)))
+        return TensorTrain(n, r, core)
+
+    def free(self):
+        if self.h:
+            lib().ttg_tt_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            if self.ctx.h:
+                self.free()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(int(os.environ.get("TTG_DEVICE", "0")))
+    return _default_ctx
+
+
+# ---------------------------------------------------------------------------
+# Reference-facing operations
+# ---------------------------------------------------------------------------
+
+def round(tt, eps, rmax=None, precision="fp64", ctx=None, stats=None):
+    """``tt = round(tt, eps[, rmax])`` (``@tt_tensor/round.m:1-110``).
+
+    ``tt`` is a host ``TensorTrain`` or a ``DeviceTT``; the result has the same
+    kind.  ``rmax``: scalar or ``d+1`` values (``round.m:20-32``).
+    """
+    ctx = ctx or (tt.ctx if isinstance(tt, DeviceTT) else default_context())
+    dev_in = tt if isinstance(tt, DeviceTT) else DeviceTT.upload(ctx, tt)
+    if rmax is None:
+        rp, nr = None, 0
+    else:
+        rm = _i64arr(np.atleast_1d(rmax))
+        rp, nr = _ptr64(rm), rm.size
+    out = _vp()
+    st = RoundStats()
+    _check(lib().ttg_round(dev_in.h, float(eps), rp, nr, _PREC[precision], C.byref(out),
+                           C.byref(st)))
+    res = DeviceTT(ctx, out)
+    if stats is not None:
+        stats.update(ms_total=st.ms_total, ms_qr_sweep=st.ms_qr_sweep,
+                     ms_svd_sweep=st.ms_svd_sweep, max_rank=int(st.max_rank))
+    if isinstance(tt, DeviceTT):
+        return res
+    host = res.download()
+    res.free()
+    dev_in.free()
+    return host
+
+
+_AMEN_KEYS = {"nswp", "rmax", "x0", "z0", "verb", "local_prec", "local_restart", "local_iters",
+              "kickrank", "kicktype", "ismex", "max_full_size", "resid_damp", "trunc_norm",
+              "tol_exit", "precision", "seed"}
+
+
+def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
+    """``[x] = amen_solve2(A, y, tol, 'name', value, ...)`` (``solve/amen_solve2.m:1``).
+
+    Options follow ``amen_solve2.m:161-203``; unknown names raise
+    ``ValueError('Unrecognized option')`` as the reference errors (``:200-201``).
+    ``A``: host ``TTMatrix`` or ``DeviceTT``; ``y``/``x0``/``z0``: host
+    ``TensorTrain`` or ``DeviceTT``.  Returns a host ``TensorTrain`` when ``y``
+    is a host tensor, else a ``DeviceTT``.
+    """
+    for k in opts:
+        if k.lower() not in _AMEN_KEYS:
+            raise ValueError("Unrecognized option: %s" % k)
+    opts = {k.lower(): v for k, v in opts.items()}
+    if opts.get("kicktype", "als") != "als":
+        raise TTGError(7, "kicktype %r is not implemented (only 'als')" % opts["kicktype"])
+    if opts.get("trunc_norm", "residual") not in ("residual", "resid", 1):
+        raise TTGError(7, "trunc_norm %r is not implemented (only 'residual')" % opts["trunc_norm"])
+    lp = opts.get("local_prec", "")
+    if lp not in ("", 0, None):
+        raise TTGError(7, "local_prec %r is not implemented" % (lp,))
+    ctx = ctx or (A.ctx if isinstance(A, DeviceTT) else default_context())
+    o = AmenOpts()
+    lib().ttg_amen_opts_default(C.byref(o))
+    for k in ("nswp", "rmax", "max_full_size", "local_restart", "local_iters", "kickrank"):
+        if k in opts:
+            setattr(o, k, int(opts[k]))
+    if "resid_damp" in opts:
+        o.resid_damp = float(opts["resid_damp"])
+    if "tol_exit" in opts and opts["tol_exit"] is not None:
+        o.tol_exit = float(opts["tol_exit"])
+    if "verb" in opts:
+        o.verb = int(opts["verb"])
+    if "seed" in opts:
+        o.seed = int(opts["seed"])
+    o.precision = _PREC[opts.get("precision", "fp64")]
+    owned = []
+
+    def dev(t):
+        if t is None or isinstance(t, DeviceTT):
+            return t
+        h = DeviceTT.upload(ctx, t)
+        owned.append(h)
+        return h
+
+    dA, dy = dev(A), dev(y)
+    dx0, dz0 = dev(opts.get("x0")), dev(opts.get("z0"))
+    out = _vp()
+    st = AmenStats()
+    try:
+        _check(lib().ttg_amen_solve(dA.h, dy.h, float(tol), C.byref(o),
+                                    dx0.h if dx0 is not None else None,
+                                    dz0.h if dz0 is not None else None, C.byref(out),
+                                    C.byref(st)))
+    finally:
+        pass
+    if stats is not None:
+        stats.update(st.to_dict())
+    res = DeviceTT(ctx, out)
+    if isinstance(y, DeviceTT):
+        for h in owned:
+            h.free()
+        return res
+    host = res.download()
+    res.free()
+    for h in owned:
+        h.free()
+    return host
+
+
+def _shape3(a):
+    a = np.asarray(a)
+    s = list(a.shape) + [1] * (3 - a.ndim)
+    return s[:3]
+
+
+def bfun3(Phi1, A, Phi2, x, ctx=None, precision="fp64"):
+    """Local matvec ``y = bfun3(Phi1, A, Phi2, x)`` (square: ry = rx)."""
+    ctx = ctx or default_context()
+    rx1, _, ra1 = _shape3(Phi1)
+    A4 = np.asarray(A)
+    A4 = A4.reshape(list(A4.shape) + [1] * (4 - A4.ndim), order="F")
+    n = A4.shape[1]
+    rx2, ra2, _ = _shape3(Phi2)
+    dP1, dA, dP2 = ctx.to_device(Phi1), ctx.to_device(A4), ctx.to_device(Phi2)
+    dx = ctx.to_device(np.asarray(x).ravel(order="F"))
+    dy = ctx.empty(rx1 * n * rx2)
+    _check(lib().ttg_local_matvec(ctx.h, rx1, n, rx2, ra1, ra2, dP1.p, dA.p, dP2.p, dx.p, dy.p,
+                                  _PREC[precision]))
+    return dy.get()
+
+
+def compute_next_Phi(Phi_prev, x, A, y, direction, extnrm=None, want_norm=False, ctx=None):
+    """``[Phi, nrm] = compute_next_Phi(Phi_prev, x, A, y, direction[, extnrm])``."""
+    ctx = ctx or default_context()
+    x = np.asarray(x)
+    y = np.asarray(y)
+    rx1, n, rx2 = _shape3(x)
+    ry1, _, ry2 = _shape3(y)
+    if A is not None:
+        A4 = np.asarray(A)
+        A4 = A4.reshape(list(A4.shape) + [1] * (4 - A4.ndim), order="F")
+        ra1, ra2 = A4.shape[0], A4.shape[3]
+        dA = ctx.to_device(A4)
+        Ap = dA.p
+    else:
+        ra1 = ra2 = 1
+        Ap = None
+    d = 0 if direction == "lr" else 1
+    cnt = rx2 * ry2 * ra2 if d == 0 else ry1 * ra1 * rx1
+    dP, dx, dy = ctx.to_device(Phi_prev), ctx.to_device(x), ctx.to_device(y)
+    out = ctx.empty(cnt)
+    nrm = C.c_double(0.0)
+    _check(lib().ttg_next_phi(ctx.h, d, rx1, n, rx2, ry1, ry2, ra1, ra2, dP.p, dx.p, Ap, dy.p,
+                              out.p, C.byref(nrm) if want_norm else None))
+    res = out.get()
+    if extnrm is not None and not want_norm:
+        res = res / extnrm
+    if d == 0:
+        shape = (rx2, ry2, ra2) if A is not None else (rx2, ry2)
+    else:
+        shape = (ry1, ra1, rx1) if A is not None else (ry1, rx1)
+    res = res.reshape(shape, order="F")
+    return (res, nrm.value) if want_norm else res
+
+
+def solve3d_2(Phi1, A, Phi2, rhs, tol, trunc_norm, sol_prev, prec=0, nrestart=40, niters=2,
+              verb=0, ctx=None, precision="fp64", info=None):
+    """MEX-compatible local solve (``fmex/solve3d_2.c:121-300``); residual branch."""
+    ctx = ctx or default_context()
+    rx1, rx1b, ra1 = _shape3(Phi1)
+    if rx1b != rx1:
+        raise TTGError(1, "Phi1 is not square!")            # solve3d_2.c:150
+    A4 = np.asarray(A)
+    A4 = A4.reshape(list(A4.shape) + [1] * (4 - A4.ndim), order="F")
+    if A4.shape[0] != ra1:
+        raise TTGError(1, "ra1 in Phi1 and A are not consistent!")   # :158
+    n = A4.shape[1]
+    if A4.shape[2] != n:
+        raise TTGError(1, "A is not square!")               # :160
+    ra2 = A4.shape[3]
+    rx2, ra2b, rx2b = _shape3(Phi2)
+    if rx2b != rx2:
+        raise TTGError(1, "Phi2 is not square!")            # :169
+    if ra2b != ra2:
+        raise TTGError(1, "ra2 in Phi2 and A are not consistent!")   # :170
+    sz = rx1 * n * rx2
+    if np.asarray(rhs).size != sz:
+        raise TTGError(1, "RHS size is not consistent!")    # :173
+    if np.asarray(sol_prev).size != sz:
+        raise TTGError(1, "SOL_PREV size is not consistent!")  # :182
+    dP1, dA, dP2 = ctx.to_device(Phi1), ctx.to_device(A4), ctx.to_device(Phi2)
+    dr = ctx.to_device(np.asarray(rhs, dtype=np.float64).ravel(order="F"))
+    ds = ctx.to_device(np.asarray(sol_prev, dtype=np.float64).ravel(order="F"))
+    out = ctx.empty(sz)
+    it = _i64(0)
+    _check(lib().ttg_local_solve(ctx.h, rx1, n, rx2, ra1, ra2, dP1.p, dA.p, dP2.p, dr.p,
+                                 float(tol), int(round_half(trunc_norm)), ds.p, int(prec),
+                                 int(nrestart), int(niters), out.p, _PREC[precision],
+                                 C.byref(it)))
+    if info is not None:
+        info["iters"] = it.value
+    return out.get()
+
+
+def round_half(v):
+    """MATLAB's ``round`` of a scalar option (``solve3d_2.c:138-141,179``)."""
+    return int(np.floor(float(v) + 0.5))
