@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: AMEn time-to-1e-8 residual on one B200 (and N independent replicas).
+
+Workload (one "step" = one full AMEn solve to tol 1e-8 from the same seeded
+initial guess): d=10, n=64 anisotropic diffusion + separable reaction TT
+operator (rank 3), seeded rank-4 Gaussian right-hand side, rmax 128,
+amen_solve2 default options otherwise.  Inputs are synthetic (seeded numpy
+PCG64), generated by ``ttgpu.workloads``.
+
+Prints ONE JSON line (rank 0).  ``value`` is the device time of one solve
+(CUDA events on the library's stream, inputs resident in HBM, L2 flushed
+between steps); ``e2e`` is the same solve through the C ABI with host
+buffers (upload + solve + download, host clock).  ``--impl reference`` times
+the reference algorithm's CPU restatement (the FP64 oracle) instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tt-toolbox_b200"))
+
+WORKLOAD = dict(d=10, n=64, rmax=128, tol=1e-8, seed=3)
+METRIC = "AMEn time-to-1e-8 residual (d=10, n=64, rank-3 TT operator, rmax 128)"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-compare", action="store_true",
+                   help="skip timing the other precision")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only: no data-path collective)
+# ---------------------------------------------------------------------------
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            # The library is loaded before torch so that its CUDA 12.9
+            # cuBLAS/cuSOLVER are the ones the process uses.
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([float(v)], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# correctness check of the measured run (host numpy, outside the timed region)
+# ---------------------------------------------------------------------------
+
+def true_residual(A, x, y):
+    """||A x - y|| / ||y|| for host TT objects (matvec by core products, norm
+    by a left-to-right QR sweep)."""
+    import numpy as np
+
+    def cores_of(t):
+        return t.cores()
+
+    def mat_cores(M):
+        out, pos = [], 0
+        for k in range(M.d):
+            sz = int(M.r[k] * M.n[k] * M.m[k] * M.r[k + 1])
+            out.append(M.core[pos:pos + sz].reshape(
+                (int(M.r[k]), int(M.n[k]), int(M.m[k]), int(M.r[k + 1])), order="F"))
+            pos += sz
+        return out
+
+    Ac, xc, yc = mat_cores(A), cores_of(x), cores_of(y)
+    d = len(xc)
+    res = []
+    for k in range(d):
+        ax = np.einsum("anmb,cmd->acnbd", Ac[k], xc[k])
+        ra1, rx1, n, ra2, rx2 = ax.shape
+        ax = ax.reshape(ra1 * rx1, n, ra2 * rx2, order="F")
+        yk = -yc[k] if k == 0 else yc[k]
+        r1a, _, r2a = ax.shape
+        r1b, _, r2b = yk.shape
+        if k == 0:
+            c = np.concatenate([ax, yk], axis=2)
+        elif k == d - 1:
+            c = np.concatenate([ax, yk], axis=0)
+        else:
+            c = np.zeros((r1a + r1b, n, r2a + r2b))
+            c[:r1a, :, :r2a] = ax
+            c[r1a:, :, r2a:] = yk
+        res.append(c)
+
+    def norm(cs):
+        nrm = 1.0
+        core = cs[0]
+        for k in range(len(cs) - 1):
+            r1, n, r2 = core.shape
+            q, rr = np.linalg.qr(core.reshape(r1 * n, r2, order="F"))
+            s = np.linalg.norm(rr)
+            nrm *= s
+            rr = rr / s
+            nxt = cs[k + 1]
+            core = (rr @ nxt.reshape(nxt.shape[0], -1, order="F")).reshape(
+                rr.shape[0], nxt.shape[1], nxt.shape[2], order="F")
+        return nrm * np.linalg.norm(core)
+
+    return norm(res) / norm(yc)
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+def load_peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per launch of the roofline kernel, from the committed ncu
+    summary (profiles/roofline_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            return json.load(f).get("bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline_run(W, reps=1):
+    """The FP64 oracle (reference algorithm restated) on the same workload."""
+    sys.path.insert(0, ROOT)
+    from oracle.amen import amen_solve2 as ref_solve
+    from oracle.builders import aniso_config
+    A, y, x0, z0 = aniso_config(d=W["d"], n=W["n"], seed=W["seed"])
+    times = []
+    info = None
+    for _ in range(reps):
+        t = time.perf_counter()
+        x, info = ref_solve(A, y, W["tol"], x0, z0, rmax=W["rmax"], nswp=50)
+        times.append(time.perf_counter() - t)
+    return times, info
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return None
+    W = WORKLOAD
+    n_total = args.warmup + args.steps
+    times, info = cpu_baseline_run(W, reps=max(1, n_total))
+    timed = times[-args.steps:] if args.steps > 0 else times
+    v = statistics.mean(timed)
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+        "config": {"workload": "amen_solve2 d=10 n=64 rank-3 anisotropic operator, rank-4 rhs, "
+                               "rmax 128, tol 1e-8", "parallelism": "replicas", "sweeps": info["sweeps"]},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
+                         "sample": "full FP64 oracle solve of the workload (numpy/OpenBLAS, all threads)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def run_ours(args, dist):
+    import ttgpu
+    from ttgpu import workloads
+    ttgpu.lib()
+    W = WORKLOAD
+    dev = dist.local if dist.world > 1 else int(os.environ.get("TTG_DEVICE", "0"))
+    ctx = ttgpu.Context(dev)
+    A, y, x0, z0 = workloads.aniso(d=W["d"], n=W["n"], seed=W["seed"])
+    dA, dy = ttgpu.DeviceTT.upload(ctx, A), ttgpu.DeviceTT.upload(ctx, y)
+    dx0, dz0 = ttgpu.DeviceTT.upload(ctx, x0), ttgpu.DeviceTT.upload(ctx, z0)
+    opts = dict(rmax=W["rmax"], nswp=50)
+
+    def solve(prec, st, timing=False):
+        out = ttgpu.amen_solve2(dA, dy, W["tol"], x0=dx0, z0=dz0, ctx=ctx, stats=st,
+                                precision=prec, timing=timing, **opts)
+        return out
+
+    agg = {}
+
+    def timed_steps(prec, K, timing=False):
+        ms, launches, sweeps, gflop = [], 0, [], 0.0
+        last = None
+        acc = {"gflop_lp": 0.0, "ms_lp": 0.0, "gflop_fp64": 0.0, "ms_fp64": 0.0,
+               "matvecs_lp": 0, "matvecs": 0}
+        for _ in range(K):
+            ctx.flush_l2()
+            st = {}
+            out = solve(prec, st, timing)
+            ms.append(st["ms_total"])
+            launches += st["launches"]
+            sweeps.append(st["sweeps"])
+            gflop += st["matvec_gflop"]
+            for k in acc:
+                acc[k] += st[k]
+            if last is not None:
+                last.free()
+            last = out
+        agg[prec] = acc
+        return ms, launches, sweeps, gflop, last
+
+    for _ in range(args.warmup):
+        st = {}
+        solve(args.precision, st).free()
+    dist.barrier()
+    ctx.sync()
+    clocks = Clocks(dev)
+    clocks.start()
+    t0 = time.perf_counter()
+    # Every local matvec of the timed solves is bracketed by CUDA events on
+    # the library's stream (opts.timing); the roofline below uses them.
+    ms, launches, sweeps, gflop, xdev = timed_steps(args.precision, args.steps, timing=True)
+    ctx.sync()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    dist.barrier()
+    ms_step = statistics.mean(ms)
+    ms_step_max = dist.max(ms_step)
+    x = xdev.download()
+    xdev.free()
+    res = true_residual(A, x, y)
+
+    # end to end through the C ABI with host buffers
+    e2e_t = []
+    h2d = 8 * (A.core.size + y.core.size + x0.core.size + z0.core.size)
+    d2h = 0
+    for _ in range(max(1, args.steps)):
+        ctx.flush_l2()
+        t = time.perf_counter()
+        xh = ttgpu.amen_solve2(A, y, W["tol"], x0=x0, z0=z0, ctx=ctx, precision=args.precision,
+                               **opts)
+        e2e_t.append(time.perf_counter() - t)
+        d2h = 8 * xh.core.size
+    e2e_v = dist.max(statistics.mean(e2e_t))
+
+    other = None
+    if not args.no_compare:
+        op = "fp64" if args.precision == "mixed" else "mixed"
+        try:
+            oms, _, osw, _, ox = timed_steps(op, args.steps, timing=True)
+            xo = ox.download()
+            ox.free()
+            a = agg[op]
+            other = {"precision": op, "ms_per_step": statistics.mean(oms), "sweeps": osw,
+                     "true_residual": true_residual(A, xo, y),
+                     "speedup_of_headline": statistics.mean(oms) / ms_step}
+            if a["ms_fp64"] > 0:
+                other["fp64_matvec_tflops"] = a["gflop_fp64"] / a["ms_fp64"]
+        except ttgpu.TTGError as e:
+            other = {"precision": op, "unavailable": str(e)}
+
+    peaks, peaks_kind = load_peaks()
+    a = agg[args.precision]
+    if args.precision == "mixed" and a["ms_lp"] > 0:
+        # BF16 tcgen05 local matvec (convert + 3 tensor-core GEMMs) per launch.
+        per_launch_tflop = a["gflop_lp"] / max(1, a["matvecs_lp"]) * 1e-3
+        per_launch_ms = a["ms_lp"] / max(1, a["matvecs_lp"])
+        achieved = per_launch_tflop / (per_launch_ms * 1e-3)
+        peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1590.0))
+        roof = {"kernel": "local matvec, BF16 tcgen05 (4 launches)", "bound": "tensor",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": load_traffic(),
+                "peak_kind": "bf16 sustained, %s" % peaks_kind,
+                "launch_ms": per_launch_ms, "gflop_per_launch": per_launch_tflop * 1e3}
+    else:
+        per_launch_ms = a["ms_fp64"] / max(1, a["matvecs"])
+        achieved = a["gflop_fp64"] / max(a["ms_fp64"], 1e-9)
+        roof = {"kernel": "local matvec, FP64 DMMA (3 launches)", "bound": "tensor",
+                "achieved": achieved, "peak": None, "unit": "TFLOP/s", "frac": None,
+                "traffic": None, "peak_kind": "no measured FP64 peak", "launch_ms": per_launch_ms}
+    line = {
+        "metric": METRIC, "value": ms_step_max / 1e3, "unit": "s", "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step_max,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "bf16/f32 matvec + f64 refinement",
+        "data": "synthetic (seeded PCG64)",
+        "config": {"workload": "amen_solve2 d=10 n=64 rank-3 anisotropic operator, rank-4 rhs, "
+                               "rmax 128, tol 1e-8", "precision": args.precision,
+                   "parallelism": "replicas" if dist.world > 1 else "single",
+                   "l2": "flushed between steps (256 MiB memset)",
+                   "sweeps": sweeps, "true_residual": res},
+        "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "clocks": clk,
+        "matvec_gflop_per_step": gflop / max(1, args.steps),
+        "wall_s_timed": wall,
+        "peaks_source": peaks_kind,
+    }
+    if other is not None:
+        line["compare"] = other
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        times, info = cpu_baseline_run(W, reps=1)
+        line["cpu_baseline"] = {"value": times[0], "unit": "s", "cores": os.cpu_count(),
+                                "kind": "port",
+                                "sample": "one full FP64 oracle solve of the same workload "
+                                          "(numpy/OpenBLAS, all threads; %d sweeps)" % info["sweeps"]}
+    for h in (dA, dy, dx0, dz0):
+        h.free()
+    ctx.close()
+    return line
+
+
+def main():
+    args = parse()
+    if args.impl == "ours":
+        import ttgpu
+        ttgpu.lib()  # before torch (see Dist)
+    dist = Dist()
+    try:
+        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if dist.rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

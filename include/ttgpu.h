@@ -58,6 +58,11 @@ int ttg_malloc(ttg_context ctx, size_t bytes, void** out);
 int ttg_free(ttg_context ctx, void* p);
 int ttg_memcpy_h2d(ttg_context ctx, void* dst_dev, const void* src_host, size_t bytes);
 int ttg_memcpy_d2h(ttg_context ctx, void* dst_host, const void* src_dev, size_t bytes);
+/* Fill device memory with a byte value (e.g. to evict the L2 cache between
+ * timed runs). */
+int ttg_memset(ttg_context ctx, void* dst_dev, int value, size_t bytes);
+/* Number of kernels this library launched on the context so far. */
+int ttg_launch_count(ttg_context ctx, int64_t* out);
 
 /* ---- device-resident TT tensors / matrices -------------------------------
  * Replaces the MATLAB objects built by @tt_tensor/tt_tensor.m:33-41 and
@@ -111,6 +116,8 @@ typedef struct {
   int32_t precision;     /* TTG_FP64 or TTG_MIXED           */
   int32_t verb;          /* 0 silent, 1 per-sweep line on stderr */
   uint64_t seed;         /* seed for device-drawn x0/z0     */
+  int32_t timing;        /* 1: time every local matvec with CUDA events */
+  int32_t reserved;
 } ttg_amen_opts;
 
 #define TTG_MAX_SWEEPS_RECORDED 64
@@ -126,6 +133,12 @@ typedef struct {
   double ms_total;
   double ms_matvec;       /* device time inside local matvecs (if timed)  */
   double matvec_gflop;    /* algorithmic FLOPs of all local matvecs / 1e9 */
+  int64_t launches;       /* kernels launched by the solve                */
+  int64_t matvecs_lp;     /* BF16 tensor-core local matvecs (mixed)       */
+  double gflop_lp;        /* their algorithmic FLOPs / 1e9                */
+  double ms_lp;           /* their device time (opts.timing = 1)          */
+  double gflop_fp64;      /* FP64 local-matvec FLOPs / 1e9                */
+  double ms_fp64;         /* their device time (opts.timing = 1)          */
 } ttg_amen_stats;
 
 void ttg_amen_opts_default(ttg_amen_opts* opts);

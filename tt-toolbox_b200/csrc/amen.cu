@@ -3,8 +3,12 @@
 // preconditioner, MEX local solver).  All cores, interfaces (Phi) and local
 // vectors live on the device; the host keeps ranks, the norm bookkeeping
 // scalars (nrmsa/nrmsy/nrmsx/nrmsc) and the truncation decisions.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "amen.h"
@@ -49,6 +53,39 @@ namespace {
 struct Core {
   DBuf<double> buf;
   double* p() const { return buf.p(); }
+};
+
+// Optional phase breakdown (TTG_PROFILE=1): synchronises at phase
+// boundaries and accumulates host-clock time per phase.
+struct PhaseProf {
+  bool on = false;
+  Context* c = nullptr;
+  std::chrono::steady_clock::time_point t0;
+  std::map<std::string, double> ms;
+  int cur = -1;
+  std::string name;
+  void start(Context* cc) {
+    const char* e = getenv("TTG_PROFILE");
+    on = e && e[0] == '1';
+    c = cc;
+  }
+  void mark(const char* n) {
+    if (!on) return;
+    sync(c);
+    auto t = std::chrono::steady_clock::now();
+    if (!name.empty()) ms[name] += std::chrono::duration<double, std::milli>(t - t0).count();
+    name = n;
+    t0 = t;
+  }
+  void report() {
+    if (!on) return;
+    mark("");
+    double tot = 0;
+    for (auto& kv : ms) tot += kv.second;
+    for (auto& kv : ms)
+      fprintf(stderr, "[ttg profile] %-14s %9.2f ms  (%4.1f%%)\n", kv.first.c_str(), kv.second,
+              100.0 * kv.second / (tot > 0 ? tot : 1));
+  }
 };
 
 // ||B x - rhs|| / nrhs with the FP64 local matvec (res into host).
@@ -157,8 +194,20 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
   TTG_CUDA(cudaEventCreate(&e0));
   TTG_CUDA(cudaEventCreate(&e1));
   TTG_CUDA(cudaEventRecord(e0, c->stream));
-  const int64_t mv0 = c->matvecs, fl0 = c->matvec_flops;
+  const int64_t mv0 = c->matvecs, fl0 = c->matvec_flops, la0 = c->launches;
+  const int64_t mvk0[2] = {c->mv_count[0], c->mv_count[1]};
+  const double flk0[2] = {c->mv_flops[0], c->mv_flops[1]};
+  c->ev_collect();
+  const double msk0[2] = {c->mv_ms[0], c->mv_ms[1]};
+  c->time_matvec = o.timing != 0;
+  struct TimingOff {
+    Context* c;
+    ~TimingOff() { c->time_matvec = false; }
+  } timing_off{c};
 
+  PhaseProf prof;
+  prof.start(c);
+  prof.mark("init");
   // Initial guesses (:222-224, :250-252).
   ttg_tt_s* x0own = nullptr;
   ttg_tt_s* z0own = nullptr;
@@ -209,6 +258,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
     // ------------- right-to-left orthogonalisation (:299-438)
     int64_t rznew = 0;
     for (int64_t i = d - 1; i >= 1; --i) {
+      prof.mark("rl_z");
       if (use_z && !last_sweep) {                                       // :301-324
         DBuf<double> zt;  // (n*rz_{i+1}) x k, to be orthogonalised
         int64_t kz = 0;
@@ -243,6 +293,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         transpose_f64(c, ncols, kq, Q.p(), ncols, crz[i].p(), kq);       // :322-323
       }
       if (swp > 1) nrmsc = nrmsc / (nrmsy[i - 1] / (nrmsa[i - 1] * nrmsx[i - 1]));  // :325-328
+      prof.mark("rl_qr");
       // QR of x_i^T (:331-342)
       const int64_t ncols = n[i] * rx[i + 1];
       DBuf<double> crT(c, ncols * rx[i]);
@@ -265,6 +316,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       crx[i].buf.reset(c, kq * ncols);
       transpose_f64(c, ncols, kq, Q.p(), ncols, crx[i].p(), kq);          // :360-362
       crx[i - 1].buf = std::move(cr2);
+      prof.mark("rl_phi");
       // Interfaces (:364-365)
       phia[i].buf.reset(c, rx[i] * ra[i] * rx[i]);
       next_phi_f64(c, 1, rx[i], n[i], rx[i + 1], rx[i], rx[i + 1], ra[i], ra[i + 1],
@@ -307,6 +359,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       gemm_f64(c, false, false, rx[i] * n[i], rx[i + 1], ry[i + 1], 1.0, t.p(), rx[i] * n[i], 0,
                phiy[i + 1].p(), ry[i + 1], 0, 0.0, rhs.p(), rx[i] * n[i], 0, 1);
       const double norm_rhs = host_norm(c, N, rhs.p());                  // :462
+      prof.mark("lr_solve");
       const double real_tol = (tol / std::sqrt(double(d))) / resid_damp; // :466
       const bool full = N < max_full_size;                                // :468
       DBuf<double> sol(c, N), tmp(c, N), B, t1(c, md.t1_size()), t2(c, md.t2_size());
@@ -347,6 +400,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         max_dx = std::max(max_dx, dx);
         max_res = std::max(max_res, res_prev);                            // :521
       }
+      prof.mark("lr_trunc");
       // Truncation (:530-601)
       const int64_t M = rx[i] * n[i], r2 = rx[i + 1];
       DBuf<double> u, v;  // u: M x r ; v: r2 x r
@@ -398,6 +452,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         transpose_f64(c, K, r2, R.p(), K, v.p(), r2);
       }
 
+      prof.mark("lr_z");
       DBuf<double> uv;
       if ((use_z && !last_sweep) || (i < d - 1 && kickrank > 0 && !last_sweep)) {
         uv.reset(c, M * r2);
@@ -427,6 +482,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       }
 
       if (i < d - 1) {                                                     // :625
+        prof.mark("lr_kick");
         if (kickrank > 0 && !last_sweep) {                                 // :626
           MvDims ld{rx[i], rx[i], ra[i], n[i], n[i], rx[i + 1], ra[i + 1], rz[i + 1]};
           DBuf<double> leftresid(c, ld.out_size());
@@ -466,6 +522,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         else
           curnorm = 1.0;
         nrmsx[i] *= curnorm;
+        prof.mark("lr_phi");
         // Interfaces (:751-752)
         phia[i + 1].buf.reset(c, r * r * ra[i + 1]);
         next_phi_f64(c, 0, rx[i], n[i], r, rx[i], r, ra[i], ra[i + 1], phia[i].p(), u.p(), A1,
@@ -510,6 +567,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
     if (max_res < tol_exit) last_sweep = true;                             // :806-808
   }
 
+  prof.report();
   // Distribute the norms (:816-820) and assemble the output.
   double lsum = 0.0;
   for (double v : nrmsx) lsum += std::log(v);
@@ -543,6 +601,15 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
     stats->max_rank = mr;
     stats->ms_total = ms;
     stats->matvec_gflop = double(c->matvec_flops - fl0) * 1e-9;
+    stats->launches = c->launches - la0;
+    c->ev_collect();
+    stats->matvecs_lp = c->mv_count[1] - mvk0[1];
+    stats->gflop_lp = (c->mv_flops[1] - flk0[1]) * 1e-9;
+    stats->ms_lp = c->mv_ms[1] - msk0[1];
+    stats->gflop_fp64 = (c->mv_flops[0] - flk0[0]) * 1e-9;
+    stats->ms_fp64 = c->mv_ms[0] - msk0[0];
+    stats->ms_matvec = o.precision == TTG_MIXED ? stats->ms_lp : stats->ms_fp64;
+    (void)mvk0;
   }
   return out;
 }

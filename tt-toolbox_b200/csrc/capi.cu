@@ -4,6 +4,7 @@
 #include "amen.h"
 #include "linalg.h"
 #include "round.h"
+#include "mixed_ops.h"
 
 using namespace ttg;
 
@@ -24,6 +25,8 @@ void ttg_amen_opts_default(ttg_amen_opts* o) {
   o->precision = TTG_FP64;
   o->verb = 0;
   o->seed = 0x243F6A8885A308D3ull;
+  o->timing = 0;
+  o->reserved = 0;
 }
 
 int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax, int32_t precision,
@@ -67,13 +70,31 @@ int ttg_local_matvec(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64
   TTG_API_BEGIN
   TTG_REQUIRE(ctx && Phi1 && A && Phi2 && x && y, "NULL argument");
   TTG_REQUIRE(rx1 >= 1 && n >= 1 && rx2 >= 1 && ra1 >= 1 && ra2 >= 1, "sizes must be >= 1");
-  TTG_REQUIRE(precision == TTG_FP64, "ttg_local_matvec: precision %d not available",
-              precision);
+  TTG_REQUIRE(precision == TTG_FP64 || precision == TTG_MIXED,
+              "ttg_local_matvec: unknown precision %d", precision);
   Context* c = &ctx->c;
   TTG_CUDA(cudaSetDevice(c->device));
   MvDims d{rx1, rx1, ra1, n, n, rx2, ra2, rx2};
-  local_matvec_f64(c, d, Phi1, A, Phi2, x, y);
+  if (precision == TTG_FP64) {
+    local_matvec_f64(c, d, Phi1, A, Phi2, x, y);
+  } else {
+    // BF16 tensor-core path; vectors go through the reversed FP32 layout.
+    const int64_t sz = d.in_size();
+    MixedOp op;
+    op.prepare(c, d, Phi1, A, Phi2);
+    DBuf<float> xr(c, sz), yr(c, sz);
+    TTG_CUDA(cudaMemsetAsync(c->d_err + 1, 0, sizeof(int), c->stream));
+    nat_to_rev(c, rx1, n, rx2, x, xr.p(), 1.0);
+    op.apply(c, xr.p(), yr.p());
+    fill_f64(c, sz, 0.0, y);
+    rev_to_nat_add(c, rx1, n, rx2, yr.p(), y, 1.0);
+  }
   sync(c);
+  if (precision == TTG_MIXED) {
+    int herr = 0;
+    TTG_CUDA(cudaMemcpy(&herr, c->d_err + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) fail(TTG_ERR_TIMEOUT, "tensor-core matvec: a bounded wait timed out");
+  }
   TTG_API_END
 }
 

@@ -203,6 +203,25 @@ int ttg_memcpy_d2h(ttg_context ctx, void* dst, const void* src, size_t bytes) {
   TTG_API_END
 }
 
+int ttg_memset(ttg_context ctx, void* dst, int value, size_t bytes) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx, "ctx is NULL");
+  TTG_REQUIRE(bytes == 0 || dst, "NULL pointer");
+  TTG_CUDA(cudaSetDevice(ctx->c.device));
+  if (bytes) {
+    TTG_CUDA(cudaMemsetAsync(dst, value, bytes, ctx->c.stream));
+    sync(&ctx->c);
+  }
+  TTG_API_END
+}
+
+int ttg_launch_count(ttg_context ctx, int64_t* out) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && out, "NULL argument");
+  *out = ctx->c.launches;
+  TTG_API_END
+}
+
 // ---------------------------------------------------------------------------
 // C ABI: TT handles
 // ---------------------------------------------------------------------------

@@ -34,7 +34,7 @@ struct HhArgs {
   double* tau;   // nrestart+1
   double* J;     // 2 x nrestart
   double* R;     // nrestart x nrestart
-  double* scal;  // [0] nrmrhs [1] curres [2] nrmr [3] exact-flag
+  double* scal;  // [0] nrmrhs [1] curres [2] nrmr [3] exact-flag [4] w[j+1]
   double* part;  // 2 * gridDim.x
   unsigned* bar; // [0] count [1] generation [2] reduction parity
   int* err;
@@ -173,10 +173,15 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
     GRID_LOOP(i, sz) w[i] -= 2.0 * dot * Ur[i];
   }
   if (j < sz - 1) {
+    // The owner of w[j+1] publishes it before the barrier: after the barrier
+    // it rewrites w[j+1], so other blocks must not read w itself.
     double s = 0.0;
-    GRID_LOOP(i, sz) if (i > j) s += w[i] * w[i];
+    GRID_LOOP(i, sz) {
+      if (i > j) s += w[i] * w[i];
+      if (i == j + 1) a.scal[4] = w[i];
+    }
     double alpha = sqrt(grid_sum(s, a, parity));
-    const double wj1 = __ldcg(w + j + 1);
+    const double wj1 = __ldcg(a.scal + 4);
     double* Un = a.U + (j + 1) * sz;
     if (alpha != 0.0) {
       if (wj1 < 0.0) alpha = -alpha;

@@ -115,10 +115,57 @@ struct Context {
   int64_t launches = 0;
   int64_t matvecs = 0;
   int64_t matvec_flops = 0;
-  float ms_matvec = 0.f;
-  // Event timing of the local matvec (optional).
+  // Per-kind local-matvec counters: [0] FP64 (DMMA), [1] BF16 (tcgen05).
+  int64_t mv_count[2] = {0, 0};
+  double mv_flops[2] = {0.0, 0.0};
+  // Optional CUDA-event timing of every local matvec on the context stream.
   bool time_matvec = false;
+  struct EvPair {
+    cudaEvent_t a, b;
+    int kind;
+  };
+  std::vector<EvPair> ev_pool;
+  size_t ev_used = 0;
+  double mv_ms[2] = {0.0, 0.0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  int ev_begin(int kind) {
+    if (ev_used == ev_pool.size()) {
+      EvPair p{};
+      cudaEventCreate(&p.a);
+      cudaEventCreate(&p.b);
+      ev_pool.push_back(p);
+    }
+    ev_pool[ev_used].kind = kind;
+    cudaEventRecord(ev_pool[ev_used].a, stream);
+    return int(ev_used++);
+  }
+  void ev_end(int i) { cudaEventRecord(ev_pool[i].b, stream); }
+  // Accumulate the elapsed time of all recorded pairs into mv_ms (syncs).
+  void ev_collect() {
+    cudaStreamSynchronize(stream);
+    for (size_t i = 0; i < ev_used; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev_pool[i].a, ev_pool[i].b);
+      mv_ms[ev_pool[i].kind] += ms;
+    }
+    ev_used = 0;
+  }
+};
+
+// Scope guard: records an event pair around a local matvec when timing is on.
+struct MvTiming {
+  Context* c;
+  int idx = -1;
+  MvTiming(Context* cc, int kind) : c(cc) {
+    if (c->time_matvec) {
+      if (c->ev_used >= 4096) c->ev_collect();
+      idx = c->ev_begin(kind);
+    }
+  }
+  ~MvTiming() {
+    if (idx >= 0) c->ev_end(idx);
+  }
 };
 
 template <typename T>

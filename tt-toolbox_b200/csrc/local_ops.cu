@@ -10,6 +10,7 @@ namespace ttg {
 
 void local_matvec_f64(Context* c, const MvDims& d, const double* Phi1, const double* A,
                       const double* Phi2, const double* x, double* y, double* t1, double* t2) {
+  MvTiming timing(c, 0);
   // (1) T1[(a,m),(be,k)] = x[(a,m), b] * Phi2[b, (be,k)]
   gemm_f64(c, false, false, d.rx1 * d.m, d.ra2 * d.ry2, d.rx2, 1.0, x, d.rx1 * d.m, 0, Phi2,
            d.rx2, 0, 0.0, t1, d.rx1 * d.m, 0, 1);
@@ -21,6 +22,8 @@ void local_matvec_f64(Context* c, const MvDims& d, const double* Phi1, const dou
            d.rx1 * d.ra1, 0, 0.0, y, d.ry1, 0, 1);
   c->matvecs += 1;
   c->matvec_flops += int64_t(d.flops());
+  c->mv_count[0] += 1;
+  c->mv_flops[0] += d.flops();
 }
 
 void local_matvec_f64(Context* c, const MvDims& d, const double* Phi1, const double* A,

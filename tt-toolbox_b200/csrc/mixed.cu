@@ -1,12 +1,382 @@
-// Mixed-precision local solve (placeholder until the tensor-core path lands).
+// Mixed-precision local solve: FP64 iterative refinement around an FP32
+// GMRES whose matvecs run on BF16 tensor cores (mixed_ops.cu).
+//
+// Same contract as the MEX local solver (fmex/solve3d_2.c:254-279): start
+// from sol_prev and stop once ||rhs - B sol|| <= tol ||rhs||, with the true
+// residual always evaluated by the FP64 matvec.  Each refinement step solves
+// B dx = r approximately in low precision (relative tolerance 1e-3 or the
+// remaining target, whichever is looser), then sol += dx and r is recomputed
+// in FP64.  The inner Krylov solver is GMRES(restart) with classical
+// Gram-Schmidt applied twice (CGS2): one cooperative kernel per Arnoldi step
+// performs both projections, the normalisation and the Givens update of the
+// least-squares residual; partial sums are reduced in a fixed order.
+#include <cmath>
+
 #include "mixed.h"
+#include "mixed_ops.h"
 
 namespace ttg {
 
-LocalSolveResult local_solve_mixed(Context*, const MvDims&, const double*, const double*,
-                                   const double*, const double*, double, const double*, int64_t,
-                                   int64_t, double*) {
-  fail(TTG_ERR_UNSUPPORTED, "precision TTG_MIXED is not available in this build");
+namespace {
+
+constexpr int AR_THREADS = 256;
+constexpr int AR_WARPS = AR_THREADS / 32;
+constexpr long long AR_SPIN_LIMIT = 1LL << 24;
+constexpr int MAX_OUTER = 8;
+constexpr double INNER_TOL = 1e-3;
+
+struct ArArgs {
+  int64_t sz;
+  int m;           // restart length
+  float* V;        // sz x (m+1)
+  float* w;        // matvec output, orthogonalised in place
+  double* H;       // (m+1) x m, column-major
+  double* cs;      // m
+  double* sn;      // m
+  double* g;       // m+1
+  double* scal;    // [0] |g_{j+1}|  [1] norm of the new Arnoldi vector  [2] beta
+  double* part;    // 2 * (m+1) * gridDim.x
+  unsigned* bar;   // [0] count [1] generation
+  int* err;
+};
+
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sumd(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ void ar_barrier(unsigned* bar, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = bar + 1;
+    volatile int* verr = err;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == gen) {
+        if (*verr) break;
+        if (++spins > AR_SPIN_LIMIT) {
+          atomicExch(err, 4);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+#define AR_LOOP(idx, n)                                                             \
+  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < (n);    \
+       idx += int64_t(gridDim.x) * blockDim.x)
+
+// part[c*nb + block] = block partial of V(:,c)'w, c < ncol.  red: AR_WARPS*(m+1) floats.
+__device__ void partial_dots(const ArArgs& a, int ncol, double* part, float* red) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = 0; c < ncol; ++c) {
+    const float* Vc = a.V + int64_t(c) * a.sz;
+    float s = 0.f;
+    AR_LOOP(i, a.sz) s += Vc[i] * a.w[i];
+    s = warp_sumf(s);
+    if (lane == 0) red[warp * (a.m + 1) + c] = s;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < AR_WARPS; ++q) s += double(red[q * (a.m + 1) + c]);
+    part[int64_t(c) * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// Sum the block partials of ncol columns (same fixed order in every block).
+__device__ void reduce_parts(const double* part, int ncol, double* out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = warp; c < ncol; c += AR_WARPS) {
+    double s = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) s += __ldcg(part + int64_t(c) * gridDim.x + b);
+    s = warp_sumd(s);
+    if (lane == 0) out[c] = s;
+  }
+  __syncthreads();
+}
+
+// One Arnoldi step for column j: w -= V h twice (CGS2), normalise into
+// V(:, j+1), Givens update of H(:, j) and g; scal[0] = |g_{j+1}|.
+__global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
+  extern __shared__ double shd[];
+  double* hp = shd;                 // m+1 : this pass's coefficients
+  double* ht = shd + (a.m + 1);     // m+2 : accumulated coefficients
+  float* red = reinterpret_cast<float*>(shd + 2 * (a.m + 2));
+  const int ncol = j + 1;
+  double* part0 = a.part;
+  double* part1 = a.part + int64_t(a.m + 1) * gridDim.x;
+  for (int c = threadIdx.x; c <= ncol; c += blockDim.x) ht[c] = 0.0;
+  for (int pass = 0; pass < 2; ++pass) {
+    double* part = pass ? part1 : part0;
+    partial_dots(a, ncol, part, red);
+    ar_barrier(a.bar, a.err);
+    reduce_parts(part, ncol, hp);
+    AR_LOOP(i, a.sz) {
+      float s = 0.f;
+      for (int c = 0; c < ncol; ++c) s += a.V[int64_t(c) * a.sz + i] * float(hp[c]);
+      a.w[i] -= s;
+    }
+    for (int c = threadIdx.x; c < ncol; c += blockDim.x) ht[c] += hp[c];
+    __syncthreads();
+  }
+  // norm of w (reuses part0: every block finished reading it before the
+  // second pass's barrier)
+  {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float s = 0.f;
+    AR_LOOP(i, a.sz) s += a.w[i] * a.w[i];
+    s = warp_sumf(s);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int q = 0; q < AR_WARPS; ++q) t += double(red[q]);
+      part0[blockIdx.x] = t;
+    }
+    ar_barrier(a.bar, a.err);
+    reduce_parts(part0, 1, hp);
+  }
+  const double nrm = sqrt(hp[0]);
+  float* Vn = a.V + int64_t(j + 1) * a.sz;
+  const float inv = nrm > 0.0 ? float(1.0 / nrm) : 0.f;
+  AR_LOOP(i, a.sz) Vn[i] = a.w[i] * inv;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double* Hj = a.H + int64_t(a.m + 1) * j;
+    for (int c = 0; c < ncol; ++c) Hj[c] = ht[c];
+    Hj[j + 1] = nrm;
+    for (int i = 0; i < j; ++i) {  // previous rotations
+      const double x = Hj[i], y = Hj[i + 1];
+      Hj[i] = a.cs[i] * x + a.sn[i] * y;
+      Hj[i + 1] = -a.sn[i] * x + a.cs[i] * y;
+    }
+    const double x = Hj[j], y = Hj[j + 1];
+    const double rho = sqrt(x * x + y * y);
+    const double c0 = rho > 0.0 ? x / rho : 1.0, s0 = rho > 0.0 ? y / rho : 0.0;
+    a.cs[j] = c0;
+    a.sn[j] = s0;
+    Hj[j] = rho;
+    Hj[j + 1] = 0.0;
+    a.g[j + 1] = -s0 * a.g[j];
+    a.g[j] = c0 * a.g[j];
+    a.scal[0] = fabs(a.g[j + 1]);
+    a.scal[1] = nrm;
+  }
+}
+
+// V(:,0) = r / ||r||, g = [||r||, 0, ...]; scal[2] = ||r||.
+__global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r) {
+  __shared__ float red[AR_WARPS];
+  __shared__ double tot[1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float s = 0.f;
+  AR_LOOP(i, a.sz) s += r[i] * r[i];
+  s = warp_sumf(s);
+  if (lane == 0) red[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < AR_WARPS; ++q) t += double(red[q]);
+    a.part[blockIdx.x] = t;
+  }
+  ar_barrier(a.bar, a.err);
+  reduce_parts(a.part, 1, tot);
+  const double beta = sqrt(tot[0]);
+  const float inv = beta > 0.0 ? float(1.0 / beta) : 0.f;
+  AR_LOOP(i, a.sz) a.V[i] = r[i] * inv;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int k = 0; k <= a.m; ++k) a.g[k] = 0.0;
+    a.g[0] = beta;
+    a.scal[2] = beta;
+    a.scal[0] = beta;
+  }
+}
+
+// x += V(:, 0:k) y with H(0:k,0:k) y = g(0:k) (upper triangular after Givens).
+__global__ void k_ar_update(ArArgs a, int k, float* x) {
+  extern __shared__ double y[];
+  if (threadIdx.x == 0) {
+    for (int row = k - 1; row >= 0; --row) {
+      double v = a.g[row];
+      for (int col = row + 1; col < k; ++col) v -= a.H[row + int64_t(a.m + 1) * col] * y[col];
+      const double d = a.H[row + int64_t(a.m + 1) * row];
+      y[row] = d != 0.0 ? v / d : 0.0;
+    }
+  }
+  __syncthreads();
+  AR_LOOP(i, a.sz) {
+    float s = 0.f;
+    for (int c = 0; c < k; ++c) s += a.V[int64_t(c) * a.sz + i] * float(y[c]);
+    x[i] += s;
+  }
+}
+
+// r = b - y (FP32)
+__global__ void k_sub_f32(int64_t n, const float* b, const float* y, float* r) {
+  AR_LOOP(i, n) r[i] = b[i] - y[i];
+}
+
+struct Gmres32 {
+  Context* c;
+  int64_t sz;
+  int m;
+  int blocks;
+  DBuf<float> V, w, r;
+  DBuf<double> small, part;
+  DBuf<unsigned> bar;
+  ArArgs a{};
+
+  Gmres32(Context* cc, int64_t n, int restart) : c(cc), sz(n), m(restart) {
+    V.reset(c, size_t(sz) * (m + 1));
+    w.reset(c, sz);
+    r.reset(c, sz);
+    small.reset(c, size_t(m + 1) * m + 2 * m + (m + 1) + 8);
+    int occ = 0;
+    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_arnoldi, AR_THREADS,
+                                                           arnoldi_smem()));
+    if (occ < 1) occ = 1;
+    int64_t want = (sz + AR_THREADS * 4 - 1) / (AR_THREADS * 4);
+    const int64_t cap = int64_t(c->num_sms) * std::min(occ, 2);
+    blocks = int(std::max<int64_t>(1, std::min(want, cap)));
+    part.reset(c, size_t(2) * (m + 1) * blocks);
+    bar.reset(c, 4);
+    TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 4 * sizeof(unsigned), c->stream));
+    a.sz = sz;
+    a.m = m;
+    a.V = V.p();
+    a.w = w.p();
+    a.H = small.p();
+    a.cs = a.H + size_t(m + 1) * m;
+    a.sn = a.cs + m;
+    a.g = a.sn + m;
+    a.scal = a.g + (m + 1);
+    a.part = part.p();
+    a.bar = bar.p();
+    a.err = c->d_err + 2;
+  }
+
+  size_t arnoldi_smem() const {
+    return sizeof(double) * (2 * (m + 2)) + sizeof(float) * AR_WARPS * (m + 1) + 16;
+  }
+
+  void coop(const void* k, void** args, size_t smem) {
+    TTG_CUDA(cudaLaunchCooperativeKernel(k, dim3(blocks), dim3(AR_THREADS), args, smem,
+                                         c->stream));
+    c->launches += 1;
+  }
+
+  // Solve B x = b approximately; x (FP32, zeroed here); returns Krylov steps.
+  int64_t solve(MixedOp& op, const float* b, float* x, double reltol, int64_t max_restarts) {
+    int64_t steps = 0;
+    TTG_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * sz, c->stream));
+    double bnorm = -1.0;
+    for (int64_t it = 0; it < max_restarts; ++it) {
+      const float* rr = b;
+      if (it > 0) {
+        op.apply(c, x, w.p());
+        k_sub_f32<<<blocks, AR_THREADS, 0, c->stream>>>(sz, b, w.p(), r.p());
+        c->launches += 1;
+        rr = r.p();
+      }
+      void* ai[] = {&a, &rr};
+      coop((const void*)k_ar_init, ai, 0);
+      double sc[3];
+      read_scalars(c, a.scal, sc, 3);
+      if (bnorm < 0) bnorm = sc[2];
+      if (sc[2] <= reltol * bnorm || sc[2] == 0.0) break;
+      int j = 0;
+      bool conv = false;
+      for (j = 0; j < m; ++j) {
+        op.apply(c, a.V + int64_t(j) * sz, w.p());
+        void* aa[] = {&a, &j};
+        coop((const void*)k_arnoldi, aa, arnoldi_smem());
+        ++steps;
+        double res;
+        read_scalars(c, a.scal, &res, 1);
+        if (res <= reltol * bnorm) {
+          conv = true;
+          break;
+        }
+      }
+      const int k = conv ? j + 1 : m;
+      k_ar_update<<<blocks, AR_THREADS, sizeof(double) * (m + 1), c->stream>>>(a, k, x);
+      c->launches += 1;
+      TTG_CHECK_LAUNCH();
+      if (conv) break;
+    }
+    return steps;
+  }
+};
+
+}  // namespace
+
+LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Phi1,
+                                   const double* A, const double* Phi2, const double* rhs,
+                                   double tol, const double* sol_prev, int64_t nrestart,
+                                   int64_t niters, double* sol) {
+  LocalSolveResult out;
+  const int64_t sz = d.in_size();
+  if (nrestart > sz) nrestart = sz;
+  TTG_REQUIRE(nrestart <= 1024, "mixed solve: restart length %lld too large", (long long)nrestart);
+  MixedOp op;
+  op.prepare(c, d, Phi1, A, Phi2);
+  Gmres32 gm(c, sz, int(nrestart));
+  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size()), r64(c, sz), prev(c, sz), s(c, 2);
+  DBuf<float> rrev(c, sz), dx(c, sz);
+  TTG_CUDA(cudaMemsetAsync(c->d_err + 1, 0, 2 * sizeof(int), c->stream));
+  copy_f64(c, sz, sol_prev, sol);
+  auto residual = [&]() -> double {
+    local_matvec_f64(c, d, Phi1, A, Phi2, sol, r64.p(), t1.p(), t2.p());
+    out.matvecs_fp64++;
+    axpby_f64(c, sz, 1.0, rhs, -1.0, r64.p());
+    dot_f64(c, sz, r64.p(), nullptr, s.p(), true);
+    double h;
+    read_scalars(c, s.p(), &h, 1);
+    return h;
+  };
+  const double nrhs = nrm2_host(c, sz, rhs);
+  const double target = tol * nrhs;
+  double nr = residual();
+  for (int outer = 0; outer < MAX_OUTER; ++outer) {
+    if (!(nr > target)) break;
+    nat_to_rev(c, d.rx1, d.n, d.rx2, r64.p(), rrev.p(), 1.0 / nr);
+    const double reltol = std::max(target / nr, INNER_TOL);
+    out.iters += gm.solve(op, rrev.p(), dx.p(), reltol, niters);
+    copy_f64(c, sz, sol, prev.p());
+    rev_to_nat_add(c, d.rx1, d.n, d.rx2, dx.p(), sol, nr);
+    const double nr_new = residual();
+    if (!(nr_new < nr)) {  // no progress: keep the better iterate and stop
+      copy_f64(c, sz, prev.p(), sol);
+      break;
+    }
+    const bool stagnating = nr_new > 0.5 * nr;
+    nr = nr_new;
+    if (stagnating) break;
+  }
+  int herr[2] = {0, 0};
+  TTG_CUDA(cudaMemcpyAsync(herr, c->d_err + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                           c->stream));
+  sync(c);
+  if (herr[0] || herr[1]) fail(TTG_ERR_TIMEOUT, "mixed solve: a bounded device wait timed out");
+  out.matvecs = out.iters;
+  return out;
 }
 
 }  // namespace ttg

@@ -1,0 +1,388 @@
+// BF16 tensor-core (tcgen05) local matvec for the mixed-precision path.
+//
+// y = (Phi1 x A x Phi2) x is three GEMMs (see local_ops.cu).  Here every
+// operand is stored K-major in BF16 so that each stage is one tcgen05 GEMM
+// fed by TMA (128-byte swizzle), accumulating in FP32 in tensor memory.  The
+// layouts of the two intermediates are chosen by the epilogue of the stage
+// that produces them, so no permutation pass runs between the stages:
+//
+//   vector layout ("reversed"): v[k + rx2*(j + n*i)]      (i: rx1, j: n, k: rx2)
+//   stage 1  T1[(m,a),(be,k)] = X[(m,a), b] * Phi2[b,(be,k)]        K = rx2
+//            X  = v as bf16 rows (m,a), K-major, ld ldx
+//            T1 stored [(m,be) | ld1][a][k]  (K-major operand of stage 2)
+//   stage 2  per k: T2_k[a,(al,j)] = T1_k[a,(m,be)] * AT[(al,j),(m,be)]  K = n*ra2
+//            T2 stored [(a,al) | ld2][k][j]  (K-major operand of stage 3)
+//   stage 3  y[(k,j), i] = T2[(k,j),(a,al)] * Phi1T[i,(a,al)]        K = rx1*ra1
+//            written straight into the reversed vector layout (FP32).
+//
+// One CTA computes a 128 x BN tile: warp 0 issues TMA loads into a 3-stage
+// shared-memory ring, one thread of warp 1 issues tcgen05.mma (M=128, N=BN,
+// K=16) and commits to mbarriers, and all four warps drain the FP32
+// accumulator from tensor memory (tcgen05.ld) in the epilogue.  All waits
+// are bounded; a timeout sets the context error flag.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+#include "mixed_ops.h"
+#include "umma.cuh"
+
+namespace ttg {
+
+namespace {
+
+constexpr int UM_STAGES = 3;
+constexpr int UM_BM = 128;
+constexpr int UM_BK = 64;
+constexpr int UM_A_BYTES = UM_BM * UM_BK * 2;
+
+struct OutMap {
+  void* base;
+  int64_t M, N;            // valid extents per batch
+  int64_t r_s1, r_t1, r_t2;
+  int64_t c_s1, c_t1, c_t2;
+  int64_t batch_stride;    // elements
+};
+
+__device__ __forceinline__ int64_t map2(int64_t i, int64_t s1, int64_t t1, int64_t t2) {
+  return (i % s1) * t1 + (i / s1) * t2;
+}
+
+template <int BN>
+constexpr size_t umma_smem_bytes() {
+  return 1024 + size_t(UM_STAGES) * (UM_A_BYTES + BN * UM_BK * 2) + (2 * UM_STAGES + 1) * 8 + 16;
+}
+
+template <int BN, bool OUT_BF16>
+__global__ void __launch_bounds__(128, 1)
+    k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                int K, int a_rows_pb, int b_rows_pb, OutMap om, int* err) {
+  using namespace umma;
+  constexpr int B_BYTES = BN * UM_BK * 2;
+  constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + UM_STAGES * UM_A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + UM_STAGES * B_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * UM_STAGES + 1);
+  const uint32_t bar_full = smem_u32(bars);
+  const uint32_t bar_empty = smem_u32(bars + UM_STAGES);
+  const uint32_t bar_done = smem_u32(bars + 2 * UM_STAGES);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * UM_BM, n0 = blockIdx.y * BN, bz = blockIdx.z;
+  const int nk = (K + UM_BK - 1) / UM_BK;
+
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
+    tmem_relinquish();
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < UM_STAGES; ++s) {
+      mbar_init(bar_full + 8 * s, 1);
+      mbar_init(bar_empty + 8 * s, 1);
+    }
+    mbar_init(bar_done, 1);
+    fence_barrier_init();
+    fence_proxy_async();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // TMA producer.
+    const int arow = bz * a_rows_pb + m0, brow = bz * b_rows_pb + n0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % UM_STAGES;
+      if (kb >= UM_STAGES) {
+        if (!mbar_wait(bar_empty + 8 * s, ((kb / UM_STAGES) - 1) & 1, err)) break;
+      }
+      mbar_expect_tx(bar_full + 8 * s, UM_A_BYTES + B_BYTES);
+      tma_load_2d(smem_u32(sA + s * UM_A_BYTES), &tmA, kb * UM_BK, arow, bar_full + 8 * s);
+      tma_load_2d(smem_u32(sB + s * B_BYTES), &tmB, kb * UM_BK, brow, bar_full + 8 * s);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer.
+    const uint32_t idesc = idesc_bf16_f32(UM_BM, BN);
+    bool ok = true;
+    for (int kb = 0; kb < nk && ok; ++kb) {
+      const int s = kb % UM_STAGES;
+      ok = mbar_wait(bar_full + 8 * s, (kb / UM_STAGES) & 1, err);
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(sA + s * UM_A_BYTES), b0 = smem_u32(sB + s * B_BYTES);
+#pragma unroll
+      for (int kk = 0; kk < UM_BK / 16; ++kk) {
+        mma_bf16(tmem, desc_k_sw128(a0 + kk * 32), desc_k_sw128(b0 + kk * 32), idesc,
+                 (kb > 0 || kk > 0) ? 1u : 0u);
+      }
+      mma_commit(bar_empty + 8 * s);
+    }
+    mma_commit(bar_done);
+  }
+  __syncwarp();
+
+  // Epilogue: warp w owns accumulator rows (TMEM lanes) 32w .. 32w+31.
+  const bool ok = mbar_wait(bar_done, 0, err);
+  tc_fence_after();
+  if (ok) {
+    const int row = warp * 32 + lane;
+    const int64_t m = int64_t(m0) + row;
+    const bool row_ok = m < om.M;
+    const int64_t roff = row_ok ? map2(m, om.r_s1, om.r_t1, om.r_t2) : 0;
+    const int64_t boff = int64_t(bz) * om.batch_stride;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      if (n0 + c0 >= om.N) break;  // uniform across the CTA
+      float v[16];
+      tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
+      if (row_ok) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int64_t n = int64_t(n0) + c0 + j;
+          if (n < om.N) {
+            const int64_t off = boff + roff + map2(n, om.c_s1, om.c_t1, om.c_t2);
+            if (OUT_BF16)
+              static_cast<__nv_bfloat16*>(om.base)[off] = __float2bfloat16_rn(v[j]);
+            else
+              static_cast<float*>(om.base)[off] = v[j];
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Operand conversion kernels (FP64/FP32 -> BF16, K-major layouts)
+// ---------------------------------------------------------------------------
+
+// Phi2b[b + ldp*col] = Phi2[b, col], col = (be, k)  (zero padding b >= rx2)
+__global__ void k_cvt_phi2(int64_t rx2, int64_t ncols, int64_t ldp, const double* __restrict__ P,
+                           __nv_bfloat16* __restrict__ out) {
+  const int64_t total = ldp * ncols;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = e % ldp, col = e / ldp;
+    out[e] = __float2bfloat16_rn(b < rx2 ? float(P[b + rx2 * col]) : 0.f);
+  }
+}
+
+// AT[(m + n*be) + ld1*(al + ra1*j)] = A[al, j, m, be]
+__global__ void k_cvt_AT(int64_t ra1, int64_t n, int64_t ra2, int64_t ld1,
+                         const double* __restrict__ A, __nv_bfloat16* __restrict__ out) {
+  const int64_t total = ld1 * ra1 * n;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t kk = e % ld1, row = e / ld1;
+    float v = 0.f;
+    if (kk < n * ra2) {
+      const int64_t mm = kk % n, be = kk / n, al = row % ra1, j = row / ra1;
+      v = float(A[al + ra1 * (j + n * (mm + n * be))]);
+    }
+    out[e] = __float2bfloat16_rn(v);
+  }
+}
+
+// Phi1T[(a + rx1*al) + ld2*i] = Phi1[i, a, al]
+__global__ void k_cvt_phi1(int64_t ry1, int64_t rx1, int64_t ra1, int64_t ld2,
+                           const double* __restrict__ P, __nv_bfloat16* __restrict__ out) {
+  const int64_t total = ld2 * ry1;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t kk = e % ld2, i = e / ld2;
+    float v = 0.f;
+    if (kk < rx1 * ra1) {
+      const int64_t a = kk % rx1, al = kk / rx1;
+      v = float(P[i + ry1 * (a + rx1 * al)]);
+    }
+    out[e] = __float2bfloat16_rn(v);
+  }
+}
+
+// X[b + ldx*row] = v[b + rx2*row]  (row = m + n*a; zero padding)
+__global__ void k_cvt_x(int64_t rx2, int64_t rows, int64_t ldx, const float* __restrict__ v,
+                        __nv_bfloat16* __restrict__ out) {
+  const int64_t total = ldx * rows;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = e % ldx, row = e / ldx;
+    out[e] = __float2bfloat16_rn(b < rx2 ? v[b + rx2 * row] : 0.f);
+  }
+}
+
+// Natural [i, j, k] (FP64) <-> reversed [k, j, i] (FP32) vector layouts.
+__global__ void k_nat_to_rev(int64_t r1, int64_t n, int64_t r2, const double* __restrict__ x,
+                             float* __restrict__ y, double scale) {
+  const int64_t total = r1 * n * r2;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = e % r2, j = (e / r2) % n, i = e / (r2 * n);
+    y[e] = float(x[i + r1 * (j + n * k)] * scale);
+  }
+}
+
+__global__ void k_rev_to_nat_add(int64_t r1, int64_t n, int64_t r2, const float* __restrict__ y,
+                                 double* __restrict__ x, double scale) {
+  const int64_t total = r1 * n * r2;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e % r1, j = (e / r1) % n, k = e / (r1 * n);
+    x[e] += scale * double(y[k + r2 * (j + n * i)]);
+  }
+}
+
+int blocks_for(Context* c, int64_t n) {
+  int64_t b = (n + 255) / 256;
+  const int64_t cap = int64_t(c->num_sms) * 8;
+  if (b > cap) b = cap;
+  return int(b < 1 ? 1 : b);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+void make_map(CUtensorMap* map, const void* ptr, int64_t K, int64_t rows, int64_t ld,
+              int box_rows) {
+  std::call_once(g_encode_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!g_encode) fail(TTG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  TTG_REQUIRE(ld % 8 == 0 && (reinterpret_cast<uintptr_t>(ptr) & 15) == 0,
+              "TMA operand not 16-byte aligned");
+  cuuint64_t gdim[2] = {cuuint64_t(K), cuuint64_t(rows)};
+  cuuint64_t gstride[1] = {cuuint64_t(ld) * 2};
+  cuuint32_t box[2] = {cuuint32_t(UM_BK), cuuint32_t(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), gdim,
+                        gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(TTG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+}
+
+template <int BN, bool OB>
+void launch_bn(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t K,
+               int64_t a_rows_pb, int64_t b_rows_pb, int64_t M, int64_t N, int64_t batch,
+               const OutMap& om) {
+  const size_t smem = umma_smem_bytes<BN>();
+  static bool configured = false;
+  if (!configured) {
+    TTG_CUDA(cudaFuncSetAttribute(k_umma_gemm<BN, OB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem)));
+    configured = true;
+  }
+  dim3 grid{unsigned((M + UM_BM - 1) / UM_BM), unsigned((N + BN - 1) / BN), unsigned(batch)};
+  k_umma_gemm<BN, OB><<<grid, 128, smem, c->stream>>>(ta, tb, int(K), int(a_rows_pb),
+                                                      int(b_rows_pb), om, c->d_err + 1);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void umma_gemm(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t K,
+               int64_t a_rows_pb, int64_t b_rows_pb, int64_t M, int64_t N, int64_t batch,
+               const OutMap& om, bool out_bf16, int bn) {
+  TTG_REQUIRE(M < (1ll << 31) && N < (1ll << 31) && batch <= 65535, "umma gemm too large");
+  if (out_bf16) {
+    if (bn == 64) launch_bn<64, true>(c, ta, tb, K, a_rows_pb, b_rows_pb, M, N, batch, om);
+    else if (bn == 128) launch_bn<128, true>(c, ta, tb, K, a_rows_pb, b_rows_pb, M, N, batch, om);
+    else launch_bn<256, true>(c, ta, tb, K, a_rows_pb, b_rows_pb, M, N, batch, om);
+  } else {
+    if (bn == 64) launch_bn<64, false>(c, ta, tb, K, a_rows_pb, b_rows_pb, M, N, batch, om);
+    else if (bn == 128) launch_bn<128, false>(c, ta, tb, K, a_rows_pb, b_rows_pb, M, N, batch, om);
+    else launch_bn<256, false>(c, ta, tb, K, a_rows_pb, b_rows_pb, M, N, batch, om);
+  }
+}
+
+int pick_bn(int64_t N) { return N <= 64 ? 64 : (N <= 128 ? 128 : 256); }
+
+int64_t up8(int64_t v) { return (v + 7) / 8 * 8; }
+
+}  // namespace
+
+void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const double* A,
+                      const double* Phi2) {
+  d = dd;
+  TTG_REQUIRE(d.n == d.m, "mixed matvec needs square A cores");
+  ldx = up8(d.rx2);
+  ld1 = up8(d.n * d.ra2);
+  ld2 = up8(d.rx1 * d.ra1);
+  TTG_REQUIRE(d.n * d.rx1 < (1ll << 31) && d.rx1 * d.ry2 < (1ll << 31), "mixed matvec too large");
+  phi2b.reset(c, ldx * d.ra2 * d.ry2);
+  AT.reset(c, ld1 * d.ra1 * d.n);
+  phi1T.reset(c, ld2 * d.ry1);
+  X.reset(c, ldx * d.m * d.rx1);
+  T1.reset(c, ld1 * d.rx1 * d.ry2);
+  T2.reset(c, ld2 * d.ry2 * d.n);
+  k_cvt_phi2<<<blocks_for(c, phi2b.size()), 256, 0, c->stream>>>(d.rx2, d.ra2 * d.ry2, ldx, Phi2,
+                                                                 phi2b.p());
+  k_cvt_AT<<<blocks_for(c, AT.size()), 256, 0, c->stream>>>(d.ra1, d.n, d.ra2, ld1, A, AT.p());
+  k_cvt_phi1<<<blocks_for(c, phi1T.size()), 256, 0, c->stream>>>(d.ry1, d.rx1, d.ra1, ld2, Phi1,
+                                                                 phi1T.p());
+  c->launches += 3;
+  TTG_CHECK_LAUNCH();
+  bn1 = pick_bn(d.ra2 * d.ry2);
+  bn2 = pick_bn(d.ra1 * d.n);
+  bn3 = pick_bn(d.ry1);
+  make_map(&mapX, X.p(), d.rx2, d.m * d.rx1, ldx, UM_BM);
+  make_map(&mapP2, phi2b.p(), d.rx2, d.ra2 * d.ry2, ldx, bn1);
+  make_map(&mapT1, T1.p(), d.n * d.ra2, d.rx1 * d.ry2, ld1, UM_BM);
+  make_map(&mapAT, AT.p(), d.n * d.ra2, d.ra1 * d.n, ld1, bn2);
+  make_map(&mapT2, T2.p(), d.rx1 * d.ra1, d.ry2 * d.n, ld2, UM_BM);
+  make_map(&mapP1, phi1T.p(), d.rx1 * d.ra1, d.ry1, ld2, bn3);
+}
+
+void MixedOp::apply(Context* c, const float* v, float* y) {
+  MvTiming timing(c, 1);
+  const int64_t rows = d.m * d.rx1;
+  k_cvt_x<<<blocks_for(c, ldx * rows), 256, 0, c->stream>>>(d.rx2, rows, ldx, v, X.p());
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+  // stage 1: T1[(m,a),(be,k)]
+  OutMap o1{T1.p(), rows, d.ra2 * d.ry2, d.m, 1, ld1, d.ra2, d.m, ld1 * d.rx1, 0};
+  umma_gemm(c, mapX, mapP2, d.rx2, 0, 0, rows, d.ra2 * d.ry2, 1, o1, true, bn1);
+  // stage 2: per k, T2_k[a,(al,j)]
+  OutMap o2{T2.p(), d.rx1, d.ra1 * d.n, d.rx1, 1, 0, d.ra1, d.rx1, ld2 * d.ry2, ld2};
+  umma_gemm(c, mapT1, mapAT, d.n * d.ra2, d.rx1, 0, d.rx1, d.ra1 * d.n, d.ry2, o2, true, bn2);
+  // stage 3: y[(k,j), i] in the reversed vector layout
+  const int64_t rows3 = d.ry2 * d.n;
+  OutMap o3{y, rows3, d.ry1, rows3, 1, 0, d.ry1, rows3, 0, 0};
+  umma_gemm(c, mapT2, mapP1, d.rx1 * d.ra1, 0, 0, rows3, d.ry1, 1, o3, false, bn3);
+  c->matvecs += 1;
+  c->matvec_flops += int64_t(d.flops());
+  c->mv_count[1] += 1;
+  c->mv_flops[1] += d.flops();
+}
+
+void nat_to_rev(Context* c, int64_t r1, int64_t n, int64_t r2, const double* x, float* y,
+                double scale) {
+  k_nat_to_rev<<<blocks_for(c, r1 * n * r2), 256, 0, c->stream>>>(r1, n, r2, x, y, scale);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void rev_to_nat_add(Context* c, int64_t r1, int64_t n, int64_t r2, const float* y, double* x,
+                    double scale) {
+  k_rev_to_nat_add<<<blocks_for(c, r1 * n * r2), 256, 0, c->stream>>>(r1, n, r2, y, x, scale);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+}  // namespace ttg

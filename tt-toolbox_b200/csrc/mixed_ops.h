@@ -1,0 +1,31 @@
+// BF16 tcgen05 local matvec (mixed-precision path).
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include "local_ops.h"
+
+namespace ttg {
+
+// One local operator (Phi1, A_k, Phi2) converted to BF16 K-major operands,
+// with its scratch intermediates and TMA descriptors.  apply() maps a vector
+// in the reversed layout v[k + rx2*(j + n*i)] (FP32) to y in the same layout.
+struct MixedOp {
+  MvDims d{};
+  int64_t ldx = 0, ld1 = 0, ld2 = 0;
+  int bn1 = 128, bn2 = 128, bn3 = 128;
+  DBuf<__nv_bfloat16> phi2b, AT, phi1T, X, T1, T2;
+  CUtensorMap mapX, mapP2, mapT1, mapAT, mapT2, mapP1;
+  void prepare(Context* c, const MvDims& d, const double* Phi1, const double* A,
+               const double* Phi2);
+  void apply(Context* c, const float* v, float* y);
+};
+
+// Natural [i, j, k] FP64 <-> reversed [k, j, i] FP32 vector layouts.
+void nat_to_rev(Context* c, int64_t r1, int64_t n, int64_t r2, const double* x, float* y,
+                double scale);
+// x[natural] += scale * y[reversed]
+void rev_to_nat_add(Context* c, int64_t r1, int64_t n, int64_t r2, const float* y, double* x,
+                    double scale);
+
+}  // namespace ttg

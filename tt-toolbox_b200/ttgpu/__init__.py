@@ -42,7 +42,8 @@ class AmenOpts(C.Structure):
                 ("local_restart", _i64), ("local_iters", _i64), ("kickrank", _i64),
                 ("resid_damp", C.c_double), ("tol_exit", C.c_double),
                 ("trunc_norm", C.c_int32), ("local_prec", C.c_int32),
-                ("precision", C.c_int32), ("verb", C.c_int32), ("seed", C.c_uint64)]
+                ("precision", C.c_int32), ("verb", C.c_int32), ("seed", C.c_uint64),
+                ("timing", C.c_int32), ("reserved", C.c_int32)]
 
 
 MAX_SWEEPS = 64
@@ -53,7 +54,9 @@ class AmenStats(C.Structure):
                 ("local_solves", _i64), ("gmres_iters", _i64), ("max_rank", _i64),
                 ("max_res", C.c_double * MAX_SWEEPS), ("max_dx", C.c_double * MAX_SWEEPS),
                 ("ms_total", C.c_double), ("ms_matvec", C.c_double),
-                ("matvec_gflop", C.c_double)]
+                ("matvec_gflop", C.c_double), ("launches", _i64), ("matvecs_lp", _i64),
+                ("gflop_lp", C.c_double), ("ms_lp", C.c_double), ("gflop_fp64", C.c_double),
+                ("ms_fp64", C.c_double)]
 
     def to_dict(self):
         s = int(self.sweeps)
@@ -62,7 +65,10 @@ class AmenStats(C.Structure):
                     local_solves=int(self.local_solves), gmres_iters=int(self.gmres_iters),
                     max_rank=int(self.max_rank), max_res=list(self.max_res[:k]),
                     max_dx=list(self.max_dx[:k]), ms_total=float(self.ms_total),
-                    matvec_gflop=float(self.matvec_gflop))
+                    matvec_gflop=float(self.matvec_gflop), launches=int(self.launches),
+                    ms_matvec=float(self.ms_matvec), matvecs_lp=int(self.matvecs_lp),
+                    gflop_lp=float(self.gflop_lp), ms_lp=float(self.ms_lp),
+                    gflop_fp64=float(self.gflop_fp64), ms_fp64=float(self.ms_fp64))
 
 
 class RoundStats(C.Structure):
@@ -92,6 +98,8 @@ def lib():
         "ttg_free": [_vp, _vp],
         "ttg_memcpy_h2d": [_vp, _vp, _vp, C.c_size_t],
         "ttg_memcpy_d2h": [_vp, _vp, _vp, C.c_size_t],
+        "ttg_memset": [_vp, _vp, C.c_int, C.c_size_t],
+        "ttg_launch_count": [_vp, _p64],
         "ttg_tt_upload": [_vp, _i64, _p64, _p64, _p64, _pd, C.POINTER(_vp)],
         "ttg_tt_shape": [_vp, _p64, _p64, _p64, _p64, _p64],
         "ttg_tt_download": [_vp, _pd],
@@ -220,6 +228,17 @@ class Context:
 
     def sync(self):
         _check(lib().ttg_context_sync(self.h))
+
+    def launch_count(self):
+        v = _i64(0)
+        _check(lib().ttg_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    def flush_l2(self, nbytes=256 << 20):
+        """Overwrite ``nbytes`` of device memory (larger than the 126 MB L2)."""
+        if getattr(self, "_flush", None) is None or self._flush.n * 8 < nbytes:
+            self._flush = DeviceArray(self, None, nbytes // 8)
+        _check(lib().ttg_memset(self.h, self._flush.p, 0, self._flush.n * 8))
 
     # device memory helpers
     def to_device(self, a):
@@ -359,7 +378,7 @@ def round(tt, eps, rmax=None, precision="fp64", ctx=None, stats=None):
 
 _AMEN_KEYS = {"nswp", "rmax", "x0", "z0", "verb", "local_prec", "local_restart", "local_iters",
               "kickrank", "kicktype", "ismex", "max_full_size", "resid_damp", "trunc_norm",
-              "tol_exit", "precision", "seed"}
+              "tol_exit", "precision", "seed", "timing"}
 
 
 def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
@@ -396,6 +415,8 @@ def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
         o.verb = int(opts["verb"])
     if "seed" in opts:
         o.seed = int(opts["seed"])
+    if "timing" in opts:
+        o.timing = 1 if opts["timing"] else 0
     o.precision = _PREC[opts.get("precision", "fp64")]
     owned = []
 
