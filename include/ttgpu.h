@@ -181,6 +181,16 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2,
                     int32_t prec, int64_t nrestart, int64_t niters,
                     double* sol_out, int32_t precision, int64_t* iters_out);
 
+/* ---- device FP64 factorizations used by the sweeps (device pointers) -------
+ * Thin QR A = Q R (Q m x k, R k x n, k = min(m,n); Householder with LAPACK's
+ * sign convention, as MATLAB's qr(A,0) at round.m:41 / amen_solve2.m:342) and
+ * economy SVD A = U diag(S) VT (U m x k, S k descending, VT k x n; as
+ * svd(A,'econ') at round.m:65 / amen_solve2.m:533).  Column-major, leading
+ * dimension = row count.  A is not modified. */
+int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double* Q, double* R);
+int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double* U, double* S,
+                  double* VT);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,61 @@
+"""GPU tests of the device FP64 factorizations (one-CTA Householder QR,
+one-sided Jacobi SVD, tall QR) against numpy/LAPACK, through the C ABI."""
+import numpy as np
+import pytest
+
+import ttgpu
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(64, 64), (132, 132), (4096, 64), (256, 4), (4, 256), (37, 53), (1, 5), (5, 1),
+          (8448, 132), (160, 150)]
+
+
+@pytest.mark.parametrize("m,n", SHAPES)
+def test_dense_svd_matches_lapack(ctx, m, n):
+    rng = np.random.default_rng(m * 7 + n)
+    A = rng.standard_normal((m, n))
+    U, s, VT = ttgpu.dense_svd(A, ctx=ctx)
+    s_ref = np.linalg.svd(A, compute_uv=False)
+    k = min(m, n)
+    assert np.allclose(s, s_ref, rtol=0, atol=1e-13 * s_ref[0])
+    assert np.linalg.norm(U * s @ VT - A) / np.linalg.norm(A) < 1e-13
+    assert np.linalg.norm(U.T @ U - np.eye(k)) < 1e-12
+    assert np.linalg.norm(VT @ VT.T - np.eye(k)) < 1e-12
+    assert np.all(np.diff(s) <= 0)
+
+
+def test_dense_svd_graded_spectrum(ctx):
+    """Singular values spanning 14 decades (the truncation regime of AMEn)."""
+    rng = np.random.default_rng(3)
+    n = 96
+    Q1, _ = np.linalg.qr(rng.standard_normal((512, n)))
+    Q2, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    sv = 10.0 ** (-np.linspace(0, 14, n))
+    A = (Q1 * sv) @ Q2.T
+    U, s, VT = ttgpu.dense_svd(A, ctx=ctx)
+    assert np.allclose(s, sv, rtol=0, atol=2e-14)
+    assert np.linalg.norm(U * s @ VT - A) / np.linalg.norm(A) < 1e-13
+
+
+@pytest.mark.parametrize("m,n", [(64, 64), (256, 4), (36, 9), (9, 36), (4096, 64), (130, 120)])
+def test_dense_qr_matches_lapack(ctx, m, n):
+    rng = np.random.default_rng(m + 11 * n)
+    A = rng.standard_normal((m, n))
+    Q, R = ttgpu.dense_qr(A, ctx=ctx)
+    Qr, Rr = np.linalg.qr(A)
+    k = min(m, n)
+    assert np.linalg.norm(Q @ R - A) / np.linalg.norm(A) < 1e-13
+    assert np.linalg.norm(Q.T @ Q - np.eye(k)) < 1e-12
+    assert np.allclose(np.tril(R, -1), 0)
+    # Same (LAPACK) sign convention as MATLAB's qr(A,0): R agrees entrywise.
+    assert np.allclose(R, Rr, rtol=1e-10, atol=1e-12 * np.abs(Rr).max())
+
+
+def test_dense_qr_rank_deficient(ctx):
+    rng = np.random.default_rng(9)
+    B = rng.standard_normal((200, 3))
+    A = np.hstack([B, B[:, :1] * 2.0, B[:, 1:2] - B[:, 2:3]])
+    Q, R = ttgpu.dense_qr(A, ctx=ctx)
+    assert np.linalg.norm(Q @ R - A) / np.linalg.norm(A) < 1e-13
+    assert np.linalg.norm(Q.T @ Q - np.eye(5)) < 1e-12

@@ -1,8 +1,14 @@
 // AMEn solver on the device: restates solve/amen_solve2.m:67-831 on its
 // default option path (kicktype 'als', trunc_norm 'residual', no local
-// preconditioner, MEX local solver).  All cores, interfaces (Phi) and local
-// vectors live on the device; the host keeps ranks, the norm bookkeeping
-// scalars (nrmsa/nrmsy/nrmsx/nrmsc) and the truncation decisions.
+// preconditioner, MEX local solver).
+//
+// All cores, interfaces (Phi) and local vectors live on the device, and so
+// does the scalar bookkeeping of the reference (nrmsa/nrmsy/nrmsx/nrmsc,
+// the local residuals and the per-sweep maxima): small device kernels update
+// it in stream order.  The host reads device values only where the
+// algorithm branches on them: the local-solve tolerance (one read per core),
+// the candidate ranks of the residual-based truncation (batched reads), the
+// Krylov stopping test, and the per-sweep stopping test.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -18,34 +24,47 @@
 
 namespace ttg {
 
-LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, const double* A,
-                             const double* Phi2, const double* rhs, double tol,
-                             const double* sol_prev, int64_t nrestart, int64_t niters,
-                             double* sol, int precision) {
+LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const double* Phi1,
+                                           const double* A, const double* Phi2,
+                                           const double* rhs, const double* dres, double nres,
+                                           double nrhs, double tol, const double* sol_prev,
+                                           int64_t nrestart, int64_t niters, double* sol,
+                                           int precision) {
   if (precision == TTG_MIXED)
-    return local_solve_mixed(c, d, Phi1, A, Phi2, rhs, tol, sol_prev, nrestart, niters, sol);
+    return local_solve_mixed(c, d, Phi1, A, Phi2, rhs, dres, nres, nrhs, tol, sol_prev, nrestart,
+                             niters, sol);
   LocalSolveResult out;
   const int64_t sz = d.in_size();
   if (nrestart > sz) nrestart = sz;                                   // solve3d_2.c:184
-  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size()), dres(c, sz);
+  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size());
   auto mv = [&](const double* x, double* y) {
     local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
   };
-  mv(sol_prev, dres.p());                                             // solve3d_2.c:257
-  out.matvecs_fp64++;
-  axpby_f64(c, sz, 1.0, rhs, -1.0, dres.p());                         // :259-262
-  DBuf<double> s2(c, 2);
-  dot_f64(c, sz, dres.p(), nullptr, s2.p(), true);
-  dot_f64(c, sz, rhs, nullptr, s2.p() + 1, true);
-  double h[2];
-  read_scalars(c, s2.p(), h, 2);
-  double tol_prev = h[0] / h[1];                                      // :263
+  double tol_prev = nres / nrhs;                                      // :263
   if (tol_prev < tol) tol_prev = tol;                                 // :264
-  GmresResult g = gmres_hh_f64(c, mv, dres.p(), sz, nrestart, tol / tol_prev, niters, sol);  // :267
+  GmresResult g = gmres_hh_f64(c, mv, dres, sz, nrestart, tol / tol_prev, niters, sol);  // :267
   axpby_f64(c, sz, 1.0, sol_prev, 1.0, sol);                          // :277-278
   out.iters = g.iters;
   out.matvecs_fp64 += g.matvecs;
   return out;
+}
+
+LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, const double* A,
+                             const double* Phi2, const double* rhs, double tol,
+                             const double* sol_prev, int64_t nrestart, int64_t niters,
+                             double* sol, int precision) {
+  const int64_t sz = d.in_size();
+  DBuf<double> dres(c, sz), s2(c, 2);
+  local_matvec_f64(c, d, Phi1, A, Phi2, sol_prev, dres.p());          // solve3d_2.c:257
+  axpby_f64(c, sz, 1.0, rhs, -1.0, dres.p());                         // :259-262
+  dot_f64(c, sz, dres.p(), nullptr, s2.p(), true);
+  dot_f64(c, sz, rhs, nullptr, s2.p() + 1, true);
+  double h[2];
+  read_scalars(c, s2.p(), h, 2);
+  LocalSolveResult r = local_solve_from_residual(c, d, Phi1, A, Phi2, rhs, dres.p(), h[0], h[1],
+                                                 tol, sol_prev, nrestart, niters, sol, precision);
+  r.matvecs_fp64 += 1;
+  return r;
 }
 
 namespace {
@@ -62,7 +81,6 @@ struct PhaseProf {
   Context* c = nullptr;
   std::chrono::steady_clock::time_point t0;
   std::map<std::string, double> ms;
-  int cur = -1;
   std::string name;
   void start(Context* cc) {
     const char* e = getenv("TTG_PROFILE");
@@ -88,40 +106,46 @@ struct PhaseProf {
   }
 };
 
-// ||B x - rhs|| / nrhs with the FP64 local matvec (res into host).
-double local_residual(Context* c, const MvDims& d, const double* Phi1, const double* A,
-                      const double* Phi2, const double* x, const double* rhs, double nrhs,
-                      double* tmp, double* t1, double* t2) {
-  local_matvec_f64(c, d, Phi1, A, Phi2, x, tmp, t1, t2);
-  DBuf<double> s(c, 1);
-  diffnrm_f64(c, d.out_size(), tmp, rhs, s.p(), true);
-  double h;
-  read_scalars(c, s.p(), &h, 1);
-  return h / nrhs;
-}
-
-double dense_residual(Context* c, int64_t N, const double* B, const double* x, const double* rhs,
-                      double nrhs, double* tmp) {
-  gemm_f64(c, false, false, N, 1, N, 1.0, B, N, 0, x, N, 0, 0.0, tmp, N, 0, 1);
-  DBuf<double> s(c, 1);
-  diffnrm_f64(c, N, tmp, rhs, s.p(), true);
-  double h;
-  read_scalars(c, s.p(), &h, 1);
-  return h / nrhs;
-}
-
-double host_norm(Context* c, int64_t n, const double* x) { return nrm2_host(c, n, x); }
-
-// Normalise in place by the Frobenius norm; returns the norm (1 if zero),
-// as compute_next_Phi with nargout > 1 (amen_solve2.m:907-914).
-double normalize(Context* c, int64_t n, double* x) {
-  double nrm = host_norm(c, n, x);
-  if (nrm > 0) {
-    axpby_f64(c, n, 1.0 / nrm, x, 0.0, x);
-  } else {
-    nrm = 1.0;
+// Device scalar slots of one solve.
+struct Scalars {
+  DBuf<double> buf;
+  int64_t d = 0;
+  enum Fixed : int64_t {
+    NRMSC = 0, NRHS, RES_PREV, RES_NEW, THR, MAXRES, MAXDX, T0, T1, T2, T3, NFIXED
+  };
+  static constexpr int64_t NCAND = 64;  // candidate residual slots
+  double* p(int64_t k) const { return buf.p() + k; }
+  double* a(int64_t i) const { return buf.p() + NFIXED + NCAND + i; }            // nrmsa
+  double* y(int64_t i) const { return buf.p() + NFIXED + NCAND + (d - 1) + i; }  // nrmsy
+  double* x(int64_t i) const { return buf.p() + NFIXED + NCAND + 2 * (d - 1) + i; }  // nrmsx
+  double* cand(int64_t k) const { return buf.p() + NFIXED + k; }
+  void init(Context* c, int64_t dd) {
+    d = dd;
+    const int64_t total = NFIXED + NCAND + 3 * (d - 1);
+    buf.reset(c, total);
+    fill_f64(c, total, 1.0, buf.p());                                 // :277-282
   }
-  return nrm;
+};
+
+// ||B x - rhs|| into *out (device), FP64 local matvec.
+void local_residual_dev(Context* c, const MvDims& d, const double* Phi1, const double* A,
+                        const double* Phi2, const double* x, const double* rhs, double* tmp,
+                        double* t1, double* t2, double* out) {
+  local_matvec_f64(c, d, Phi1, A, Phi2, x, tmp, t1, t2);
+  diffnrm_f64(c, d.out_size(), tmp, rhs, out, true);
+}
+
+void dense_residual_dev(Context* c, int64_t N, const double* B, const double* x,
+                        const double* rhs, double* tmp, double* out) {
+  gemm_f64(c, false, false, N, 1, N, 1.0, B, N, 0, x, N, 0, 0.0, tmp, N, 0, 1);
+  diffnrm_f64(c, N, tmp, rhs, out, true);
+}
+
+// Normalise in place by the Frobenius norm, the norm (1 if zero) into *slot
+// (compute_next_Phi with nargout > 1, amen_solve2.m:907-914).
+void normalize_dev(Context* c, int64_t n, double* x, double* slot) {
+  dot_f64(c, n, x, nullptr, slot, true);
+  normalize_by_dev(c, n, x, slot);
 }
 
 }  // namespace
@@ -189,14 +213,15 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
   const double resid_damp = o.resid_damp;
   const double tol_exit = o.tol_exit > 0 ? o.tol_exit : tol;            // :156-158
   const bool use_z = kickrank > 0;                                      // :246
+  const double real_tol = (tol / std::sqrt(double(d))) / resid_damp;   // :466
 
   cudaEvent_t e0, e1;
   TTG_CUDA(cudaEventCreate(&e0));
   TTG_CUDA(cudaEventCreate(&e1));
   TTG_CUDA(cudaEventRecord(e0, c->stream));
   const int64_t mv0 = c->matvecs, fl0 = c->matvec_flops, la0 = c->launches;
-  const int64_t mvk0[2] = {c->mv_count[0], c->mv_count[1]};
   const double flk0[2] = {c->mv_flops[0], c->mv_flops[1]};
+  const int64_t mvk0[2] = {c->mv_count[0], c->mv_count[1]};
   c->ev_collect();
   const double msk0[2] = {c->mv_ms[0], c->mv_ms[1]};
   c->time_matvec = o.timing != 0;
@@ -204,6 +229,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
     Context* c;
     ~TimingOff() { c->time_matvec = false; }
   } timing_off{c};
+  TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 8 * sizeof(int), c->stream));
 
   PhaseProf prof;
   prof.start(c);
@@ -247,12 +273,12 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       fill_f64(c, 1, 1.0, (*v)[k].p());
     }
   }
-  std::vector<double> nrmsa(d - 1, 1.0), nrmsy(d - 1, 1.0), nrmsx(d - 1, 1.0);  // :277-279
-  double nrmsc = 1.0;                                                   // :282
+  Scalars S;
+  S.init(c, d);                                  // nrmsa = nrmsy = nrmsx = nrmsc = 1 (:277-282)
+  double* NC = S.p(Scalars::NRMSC);
   bool last_sweep = false;
   int64_t local_solves = 0, gmres_iters = 0, mv_fp64 = 0;
   int64_t swp_done = 0;
-  std::vector<double> hs;
 
   for (int64_t swp = 1; swp <= nswp; ++swp) {                           // :296
     // ------------- right-to-left orthogonalisation (:299-438)
@@ -273,10 +299,10 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
                    cry(i), ry[i], 0, 0.0, t.p(), rz[i], 0, 1);
           gemm_f64(c, false, false, rz[i] * n[i], rz[i + 1], ry[i + 1], 1.0, t.p(), rz[i] * n[i], 0,
                    phizy[i + 1].p(), ry[i + 1], 0, 0.0, crzy.p(), rz[i] * n[i], 0, 1);
-          axpby_f64(c, zd.out_size(), -1.0, crzAt.p(), nrmsc, crzy.p());  // crzy*nrmsc - crzAt
+          axpby_dev(c, zd.out_size(), -1.0, crzAt.p(), NC, crzy.p());  // :309 crzy*nrmsc - crzAt
           const int64_t K = std::min(rz[i], ncols);
-          DBuf<double> U(c, rz[i] * K), S(c, K), VT(c, K * ncols);
-          svd_f64(c, rz[i], ncols, crzy.p(), U.p(), S.p(), VT.p());       // :311
+          DBuf<double> U(c, rz[i] * K), Sv(c, K), VT(c, K * ncols);
+          svd_f64(c, rz[i], ncols, crzy.p(), U.p(), Sv.p(), VT.p());     // :311
           kz = std::min(kickrank, K);                                     // :312
           zt.reset(c, ncols * kz);
           transpose_f64(c, kz, ncols, VT.p(), K, zt.p(), ncols);
@@ -292,7 +318,8 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         crz[i].buf.reset(c, kq * ncols);
         transpose_f64(c, ncols, kq, Q.p(), ncols, crz[i].p(), kq);       // :322-323
       }
-      if (swp > 1) nrmsc = nrmsc / (nrmsy[i - 1] / (nrmsa[i - 1] * nrmsx[i - 1]));  // :325-328
+      if (swp > 1)                                                      // :325-328
+        scalar_op(c, SC_NRMSC_DIV, NC, S.y(i - 1), S.a(i - 1), S.x(i - 1));
       prof.mark("rl_qr");
       // QR of x_i^T (:331-342)
       const int64_t ncols = n[i] * rx[i + 1];
@@ -306,12 +333,8 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       DBuf<double> cr2(c, m2 * kq);
       gemm_f64(c, false, true, m2, kq, rx[i], 1.0, crx[i - 1].p(), m2, 0, rv.p(), kq, 0, 0.0,
                cr2.p(), m2, 0, 1);
-      double curnorm = host_norm(c, m2 * kq, cr2.p());                   // :351-357
-      if (curnorm > 0)
-        axpby_f64(c, m2 * kq, 1.0 / curnorm, cr2.p(), 0.0, cr2.p());
-      else
-        curnorm = 1.0;
-      nrmsx[i - 1] *= curnorm;
+      normalize_dev(c, m2 * kq, cr2.p(), S.p(Scalars::T0));            // :351-356
+      scalar_op(c, SC_MUL, S.x(i - 1), S.p(Scalars::T0));              // :357
       rx[i] = kq;                                                         // :359
       crx[i].buf.reset(c, kq * ncols);
       transpose_f64(c, ncols, kq, Q.p(), ncols, crx[i].p(), kq);          // :360-362
@@ -321,28 +344,29 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       phia[i].buf.reset(c, rx[i] * ra[i] * rx[i]);
       next_phi_f64(c, 1, rx[i], n[i], rx[i + 1], rx[i], rx[i + 1], ra[i], ra[i + 1],
                    phia[i + 1].p(), crx[i].p(), crA(i), crx[i].p(), phia[i].p());
-      nrmsa[i - 1] = normalize(c, rx[i] * ra[i] * rx[i], phia[i].p());
+      normalize_dev(c, rx[i] * ra[i] * rx[i], phia[i].p(), S.a(i - 1));
       phiy[i].buf.reset(c, ry[i] * rx[i]);
       next_phi_f64(c, 1, rx[i], n[i], rx[i + 1], ry[i], ry[i + 1], 1, 1, phiy[i + 1].p(),
                    crx[i].p(), nullptr, cry(i), phiy[i].p());
-      nrmsy[i - 1] = normalize(c, ry[i] * rx[i], phiy[i].p());
-      nrmsc = nrmsc * (nrmsy[i - 1] / (nrmsa[i - 1] * nrmsx[i - 1]));    // :372
+      normalize_dev(c, ry[i] * rx[i], phiy[i].p(), S.y(i - 1));
+      scalar_op(c, SC_NRMSC_MUL, NC, S.y(i - 1), S.a(i - 1), S.x(i - 1));  // :372
       if (use_z && !last_sweep) {                                         // :432-436
         rz[i] = rznew;
         phiza[i].buf.reset(c, rx[i] * ra[i] * rz[i]);
         next_phi_f64(c, 1, rz[i], n[i], rz[i + 1], rx[i], rx[i + 1], ra[i], ra[i + 1],
                      phiza[i + 1].p(), crz[i].p(), crA(i), crx[i].p(), phiza[i].p());
-        axpby_f64(c, rx[i] * ra[i] * rz[i], 1.0 / nrmsa[i - 1], phiza[i].p(), 0.0, phiza[i].p());
+        scale_dev_f64(c, rx[i] * ra[i] * rz[i], phiza[i].p(), phiza[i].p(), nullptr, S.a(i - 1));
         phizy[i].buf.reset(c, ry[i] * rz[i]);
         next_phi_f64(c, 1, rz[i], n[i], rz[i + 1], ry[i], ry[i + 1], 1, 1, phizy[i + 1].p(),
                      crz[i].p(), nullptr, cry(i), phizy[i].p());
-        axpby_f64(c, ry[i] * rz[i], 1.0 / nrmsy[i - 1], phizy[i].p(), 0.0, phizy[i].p());
+        scale_dev_f64(c, ry[i] * rz[i], phizy[i].p(), phizy[i].p(), nullptr, S.y(i - 1));
       }
     }
 
     // ------------- left-to-right solve sweep (:444-791)
-    double max_res = 0.0, max_dx = 0.0;
+    fill_f64(c, 2, 0.0, S.p(Scalars::MAXRES));  // max_res = max_dx = 0 (:440-441)
     for (int64_t i = 0; i < d; ++i) {
+      prof.mark("lr_rhs");
       const double* Phi1 = phia[i].p();
       const double* Phi2 = phia[i + 1].p();
       const double* A1 = crA(i);
@@ -352,54 +376,61 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       // y1 = y_i * nrmsc (:453); rhs = phiy_i * y1 * phiy_{i+1} (:456-461)
       const int64_t ysz = ry[i] * n[i] * ry[i + 1];
       DBuf<double> y1(c, ysz);
-      axpby_f64(c, ysz, nrmsc, cry(i), 0.0, y1.p());
+      scale_dev_f64(c, ysz, cry(i), y1.p(), NC, nullptr);
       DBuf<double> t(c, rx[i] * n[i] * ry[i + 1]), rhs(c, N);
       gemm_f64(c, false, false, rx[i], n[i] * ry[i + 1], ry[i], 1.0, phiy[i].p(), rx[i], 0,
                y1.p(), ry[i], 0, 0.0, t.p(), rx[i], 0, 1);
       gemm_f64(c, false, false, rx[i] * n[i], rx[i + 1], ry[i + 1], 1.0, t.p(), rx[i] * n[i], 0,
                phiy[i + 1].p(), ry[i + 1], 0, 0.0, rhs.p(), rx[i] * n[i], 0, 1);
-      const double norm_rhs = host_norm(c, N, rhs.p());                  // :462
+      dot_f64(c, N, rhs.p(), nullptr, S.p(Scalars::NRHS), true);         // :462
       prof.mark("lr_solve");
-      const double real_tol = (tol / std::sqrt(double(d))) / resid_damp; // :466
       const bool full = N < max_full_size;                                // :468
       DBuf<double> sol(c, N), tmp(c, N), B, t1(c, md.t1_size()), t2(c, md.t2_size());
-      double res_prev = 0.0, res_new = 0.0;
       if (full) {
         B.reset(c, N * N);
         assemble_local_f64(c, rx[i], n[i], rx[i + 1], ra[i], ra[i + 1], Phi1, A1, Phi2, B.p());
-        res_prev = dense_residual(c, N, B.p(), sol_prev, rhs.p(), norm_rhs, tmp.p());  // :482
+        dense_residual_dev(c, N, B.p(), sol_prev, rhs.p(), tmp.p(), S.p(Scalars::T0));  // :482
         copy_f64(c, N, rhs.p(), sol.p());
         lu_solve_f64(c, N, B.p(), sol.p(), 1);                            // :486
-        res_new = dense_residual(c, N, B.p(), sol.p(), rhs.p(), norm_rhs, tmp.p());    // :487
+        dense_residual_dev(c, N, B.p(), sol.p(), rhs.p(), tmp.p(), S.p(Scalars::T1));   // :487
+        scalar_op(c, SC_DIV, S.p(Scalars::RES_PREV), S.p(Scalars::T0), S.p(Scalars::NRHS));
+        scalar_op(c, SC_DIV, S.p(Scalars::RES_NEW), S.p(Scalars::T1), S.p(Scalars::NRHS));
       } else {
-        res_prev = local_residual(c, md, Phi1, A1, Phi2, sol_prev, rhs.p(), norm_rhs, tmp.p(),
-                                  t1.p(), t2.p());                        // :495
+        // dres = rhs - B sol_prev serves both res_prev (:495) and the MEX
+        // local solver's initial residual (solve3d_2.c:257-263).
+        DBuf<double> dres(c, N);
+        local_matvec_f64(c, md, Phi1, A1, Phi2, sol_prev, dres.p(), t1.p(), t2.p());
         mv_fp64++;
+        axpby_f64(c, N, 1.0, rhs.p(), -1.0, dres.p());
+        dot_f64(c, N, dres.p(), nullptr, S.p(Scalars::T0), true);
+        scalar_op(c, SC_DIV, S.p(Scalars::RES_PREV), S.p(Scalars::T0), S.p(Scalars::NRHS));
+        double h[2];
+        read_scalars(c, S.p(Scalars::NRHS), h, 1);
+        read_scalars(c, S.p(Scalars::T0), h + 1, 1);
+        const double norm_rhs = h[0], nres = h[1];
         if (norm_rhs > 0) {                                               // :497
-          LocalSolveResult lr = local_solve(c, md, Phi1, A1, Phi2, rhs.p(), real_tol, sol_prev,
-                                            o.local_restart, o.local_iters, sol.p(),
-                                            o.precision);                 // :501
+          LocalSolveResult lr = local_solve_from_residual(
+              c, md, Phi1, A1, Phi2, rhs.p(), dres.p(), nres, norm_rhs, real_tol, sol_prev,
+              o.local_restart, o.local_iters, sol.p(), o.precision);      // :501
           local_solves++;
           gmres_iters += lr.iters;
           mv_fp64 += lr.matvecs_fp64;
-          res_new = local_residual(c, md, Phi1, A1, Phi2, sol.p(), rhs.p(), norm_rhs, tmp.p(),
-                                   t1.p(), t2.p());                       // :504
+          local_residual_dev(c, md, Phi1, A1, Phi2, sol.p(), rhs.p(), tmp.p(), t1.p(), t2.p(),
+                             S.p(Scalars::T1));                           // :504
           mv_fp64++;
+          scalar_op(c, SC_DIV, S.p(Scalars::RES_NEW), S.p(Scalars::T1), S.p(Scalars::NRHS));
         } else {
           fill_f64(c, N, 0.0, sol.p());
-          res_new = 0.0;
+          fill_f64(c, 1, 0.0, S.p(Scalars::RES_NEW));
         }
       }
-      {
-        DBuf<double> s(c, 2);
-        diffnrm_f64(c, N, sol.p(), sol_prev, s.p(), true);
-        dot_f64(c, N, sol.p(), nullptr, s.p() + 1, true);
-        double h[2];
-        read_scalars(c, s.p(), h, 2);
-        const double dx = h[1] > 0 ? h[0] / h[1] : 0.0;                    // :519
-        max_dx = std::max(max_dx, dx);
-        max_res = std::max(max_res, res_prev);                            // :521
-      }
+      // dx = ||sol - sol_prev|| / ||sol|| ; max_dx, max_res (:519-521)
+      diffnrm_f64(c, N, sol.p(), sol_prev, S.p(Scalars::T2), true);
+      dot_f64(c, N, sol.p(), nullptr, S.p(Scalars::T3), true);
+      scalar_op(c, SC_DIV_NZ, S.p(Scalars::T2), S.p(Scalars::T2), S.p(Scalars::T3));
+      scalar_op(c, SC_MAXUPD, S.p(Scalars::MAXDX), S.p(Scalars::T2));
+      scalar_op(c, SC_MAXUPD, S.p(Scalars::MAXRES), S.p(Scalars::RES_PREV));
+
       prof.mark("lr_trunc");
       // Truncation (:530-601)
       const int64_t M = rx[i] * n[i], r2 = rx[i + 1];
@@ -407,33 +438,42 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
       int64_t r = 0;
       if (kickrank >= 0 && i < d - 1) {
         const int64_t K = std::min(M, r2);
-        DBuf<double> U(c, M * K), S(c, K), VT(c, K * r2);
-        svd_f64(c, M, r2, sol.p(), U.p(), S.p(), VT.p());                // :533
-        hs.resize(K);
-        TTG_CUDA(cudaMemcpyAsync(hs.data(), S.p(), sizeof(double) * K, cudaMemcpyDeviceToHost,
-                                 c->stream));
-        sync(c);
-        const double thr = std::max(real_tol * resid_damp, res_new);
-        int64_t rr = 0;
-        bool any = false;
+        DBuf<double> U(c, M * K), Sv(c, K), VT(c, K * r2);
+        svd_f64(c, M, r2, sol.p(), U.p(), Sv.p(), VT.p());               // :533
+        // thr = max(real_tol*resid_damp, res_new) (:547)
+        scalar_op(c, SC_MAX_CONST, S.p(Scalars::THR), S.p(Scalars::RES_NEW), nullptr, nullptr,
+                  real_tol * resid_damp);
+        // Candidate ranks rr = K-1, K-2, ..., 1 (:539-550): residuals are
+        // evaluated in growing batches and read back once per batch; the rank
+        // is the first candidate whose residual exceeds thr, as in the loop.
         DBuf<double> us(c, M * K), cursol(c, M * r2);
-        for (rr = K - 1; rr >= 1; --rr) {                                 // :539-550
-          any = true;
-          copy2d_f64(c, M, rr, U.p(), M, us.p(), M, S.p());
-          gemm_f64(c, false, false, M, r2, rr, 1.0, us.p(), M, 0, VT.p(), K, 0, 0.0, cursol.p(),
-                   M, 0, 1);
-          double res;
-          if (full) {
-            res = dense_residual(c, N, B.p(), cursol.p(), rhs.p(), norm_rhs, tmp.p());
-          } else {
-            res = local_residual(c, md, Phi1, A1, Phi2, cursol.p(), rhs.p(), norm_rhs, tmp.p(),
-                                 t1.p(), t2.p());
-            mv_fp64++;
+        int64_t found = -1, next = K - 1, batch = 2;
+        while (next >= 1 && found < 0) {
+          const int64_t nb = std::min<int64_t>(std::min(batch, next), Scalars::NCAND);
+          for (int64_t b = 0; b < nb; ++b) {
+            const int64_t rr = next - b;
+            copy2d_f64(c, M, rr, U.p(), M, us.p(), M, Sv.p());
+            gemm_f64(c, false, false, M, r2, rr, 1.0, us.p(), M, 0, VT.p(), K, 0, 0.0,
+                     cursol.p(), M, 0, 1);
+            if (full) {
+              dense_residual_dev(c, N, B.p(), cursol.p(), rhs.p(), tmp.p(), S.cand(b));
+            } else {
+              local_residual_dev(c, md, Phi1, A1, Phi2, cursol.p(), rhs.p(), tmp.p(), t1.p(),
+                                 t2.p(), S.cand(b));
+              mv_fp64++;
+            }
           }
-          if (res > thr) break;
+          first_exceeding(c, nb, S.cand(0), S.p(Scalars::NRHS), S.p(Scalars::THR),
+                          S.p(Scalars::T3));
+          double hb;
+          read_scalars(c, S.p(Scalars::T3), &hb, 1);
+          if (hb >= 0.0) found = next - int64_t(hb);
+          next -= nb;
+          batch *= 2;
         }
-        if (any && rr < 1) rr = 1;  // MATLAB leaves the loop variable at 1
-        r = (any ? rr : K - 1) + 1;                                       // :551
+        // MATLAB leaves the loop variable at 1 when no candidate breaks the
+        // loop; an empty loop (K == 1) gives K.
+        r = (found >= 1 ? found : (K - 1 >= 1 ? 1 : K - 1)) + 1;          // :551
         r = std::min(r, K);                                               // :593
         r = std::min(r, rmax);                                            // :594
         u.reset(c, M * r);
@@ -441,7 +481,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         v.reset(c, r2 * r);                                               // :604 v = V(:,1:r)*diag(s)
         DBuf<double> vtmp(c, r2 * r);
         transpose_f64(c, r, r2, VT.p(), K, vtmp.p(), r2);
-        copy2d_f64(c, r2, r, vtmp.p(), r2, v.p(), r2, S.p());
+        copy2d_f64(c, r2, r, vtmp.p(), r2, v.p(), r2, Sv.p());
       } else {                                                             // :596-601
         const int64_t K = std::min(M, r2);
         DBuf<double> Q(c, M * K), R(c, K * r2);
@@ -471,8 +511,8 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         axpby_f64(c, zd.out_size(), -1.0, crzAt.p(), 1.0, crzy.p());       // :612
         const int64_t mz = rz[i] * n[i];
         const int64_t K = std::min(mz, rz[i + 1]);
-        DBuf<double> U(c, mz * K), S(c, K), VT(c, K * rz[i + 1]);
-        svd_f64(c, mz, rz[i + 1], crzy.p(), U.p(), S.p(), VT.p());       // :613
+        DBuf<double> U(c, mz * K), Sv(c, K), VT(c, K * rz[i + 1]);
+        svd_f64(c, mz, rz[i + 1], crzy.p(), U.p(), Sv.p(), VT.p());       // :613
         const int64_t kz = std::min(kickrank, K);                          // :614
         const int64_t kq = std::min(mz, kz);
         DBuf<double> Q(c, mz * kq), R(c, kq * kz);
@@ -515,24 +555,20 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         DBuf<double> vx(c, r * nc);
         gemm_f64(c, true, false, r, nc, r2, 1.0, v.p(), r2, 0, crx[i + 1].p(), r2, 0, 0.0, vx.p(),
                  r, 0, 1);
-        nrmsc = nrmsc / (nrmsy[i] / (nrmsa[i] * nrmsx[i]));               // :737
-        double curnorm = host_norm(c, r * nc, vx.p());                     // :739-745
-        if (curnorm > 0)
-          axpby_f64(c, r * nc, 1.0 / curnorm, vx.p(), 0.0, vx.p());
-        else
-          curnorm = 1.0;
-        nrmsx[i] *= curnorm;
+        scalar_op(c, SC_NRMSC_DIV, NC, S.y(i), S.a(i), S.x(i));           // :737
+        normalize_dev(c, r * nc, vx.p(), S.p(Scalars::T0));               // :739-744
+        scalar_op(c, SC_MUL, S.x(i), S.p(Scalars::T0));                   // :745
         prof.mark("lr_phi");
         // Interfaces (:751-752)
         phia[i + 1].buf.reset(c, r * r * ra[i + 1]);
         next_phi_f64(c, 0, rx[i], n[i], r, rx[i], r, ra[i], ra[i + 1], phia[i].p(), u.p(), A1,
                      u.p(), phia[i + 1].p());
-        nrmsa[i] = normalize(c, r * r * ra[i + 1], phia[i + 1].p());
+        normalize_dev(c, r * r * ra[i + 1], phia[i + 1].p(), S.a(i));
         phiy[i + 1].buf.reset(c, r * ry[i + 1]);
         next_phi_f64(c, 0, rx[i], n[i], r, ry[i], ry[i + 1], 1, 1, phiy[i].p(), u.p(), nullptr,
                      cry(i), phiy[i + 1].p());
-        nrmsy[i] = normalize(c, r * ry[i + 1], phiy[i + 1].p());
-        nrmsc = nrmsc * (nrmsy[i] / (nrmsa[i] * nrmsx[i]));               // :754
+        normalize_dev(c, r * ry[i + 1], phiy[i + 1].p(), S.y(i));
+        scalar_op(c, SC_NRMSC_MUL, NC, S.y(i), S.a(i), S.x(i));           // :754
         rx[i + 1] = r;                                                     // :765-767
         crx[i].buf = std::move(u);
         crx[i + 1].buf = std::move(vx);
@@ -541,19 +577,22 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
           phiza[i + 1].buf.reset(c, rz[i + 1] * rx[i + 1] * ra[i + 1]);
           next_phi_f64(c, 0, rz[i], n[i], rz[i + 1], rx[i], rx[i + 1], ra[i], ra[i + 1],
                        phiza[i].p(), crz[i].p(), A1, crx[i].p(), phiza[i + 1].p());
-          axpby_f64(c, rz[i + 1] * rx[i + 1] * ra[i + 1], 1.0 / nrmsa[i], phiza[i + 1].p(), 0.0,
-                    phiza[i + 1].p());
+          scale_dev_f64(c, rz[i + 1] * rx[i + 1] * ra[i + 1], phiza[i + 1].p(), phiza[i + 1].p(),
+                        nullptr, S.a(i));
           phizy[i + 1].buf.reset(c, rz[i + 1] * ry[i + 1]);
           next_phi_f64(c, 0, rz[i], n[i], rz[i + 1], ry[i], ry[i + 1], 1, 1, phizy[i].p(),
                        crz[i].p(), nullptr, cry(i), phizy[i + 1].p());
-          axpby_f64(c, rz[i + 1] * ry[i + 1], 1.0 / nrmsy[i], phizy[i + 1].p(), 0.0,
-                    phizy[i + 1].p());
+          scale_dev_f64(c, rz[i + 1] * ry[i + 1], phizy[i + 1].p(), phizy[i + 1].p(), nullptr,
+                        S.y(i));
         }
       } else {
         crx[i].buf = std::move(sol);                                       // :778-779
       }
     }
     swp_done = swp;
+    double mm[2];
+    read_scalars(c, S.p(Scalars::MAXRES), mm, 2);
+    const double max_res = mm[0], max_dx = mm[1];
     int64_t maxr = 0;
     for (auto v : rx) maxr = std::max(maxr, v);
     if (stats && swp <= TTG_MAX_SWEEPS_RECORDED) {
@@ -569,8 +608,10 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
 
   prof.report();
   // Distribute the norms (:816-820) and assemble the output.
+  std::vector<double> hx(d - 1);
+  read_scalars(c, S.x(0), hx.data(), int(d - 1));
   double lsum = 0.0;
-  for (double v : nrmsx) lsum += std::log(v);
+  for (double v : hx) lsum += std::log(v);
   const double nx = std::exp(lsum / double(d));
   auto* out = new ttg_tt_s();
   out->ctx = c;
@@ -590,6 +631,17 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  int herr[8];
+  TTG_CUDA(cudaMemcpy(herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
+  if (herr[0] || herr[1] || herr[2]) {
+    ttg_tt_free(out);
+    fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out (codes %d %d %d)", herr[0],
+         herr[1], herr[2]);
+  }
+  if (herr[4]) {
+    ttg_tt_free(out);
+    fail(TTG_ERR_SOLVER, "a device factorization reported a non-zero LAPACK info");
+  }
   if (stats) {
     stats->sweeps = swp_done;
     stats->matvecs = c->matvecs - mv0;
@@ -609,7 +661,6 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
     stats->gflop_fp64 = (c->mv_flops[0] - flk0[0]) * 1e-9;
     stats->ms_fp64 = c->mv_ms[0] - msk0[0];
     stats->ms_matvec = o.precision == TTG_MIXED ? stats->ms_lp : stats->ms_fp64;
-    (void)mvk0;
   }
   return out;
 }

@@ -43,6 +43,7 @@ int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax, int32_t
     for (auto v : rm) TTG_REQUIRE(v >= 1, "rmax entries must be >= 1");
   }
   *out = round_tt(in, eps, rm, precision, stats);
+  check_factorizations(in->ctx);
   TTG_API_END
 }
 
@@ -122,6 +123,34 @@ int ttg_next_phi(ttg_context ctx, int32_t dir, int64_t rx1, int64_t n, int64_t r
   TTG_API_END
 }
 
+int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double* Q, double* R) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && A && Q && R, "NULL argument");
+  TTG_REQUIRE(m >= 1 && n >= 1, "sizes must be >= 1");
+  Context* c = &ctx->c;
+  TTG_CUDA(cudaSetDevice(c->device));
+  qr_f64(c, m, n, A, Q, R);
+  check_factorizations(c);
+  TTG_API_END
+}
+
+int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double* U, double* S,
+                  double* VT) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && A && U && S && VT, "NULL argument");
+  TTG_REQUIRE(m >= 1 && n >= 1, "sizes must be >= 1");
+  Context* c = &ctx->c;
+  TTG_CUDA(cudaSetDevice(c->device));
+  TTG_CUDA(cudaMemsetAsync(c->d_err + 3, 0, sizeof(int), c->stream));
+  svd_f64(c, m, n, A, U, S, VT);
+  int herr = 0;
+  TTG_CUDA(cudaMemcpyAsync(&herr, c->d_err + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  if (herr) fail(TTG_ERR_NOCONV, "Jacobi SVD reached its sweep limit");
+  check_factorizations(c);
+  TTG_API_END
+}
+
 int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
                     int64_t ra2, const double* Phi1, const double* A, const double* Phi2,
                     const double* rhs, double tol, int32_t trunc_norm, const double* sol_prev,
@@ -137,9 +166,14 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_
   Context* c = &ctx->c;
   TTG_CUDA(cudaSetDevice(c->device));
   MvDims d{rx1, rx1, ra1, n, n, rx2, ra2, rx2};
+  TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 8 * sizeof(int), c->stream));
   LocalSolveResult r =
       local_solve(c, d, Phi1, A, Phi2, rhs, tol, sol_prev, nrestart, niters, sol_out, precision);
+  int herr[8];
+  TTG_CUDA(cudaMemcpyAsync(herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost, c->stream));
   sync(c);
+  if (herr[0] || herr[1] || herr[2])
+    fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out in the local solve");
   if (iters_out) *iters_out = r.iters;
   TTG_API_END
 }

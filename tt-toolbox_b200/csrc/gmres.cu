@@ -13,6 +13,7 @@
 // the kernel raises the context error flag and runs to completion, and the
 // host returns TTG_ERR_TIMEOUT.
 #include <cmath>
+#include <cstring>
 
 #include "gmres.h"
 
@@ -38,6 +39,8 @@ struct HhArgs {
   double* part;  // 2 * gridDim.x
   unsigned* bar; // [0] count [1] generation [2] reduction parity
   int* err;
+  int* stop;     // [0] converged flag, [1] step at which it converged
+  double tol;    // relative stopping tolerance of the current solve
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -142,6 +145,7 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_init(HhArgs a, int it) {
 
 // v_j = P_0 ... P_{j-1} (P_j e_j), normalised, into w  (:396-406)
 __global__ void __launch_bounds__(HH_THREADS) k_hh_build(HhArgs a, int64_t j) {
+  if (*(volatile int*)a.stop) return;  // queued after convergence
   unsigned parity = 0;
   const int64_t sz = a.sz;
   const double* Uj = a.U + j * sz;
@@ -162,6 +166,7 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_build(HhArgs a, int64_t j) {
 
 // w2 = P_j ... P_0 w2 ; new reflector U_{j+1} ; Givens ; R(:,j) ; residual (:421-473)
 __global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
+  if (*(volatile int*)a.stop) return;  // queued after convergence
   unsigned parity = 0;
   const int64_t sz = a.sz;
   double* w = a.w2;
@@ -225,7 +230,13 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
       w[j + 1] = 0.0;
     }
     for (int64_t k = 0; k < a.nrestart; ++k) a.R[k + j * a.nrestart] = (k < sz) ? __ldcg(w + k) : 0.0;
-    a.scal[1] = fabs(a.tau[j + 1]) / a.scal[0];
+    const double curres = fabs(a.tau[j + 1]) / a.scal[0];
+    a.scal[1] = curres;
+    if (curres < a.tol) {  // (:476) later queued steps see the flag and return
+      a.stop[1] = int(j);
+      __threadfence();
+      a.stop[0] = 1;
+    }
   }
 }
 
@@ -291,6 +302,7 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
                coop_blocks(c, (const void*)k_hh_correct, sizeof(double) * nrestart, sz)));
   DBuf<double> part(c, 2 * blocks);
   DBuf<unsigned> bar(c, 4);
+  DBuf<int> stop(c, 4);
   TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 4 * sizeof(unsigned), c->stream));
   TTG_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
 
@@ -309,8 +321,28 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
   a.part = part.p();
   a.bar = bar.p();
   a.err = c->d_err;
+  a.stop = stop.p();
+  a.tol = tol;
   fill_f64(c, sz, 0.0, sol);
 
+  // Arnoldi steps are queued in chunks of growing length without a host
+  // round trip per step; k_hh_tail raises a device flag on convergence and
+  // every kernel queued after it (reflector kernels and the matvec GEMMs,
+  // through Context::skip) returns at once.  The host reads the flag, the
+  // converged step and the residual estimate once per chunk.
+  struct Probe {
+    int flag[2];
+    double curres;
+  };
+  auto probe = [&](Probe& p) {
+    TTG_CUDA(cudaMemcpyAsync(c->h_scal, stop.p(), 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                             c->stream));
+    TTG_CUDA(cudaMemcpyAsync(c->h_scal + 1, a.scal + 1, sizeof(double), cudaMemcpyDeviceToHost,
+                             c->stream));
+    sync(c);
+    memcpy(p.flag, c->h_scal, 2 * sizeof(int));
+    p.curres = c->h_scal[1];
+  };
   double curres = INFINITY;
   for (int64_t it = 0; it < niters; ++it) {
     apply(sol, w2.p());
@@ -318,6 +350,7 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
     int itv = int(it);
     void* args_init[] = {&a, &itv};
     launch_coop(c, (const void*)k_hh_init, blocks, 0, args_init);
+    TTG_CUDA(cudaMemsetAsync(stop.p(), 0, 2 * sizeof(int), c->stream));
     double hs[4];
     read_scalars(c, a.scal, hs, 4);
     if (hs[3] != 0.0) {  // exact solution: nothing to correct
@@ -325,21 +358,33 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
       break;
     }
     bool broke = false;
-    int64_t j = 0;
-    for (j = 0; j < nrestart; ++j) {
-      void* args_b[] = {&a, &j};
-      launch_coop(c, (const void*)k_hh_build, blocks, 0, args_b);
-      apply(w.p(), w2.p());
-      res.matvecs++;
-      void* args_t[] = {&a, &j};
-      launch_coop(c, (const void*)k_hh_tail, blocks, 0, args_t);
-      res.iters++;
-      read_scalars(c, a.scal + 1, &curres, 1);
-      if (curres < tol) {
+    int64_t j = 0, chunk = 3;
+    SkipGuard guard(c, stop.p());
+    while (j < nrestart) {
+      const int64_t jend = std::min(nrestart, j + chunk);
+      for (int64_t jj = j; jj < jend; ++jj) {
+        int64_t jv = jj;
+        void* args_b[] = {&a, &jv};
+        launch_coop(c, (const void*)k_hh_build, blocks, 0, args_b);
+        apply(w.p(), w2.p());
+        void* args_t[] = {&a, &jv};
+        launch_coop(c, (const void*)k_hh_tail, blocks, 0, args_t);
+      }
+      Probe p;
+      probe(p);
+      curres = p.curres;
+      if (p.flag[0]) {
         broke = true;
+        j = p.flag[1];
         break;
       }
+      j = jend;
+      chunk *= 2;
     }
+    guard.release();
+    const int64_t steps = broke ? j + 1 : nrestart;
+    res.iters += steps;
+    res.matvecs += steps;
     int64_t ni;
     if (!broke) {
       j = nrestart - 1;
@@ -351,10 +396,6 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
     launch_coop(c, (const void*)k_hh_correct, blocks, sizeof(double) * nrestart, args_c);
     if (curres < tol) break;
   }
-  int herr = 0;
-  TTG_CUDA(cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  sync(c);
-  if (herr) fail(TTG_ERR_TIMEOUT, "GMRES grid barrier timed out");
   res.relres = curres;
   return res;
 }

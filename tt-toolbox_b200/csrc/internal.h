@@ -128,6 +128,10 @@ struct Context {
   size_t ev_used = 0;
   double mv_ms[2] = {0.0, 0.0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // While non-null, GEMM and matvec kernels launched on this context return
+  // immediately when *skip != 0 (speculatively queued Krylov steps after
+  // convergence).
+  const int* skip = nullptr;
 
   int ev_begin(int kind) {
     if (ev_used == ev_pool.size()) {
@@ -151,6 +155,14 @@ struct Context {
     }
     ev_used = 0;
   }
+};
+
+// Sets Context::skip for a scope (cleared on every exit path).
+struct SkipGuard {
+  Context* c;
+  SkipGuard(Context* cc, const int* flag) : c(cc) { c->skip = flag; }
+  void release() { c->skip = nullptr; }
+  ~SkipGuard() { c->skip = nullptr; }
 };
 
 // Scope guard: records an event pair around a local matvec when timing is on.

@@ -42,4 +42,28 @@ void copy2d_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_
 // counter-based hash (seed, offset).
 void randn_f64(Context* c, int64_t n, uint64_t seed, uint64_t offset, double* y);
 
+// ---- device-resident scalar bookkeeping (no host round trip) -------------
+// x /= *nrm in place (nothing when *nrm == 0, and *nrm is then set to 1) --
+// the normalisation of compute_next_Phi with nargout > 1.
+void normalize_by_dev(Context* c, int64_t n, double* x, double* nrm);
+// y = a*x + (*b)*y with a host scalar a and a device scalar b.
+void axpby_dev(Context* c, int64_t n, double a, const double* x, const double* b, double* y);
+// Scalar program on device memory (one thread): see ScalOp.
+enum ScalOp : int {
+  SC_DIV = 0,        // out = p0 / p1
+  SC_MAXUPD = 1,     // out = max(out, p0)
+  SC_NRMSC_DIV = 2,  // out /= (p0 / (p1 * p2))      (amen_solve2.m:327,737)
+  SC_NRMSC_MUL = 3,  // out *= (p0 / (p1 * p2))      (amen_solve2.m:372,754)
+  SC_MUL = 4,        // out *= p0
+  SC_MAX_CONST = 5,  // out = max(p0, host constant)
+  SC_DIV_NZ = 6,     // out = p1 > 0 ? p0 / p1 : 0
+};
+void scalar_op(Context* c, int op, double* out, const double* p0, const double* p1 = nullptr,
+               const double* p2 = nullptr, double k = 0.0);
+// *out = first b < nb with cand[b] / *den > *thr, or -1 (one thread).
+void first_exceeding(Context* c, int64_t nb, const double* cand, const double* den,
+                     const double* thr, double* out);
+// err_slot |= (*info != 0): LAPACK-style status accumulated without a host sync.
+void accumulate_info(Context* c, const int* info, int* err_slot);
+
 }  // namespace ttg

@@ -25,6 +25,7 @@ struct GemmP {
   double* C;
   int64_t ldc, sC;
   double alpha, beta;
+  const int* skip;  // optional: return at once when *skip != 0
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
@@ -48,6 +49,7 @@ template <bool TA, bool TB>
 __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
   __shared__ double As[2][BK][BM + PADS];
   __shared__ double Bs[2][BK][BN + PADS];
+  if (p.skip && *p.skip) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t bz = blockIdx.z;
   const double* __restrict__ A = p.A + bz * p.sA;
@@ -301,6 +303,54 @@ __global__ void k_randn(int64_t n, uint64_t seed, uint64_t offset, double* y) {
   }
 }
 
+__global__ void k_normalize_by(int64_t n, double* __restrict__ x, double* nrm) {
+  const double v = *nrm;
+  const double s = v > 0.0 ? 1.0 / v : 1.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    x[i] *= s;
+  // Every block has read *nrm above; a zero norm is reported as 1.
+  if (blockIdx.x == 0 && threadIdx.x == 0 && !(v > 0.0)) *nrm = 1.0;
+}
+
+__global__ void k_axpby_dev(int64_t n, double a, const double* __restrict__ x,
+                            const double* __restrict__ b, double* __restrict__ y) {
+  const double bv = *b;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = bv * y[i] + a * x[i];
+}
+
+__global__ void k_scalar_op(int op, double* out, const double* p0, const double* p1,
+                            const double* p2, double k) {
+  switch (op) {
+    case 0: *out = *p0 / *p1; break;
+    case 1: *out = fmax(*out, *p0); break;
+    case 2: *out = *out / (*p0 / (*p1 * *p2)); break;
+    case 3: *out = *out * (*p0 / (*p1 * *p2)); break;
+    case 4: *out = *out * *p0; break;
+    case 5: *out = fmax(*p0, k); break;
+    case 6: *out = (*p1 > 0.0) ? *p0 / *p1 : 0.0; break;
+    default: break;
+  }
+}
+
+__global__ void k_first_exceeding(int64_t nb, const double* cand, const double* den,
+                                  const double* thr, double* out) {
+  double r = -1.0;
+  for (int64_t b = 0; b < nb; ++b) {
+    if (cand[b] / *den > *thr) {
+      r = double(b);
+      break;
+    }
+  }
+  *out = r;
+}
+
+__global__ void k_accumulate_info(const int* info, int* err_slot) {
+  if (*info != 0) atomicOr(err_slot, 1);
+}
+
 int grid_for(Context* c, int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
   int64_t cap = int64_t(c->num_sms) * 8;
@@ -329,7 +379,7 @@ void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, dou
   TTG_REQUIRE(batch <= 65535, "gemm batch %lld too large", (long long)batch);
   const int64_t gx = (M + BM - 1) / BM, gy = (N + BN - 1) / BN;
   TTG_REQUIRE(gy <= 65535 && gx <= 0x7fffffff, "gemm too large");
-  GemmP p{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta};
+  GemmP p{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta, c->skip};
   dim3 grid{unsigned(gx), unsigned(gy), unsigned(batch)};
   if (!tA && !tB)
     k_gemm_f64<false, false><<<grid, 128, 0, c->stream>>>(p);
@@ -402,6 +452,40 @@ void copy2d_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_
   if (rows <= 0 || cols <= 0) return;
   k_copy2d<<<grid_for(c, rows * cols), 256, 0, c->stream>>>(rows, cols, in, ldi, out, ldo,
                                                             scale_col);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void normalize_by_dev(Context* c, int64_t n, double* x, double* nrm) {
+  if (n <= 0) return;
+  k_normalize_by<<<grid_for(c, n), 256, 0, c->stream>>>(n, x, nrm);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void axpby_dev(Context* c, int64_t n, double a, const double* x, const double* b, double* y) {
+  if (n <= 0) return;
+  k_axpby_dev<<<grid_for(c, n), 256, 0, c->stream>>>(n, a, x, b, y);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void scalar_op(Context* c, int op, double* out, const double* p0, const double* p1,
+               const double* p2, double k) {
+  k_scalar_op<<<1, 1, 0, c->stream>>>(op, out, p0, p1, p2, k);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void first_exceeding(Context* c, int64_t nb, const double* cand, const double* den,
+                     const double* thr, double* out) {
+  k_first_exceeding<<<1, 1, 0, c->stream>>>(nb, cand, den, thr, out);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void accumulate_info(Context* c, const int* info, int* err_slot) {
+  k_accumulate_info<<<1, 1, 0, c->stream>>>(info, err_slot);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
 }

@@ -1,6 +1,7 @@
 // FP64 QR / SVD / LU on the device through cuSOLVER (library factorizations;
 // the contractions around them are this library's own kernels).
 #include "linalg.h"
+#include "small_dense.h"
 
 namespace ttg {
 
@@ -16,11 +17,10 @@ __global__ void k_triu(int64_t k, int64_t n, const double* __restrict__ A, int64
   }
 }
 
-void check_info(Context* c, const int* dinfo, const char* what) {
-  int info = 0;
-  TTG_CUDA(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  sync(c);
-  if (info != 0) fail(TTG_ERR_SOLVER, "%s returned info = %d", what, info);
+// A non-zero info is folded into the context error slot 4 on the device (no
+// host round trip); callers check the slot once their sequence is done.
+void check_info(Context* c, const int* dinfo, const char* /*what*/) {
+  accumulate_info(c, dinfo, c->d_err + 4);
 }
 
 int as_int(int64_t v, const char* what) {
@@ -30,6 +30,16 @@ int as_int(int64_t v, const char* what) {
 }
 
 }  // namespace
+
+void check_factorizations(Context* c) {
+  int h = 0;
+  TTG_CUDA(cudaMemcpyAsync(&h, c->d_err + 4, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  if (h) {
+    TTG_CUDA(cudaMemsetAsync(c->d_err + 4, 0, sizeof(int), c->stream));
+    fail(TTG_ERR_SOLVER, "a device factorization reported a non-zero LAPACK info");
+  }
+}
 
 void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t lda, double* R) {
   if (k <= 0 || n <= 0) return;
@@ -42,6 +52,10 @@ void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t
 
 int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R) {
   const int64_t k = std::min(m, n);
+  if (small_qr_fits(m, n)) {
+    small_qr_f64(c, m, n, A, m, Q, R);
+    return k;
+  }
   const int mi = as_int(m, "m"), ni = as_int(n, "n"), ki = as_int(k, "k");
   DBuf<double> work(c, m * n), tau(c, k > 0 ? k : 1);
   DBuf<int> info(c, 1);
@@ -59,17 +73,18 @@ int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, dou
 }
 
 namespace {
-// gesvd on m >= n, econ; A is overwritten.
-void gesvd_tall(Context* c, int64_t m, int64_t n, double* A, double* U, double* S, double* VT) {
-  const int mi = as_int(m, "m"), ni = as_int(n, "n");
-  int lwork = 0;
-  TTG_SOLVER(cusolverDnDgesvd_bufferSize(c->solver, mi, ni, &lwork));
-  DBuf<double> ws(c, std::max(lwork, 1)), rwork(c, std::max<int64_t>(n, 1));
-  DBuf<int> info(c, 1);
-  signed char jobu = 'S', jobvt = 'S';
-  TTG_SOLVER(cusolverDnDgesvd(c->solver, jobu, jobvt, mi, ni, A, mi, S, U, mi, VT, ni, ws.p(),
-                              lwork, rwork.p(), info.p()));
-  check_info(c, info.p(), "gesvd");
+// Economy SVD of a tall m x n (m >= n) matrix: QR, then one-sided Jacobi SVD
+// of the n x n triangular factor (small_dense.cu), U = Q Ur.
+void svd_tall(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
+              double* VT) {
+  if (m == n) {
+    jacobi_svd_f64(c, n, A, m, U, S, VT);
+    return;
+  }
+  DBuf<double> Q(c, m * n), R(c, n * n), Ur(c, n * n);
+  qr_f64(c, m, n, A, Q.p(), R.p());
+  jacobi_svd_f64(c, n, R.p(), n, Ur.p(), S, VT);
+  gemm_f64(c, false, false, m, n, n, 1.0, Q.p(), m, 0, Ur.p(), n, 0, 0.0, U, m, 0, 1);
 }
 }  // namespace
 
@@ -78,29 +93,12 @@ int64_t svd_f64(Context* c, int64_t m, int64_t n, const double* A, double* U, do
   const int64_t k = std::min(m, n);
   if (k <= 0) return 0;
   if (m >= n) {
-    if (m >= 2 * n && n > 1) {
-      // A = Q R ; R = Ur S VT ; U = Q Ur
-      DBuf<double> Q(c, m * n), R(c, n * n), Ur(c, n * n);
-      qr_f64(c, m, n, A, Q.p(), R.p());
-      gesvd_tall(c, n, n, R.p(), Ur.p(), S, VT);
-      gemm_f64(c, false, false, m, n, n, 1.0, Q.p(), m, 0, Ur.p(), n, 0, 0.0, U, m, 0, 1);
-    } else {
-      DBuf<double> W(c, m * n);
-      copy_f64(c, m * n, A, W.p());
-      gesvd_tall(c, m, n, W.p(), U, S, VT);
-    }
+    svd_tall(c, m, n, A, U, S, VT);
   } else {
     // A^T (n x m) = U' S V'^T  ->  A = V' S U'^T : U = V' = (VT')^T, VT = U'^T
     DBuf<double> At(c, n * m), Up(c, n * m), VTp(c, m * m);
     transpose_f64(c, m, n, A, m, At.p(), n);
-    if (n >= 2 * m && m > 1) {
-      DBuf<double> Q(c, n * m), R(c, m * m), Ur(c, m * m);
-      qr_f64(c, n, m, At.p(), Q.p(), R.p());
-      gesvd_tall(c, m, m, R.p(), Ur.p(), S, VTp.p());
-      gemm_f64(c, false, false, n, m, m, 1.0, Q.p(), n, 0, Ur.p(), m, 0, 0.0, Up.p(), n, 0, 1);
-    } else {
-      gesvd_tall(c, n, m, At.p(), Up.p(), S, VTp.p());
-    }
+    svd_tall(c, n, m, At.p(), Up.p(), S, VTp.p());
     transpose_f64(c, m, m, VTp.p(), m, U, m);     // U (m x m) = VT'^T
     transpose_f64(c, n, m, Up.p(), n, VT, m);     // VT (m x n) = U'^T
   }

@@ -4,6 +4,11 @@
 
 namespace ttg {
 
+// Failures of the library factorizations (LAPACK info != 0) are accumulated
+// into the context's device error slot 4 without a host round trip; call
+// check_factorizations() after a sequence to turn them into an error.
+void check_factorizations(Context* c);
+
 // Thin QR of the m x n column-major A (lda = m): Q (m x k, ld m) and
 // R (k x n, ld k), k = min(m, n).  A is not modified.  Householder QR with
 // LAPACK's sign convention (geqrf/orgqr), as MATLAB's qr(A,0).

@@ -5,9 +5,11 @@
 
 namespace ttg {
 
+// dres = rhs - B sol_prev (FP64), nres = ||dres||, nrhs = ||rhs|| are given.
 LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Phi1,
                                    const double* A, const double* Phi2, const double* rhs,
-                                   double tol, const double* sol_prev, int64_t nrestart,
-                                   int64_t niters, double* sol);
+                                   const double* dres, double nres, double nrhs, double tol,
+                                   const double* sol_prev, int64_t nrestart, int64_t niters,
+                                   double* sol);
 
 }  // namespace ttg

@@ -58,8 +58,9 @@ constexpr size_t umma_smem_bytes() {
 template <int BN, bool OUT_BF16>
 __global__ void __launch_bounds__(128, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                int K, int a_rows_pb, int b_rows_pb, OutMap om, int* err) {
+                int K, int a_rows_pb, int b_rows_pb, OutMap om, int* err, const int* skip) {
   using namespace umma;
+  if (skip && *skip) return;  // queued Krylov step after convergence
   constexpr int B_BYTES = BN * UM_BK * 2;
   constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
   extern __shared__ uint8_t smem_raw[];
@@ -137,22 +138,27 @@ __global__ void __launch_bounds__(128, 1)
     const bool row_ok = m < om.M;
     const int64_t roff = row_ok ? map2(m, om.r_s1, om.r_t1, om.r_t2) : 0;
     const int64_t boff = int64_t(bz) * om.batch_stride;
+    // Column offsets advance incrementally: (n % c_s1, n / c_s1) -> no
+    // division per element.
+    int64_t cq = (int64_t(n0)) / om.c_s1, cr = (int64_t(n0)) % om.c_s1;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
       if (n0 + c0 >= om.N) break;  // uniform across the CTA
       float v[16];
       tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
-      if (row_ok) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int64_t n = int64_t(n0) + c0 + j;
-          if (n < om.N) {
-            const int64_t off = boff + roff + map2(n, om.c_s1, om.c_t1, om.c_t2);
-            if (OUT_BF16)
-              static_cast<__nv_bfloat16*>(om.base)[off] = __float2bfloat16_rn(v[j]);
-            else
-              static_cast<float*>(om.base)[off] = v[j];
-          }
+      for (int j = 0; j < 16; ++j) {
+        const int64_t n = int64_t(n0) + c0 + j;
+        if (row_ok && n < om.N) {
+          const int64_t off = boff + roff + cr * om.c_t1 + cq * om.c_t2;
+          if (OUT_BF16)
+            static_cast<__nv_bfloat16*>(om.base)[off] = __float2bfloat16_rn(v[j]);
+          else
+            static_cast<float*>(om.base)[off] = v[j];
+        }
+        if (++cr == om.c_s1) {
+          cr = 0;
+          ++cq;
         }
       }
     }
@@ -214,7 +220,8 @@ __global__ void k_cvt_phi1(int64_t ry1, int64_t rx1, int64_t ra1, int64_t ld2,
 
 // X[b + ldx*row] = v[b + rx2*row]  (row = m + n*a; zero padding)
 __global__ void k_cvt_x(int64_t rx2, int64_t rows, int64_t ldx, const float* __restrict__ v,
-                        __nv_bfloat16* __restrict__ out) {
+                        __nv_bfloat16* __restrict__ out, const int* skip) {
+  if (skip && *skip) return;
   const int64_t total = ldx * rows;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -291,7 +298,7 @@ void launch_bn(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t
   }
   dim3 grid{unsigned((M + UM_BM - 1) / UM_BM), unsigned((N + BN - 1) / BN), unsigned(batch)};
   k_umma_gemm<BN, OB><<<grid, 128, smem, c->stream>>>(ta, tb, int(K), int(a_rows_pb),
-                                                      int(b_rows_pb), om, c->d_err + 1);
+                                                      int(b_rows_pb), om, c->d_err + 1, c->skip);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
 }
@@ -352,7 +359,7 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
 void MixedOp::apply(Context* c, const float* v, float* y) {
   MvTiming timing(c, 1);
   const int64_t rows = d.m * d.rx1;
-  k_cvt_x<<<blocks_for(c, ldx * rows), 256, 0, c->stream>>>(d.rx2, rows, ldx, v, X.p());
+  k_cvt_x<<<blocks_for(c, ldx * rows), 256, 0, c->stream>>>(d.rx2, rows, ldx, v, X.p(), c->skip);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
   // stage 1: T1[(m,a),(be,k)]

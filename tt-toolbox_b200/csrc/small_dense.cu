@@ -1,0 +1,271 @@
+// Single-CTA FP64 dense factorizations for the small matrices of the AMEn
+// and rounding sweeps (replacing library calls whose host-side sequencing
+// cost milliseconds on 64x64 inputs):
+//
+//   k_jacobi_svd : one-sided (Hestenes) Jacobi SVD of a square n x n matrix,
+//                  round-robin pairing, one warp per column pair, the matrix
+//                  held in shared memory (global memory above ~160 columns),
+//                  V accumulated in global memory.  Singular values sorted
+//                  descending.  One launch, no host round trip.
+//   k_house_qr   : Householder QR (LAPACK sign convention: beta =
+//                  -sign(alpha) ||x||, as geqrf/orgqr and MATLAB's qr(A,0))
+//                  of an m x n matrix that fits in shared memory; forms the
+//                  thin Q and R.
+#include <cmath>
+
+#include "small_dense.h"
+
+namespace ttg {
+
+namespace {
+
+constexpr int SD_THREADS = 1024;
+constexpr int SD_WARPS = SD_THREADS / 32;
+constexpr int JAC_MAX_SWEEPS = 40;
+constexpr size_t SMEM_LIMIT = 200 * 1024;
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Column index of slot k in round r of a round-robin tournament on ne (even)
+// players: slot 0 is fixed, the others rotate.
+__device__ __forceinline__ int rr_player(int k, int r, int ne) {
+  return k == 0 ? 0 : 1 + ((k - 1 + r) % (ne - 1));
+}
+
+// A: n x n (column-major, lda) input; U (n x n, ld n), S (n), VT (n x n, ld n)
+// outputs.  work: n*n doubles of global scratch used when A does not fit in
+// shared memory.  Status: *err = 5 if the sweep limit is reached.
+__global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* __restrict__ Ain,
+                                                          int lda, double* __restrict__ U,
+                                                          double* __restrict__ S,
+                                                          double* __restrict__ VT,
+                                                          double* __restrict__ Vg,
+                                                          double* __restrict__ work, int in_smem,
+                                                          int* err) {
+  extern __shared__ double sm[];
+  __shared__ double s_off[SD_WARPS];
+  __shared__ int s_done;
+  // in_smem: 0 = A and V in global memory, 1 = A in shared memory,
+  // 2 = A and V in shared memory.
+  double* A = in_smem ? sm : work;
+  double* V = in_smem == 2 ? sm + int64_t(n) * n : Vg;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < n * n; e += SD_THREADS) {
+    const int i = e % n, j = e / n;
+    A[e] = Ain[i + int64_t(j) * lda];
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int ne = (n + 1) & ~1;  // even number of players (dummy column n if odd)
+  const double tol = 4.0 * 2.220446049250313e-16;
+  int sweep = 0;
+  for (sweep = 0; sweep < JAC_MAX_SWEEPS; ++sweep) {
+    double off = 0.0;
+    for (int r = 0; r < ne - 1; ++r) {
+      for (int pr = warp; pr < ne / 2; pr += SD_WARPS) {
+        int p = rr_player(pr, r, ne), q = rr_player(ne - 1 - pr, r, ne);
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        if (q >= n) continue;  // dummy player
+        double* ap = A + int64_t(p) * n;
+        double* aq = A + int64_t(q) * n;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int i = lane; i < n; i += 32) {
+          const double x = ap[i], y = aq[i];
+          al += x * x;
+          be += y * y;
+          ga += x * y;
+        }
+        al = wsum(al);
+        be = wsum(be);
+        ga = wsum(ga);
+        const double nrm = sqrt(al * be);
+        if (nrm == 0.0 || fabs(ga) <= tol * nrm) continue;
+        off = fmax(off, fabs(ga) / nrm);
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        double* vp = V + int64_t(p) * n;
+        double* vq = V + int64_t(q) * n;
+        for (int i = lane; i < n; i += 32) {
+          const double x = ap[i], y = aq[i];
+          ap[i] = c * x - s * y;
+          aq[i] = s * x + c * y;
+          const double vx = vp[i], vy = vq[i];
+          vp[i] = c * vx - s * vy;
+          vq[i] = s * vx + c * vy;
+        }
+      }
+      __syncthreads();
+    }
+    if (lane == 0) s_off[warp] = off;
+    __syncthreads();
+    if (tid == 0) {
+      double m = 0.0;
+      for (int w = 0; w < SD_WARPS; ++w) m = fmax(m, s_off[w]);
+      s_done = (m <= tol) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_done) break;
+  }
+  if (tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(err, 5);
+  // Column norms -> singular values; rank by value (descending, stable on index).
+  double* sig = work + int64_t(n) * n;  // n scratch
+  for (int j = warp; j < n; j += SD_WARPS) {
+    const double* aj = A + int64_t(j) * n;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += aj[i] * aj[i];
+    s = wsum(s);
+    if (lane == 0) sig[j] = sqrt(s);
+  }
+  __syncthreads();
+  for (int j = tid; j < n; j += SD_THREADS) {
+    const double sj = sig[j];
+    int pos = 0;
+    for (int k = 0; k < n; ++k) {
+      const double sk = sig[k];
+      pos += (sk > sj) || (sk == sj && k < j);
+    }
+    S[pos] = sj;
+    sig[n + j] = double(pos);
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += SD_THREADS) {
+    const int i = e % n, j = e / n;
+    const int pos = int(sig[n + j]);
+    const double sj = sig[j];
+    U[i + int64_t(pos) * n] = sj > 0.0 ? A[e] / sj : (i == pos ? 1.0 : 0.0);
+    VT[pos + int64_t(i) * n] = V[e];
+  }
+}
+
+// Householder QR of the m x n matrix A (column-major, lda) held in shared
+// memory: Q (m x k, ld m), R (k x n, ld k), k = min(m, n).
+__global__ void __launch_bounds__(SD_THREADS) k_house_qr(int m, int n, const double* __restrict__ Ain,
+                                                        int lda, double* __restrict__ Q,
+                                                        double* __restrict__ R) {
+  extern __shared__ double sm[];
+  double* A = sm;                 // m x n
+  double* tau = sm + int64_t(m) * n;  // k
+  __shared__ double red[SD_WARPS];
+  __shared__ double bcast[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int k = m < n ? m : n;
+  for (int e = tid; e < m * n; e += SD_THREADS) A[e] = Ain[(e % m) + int64_t(e / m) * lda];
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    double* aj = A + int64_t(j) * m;
+    // ||x(2:end)||^2
+    double s = 0.0;
+    for (int i = j + 1 + tid; i < m; i += SD_THREADS) s += aj[i] * aj[i];
+    s = wsum(s);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < SD_WARPS; ++w) t += red[w];
+      const double alpha = aj[j];
+      double beta, tj, scal;
+      if (t == 0.0) {
+        beta = alpha;
+        tj = 0.0;
+        scal = 0.0;
+      } else {
+        beta = -copysign(sqrt(alpha * alpha + t), alpha);
+        tj = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      tau[j] = tj;
+      aj[j] = beta;
+      bcast[0] = scal;
+    }
+    __syncthreads();
+    const double scal = bcast[0];
+    for (int i = j + 1 + tid; i < m; i += SD_THREADS) aj[i] *= scal;  // v(2:end), v(1) = 1
+    __syncthreads();
+    const double tj = tau[j];
+    if (tj != 0.0) {
+      for (int c = j + 1 + warp; c < n; c += SD_WARPS) {
+        double* ac = A + int64_t(c) * m;
+        double w = 0.0;
+        for (int i = j + lane; i < m; i += 32) w += (i == j ? 1.0 : aj[i]) * ac[i];
+        w = wsum(w) * tj;
+        for (int i = j + lane; i < m; i += 32) ac[i] -= w * (i == j ? 1.0 : aj[i]);
+      }
+    }
+    __syncthreads();
+  }
+  // R
+  for (int e = tid; e < k * n; e += SD_THREADS) {
+    const int i = e % k, c = e / k;
+    R[e] = (i <= c) ? A[i + int64_t(c) * m] : 0.0;
+  }
+  // Q = H_0 H_1 ... H_{k-1} I(:, 0:k), applied right to left into global Q.
+  for (int e = tid; e < m * k; e += SD_THREADS) {
+    const int i = e % m, c = e / m;
+    Q[e] = (i == c) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int j = k - 1; j >= 0; --j) {
+    const double tj = tau[j];
+    const double* v = A + int64_t(j) * m;
+    if (tj != 0.0) {
+      for (int c = j + warp; c < k; c += SD_WARPS) {
+        double* qc = Q + int64_t(c) * m;
+        double w = 0.0;
+        for (int i = j + lane; i < m; i += 32) w += (i == j ? 1.0 : v[i]) * qc[i];
+        w = wsum(w) * tj;
+        for (int i = j + lane; i < m; i += 32) qc[i] -= w * (i == j ? 1.0 : v[i]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+bool small_qr_fits(int64_t m, int64_t n) {
+  return m * n + std::min(m, n) <= int64_t(SMEM_LIMIT / sizeof(double)) && m <= 0x7fffffff;
+}
+
+void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
+                  double* R) {
+  const size_t smem = sizeof(double) * size_t(m * n + std::min(m, n));
+  static bool attr = false;
+  if (!attr) {
+    TTG_CUDA(cudaFuncSetAttribute(k_house_qr, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(SMEM_LIMIT + 1024)));
+    attr = true;
+  }
+  k_house_qr<<<1, SD_THREADS, smem, c->stream>>>(int(m), int(n), A, int(lda), Q, R);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
+                    double* VT) {
+  TTG_REQUIRE(n >= 1 && n <= 4096, "jacobi_svd: n = %lld out of range", (long long)n);
+  const size_t mat = size_t(n * n) * sizeof(double);
+  const int mode = 2 * mat <= SMEM_LIMIT ? 2 : (mat <= SMEM_LIMIT ? 1 : 0);
+  DBuf<double> V(c, n * n), work(c, n * n + 2 * n);
+  static bool attr = false;
+  if (!attr) {
+    TTG_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(SMEM_LIMIT + 1024)));
+    attr = true;
+  }
+  const size_t smem = size_t(mode) * mat;
+  k_jacobi_svd<<<1, SD_THREADS, smem, c->stream>>>(int(n), A, int(lda), U, S, VT, V.p(),
+                                                    work.p(), mode, c->d_err + 3);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+}  // namespace ttg

@@ -1,0 +1,17 @@
+// Single-CTA FP64 factorizations of small matrices (small_dense.cu).
+#pragma once
+#include "kernels.h"
+
+namespace ttg {
+
+// True when an m x n Householder QR fits in one CTA's shared memory.
+bool small_qr_fits(int64_t m, int64_t n);
+// Thin Householder QR in one CTA: Q (m x k, ld m), R (k x n, ld k).
+void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
+                  double* R);
+// One-sided Jacobi SVD of a square n x n matrix: U (n x n), S (n, descending),
+// VT (n x n), all with leading dimension n.
+void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
+                    double* VT);
+
+}  // namespace ttg

@@ -115,6 +115,8 @@ def lib():
         "ttg_local_solve": [_vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp, C.c_double,
                             C.c_int32, _vp, C.c_int32, _i64, _i64, _vp, C.c_int32, _p64],
     }
+    sigs["ttg_dense_qr"] = [_vp, _i64, _i64, _vp, _vp, _vp]
+    sigs["ttg_dense_svd"] = [_vp, _i64, _i64, _vp, _vp, _vp, _vp]
     for name, args in sigs.items():
         f = getattr(L, name)
         f.argtypes = args
@@ -545,6 +547,28 @@ def solve3d_2(Phi1, A, Phi2, rhs, tol, trunc_norm, sol_prev, prec=0, nrestart=40
     if info is not None:
         info["iters"] = it.value
     return out.get()
+
+
+def dense_qr(A, ctx=None):
+    """Thin QR of a host matrix on the device: ``(Q, R)`` (as ``qr(A, 0)``)."""
+    ctx = ctx or default_context()
+    A = np.asarray(A, dtype=np.float64)
+    m, n = A.shape
+    k = min(m, n)
+    dA, dQ, dR = ctx.to_device(A), ctx.empty(m * k), ctx.empty(k * n)
+    _check(lib().ttg_dense_qr(ctx.h, m, n, dA.p, dQ.p, dR.p))
+    return dQ.get().reshape(m, k, order="F"), dR.get().reshape(k, n, order="F")
+
+
+def dense_svd(A, ctx=None):
+    """Economy SVD of a host matrix on the device: ``(U, s, VT)`` (as ``svd(A,'econ')``)."""
+    ctx = ctx or default_context()
+    A = np.asarray(A, dtype=np.float64)
+    m, n = A.shape
+    k = min(m, n)
+    dA, dU, dS, dV = ctx.to_device(A), ctx.empty(m * k), ctx.empty(k), ctx.empty(k * n)
+    _check(lib().ttg_dense_svd(ctx.h, m, n, dA.p, dU.p, dS.p, dV.p))
+    return (dU.get().reshape(m, k, order="F"), dS.get(), dV.get().reshape(k, n, order="F"))
 
 
 def round_half(v):
