@@ -181,6 +181,26 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2,
                     int32_t prec, int64_t nrestart, int64_t niters,
                     double* sol_out, int32_t precision, int64_t* iters_out);
 
+/* Local matvec that allocates nothing.  No counterpart in the reference: it
+ * is ttg_local_matvec (FP64) for callers that may not allocate device memory
+ * -- hosts whose memory budget is owned by another pool, time-critical loops
+ * that must not hit cudaMalloc's implicit synchronisation or out-of-memory
+ * failure, plugin hosts whose memory manager forbids untracked allocations.
+ * The caller passes device inputs and outputs only; the two contraction
+ * intermediates use a fixed scratch array built into the library, 64 MiB per
+ * GPU (8 Mi doubles), held by every GPU that loads the library until exit.
+ * Sizes whose intermediates (rx1*n*ra2*rx2 + rx1*ra1*n*rx2 doubles) exceed
+ * it are rejected with TTG_ERR_INVALID.  stream: a cudaStream_t (NULL = the
+ * legacy default stream) of the current device; the call returns after the
+ * stream has finished.  The first call on a device looks up the array's
+ * device address, so make it before any stream capture.  All calls on a
+ * device share the array: calls whose GPU work overlaps (other streams,
+ * other host threads) race on it and must be serialised by the caller. */
+int ttg_local_matvec_noalloc(void* stream, int64_t rx1, int64_t n, int64_t rx2,
+                             int64_t ra1, int64_t ra2, const double* Phi1,
+                             const double* A, const double* Phi2, const double* x,
+                             double* y);
+
 /* ---- device FP64 factorizations used by the sweeps (device pointers) -------
  * Thin QR A = Q R (Q m x k, R k x n, k = min(m,n); Householder with LAPACK's
  * sign convention, as MATLAB's qr(A,0) at round.m:41 / amen_solve2.m:342) and

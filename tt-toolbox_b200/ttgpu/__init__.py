@@ -115,6 +115,8 @@ def lib():
         "ttg_local_solve": [_vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp, C.c_double,
                             C.c_int32, _vp, C.c_int32, _i64, _i64, _vp, C.c_int32, _p64],
     }
+    sigs["ttg_local_matvec_noalloc"] = [_vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp,
+                                        _vp]
     sigs["ttg_dense_qr"] = [_vp, _i64, _i64, _vp, _vp, _vp]
     sigs["ttg_dense_svd"] = [_vp, _i64, _i64, _vp, _vp, _vp, _vp]
     for name, args in sigs.items():
