@@ -211,6 +211,29 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
 int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double* U, double* S,
                   double* VT);
 
+/* ---- Gradients with respect to every core (FP64) ----------------------
+ * No counterpart in the reference: TT-Toolbox has no derivative code.  The
+ * forward maps are the reference's own, cited per entry.  x is a TT tensor
+ * with boundary ranks 1; grad is a DEVICE buffer of numel(x) doubles
+ * (ttg_malloc), written in x's flat core layout (grad of core k at the
+ * offset of core k); value (nullable, host) receives f(x).  Operands must
+ * belong to the same context. */
+
+/* f(x) = <x, A x>: @tt_matrix/mtimes.m:38-65 then @tt_tensor/dot.m:92-111.
+ * A: TT matrix with A.n = A.m = x.n. */
+int ttg_grad_xAx(ttg_tt x, ttg_tt A, double* grad, double* value);
+
+/* f(x) = <x, b>: @tt_tensor/dot.m:92-111.  b: TT tensor with b.n = x.n. */
+int ttg_grad_xb(ttg_tt x, ttg_tt b, double* grad, double* value);
+
+/* f(x) = sum_s (X[idx_s] - y_s)^2 with X[idx_s] the entry of the element
+ * path @tt_tensor/subsref.m:93-123.  idx: DEVICE int32 array, column-major
+ * nsamples x d (column k holds the mode-k indices, as MATLAB's ind(:,k)),
+ * 0-based; an index outside [0, n_k) fails with TTG_ERR_INVALID.
+ * y: DEVICE array of nsamples doubles.  Mode sizes up to 8192. */
+int ttg_grad_sampled(ttg_tt x, int64_t nsamples, const int32_t* idx, const double* y,
+                     double* grad, double* value);
+
 #ifdef __cplusplus
 }
 #endif

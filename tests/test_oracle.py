@@ -165,3 +165,37 @@ def test_aniso_operator_rank3_matches_dense():
     dense = (np.kron(I, np.kron(I, c[0] * L)) + np.kron(I, np.kron(c[1] * L, I)) +
              np.kron(c[2] * L, np.kron(I, I)) + 36.0 * np.kron(M, np.kron(M, M)))
     assert np.allclose(A.full(), dense)
+
+
+def _fd_grad_check(f, cs, G, rng, nprobe=10, h=1e-6):
+    f0 = abs(f(cs))
+    for _ in range(nprobe):
+        k = int(rng.integers(len(cs)))
+        i = tuple(int(rng.integers(s)) for s in cs[k].shape)
+        cp = [c.copy() for c in cs]
+        cm = [c.copy() for c in cs]
+        cp[k][i] += h
+        cm[k][i] -= h
+        fd = (f(cp) - f(cm)) / (2 * h)
+        assert abs(fd - G[k][i]) <= 1e-6 * abs(G[k][i]) + 1e-8 * max(1.0, f0)
+
+
+def test_grad_oracle_vs_full_tensor_and_fd():
+    """The oracle's sweep gradients against the full-tensor functionals
+    (value) and central differences (h = 1e-6) on a nonsymmetric operator."""
+    from oracle import grad as og
+    rng = np.random.default_rng(21)
+    n, r, ra, rb = [3, 4, 2, 3], [1, 2, 3, 2, 1], [1, 2, 3, 2, 1], [1, 3, 2, 2, 1]
+    xs = [rng.standard_normal((r[k], n[k], r[k + 1])) for k in range(4)]
+    As = [rng.standard_normal((ra[k], n[k], n[k], ra[k + 1])) for k in range(4)]
+    bs = [rng.standard_normal((rb[k], n[k], rb[k + 1])) for k in range(4)]
+    idx = np.stack([rng.integers(0, n[k], 60) for k in range(4)], axis=1)
+    y = rng.standard_normal(60)
+    for f_sweep, f_full, arg in [(og.xAx, og.full_xAx, As), (og.xb, og.full_xb, bs)]:
+        v, G = f_sweep(xs, arg)
+        assert v == pytest.approx(f_full(xs, arg), rel=1e-12)
+        _fd_grad_check(lambda cs: f_full(cs, arg), xs, G, rng)
+    v, G = og.sampled(xs, idx, y)
+    assert v == pytest.approx(og.full_sampled(xs, idx, y), rel=1e-12)
+    assert np.allclose(og.entries(xs, idx), og.full_tensor(xs)[tuple(idx.T)], rtol=1e-13)
+    _fd_grad_check(lambda cs: og.full_sampled(cs, idx, y), xs, G, rng)

@@ -447,7 +447,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
         // evaluated in growing batches and read back once per batch; the rank
         // is the first candidate whose residual exceeds thr, as in the loop.
         DBuf<double> us(c, M * K), cursol(c, M * r2);
-        int64_t found = -1, next = K - 1, batch = 2;
+        int64_t found = -1, next = K - 1, batch = 1;
         while (next >= 1 && found < 0) {
           const int64_t nb = std::min<int64_t>(std::min(batch, next), Scalars::NCAND);
           for (int64_t b = 0; b < nb; ++b) {

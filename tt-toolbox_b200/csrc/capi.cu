@@ -2,11 +2,28 @@
 #include <cmath>
 
 #include "amen.h"
+#include "grad.h"
 #include "linalg.h"
 #include "round.h"
 #include "mixed_ops.h"
 
 using namespace ttg;
+
+namespace {
+
+// Shared checks of the gradient entries: same context, a device output.
+ttg::Context* grad_ctx(ttg_tt x, ttg_tt other, double* grad) {
+  TTG_REQUIRE(x && grad, "NULL argument");
+  if (other) TTG_REQUIRE(other->ctx == x->ctx, "operands belong to different contexts");
+  TTG_CUDA(cudaSetDevice(x->ctx->device));
+  return x->ctx;
+}
+
+void grad_value_out(ttg::Context* c, const double* dval, double* value) {
+  if (value) ttg::read_scalars(c, dval, value, 1);
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -175,6 +192,40 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_
   if (herr[0] || herr[1] || herr[2])
     fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out in the local solve");
   if (iters_out) *iters_out = r.iters;
+  TTG_API_END
+}
+
+int ttg_grad_xAx(ttg_tt x, ttg_tt A, double* grad, double* value) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(A, "NULL argument");
+  Context* c = grad_ctx(x, A, grad);
+  DBuf<double> v(c, 1);
+  grad_xAx(c, x, A, grad, v.p());
+  grad_value_out(c, v.p(), value);
+  sync(c);
+  TTG_API_END
+}
+
+int ttg_grad_xb(ttg_tt x, ttg_tt b, double* grad, double* value) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(b, "NULL argument");
+  Context* c = grad_ctx(x, b, grad);
+  DBuf<double> v(c, 1);
+  grad_xb(c, x, b, grad, v.p());
+  grad_value_out(c, v.p(), value);
+  sync(c);
+  TTG_API_END
+}
+
+int ttg_grad_sampled(ttg_tt x, int64_t nsamples, const int32_t* idx, const double* y,
+                     double* grad, double* value) {
+  TTG_API_BEGIN
+  Context* c = grad_ctx(x, nullptr, grad);
+  TTG_REQUIRE(nsamples >= 0, "nsamples must be >= 0");
+  DBuf<double> v(c, 1);
+  grad_sampled(c, x, nsamples, idx, y, grad, v.p());
+  grad_value_out(c, v.p(), value);
+  sync(c);
   TTG_API_END
 }
 

@@ -9,6 +9,7 @@
 // has no FP64 kind).  Global->shared staging with cp.async (8-byte granules so
 // any leading dimension works), double buffered.
 #include "kernels.h"
+#include "dmma.cuh"
 
 namespace ttg {
 
@@ -27,23 +28,6 @@ struct GemmP {
   double alpha, beta;
   const int* skip;  // optional: return at once when *skip != 0
 };
-
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
-  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  int bytes = pred ? 8 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
 
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {

@@ -119,6 +119,9 @@ def lib():
                                         _vp]
     sigs["ttg_dense_qr"] = [_vp, _i64, _i64, _vp, _vp, _vp]
     sigs["ttg_dense_svd"] = [_vp, _i64, _i64, _vp, _vp, _vp, _vp]
+    sigs["ttg_grad_xAx"] = [_vp, _vp, _vp, _pd]
+    sigs["ttg_grad_xb"] = [_vp, _vp, _vp, _pd]
+    sigs["ttg_grad_sampled"] = [_vp, _i64, _vp, _vp, _vp, _pd]
     for name, args in sigs.items():
         f = getattr(L, name)
         f.argtypes = args
@@ -576,3 +579,99 @@ def dense_svd(A, ctx=None):
 def round_half(v):
     """MATLAB's ``round`` of a scalar option (``solve3d_2.c:138-141,179``)."""
     return int(np.floor(float(v) + 0.5))
+
+
+# ---------------------------------------------------------------------------
+# Gradients with respect to every core (no reference counterpart; the forward
+# maps are @tt_matrix/mtimes.m:38-65, @tt_tensor/dot.m:92-111 and the element
+# path of @tt_tensor/subsref.m:93-123)
+# ---------------------------------------------------------------------------
+
+def _grad_call(fn, x, other, ctx, *extra, out=None):
+    """Run one gradient entry.  With ``out`` (a ``DeviceArray`` of numel(x)
+    doubles) the gradient stays on the device and ``(f, out)`` is returned;
+    otherwise ``(f, TensorTrain)`` with the gradient downloaded."""
+    ctx = ctx or (x.ctx if isinstance(x, DeviceTT) else default_context())
+    owned = []
+
+    def dev(t):
+        if t is None or isinstance(t, DeviceTT):
+            return t
+        h = DeviceTT.upload(ctx, t)
+        owned.append(h)
+        return h
+    dx, do = dev(x), dev(other)
+    n, m, r, numel = dx.shape()
+    g = out if out is not None else ctx.empty(numel)
+    if g.n < numel:
+        raise ValueError("out holds %d doubles, the gradient needs %d" % (g.n, numel))
+    val = C.c_double(0.0)
+    try:
+        if do is None:
+            _check(fn(dx.h, *extra, g.p, C.byref(val)))
+        else:
+            _check(fn(dx.h, do.h, g.p, C.byref(val)))
+        if out is not None:
+            return val.value, out
+        return val.value, TensorTrain(n, r, g.get())
+    finally:
+        if out is None:
+            g.free()
+        for h in owned:
+            h.free()
+
+
+def grad_xAx(x, A, ctx=None, out=None):
+    """``(f, G)`` with ``f = <x, A x>`` and ``G`` the gradient with respect to
+    every core of ``x`` (a ``TensorTrain`` with x's shapes, or ``out``)."""
+    return _grad_call(lib().ttg_grad_xAx, x, A, ctx, out=out)
+
+
+def grad_xb(x, b, ctx=None, out=None):
+    """``(f, G)`` with ``f = <x, b>``."""
+    return _grad_call(lib().ttg_grad_xb, x, b, ctx, out=out)
+
+
+class SampleSet:
+    """Device-resident samples for ``grad_sampled``: ``idx`` [S, d] 0-based
+    multi-indices (stored column-major int32) and values ``y`` [S]."""
+
+    def __init__(self, ctx, idx, y):
+        idx = np.asarray(idx)
+        if idx.ndim != 2:
+            raise ValueError("idx must be [S, d]")
+        self.ctx = ctx
+        self.S, self.d = idx.shape
+        col = np.asfortranarray(idx.astype(np.int32, copy=False))
+        yv = np.ascontiguousarray(np.asarray(y, dtype=np.float64).ravel())
+        if yv.size != self.S:
+            raise ValueError("y must have one value per sample")
+        self.idx = DeviceArray(ctx, None, max(1, (self.S * self.d + 1) // 2))
+        if self.S:
+            _check(lib().ttg_memcpy_h2d(ctx.h, self.idx.p, col.ctypes.data_as(_vp), col.nbytes))
+        self.y = DeviceArray(ctx, yv) if self.S else DeviceArray(ctx, None, 1)
+
+    def free(self):
+        self.idx.free()
+        self.y.free()
+
+
+def grad_sampled(x, idx, y=None, ctx=None, out=None):
+    """``(f, G)`` with ``f = sum_s (X[idx[s]] - y[s])^2``.
+
+    ``idx``: integer array ``[S, d]`` of 0-based multi-indices with ``y``
+    ``[S]``, or a ``SampleSet`` already on the device (``y`` omitted)."""
+    ctx = ctx or (x.ctx if isinstance(x, DeviceTT) else default_context())
+    own = not isinstance(idx, SampleSet)
+    ss = SampleSet(ctx, idx, y) if own else idx
+    d = x.d if not isinstance(x, DeviceTT) else len(x.shape()[0])
+    if ss.S and ss.d != d:
+        if own:
+            ss.free()
+        raise ValueError("idx must be [S, d] with d = %d" % d)
+    try:
+        return _grad_call(lib().ttg_grad_sampled, x, None, ctx, ss.S, ss.idx.p, ss.y.p,
+                          out=out)
+    finally:
+        if own:
+            ss.free()

@@ -1,0 +1,210 @@
+"""Fixed-shape runs of the hot kernels through the C ABI.
+
+``python -m ttgpu.kernel_bench matvec --r 64 --n 64 --ra 3 --reps 20``
+    runs ``ttg_local_matvec`` (``bfun3``, ``solve/amen_solve2.m:924-951``) on
+    seeded operands of one shape, in FP64 and in mixed (BF16 tcgen05)
+    precision, and prints the mean wall time per call.  The call is
+    synchronous, so the time includes the call's own conversions (FP64 ->
+    BF16 operands, natural <-> reversed vector layout) and one stream
+    synchronisation; it is the target of the kernel-level ncu captures.
+
+``python -m ttgpu.kernel_bench round --d 20 --n 16 --r 64 --terms 4``
+    rounds a sum of ``terms`` rank-``r`` Gaussian TTs (``@tt_tensor/round.m``)
+    on the device and prints the time, ranks and the relative error of the
+    rounded tensor against the input.
+
+``python -m ttgpu.kernel_bench grad --d 12 --n 32 --r 64 --samples 1000000``
+    gradients of <x,Ax>, <x,b> and the sampled-entry loss with respect to
+    every core, inputs resident on the device; time and FLOP/s (parity at
+    this size is checked in the GPU tests).
+
+``python -m ttgpu.kernel_bench dgemm``
+    cuBLAS FP64 GEMM throughput (torch.matmul, 8192^3) as the measured FP64
+    tensor-core reference for the FP64 kernels.
+"""
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import (Context, DeviceArray, DeviceTT, _check, _PREC, lib, round as tt_round,
+               workloads)
+
+
+def matvec(args):
+    ctx = Context(args.device)
+    rng = np.random.default_rng(args.seed)
+    r1 = r2 = args.r
+    n, ra = args.n, args.ra
+    P1 = DeviceArray(ctx, rng.standard_normal(r1 * r1 * ra))
+    A = DeviceArray(ctx, rng.standard_normal(ra * n * n * ra))
+    P2 = DeviceArray(ctx, rng.standard_normal(r2 * ra * r2))
+    x = DeviceArray(ctx, rng.standard_normal(r1 * n * r2))
+    y = DeviceArray(ctx, None, r1 * n * r2)
+    flops = 2.0 * n * r1 * r2 * (r1 * ra + ra * ra * n + r2 * ra)
+    out = {"shape": {"r1": r1, "n": n, "r2": r2, "ra1": ra, "ra2": ra}, "gflop": flops * 1e-9}
+    for prec in args.precision.split(","):
+        def call():
+            _check(lib().ttg_local_matvec(ctx.h, r1, n, r2, ra, ra, P1.p, A.p, P2.p, x.p, y.p,
+                                          _PREC[prec]))
+        for _ in range(3):
+            call()
+        ctx.sync()
+        t = time.perf_counter()
+        for _ in range(args.reps):
+            call()
+        ctx.sync()
+        ms = (time.perf_counter() - t) / args.reps * 1e3
+        out[prec] = {"ms_per_call": ms, "tflops_per_call": flops / (ms * 1e-3) * 1e-12}
+    print(json.dumps(out))
+    ctx.close()
+
+
+def round_bench(args):
+    ctx = Context(args.device)
+    X = workloads.round_input(d=args.d, n=args.n, r=args.r, terms=args.terms, seed=args.seed)
+    dX = DeviceTT.upload(ctx, X)
+    out = {"workload": "round: d=%d n=%d, sum of %d rank-%d Gaussian TTs, eps=%g"
+                       % (args.d, args.n, args.terms, args.r, args.eps)}
+    for prec in args.precision.split(","):
+        times, st = [], {}
+        for it in range(args.reps + 1):
+            ctx.flush_l2()
+            ctx.sync()
+            t = time.perf_counter()
+            Y = tt_round(dX, args.eps, precision=prec, ctx=ctx, stats=st)
+            ctx.sync()
+            if it:
+                times.append(time.perf_counter() - t)
+            if it < args.reps:
+                Y.free()
+        r = Y.shape()[2]
+        Yh = Y.download()
+        Y.free()
+        out[prec] = {"ms": float(np.median(times)) * 1e3, "ranks": [int(v) for v in r],
+                     "ms_qr_sweep": st["ms_qr_sweep"], "ms_svd_sweep": st["ms_svd_sweep"]}
+        if args.check:
+            out[prec]["rel_err"] = _rel_diff(X, Yh)
+    print(json.dumps(out))
+    dX.free()
+    ctx.close()
+
+
+def _time(ctx, fn, reps):
+    fn()
+    ctx.sync()
+    ts = []
+    for _ in range(reps):
+        ctx.flush_l2()
+        ctx.sync()
+        t = time.perf_counter()
+        fn()
+        ctx.sync()
+        ts.append(time.perf_counter() - t)
+    return float(np.median(ts)) * 1e3
+
+
+def grad_bench(args):
+    from . import SampleSet, grad_sampled, grad_xAx, grad_xb
+    ctx = Context(args.device)
+    x, A, b, idx, y = workloads.grad_inputs(d=args.d, n=args.n, r=args.r, nsamples=args.samples,
+                                            seed=args.seed)
+    dx, dA, db = DeviceTT.upload(ctx, x), DeviceTT.upload(ctx, A), DeviceTT.upload(ctx, b)
+    ss = SampleSet(ctx, idx, y)
+    g = DeviceArray(ctx, None, x.core.size)
+    r, n, ra, rb = list(x.r), list(x.n), list(A.r), list(b.r)
+    d = len(n)
+    f_mv = [2.0 * n[k] * r[k] * r[k + 1] * (r[k] * ra[k + 1] + ra[k] * ra[k + 1] * n[k]
+                                             + r[k + 1] * ra[k]) for k in range(d)]
+    # two interface sweeps (d updates each, same flop formula) + two local matvecs per core
+    fl_xAx = 2 * sum(f_mv) + 2 * sum(f_mv)
+    fl_xb = sum(2.0 * n[k] * (r[k] * rb[k] * rb[k + 1] + 2 * r[k] * r[k + 1] * rb[k + 1]
+                              + rb[k] * rb[k + 1] * r[k + 1] + r[k] * rb[k] * r[k + 1])
+                for k in range(d))
+    fl_s = 6.0 * args.samples * sum(r[k] * r[k + 1] for k in range(d))
+    out = {"workload": "grad: d=%d n=%d rank-%d x, rank-3 operator, rank-%d b, %d samples"
+                       % (args.d, args.n, args.r, rb[1], args.samples)}
+    runs = [("xAx", lambda: grad_xAx(dx, dA, ctx=ctx, out=g), fl_xAx),
+            ("xb", lambda: grad_xb(dx, db, ctx=ctx, out=g), fl_xb),
+            ("sampled", lambda: grad_sampled(dx, ss, ctx=ctx, out=g), fl_s)]
+    for name, fn, fl in runs:
+        ms = _time(ctx, fn, args.reps)
+        out[name] = {"ms": ms, "gflop": fl * 1e-9, "tflops": fl / (ms * 1e-3) * 1e-12}
+    print(json.dumps(out))
+    g.free()
+    ss.free()
+    for h in (dx, dA, db):
+        h.free()
+    ctx.close()
+
+
+def dgemm_bench(args):
+    import torch
+    n = args.size
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(args.reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    print(json.dumps({"dgemm": {"n": n, "ms": best, "tflops": 2.0 * n ** 3 / (best * 1e-3) * 1e-12}}))
+
+
+def _rel_diff(X, Y):
+    """||Y - X|| / ||X|| by TT inner products in FP64 on the host."""
+    xs, ys = X.cores(), Y.cores()
+
+    def gram(a, b):
+        G = np.ones((1, 1))
+        for ca, cb in zip(a, b):
+            G = np.einsum("ij,ink,jnl->kl", G, ca, cb)
+        return G[0, 0]
+    xx, yy, xy = gram(xs, xs), gram(ys, ys), gram(xs, ys)
+    return float(np.sqrt(max(xx + yy - 2 * xy, 0.0) / xx))
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    sub = p.add_subparsers(dest="what", required=True)
+    m = sub.add_parser("matvec")
+    m.add_argument("--r", type=int, default=64)
+    m.add_argument("--n", type=int, default=64)
+    m.add_argument("--ra", type=int, default=3)
+    m.add_argument("--reps", type=int, default=20)
+    m.add_argument("--precision", default="fp64,mixed")
+    r = sub.add_parser("round")
+    r.add_argument("--d", type=int, default=20)
+    r.add_argument("--n", type=int, default=16)
+    r.add_argument("--r", type=int, default=64)
+    r.add_argument("--terms", type=int, default=4)
+    r.add_argument("--eps", type=float, default=1e-8)
+    r.add_argument("--reps", type=int, default=3)
+    r.add_argument("--precision", default="fp64")
+    r.add_argument("--check", action="store_true")
+    g = sub.add_parser("grad")
+    g.add_argument("--d", type=int, default=12)
+    g.add_argument("--n", type=int, default=32)
+    g.add_argument("--r", type=int, default=64)
+    g.add_argument("--samples", type=int, default=1_000_000)
+    g.add_argument("--reps", type=int, default=5)
+    dg = sub.add_parser("dgemm")
+    dg.add_argument("--size", type=int, default=8192)
+    dg.add_argument("--reps", type=int, default=10)
+    for s in (m, r, g, dg):
+        s.add_argument("--device", type=int, default=0)
+        s.add_argument("--seed", type=int, default=5)
+    args = p.parse_args()
+    {"matvec": matvec, "round": round_bench, "grad": grad_bench, "dgemm": dgemm_bench}[args.what](args)
+
+
+if __name__ == "__main__":
+    main()

@@ -143,3 +143,32 @@ def round_input(d=20, n=16, r=64, terms=4, seed=2):
         t = randn_cores(n, d, r, rng, scale=lambda r1, nn, r2: 1.0 / np.sqrt(r1 * nn))
         x = t if x is None else tt_sum_cores(x, t)
     return TensorTrain.from_cores(x)
+
+
+def grad_inputs(d=12, n=32, r=64, rb=4, nsamples=1_000_000, hidden_rank=8, noise=1e-3,
+                seed=9):
+    """Differentiation workload: x rank ``r`` with N(0, 1/(r_k n)) entries;
+    A the rank-3 operator of ``aniso`` with c_k = 1; b rank ``rb`` Gaussian;
+    ``nsamples`` uniform 0-based multi-indices (int32 ``[S, d]``) and values
+    of a hidden rank-``hidden_rank`` TT at them plus N(0, noise^2)."""
+    rng = np.random.default_rng(seed)
+    sc = lambda r1, nn, r2: 1.0 / np.sqrt(r1 * nn)  # noqa: E731
+    x = TensorTrain.from_cores(randn_cores(n, d, r, rng, scale=sc))
+    M = mass1d(n)
+    sigma = (n + 1) ** 2
+    react = [M * (sigma if k == 0 else 1.0) for k in range(d)]
+    A = TTMatrix.from_cores(kron_sum_cores([lap1d(n)] * d, react))
+    b = TensorTrain.from_cores(randn_cores(n, d, rb, rng, scale=sc))
+    idx = rng.integers(0, n, size=(nsamples, d), dtype=np.int32)
+    hidden = randn_cores(n, d, hidden_rank, rng, scale=sc)
+    v = np.ones((nsamples, 1))
+    for k in range(d):
+        core = hidden[k]
+        out = np.empty((nsamples, core.shape[2]))
+        col = idx[:, k]
+        for j in range(n):
+            m = col == j
+            out[m] = v[m] @ core[:, j, :]
+        v = out
+    y = v[:, 0] + noise * rng.standard_normal(nsamples)
+    return x, A, b, idx, y
