@@ -211,6 +211,24 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
 int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double* U, double* S,
                   double* VT);
 
+/* Batched amen_solve2: `count` independent systems A[i] x = y[i] solved
+ * concurrently on the context's device.  No single reference counterpart:
+ * each system is amen_solve2(A{i}, y{i}, tol(i), opts{i}) (solve/amen_solve2.m:1);
+ * the batch replaces a MATLAB loop over systems.  `workers` host threads
+ * (0 = 8; at most count and 64), each with its own CUDA stream, allocator
+ * and solver handle, take systems in index order, so the systems' kernels
+ * overlap on the GPU.  All handles belong to ctx; x0 / z0 (nullable arrays,
+ * NULL entries allowed) as in ttg_amen_solve; tol[i] per system; opts
+ * (nullable = defaults) is an array of `count` option sets; stats
+ * (nullable) an array of `count`.  x_out[i] receives a new handle of ctx, or
+ * NULL when system i failed; status (nullable) receives each system's code.
+ * Every system runs even when some fail; the call then returns the code of
+ * the lowest-numbered failing system with its message. */
+int ttg_amen_solve_batch(ttg_context ctx, int64_t count, const ttg_tt* A, const ttg_tt* y,
+                         const double* tol, const ttg_amen_opts* opts, const ttg_tt* x0,
+                         const ttg_tt* z0, int32_t workers, ttg_tt* x_out,
+                         ttg_amen_stats* stats, int32_t* status);
+
 /* ---- Gradients with respect to every core (FP64) ----------------------
  * No counterpart in the reference: TT-Toolbox has no derivative code.  The
  * forward maps are the reference's own, cited per entry.  x is a TT tensor

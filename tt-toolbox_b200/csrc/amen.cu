@@ -184,12 +184,12 @@ ttg_tt_s* tt_rand_device(Context* c, const std::vector<int64_t>& n, int64_t r, u
   return t;
 }
 
-ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts& o,
-                     ttg_tt_s* x0h, ttg_tt_s* z0h, ttg_amen_stats* stats) {
-  Context* c = Ah->ctx;
+ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts& o,
+                     ttg_tt_s* x0h, ttg_tt_s* z0h, ttg_amen_stats* stats, Context* out_ctx) {
+  if (!out_ctx) out_ctx = c;
   TTG_REQUIRE(Ah->is_matrix, "A must be a TT matrix");
   TTG_REQUIRE(!yh->is_matrix, "y must be a TT tensor");
-  TTG_REQUIRE(yh->ctx == c, "A and y belong to different contexts");
+  TTG_REQUIRE(yh->ctx == Ah->ctx, "A and y belong to different contexts");
   TTG_REQUIRE(Ah->d == yh->d, "A.d != y.d");
   const int64_t d = yh->d;
   TTG_REQUIRE(d >= 2, "amen_solve needs d >= 2");
@@ -614,7 +614,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
   for (double v : hx) lsum += std::log(v);
   const double nx = std::exp(lsum / double(d));
   auto* out = new ttg_tt_s();
-  out->ctx = c;
+  out->ctx = out_ctx;
   out->d = d;
   out->is_matrix = false;
   out->n = n;
@@ -622,7 +622,7 @@ ttg_tt_s* amen_solve(ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const ttg_amen_opts
   out->ps.assign(d + 1, 0);
   for (int64_t k = 0; k < d; ++k) out->ps[k + 1] = out->ps[k] + rx[k] * n[k] * rx[k + 1];
   out->numel = out->ps[d];
-  out->core = static_cast<double*>(c->alloc->get(sizeof(double) * out->numel));
+  out->core = static_cast<double*>(out_ctx->alloc->get(sizeof(double) * out->numel));
   for (int64_t k = 0; k < d; ++k)
     axpby_f64(c, out->ps[k + 1] - out->ps[k], nx, crx[k].p(), 0.0, out->core + out->ps[k]);
   TTG_CUDA(cudaEventRecord(e1, c->stream));

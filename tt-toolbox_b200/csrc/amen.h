@@ -18,8 +18,13 @@ LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, co
                              const double* sol_prev, int64_t nrestart, int64_t niters,
                              double* sol, int precision);
 
-ttg_tt_s* amen_solve(ttg_tt_s* A, ttg_tt_s* y, double tol, const ttg_amen_opts& o,
-                     ttg_tt_s* x0, ttg_tt_s* z0, ttg_amen_stats* stats);
+// Solve on context c (its stream, allocator and solver handle); the inputs
+// may belong to another context of the same device.  The result handle
+// belongs to out_ctx (nullptr: c) and its core is drawn from out_ctx's
+// allocator.
+ttg_tt_s* amen_solve(Context* c, ttg_tt_s* A, ttg_tt_s* y, double tol, const ttg_amen_opts& o,
+                     ttg_tt_s* x0, ttg_tt_s* z0, ttg_amen_stats* stats,
+                     Context* out_ctx = nullptr);
 
 // Right-orthogonal random TT of rank r (tt_rand(n,d,r,-1), core/tt_rand.m:40-62)
 // with entries from the device hash generator.

@@ -1,5 +1,7 @@
 // extern "C" entry points of the hot path (include/ttgpu.h).
+#include <atomic>
 #include <cmath>
+#include <thread>
 
 #include "amen.h"
 #include "grad.h"
@@ -78,7 +80,7 @@ int ttg_amen_solve(ttg_tt A, ttg_tt y, double tol, const ttg_amen_opts* opts, tt
   TTG_CUDA(cudaSetDevice(A->ctx->device));
   if (x0) TTG_REQUIRE(x0->ctx == A->ctx, "x0 belongs to another context");
   if (z0) TTG_REQUIRE(z0->ctx == A->ctx, "z0 belongs to another context");
-  *x_out = amen_solve(A, y, tol, o, x0, z0, stats);
+  *x_out = amen_solve(A->ctx, A, y, tol, o, x0, z0, stats);
   TTG_API_END
 }
 
@@ -226,6 +228,97 @@ int ttg_grad_sampled(ttg_tt x, int64_t nsamples, const int32_t* idx, const doubl
   grad_sampled(c, x, nsamples, idx, y, grad, v.p());
   grad_value_out(c, v.p(), value);
   sync(c);
+  TTG_API_END
+}
+
+int ttg_amen_solve_batch(ttg_context ctx, int64_t count, const ttg_tt* A, const ttg_tt* y,
+                         const double* tol, const ttg_amen_opts* opts, const ttg_tt* x0,
+                         const ttg_tt* z0, int32_t workers, ttg_tt* x_out,
+                         ttg_amen_stats* stats, int32_t* status) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && x_out, "NULL argument");
+  TTG_REQUIRE(count >= 0, "count must be >= 0");
+  if (count == 0) return TTG_OK;
+  TTG_REQUIRE(A && y && tol, "NULL argument");
+  Context* owner = &ctx->c;
+  TTG_CUDA(cudaSetDevice(owner->device));
+  for (int64_t i = 0; i < count; ++i) {
+    x_out[i] = nullptr;
+    if (status) status[i] = TTG_OK;
+    if (stats) stats[i] = ttg_amen_stats{};
+    TTG_REQUIRE(A[i] && y[i], "system %lld: NULL handle", (long long)i);
+    TTG_REQUIRE(A[i]->ctx == owner && y[i]->ctx == owner,
+                "system %lld: handles belong to another context", (long long)i);
+    if (x0 && x0[i]) TTG_REQUIRE(x0[i]->ctx == owner, "system %lld: x0 context", (long long)i);
+    if (z0 && z0[i]) TTG_REQUIRE(z0[i]->ctx == owner, "system %lld: z0 context", (long long)i);
+    TTG_REQUIRE(std::isfinite(tol[i]) && tol[i] > 0, "system %lld: tol must be > 0",
+                (long long)i);
+  }
+  int64_t nw = workers > 0 ? workers : 8;
+  nw = std::max<int64_t>(1, std::min<int64_t>({nw, count, 64}));
+  // Inputs uploaded on the owner's stream are complete before other streams
+  // read them, and no block of the owner's allocator is still in flight.
+  sync(owner);
+  std::vector<Context*> w(nw);
+  {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    while (int64_t(ctx->workers.size()) < nw) {
+      std::unique_ptr<Context> c(new Context());
+      try {
+        context_init(*c, owner->device);
+      } catch (...) {
+        context_release(*c);
+        throw;
+      }
+      ctx->workers.push_back(std::move(c));
+    }
+    const int share = std::max(4, owner->num_sms / int(nw));
+    for (int64_t k = 0; k < nw; ++k) {
+      w[k] = ctx->workers[k].get();
+      // Cooperative Krylov grids are sized from num_sms: a share of the SMs
+      // per worker lets the workers' grids be resident together.
+      w[k]->num_sms = share;
+    }
+  }
+  ttg_amen_opts dflt;
+  ttg_amen_opts_default(&dflt);
+  std::atomic<int64_t> next{0};
+  std::mutex emu;
+  int64_t first_bad = -1;
+  int first_code = TTG_OK;
+  std::string first_msg;
+  auto record = [&](int64_t i, int code, const char* msg) {
+    if (status) status[i] = code;
+    std::lock_guard<std::mutex> lock(emu);
+    if (first_bad < 0 || i < first_bad) {
+      first_bad = i;
+      first_code = code;
+      first_msg = msg;
+    }
+  };
+  auto run = [&](Context* c) {
+    cudaSetDevice(c->device);
+    for (;;) {
+      const int64_t i = next.fetch_add(1);
+      if (i >= count) break;
+      try {
+        x_out[i] = amen_solve(c, A[i], y[i], tol[i], opts ? opts[i] : dflt,
+                              x0 ? x0[i] : nullptr, z0 ? z0[i] : nullptr,
+                              stats ? &stats[i] : nullptr, owner);
+      } catch (const Error& e) {
+        record(i, e.code, e.msg.c_str());
+      } catch (const std::exception& e) {
+        record(i, TTG_ERR_INVALID, e.what());
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int64_t k = 1; k < nw; ++k) th.emplace_back(run, w[k]);
+  run(w[0]);
+  for (auto& t : th) t.join();
+  for (int64_t k = 0; k < nw; ++k) w[k]->num_sms = owner->num_sms;
+  if (first_bad >= 0)
+    fail(first_code, "system %lld: %s", (long long)first_bad, first_msg.c_str());
   TTG_API_END
 }
 

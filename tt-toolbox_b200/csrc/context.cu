@@ -1,6 +1,7 @@
 // Context, caching allocator, error reporting and TT handles of libttgpu.
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 
 #include "internal.h"
 
@@ -40,6 +41,7 @@ size_t Allocator::size_class(size_t bytes) {
 }
 
 void* Allocator::get(size_t bytes) {
+  std::lock_guard<std::mutex> lock(mu_);
   size_t cls = size_class(bytes);
   auto it = free_.find(cls);
   void* p = nullptr;
@@ -70,6 +72,7 @@ void* Allocator::get(size_t bytes) {
 }
 
 void Allocator::put(void* p) {
+  std::lock_guard<std::mutex> lock(mu_);
   auto it = live_.find(p);
   if (it == live_.end()) return;
   size_t cls = it->second;
@@ -82,6 +85,52 @@ void Allocator::put(void* p) {
 void set_last_error(const char* msg) { g_last_error = msg; }
 
 void sync(Context* c) { TTG_CUDA(cudaStreamSynchronize(c->stream)); }
+
+void context_init(Context& c, int device) {
+  c.device = device;
+  TTG_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
+  TTG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  TTG_SOLVER(cusolverDnCreate(&c.solver));
+  TTG_SOLVER(cusolverDnSetStream(c.solver, c.stream));
+  c.alloc = new Allocator(device);
+  TTG_CUDA(cudaMallocHost(&c.h_scal, 4096 * sizeof(double)));
+  TTG_CUDA(cudaMalloc(&c.d_err, 64 * sizeof(int)));
+  TTG_CUDA(cudaMemset(c.d_err, 0, 64 * sizeof(int)));
+  TTG_CUDA(cudaEventCreate(&c.ev0));
+  TTG_CUDA(cudaEventCreate(&c.ev1));
+}
+
+void context_release(Context& c) {
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  delete c.alloc;
+  c.alloc = nullptr;
+  if (c.solver) cusolverDnDestroy(c.solver);
+  if (c.h_scal) cudaFreeHost(c.h_scal);
+  if (c.d_err) cudaFree(c.d_err);
+  if (c.ev0) cudaEventDestroy(c.ev0);
+  if (c.ev1) cudaEventDestroy(c.ev1);
+  for (auto& e : c.ev_pool) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  c.ev_pool.clear();
+  if (c.stream) cudaStreamDestroy(c.stream);
+  c.solver = nullptr;
+  c.h_scal = nullptr;
+  c.d_err = nullptr;
+  c.ev0 = c.ev1 = nullptr;
+  c.stream = nullptr;
+}
+
+void ensure_smem_attr(const void* func, int device, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find({func, device});
+  if (it != done.end() && it->second >= bytes) return;
+  TTG_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done[{func, device}] = bytes;
+}
 
 void read_scalars(Context* c, const double* d, double* h, int count) {
   TTG_CUDA(cudaMemcpyAsync(c->h_scal, d, sizeof(double) * count, cudaMemcpyDeviceToHost,
@@ -111,36 +160,27 @@ int ttg_context_create(int device, ttg_context* out) {
   TTG_CUDA(cudaGetDeviceCount(&ndev));
   TTG_REQUIRE(device >= 0 && device < ndev, "device %d out of range (%d devices)", device, ndev);
   TTG_CUDA(cudaSetDevice(device));
-  auto* h = new ttg_context_s();
-  Context& c = h->c;
-  c.device = device;
-  TTG_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
-  TTG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-  TTG_SOLVER(cusolverDnCreate(&c.solver));
-  TTG_SOLVER(cusolverDnSetStream(c.solver, c.stream));
-  c.alloc = new Allocator(device);
-  TTG_CUDA(cudaMallocHost(&c.h_scal, 4096 * sizeof(double)));
-  TTG_CUDA(cudaMalloc(&c.d_err, 64 * sizeof(int)));
-  TTG_CUDA(cudaMemset(c.d_err, 0, 64 * sizeof(int)));
-  TTG_CUDA(cudaEventCreate(&c.ev0));
-  TTG_CUDA(cudaEventCreate(&c.ev1));
-  *out = h;
+  std::unique_ptr<ttg_context_s> h(new ttg_context_s());
+  try {
+    context_init(h->c, device);
+  } catch (...) {
+    context_release(h->c);
+    throw;
+  }
+  *out = h.release();
   TTG_API_END
 }
 
 int ttg_context_destroy(ttg_context ctx) {
   TTG_API_BEGIN
   if (!ctx) return TTG_OK;
-  Context& c = ctx->c;
-  cudaSetDevice(c.device);
-  cudaStreamSynchronize(c.stream);
-  delete c.alloc;
-  if (c.solver) cusolverDnDestroy(c.solver);
-  if (c.h_scal) cudaFreeHost(c.h_scal);
-  if (c.d_err) cudaFree(c.d_err);
-  if (c.ev0) cudaEventDestroy(c.ev0);
-  if (c.ev1) cudaEventDestroy(c.ev1);
-  if (c.stream) cudaStreamDestroy(c.stream);
+  cudaSetDevice(ctx->c.device);
+  {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    for (auto& w : ctx->workers) context_release(*w);
+    ctx->workers.clear();
+  }
+  context_release(ctx->c);
   delete ctx;
   TTG_API_END
 }

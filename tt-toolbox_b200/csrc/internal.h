@@ -12,6 +12,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -51,7 +53,11 @@ struct Error {
 
 // Caching device allocator: blocks are rounded up to a size class and kept
 // on per-class free lists, so a solve that reaches steady state performs no
-// cudaMalloc.  Not thread-safe (a context is single-threaded by contract).
+// cudaMalloc.  get/put are serialised by a mutex: the batched solve draws its
+// result handles from the owning context's allocator on worker threads.  A
+// block put back is reused in stream order only on the stream of the thread
+// that takes it, so blocks shared across streams are handed over only at
+// points where both streams have been synchronised.
 class Allocator {
  public:
   explicit Allocator(int device) : device_(device) {}
@@ -64,6 +70,7 @@ class Allocator {
  private:
   static size_t size_class(size_t bytes);
   int device_;
+  std::mutex mu_;
   std::map<size_t, std::vector<void*>> free_;
   std::map<void*, size_t> live_;
   size_t in_use_ = 0, cached_ = 0;
@@ -218,6 +225,13 @@ void set_last_error(const char* msg);
 // Copy a device scalar (or a few) to the host; synchronises the stream.
 void read_scalars(Context* c, const double* d, double* h, int count);
 void sync(Context* c);
+// Stream, solver handle, allocator, pinned scalars and error slots of a
+// context on `device` (the current device must be `device`).
+void context_init(Context& c, int device);
+void context_release(Context& c);
+// Raise a kernel's dynamic shared-memory limit to `bytes` on `device`, once
+// per (kernel, device); thread-safe (contexts on several host threads).
+void ensure_smem_attr(const void* func, int device, int bytes);
 
 }  // namespace ttg
 
@@ -233,4 +247,8 @@ struct ttg_tt_s {
 
 struct ttg_context_s {
   ttg::Context c;
+  // Worker contexts of the batched solve (created on first use, each with
+  // its own stream), guarded by mu.
+  std::mutex mu;
+  std::vector<std::unique_ptr<ttg::Context>> workers;
 };

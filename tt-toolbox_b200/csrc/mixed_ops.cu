@@ -290,12 +290,7 @@ void launch_bn(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t
                int64_t a_rows_pb, int64_t b_rows_pb, int64_t M, int64_t N, int64_t batch,
                const OutMap& om) {
   const size_t smem = umma_smem_bytes<BN>();
-  static bool configured = false;
-  if (!configured) {
-    TTG_CUDA(cudaFuncSetAttribute(k_umma_gemm<BN, OB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(smem)));
-    configured = true;
-  }
+  ensure_smem_attr(reinterpret_cast<const void*>(k_umma_gemm<BN, OB>), c->device, int(smem));
   dim3 grid{unsigned((M + UM_BM - 1) / UM_BM), unsigned((N + BN - 1) / BN), unsigned(batch)};
   k_umma_gemm<BN, OB><<<grid, 128, smem, c->stream>>>(ta, tb, int(K), int(a_rows_pb),
                                                       int(b_rows_pb), om, c->d_err + 1, c->skip);

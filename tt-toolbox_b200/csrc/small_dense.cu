@@ -238,12 +238,7 @@ bool small_qr_fits(int64_t m, int64_t n) {
 void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
                   double* R) {
   const size_t smem = sizeof(double) * size_t(m * n + std::min(m, n));
-  static bool attr = false;
-  if (!attr) {
-    TTG_CUDA(cudaFuncSetAttribute(k_house_qr, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(SMEM_LIMIT + 1024)));
-    attr = true;
-  }
+  ensure_smem_attr(reinterpret_cast<const void*>(k_house_qr), c->device, int(SMEM_LIMIT + 1024));
   k_house_qr<<<1, SD_THREADS, smem, c->stream>>>(int(m), int(n), A, int(lda), Q, R);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
@@ -255,12 +250,8 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
   const size_t mat = size_t(n * n) * sizeof(double);
   const int mode = 2 * mat <= SMEM_LIMIT ? 2 : (mat <= SMEM_LIMIT ? 1 : 0);
   DBuf<double> V(c, n * n), work(c, n * n + 2 * n);
-  static bool attr = false;
-  if (!attr) {
-    TTG_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(SMEM_LIMIT + 1024)));
-    attr = true;
-  }
+  ensure_smem_attr(reinterpret_cast<const void*>(k_jacobi_svd), c->device,
+                   int(SMEM_LIMIT + 1024));
   const size_t smem = size_t(mode) * mat;
   k_jacobi_svd<<<1, SD_THREADS, smem, c->stream>>>(int(n), A, int(lda), U, S, VT, V.p(),
                                                     work.p(), mode, c->d_err + 3);

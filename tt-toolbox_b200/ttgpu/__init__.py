@@ -120,6 +120,10 @@ def lib():
     sigs["ttg_dense_qr"] = [_vp, _i64, _i64, _vp, _vp, _vp]
     sigs["ttg_dense_svd"] = [_vp, _i64, _i64, _vp, _vp, _vp, _vp]
     sigs["ttg_grad_xAx"] = [_vp, _vp, _vp, _pd]
+    sigs["ttg_amen_solve_batch"] = [_vp, _i64, C.POINTER(_vp), C.POINTER(_vp), _pd,
+                                    C.POINTER(AmenOpts), C.POINTER(_vp), C.POINTER(_vp),
+                                    C.c_int32, C.POINTER(_vp), C.POINTER(AmenStats),
+                                    C.POINTER(C.c_int32)]
     sigs["ttg_grad_xb"] = [_vp, _vp, _vp, _pd]
     sigs["ttg_grad_sampled"] = [_vp, _i64, _vp, _vp, _vp, _pd]
     for name, args in sigs.items():
@@ -388,15 +392,7 @@ _AMEN_KEYS = {"nswp", "rmax", "x0", "z0", "verb", "local_prec", "local_restart",
               "tol_exit", "precision", "seed", "timing"}
 
 
-def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
-    """``[x] = amen_solve2(A, y, tol, 'name', value, ...)`` (``solve/amen_solve2.m:1``).
-
-    Options follow ``amen_solve2.m:161-203``; unknown names raise
-    ``ValueError('Unrecognized option')`` as the reference errors (``:200-201``).
-    ``A``: host ``TTMatrix`` or ``DeviceTT``; ``y``/``x0``/``z0``: host
-    ``TensorTrain`` or ``DeviceTT``.  Returns a host ``TensorTrain`` when ``y``
-    is a host tensor, else a ``DeviceTT``.
-    """
+def _check_amen_opts(opts):
     for k in opts:
         if k.lower() not in _AMEN_KEYS:
             raise ValueError("Unrecognized option: %s" % k)
@@ -408,7 +404,12 @@ def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
     lp = opts.get("local_prec", "")
     if lp not in ("", 0, None):
         raise TTGError(7, "local_prec %r is not implemented" % (lp,))
-    ctx = ctx or (A.ctx if isinstance(A, DeviceTT) else default_context())
+    return opts
+
+
+def _amen_opts(opts):
+    """``ttg_amen_opts`` from checked name/value options (defaults of
+    ``amen_solve2.m:75-107`` for the rest)."""
     o = AmenOpts()
     lib().ttg_amen_opts_default(C.byref(o))
     for k in ("nswp", "rmax", "max_full_size", "local_restart", "local_iters", "kickrank"):
@@ -425,6 +426,21 @@ def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
     if "timing" in opts:
         o.timing = 1 if opts["timing"] else 0
     o.precision = _PREC[opts.get("precision", "fp64")]
+    return o
+
+
+def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
+    """``[x] = amen_solve2(A, y, tol, 'name', value, ...)`` (``solve/amen_solve2.m:1``).
+
+    Options follow ``amen_solve2.m:161-203``; unknown names raise
+    ``ValueError('Unrecognized option')`` as the reference errors (``:200-201``).
+    ``A``: host ``TTMatrix`` or ``DeviceTT``; ``y``/``x0``/``z0``: host
+    ``TensorTrain`` or ``DeviceTT``.  Returns a host ``TensorTrain`` when ``y``
+    is a host tensor, else a ``DeviceTT``.
+    """
+    opts = _check_amen_opts(opts)
+    ctx = ctx or (A.ctx if isinstance(A, DeviceTT) else default_context())
+    o = _amen_opts(opts)
     owned = []
 
     def dev(t):
@@ -457,6 +473,78 @@ def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
     for h in owned:
         h.free()
     return host
+
+
+def amen_solve2_batch(As, ys, tol, x0s=None, z0s=None, workers=0, ctx=None, stats=None,
+                      per_system=None, **opts):
+    """Batched ``amen_solve2`` (``ttg_amen_solve_batch``): solves
+    ``As[i] x = ys[i]`` for every i, concurrently on one device.
+
+    ``tol``: scalar or one per system; ``opts``: options shared by all
+    systems; ``per_system``: optional list of option dicts merged over
+    ``opts`` for each system (e.g. its own ``rmax``).  ``x0s``/``z0s``:
+    optional lists (entries may be None).  Returns a list of host
+    ``TensorTrain`` (``DeviceTT`` when the ys are device handles).  ``stats``:
+    optional list filled with one dict per system.  Raises ``TTGError`` for
+    the first failing system after all systems ran."""
+    count = len(As)
+    if len(ys) != count:
+        raise ValueError("As and ys differ in length")
+    ctx = ctx or (As[0].ctx if count and isinstance(As[0], DeviceTT) else default_context())
+    base = _check_amen_opts(opts)
+    for k in ("x0", "z0"):
+        if k in base:
+            raise ValueError("pass initial guesses as x0s / z0s")
+    olist = (AmenOpts * max(count, 1))()
+    for i in range(count):
+        oi = dict(base)
+        if per_system is not None and per_system[i]:
+            oi.update(_check_amen_opts(per_system[i]))
+        olist[i] = _amen_opts(oi)
+    tols = np.ascontiguousarray(np.broadcast_to(np.asarray(tol, np.float64), (count,)))
+    owned = []
+
+    def dev(t):
+        if t is None or isinstance(t, DeviceTT):
+            return t
+        h = DeviceTT.upload(ctx, t)
+        owned.append(h)
+        return h
+
+    HA = (_vp * max(count, 1))()
+    HY = (_vp * max(count, 1))()
+    HX0 = (_vp * max(count, 1))()
+    HZ0 = (_vp * max(count, 1))()
+    for i in range(count):
+        HA[i] = dev(As[i]).h
+        HY[i] = dev(ys[i]).h
+        HX0[i] = dev(x0s[i]).h if x0s is not None and x0s[i] is not None else None
+        HZ0[i] = dev(z0s[i]).h if z0s is not None and z0s[i] is not None else None
+    out = (_vp * max(count, 1))()
+    st = (AmenStats * max(count, 1))()
+    status = (C.c_int32 * max(count, 1))()
+    try:
+        code = lib().ttg_amen_solve_batch(ctx.h, count, HA, HY, _ptrd(tols), olist,
+                                          HX0 if x0s is not None else None,
+                                          HZ0 if z0s is not None else None, int(workers), out,
+                                          st, status)
+        msg = lib().ttg_last_error().decode(errors="replace") if code else ""
+        res = []
+        for i in range(count):
+            h = DeviceTT(ctx, out[i]) if out[i] else None
+            if h is not None and not (count and isinstance(ys[0], DeviceTT)):
+                t = h.download()
+                h.free()
+                h = t
+            res.append(h)
+        if stats is not None:
+            stats[:] = [dict(st[i].to_dict(), status=int(status[i])) for i in range(count)]
+        if code:
+            raise TTGError(code, msg)
+        return res
+    finally:
+        for h in owned:
+            h.free()
 
 
 def _shape3(a):

@@ -172,3 +172,28 @@ def grad_inputs(d=12, n=32, r=64, rb=4, nsamples=1_000_000, hidden_rank=8, noise
         v = out
     y = v[:, 0] + noise * rng.standard_normal(nsamples)
     return x, A, b, idx, y
+
+
+def batch_systems(count=512, seed=4, d_range=(6, 14), n_choices=(8, 16, 32, 64),
+                  rmax_range=(8, 64)):
+    """Batched-solve workload: ``count`` independent Laplacian systems
+    (operator rank 2, RHS all-ones rank 1), d ~ U{d_range}, n from
+    ``n_choices``, rmax ~ U{rmax_range}, all from one seeded generator.
+    Returns (As, ys, rmaxs, shapes)."""
+    rng = np.random.default_rng(seed)
+    As, ys, rmaxs, shapes = [], [], [], []
+    cache = {}
+    for _ in range(count):
+        d = int(rng.integers(d_range[0], d_range[1] + 1))
+        n = int(rng.choice(n_choices))
+        r = int(rng.integers(rmax_range[0], rmax_range[1] + 1))
+        key = (d, n)
+        if key not in cache:
+            cache[key] = (TTMatrix.from_cores(kron_sum_cores([lap1d(n)] * d)),
+                          TensorTrain.from_cores([np.ones((1, n, 1)) for _ in range(d)]))
+        A, y = cache[key]
+        As.append(A)
+        ys.append(y)
+        rmaxs.append(r)
+        shapes.append((d, n, r))
+    return As, ys, rmaxs, shapes
