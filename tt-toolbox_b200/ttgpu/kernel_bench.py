@@ -18,6 +18,11 @@
     every core, inputs resident on the device; time and FLOP/s (parity at
     this size is checked in the GPU tests).
 
+``python -m ttgpu.kernel_bench batch --count 512 --workers 8``
+    the batched AMEn workload (uneven d, n, rmax; Laplacian systems, ones
+    right-hand sides, tol 1e-8) through ``ttg_amen_solve_batch``, against
+    the same systems solved one after another (the first ``--serial``).
+
 ``python -m ttgpu.kernel_bench dgemm``
     cuBLAS FP64 GEMM throughput (torch.matmul, 8192^3) as the measured FP64
     tensor-core reference for the FP64 kernels.
@@ -140,6 +145,46 @@ def grad_bench(args):
     ctx.close()
 
 
+def batch_bench(args):
+    from . import amen_solve2, amen_solve2_batch
+    ctx = Context(args.device)
+    As, ys, rmaxs, shapes = workloads.batch_systems(count=args.count, seed=args.seed)
+    dAs = [DeviceTT.upload(ctx, a) for a in As]
+    dys = [DeviceTT.upload(ctx, y) for y in ys]
+    per = [dict(rmax=r) for r in rmaxs]
+    out = {"workload": "batch: %d Laplacian systems, d U{6..14}, n in {8,16,32,64}, "
+                       "rmax U{8..64}, ones rhs, tol %g" % (args.count, args.tol),
+           "workers": args.workers}
+    for prec in args.precision.split(","):
+        st = []
+        ctx.sync()
+        t = time.perf_counter()
+        xs = amen_solve2_batch(dAs, dys, args.tol, workers=args.workers, ctx=ctx, stats=st,
+                               per_system=per, precision=prec)
+        ctx.sync()
+        wall = time.perf_counter() - t
+        conv = sum(1 for s in st if s["sweeps"] and s["max_res"][s["sweeps"] - 1] < args.tol)
+        fl = sum(s["matvec_gflop"] for s in st)
+        for x in xs:
+            x.free()
+        k = min(args.serial, args.count)
+        t = time.perf_counter()
+        for i in range(k):
+            amen_solve2(dAs[i], dys[i], args.tol, ctx=ctx, rmax=rmaxs[i], precision=prec).free()
+        ctx.sync()
+        ser = time.perf_counter() - t
+        bt = sum(s["ms_total"] for s in st[:k]) * 1e-3
+        out[prec] = {"batch_s": wall, "converged": conv, "matvec_gflop": fl,
+                     "matvec_tflops": fl / wall * 1e-3,
+                     "serial_first_k_s": ser, "serial_k": k,
+                     "batch_speedup_est": (ser / k * args.count) / wall,
+                     "sum_ms_first_k_in_batch": bt * 1e3}
+    print(json.dumps(out))
+    for h in dAs + dys:
+        h.free()
+    ctx.close()
+
+
 def dgemm_bench(args):
     import torch
     n = args.size
@@ -196,14 +241,21 @@ def main():
     g.add_argument("--r", type=int, default=64)
     g.add_argument("--samples", type=int, default=1_000_000)
     g.add_argument("--reps", type=int, default=5)
+    b = sub.add_parser("batch")
+    b.add_argument("--count", type=int, default=512)
+    b.add_argument("--workers", type=int, default=8)
+    b.add_argument("--serial", type=int, default=64)
+    b.add_argument("--tol", type=float, default=1e-8)
+    b.add_argument("--precision", default="fp64,mixed")
     dg = sub.add_parser("dgemm")
     dg.add_argument("--size", type=int, default=8192)
     dg.add_argument("--reps", type=int, default=10)
-    for s in (m, r, g, dg):
+    for s in (m, r, g, b, dg):
         s.add_argument("--device", type=int, default=0)
         s.add_argument("--seed", type=int, default=5)
     args = p.parse_args()
-    {"matvec": matvec, "round": round_bench, "grad": grad_bench, "dgemm": dgemm_bench}[args.what](args)
+    {"matvec": matvec, "round": round_bench, "grad": grad_bench, "batch": batch_bench,
+     "dgemm": dgemm_bench}[args.what](args)
 
 
 if __name__ == "__main__":
