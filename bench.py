@@ -58,7 +58,7 @@ class Dist:
             # cuBLAS/cuSOLVER are the ones the process uses.
             import torch.distributed as dist
             from datetime import timedelta
-            dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+            dist.init_process_group("gloo", timeout=timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
