@@ -386,6 +386,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
       prof.mark("lr_solve");
       const bool full = N < max_full_size;                                // :468
       DBuf<double> sol(c, N), tmp(c, N), B, t1(c, md.t1_size()), t2(c, md.t2_size());
+      bool have_bsol = false;  // tmp = B sol (FP64) after the local solve
       if (full) {
         B.reset(c, N * N);
         assemble_local_f64(c, rx[i], n[i], rx[i + 1], ra[i], ra[i + 1], Phi1, A1, Phi2, B.p());
@@ -418,6 +419,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
           local_residual_dev(c, md, Phi1, A1, Phi2, sol.p(), rhs.p(), tmp.p(), t1.p(), t2.p(),
                              S.p(Scalars::T1));                           // :504
           mv_fp64++;
+          have_bsol = true;
           scalar_op(c, SC_DIV, S.p(Scalars::RES_NEW), S.p(Scalars::T1), S.p(Scalars::NRHS));
         } else {
           fill_f64(c, N, 0.0, sol.p());
@@ -446,8 +448,32 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
         // Candidate ranks rr = K-1, K-2, ..., 1 (:539-550): residuals are
         // evaluated in growing batches and read back once per batch; the rank
         // is the first candidate whose residual exceeds thr, as in the loop.
-        DBuf<double> us(c, M * K), cursol(c, M * r2);
         int64_t found = -1, next = K - 1, batch = 1;
+        if (have_bsol && next >= 1) {
+          // rhs - B(U_rr S_rr V_rr^T) = (rhs - B sol) + sum_{k >= rr} s_k B(u_k v_k^T):
+          // candidates in chunks of up to 16, each chunk one rank-one image
+          // contraction and one fused running-norm pass, one read-back.
+          const int64_t C = CUMNORM_MAXC;
+          DBuf<double> R(c, N), W(c, N * std::min(C, next)),
+              scr(c, rank1_scratch_size(md, std::min(C, next))),
+              part(c, cumulative_norms_part_size(c));
+          copy_f64(c, N, rhs.p(), R.p());
+          axpby_f64(c, N, -1.0, tmp.p(), 1.0, R.p());
+          while (next >= 1 && found < 0) {
+            const int64_t nb = std::min(C, next);
+            const int64_t k0 = next - nb + 1;  // chunk covers rr = next .. k0
+            rank1_images_f64(c, md, Phi1, A1, Phi2, U.p(), M, VT.p(), K, Sv.p(), k0, nb, W.p(),
+                             scr.p());
+            cumulative_norms_f64(c, N, nb, R.p(), W.p(), part.p(), S.cand(0));
+            first_exceeding(c, nb, S.cand(0), S.p(Scalars::NRHS), S.p(Scalars::THR),
+                            S.p(Scalars::T3));
+            double hb;
+            read_scalars(c, S.p(Scalars::T3), &hb, 1);
+            if (hb >= 0.0) found = next - int64_t(hb);
+            next -= nb;
+          }
+        }
+        DBuf<double> us(c, M * K), cursol(c, M * r2);
         while (next >= 1 && found < 0) {
           const int64_t nb = std::min<int64_t>(std::min(batch, next), Scalars::NCAND);
           for (int64_t b = 0; b < nb; ++b) {

@@ -4,6 +4,8 @@
 // every contraction is a plain (batched) column-major GEMM on the DMMA engine
 // with no permutation pass in between -- the reference interleaves its three
 // GEMMs with two explicit transposes (amen_solve2.m:937-950, :857-905).
+#include <algorithm>
+
 #include "local_ops.h"
 
 namespace ttg {
@@ -115,5 +117,103 @@ void assemble_local_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t
   c->launches += 1;
   TTG_CHECK_LAUNCH();
 }
+
+// ---------------------------------------------------------------------------
+// Candidate residuals of the truncation loop (amen_solve2.m:539-551)
+// ---------------------------------------------------------------------------
+
+void rank1_images_f64(Context* c, const MvDims& d, const double* Phi1, const double* A,
+                      const double* Phi2, const double* U, int64_t ldu, const double* VT,
+                      int64_t ldvt, const double* s, int64_t k0, int64_t cnt, double* W,
+                      double* scratch) {
+  const int64_t r1 = d.rx1, n = d.n, r2 = d.rx2, a1 = d.ra1, a2 = d.ra2;
+  const int64_t N = d.out_size();
+  double* Q = scratch;                       // [(be,c), t]   a2*r2*cnt
+  double* Qs = Q + a2 * r2 * cnt;            // scaled by s_k
+  double* Z = Qs + a2 * r2 * cnt;            // [a, al, j, be, t]  r1*a1*n*a2*cnt
+  double* P = Z + r1 * a1 * n * a2 * cnt;    // [i, j, be, t]      r1*n*a2*cnt
+  // Q[(be,c), t] = sum_b Phi2[b, (be,c)] V[b, k0+t]
+  gemm_f64(c, true, true, a2 * r2, cnt, r2, 1.0, Phi2, r2, 0, VT + k0, ldvt, 0, 0.0, Q, a2 * r2,
+           0, 1);
+  copy2d_f64(c, a2 * r2, cnt, Q, a2 * r2, Qs, a2 * r2, s + k0);
+  // Z[a, (al,j), be, t] = sum_m U[(a,m), k0+t] A[al, j, m, be]
+  for (int64_t be = 0; be < a2; ++be)
+    gemm_f64(c, false, true, r1, a1 * n, n, 1.0, U + k0 * ldu, r1, ldu, A + be * a1 * n * n,
+             a1 * n, 0, 0.0, Z + be * r1 * a1 * n, r1, r1 * a1 * n * a2, cnt);
+  // P[i, (j, be, t)] = sum_{a,al} Phi1[i, (a,al)] Z[(a,al), (j, be, t)]
+  gemm_f64(c, false, false, r1, n * a2 * cnt, r1 * a1, 1.0, Phi1, r1, 0, Z, r1 * a1, 0, 0.0, P,
+           r1, 0, 1);
+  // W_t[(i,j), c] = sum_be P_t[(i,j), be] Qs_t[be, c]
+  gemm_f64(c, false, false, r1 * n, r2, a2, 1.0, P, r1 * n, r1 * n * a2, Qs, a2, a2 * r2, 0.0,
+           W, r1 * n, N, cnt);
+}
+
+int64_t rank1_scratch_size(const MvDims& d, int64_t cnt) {
+  return cnt * (2 * d.ra2 * d.rx2 + d.rx1 * d.ra1 * d.n * d.ra2 + d.rx1 * d.n * d.ra2);
+}
+
+namespace {
+
+constexpr int CN_THREADS = 256;
+
+// part[blk * MAXC + b] = sum over this block's i of (R[i] + sum_{t >= cnt-1-b} W[i + N t])^2
+__global__ void __launch_bounds__(CN_THREADS) k_cumnorm(int64_t N, int cnt,
+                                                         double* __restrict__ R,
+                                                         const double* __restrict__ W,
+                                                         double* __restrict__ part) {
+  double acc2[CUMNORM_MAXC];
+#pragma unroll
+  for (int b = 0; b < CUMNORM_MAXC; ++b) acc2[b] = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(CN_THREADS) + threadIdx.x; i < N;
+       i += int64_t(gridDim.x) * CN_THREADS) {
+    double v = R[i];
+#pragma unroll
+    for (int b = 0; b < CUMNORM_MAXC; ++b) {
+      if (b < cnt) {
+        v += W[i + N * int64_t(cnt - 1 - b)];
+        acc2[b] += v * v;
+      }
+    }
+    R[i] = v;
+  }
+  __shared__ double sh[CN_THREADS / 32][CUMNORM_MAXC];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int b = 0; b < CUMNORM_MAXC; ++b) {
+    double x = acc2[b];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[w][b] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < CUMNORM_MAXC) {
+    double x = 0.0;
+    for (int k = 0; k < CN_THREADS / 32; ++k) x += sh[k][threadIdx.x];
+    part[int64_t(blockIdx.x) * CUMNORM_MAXC + threadIdx.x] = x;
+  }
+}
+
+__global__ void k_cumnorm_final(int nblk, int cnt, const double* __restrict__ part,
+                                double* __restrict__ out) {
+  const int b = threadIdx.x;
+  if (b >= cnt) return;
+  double x = 0.0;
+  for (int k = 0; k < nblk; ++k) x += part[int64_t(k) * CUMNORM_MAXC + b];
+  out[b] = sqrt(x);
+}
+
+}  // namespace
+
+void cumulative_norms_f64(Context* c, int64_t N, int64_t cnt, double* R, const double* W,
+                          double* part, double* out) {
+  TTG_REQUIRE(cnt >= 1 && cnt <= CUMNORM_MAXC, "cumulative_norms: cnt %lld", (long long)cnt);
+  int64_t nb = (N + CN_THREADS - 1) / CN_THREADS;
+  nb = std::max<int64_t>(1, std::min<int64_t>(nb, int64_t(c->num_sms) * 4));
+  k_cumnorm<<<unsigned(nb), CN_THREADS, 0, c->stream>>>(N, int(cnt), R, W, part);
+  k_cumnorm_final<<<1, 32, 0, c->stream>>>(int(nb), int(cnt), part, out);
+  c->launches += 2;
+  TTG_CHECK_LAUNCH();
+}
+
+int64_t cumulative_norms_part_size(Context* c) { return int64_t(c->num_sms) * 4 * CUMNORM_MAXC; }
 
 }  // namespace ttg

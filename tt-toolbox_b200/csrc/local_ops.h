@@ -42,4 +42,27 @@ void assemble_local_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t
                         int64_t ra2, const double* Phi1, const double* A, const double* Phi2,
                         double* B);
 
+// Images of rank-one terms under the local operator, for the candidate
+// residuals of the truncation loop (amen_solve2.m:539-551): with the SVD
+// sol = U diag(s) V^T, W[:, t] = s_k B (u_k v_k^T), k = k0 + t, t < cnt,
+// where B = Phi1 x A x Phi2 (square local system, d.ry* = d.rx*).
+// Because B is linear, rhs - B(U_r S_r V_r^T) = (rhs - B sol) + sum_{k>=r}
+// W_k: every candidate residual follows from one contraction per rank-one
+// term, 2 rx1 n ra2 (ra1 n + rx1 ra1 + rx2) flops each, instead of one full
+// local matvec per candidate.  W: out_size() x cnt; scratch:
+// rank1_scratch_size(d, cnt) doubles.  U: M x K (ldu), VT: K x rx2 (ldvt).
+void rank1_images_f64(Context* c, const MvDims& d, const double* Phi1, const double* A,
+                      const double* Phi2, const double* U, int64_t ldu, const double* VT,
+                      int64_t ldvt, const double* s, int64_t k0, int64_t cnt, double* W,
+                      double* scratch);
+int64_t rank1_scratch_size(const MvDims& d, int64_t cnt);
+
+// Running sums of candidate residuals: for b = 0..cnt-1,
+//   R += W[:, cnt-1-b];  out[b] = ||R||      (R updated in place)
+// deterministic two-stage reduction.  part: cumulative_norms_part_size(c).
+constexpr int CUMNORM_MAXC = 16;
+void cumulative_norms_f64(Context* c, int64_t N, int64_t cnt, double* R, const double* W,
+                          double* part, double* out);
+int64_t cumulative_norms_part_size(Context* c);
+
 }  // namespace ttg
