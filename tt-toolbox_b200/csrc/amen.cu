@@ -29,10 +29,10 @@ LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const do
                                            const double* rhs, const double* dres, double nres,
                                            double nrhs, double tol, const double* sol_prev,
                                            int64_t nrestart, int64_t niters, double* sol,
-                                           int precision) {
+                                           int precision, double* bsol_out = nullptr) {
   if (precision == TTG_MIXED)
     return local_solve_mixed(c, d, Phi1, A, Phi2, rhs, dres, nres, nrhs, tol, sol_prev, nrestart,
-                             niters, sol);
+                             niters, sol, bsol_out);
   LocalSolveResult out;
   const int64_t sz = d.in_size();
   if (nrestart > sz) nrestart = sz;                                   // solve3d_2.c:184
@@ -412,13 +412,17 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
         if (norm_rhs > 0) {                                               // :497
           LocalSolveResult lr = local_solve_from_residual(
               c, md, Phi1, A1, Phi2, rhs.p(), dres.p(), nres, norm_rhs, real_tol, sol_prev,
-              o.local_restart, o.local_iters, sol.p(), o.precision);      // :501
+              o.local_restart, o.local_iters, sol.p(), o.precision, tmp.p());  // :501
           local_solves++;
           gmres_iters += lr.iters;
           mv_fp64 += lr.matvecs_fp64;
-          local_residual_dev(c, md, Phi1, A1, Phi2, sol.p(), rhs.p(), tmp.p(), t1.p(), t2.p(),
-                             S.p(Scalars::T1));                           // :504
-          mv_fp64++;
+          if (lr.have_bsol) {  // the refinement's last FP64 matvec was B sol: reuse it
+            diffnrm_f64(c, N, tmp.p(), rhs.p(), S.p(Scalars::T1), true);  // :504
+          } else {
+            local_residual_dev(c, md, Phi1, A1, Phi2, sol.p(), rhs.p(), tmp.p(), t1.p(), t2.p(),
+                               S.p(Scalars::T1));                         // :504
+            mv_fp64++;
+          }
           have_bsol = true;
           scalar_op(c, SC_DIV, S.p(Scalars::RES_NEW), S.p(Scalars::T1), S.p(Scalars::NRHS));
         } else {

@@ -12,6 +12,9 @@ struct LocalSolveResult {
   int64_t iters = 0;
   int64_t matvecs = 0;
   int64_t matvecs_fp64 = 0;
+  // The solver's last FP64 refinement matvec was B sol for the returned sol
+  // and was stored in the caller's bsol_out buffer.
+  bool have_bsol = false;
 };
 LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, const double* A,
                              const double* Phi2, const double* rhs, double tol,

@@ -360,7 +360,7 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
                                    const double* A, const double* Phi2, const double* rhs,
                                    const double* dres, double nres, double nrhs, double tol,
                                    const double* sol_prev, int64_t nrestart, int64_t niters,
-                                   double* sol) {
+                                   double* sol, double* bsol_out) {
   LocalSolveResult out;
   const int64_t sz = d.in_size();
   if (nrestart > sz) nrestart = sz;
@@ -372,7 +372,12 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
   DBuf<float> rrev(c, sz), dx(c, sz);
   copy_f64(c, sz, sol_prev, sol);
   auto residual = [&]() -> double {
-    local_matvec_f64(c, d, Phi1, A, Phi2, sol, r64.p(), t1.p(), t2.p());
+    if (bsol_out) {
+      local_matvec_f64(c, d, Phi1, A, Phi2, sol, bsol_out, t1.p(), t2.p());
+      copy_f64(c, sz, bsol_out, r64.p());
+    } else {
+      local_matvec_f64(c, d, Phi1, A, Phi2, sol, r64.p(), t1.p(), t2.p());
+    }
     out.matvecs_fp64++;
     axpby_f64(c, sz, 1.0, rhs, -1.0, r64.p());
     dot_f64(c, sz, r64.p(), nullptr, s.p(), true);
@@ -391,8 +396,10 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
     copy_f64(c, sz, sol, prev.p());
     rev_to_nat_add(c, d.rx1, d.n, d.rx2, dx.p(), sol, nr);
     const double nr_new = residual();
+    out.have_bsol = bsol_out != nullptr;
     if (!(nr_new < nr)) {  // no progress: keep the better iterate and stop
       copy_f64(c, sz, prev.p(), sol);
+      out.have_bsol = false;
       break;
     }
     const bool stagnating = nr_new > 0.5 * nr;
