@@ -211,7 +211,8 @@ def _rel_diff(X, Y):
     def gram(a, b):
         G = np.ones((1, 1))
         for ca, cb in zip(a, b):
-            G = np.einsum("ij,ink,jnl->kl", G, ca, cb)
+            t = np.tensordot(G, ca, axes=([0], [0]))          # [j, n, k]
+            G = np.tensordot(t, cb, axes=([0, 1], [0, 1]))    # [k, l]
         return G[0, 0]
     xx, yy, xy = gram(xs, xs), gram(ys, ys), gram(xs, ys)
     return float(np.sqrt(max(xx + yy - 2 * xy, 0.0) / xx))
