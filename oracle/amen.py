@@ -3,8 +3,8 @@
 TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
 
 Restates, on the default option path of ``solve/amen_solve2.m``
-(kicktype ``'als'``, trunc_norm ``'residual'``, no local preconditioner, the
-MEX local solver ``solve3d_2``):
+(kicktype ``'als'``, trunc_norm ``'residual'``, the MEX local solver
+``solve3d_2``, with or without the block-Jacobi local preconditioners):
 
 * ``bfun3``            -- ``solve/amen_solve2.m:924-951``
 * ``compute_next_Phi`` -- ``solve/amen_solve2.m:834-920``
@@ -217,13 +217,67 @@ def dgmresr_hh(mv, rhs, nrestart, tol, niters, stats=None):
     return sol
 
 
-def solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, nrestart=40, niters=2, stats=None):
+def jac_gen(Phi1, A, Phi2, prec):
+    """Block-Jacobi local preconditioners (``solve/solve3d_2ml.m:21-70``; the
+    centre variant also in ``fmex/solve3d.c:47-112``).
+
+    prec 1 ('cjacobi'): for every rank pair (i, k) the n x n diagonal block
+      ``J[:, :, i, k] = sum_{al,be} Phi1[i,i,al] A[al,:,:,be] Phi2[k,be,k]``,
+      inverted; returned as ``[n, n, rx1, rx2]``.
+    prec 2 ('ljacobi'): for every k the (rx1 n) x (rx1 n) block
+      ``sum_{al,be} Phi1[:,:,al] (x) A[al,:,:,be] Phi2[k,be,k]``, inverted:
+      ``[rx1 n, rx1 n, rx2]``.
+    prec 3 ('rjacobi'): for every i the (n rx2) x (n rx2) block
+      ``sum_{al,be} Phi1[i,i,al] A[al,:,:,be] (x) Phi2[:,be,:]``, inverted:
+      ``[n rx2, n rx2, rx1]``."""
+    rx1, ra1 = Phi1.shape[1], Phi1.shape[2]
+    n = A.shape[1]
+    rx2, ra2 = Phi2.shape[0], Phi2.shape[1]
+    d1 = np.stack([np.diag(Phi1[:, :, a]) for a in range(ra1)], axis=1)     # [rx1, ra1]
+    d2 = np.stack([np.diag(Phi2[:, b, :]) for b in range(ra2)], axis=0)     # [ra2, rx2]
+    if prec == 1:
+        J = np.einsum("ia,ajmb,bk->jmik", d1, A, d2)                      # [n, n, rx1, rx2]
+        out = np.empty_like(J)
+        for i in range(rx1):
+            for k in range(rx2):
+                out[:, :, i, k] = np.linalg.inv(J[:, :, i, k])
+        return out
+    if prec == 2:
+        J = np.einsum("ipa,ajmb,bk->ijpmk", Phi1, A, d2)                  # [rx1,n,rx1,n,rx2]
+        J = J.reshape(rx1 * n, rx1 * n, rx2, order="F")
+        return np.stack([np.linalg.inv(J[:, :, k]) for k in range(rx2)], axis=2)
+    if prec == 3:
+        J = np.einsum("ia,ajmb,qbk->jkmqi", d1, A, Phi2)                  # [n,rx2,n,rx2,rx1]
+        J = J.reshape(n * rx2, n * rx2, rx1, order="F")
+        return np.stack([np.linalg.inv(J[:, :, i]) for i in range(rx1)], axis=2)
+    raise ValueError("unknown preconditioner %r" % (prec,))
+
+
+def jac_apply(jacs, prec, x, rx1, n, rx2):
+    """``y = P x`` for the preconditioners of ``jac_gen``
+    (``solve/solve3d_2ml.m:120-146``, ``fmex/solve3d.c:115-128``)."""
+    X = rs(x, rx1, n, rx2)
+    if prec == 1:
+        Y = np.einsum("jmik,imk->ijk", jacs, X)
+    elif prec == 2:
+        Y = np.einsum("pqk,qk->pk", jacs, rs(X, rx1 * n, rx2))
+    elif prec == 3:
+        Xt = rs(np.transpose(X, (1, 2, 0)), n * rx2, rx1)
+        Yt = np.einsum("pqi,qi->pi", jacs, Xt)
+        Y = np.transpose(rs(Yt, n, rx2, rx1), (2, 0, 1))
+    else:
+        raise ValueError("unknown preconditioner %r" % (prec,))
+    return np.asfortranarray(Y).ravel(order="F")
+
+
+def solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, nrestart=40, niters=2, stats=None, prec=0):
     """MEX local solver, residual branch (``fmex/solve3d_2.c:121-300``).
 
     ``tol`` is relative to ``||rhs||``.  Computes ``dres = rhs - B sol_prev``,
     runs ``dgmresr_hh`` with tolerance ``tol/max(||dres||/||rhs||, tol)`` and
-    returns ``sol_prev + dsol`` (``:254-279``).
-    """
+    returns ``sol_prev + dsol`` (``:254-279``).  ``prec`` 1/2/3 (cjacobi,
+    ljacobi, rjacobi) right-preconditions the Krylov solve with ``jac_gen``:
+    the matvec is ``B P`` and ``dsol = P y`` (``:226-231,272-274``)."""
     rx1, n, rx2 = Phi1.shape[1], A.shape[1], Phi2.shape[0]
     sz = rx1 * n * rx2
     if nrestart > sz:                                   # :184
@@ -234,8 +288,14 @@ def solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, nrestart=40, niters=2, stats=No
     tol_prev = np.linalg.norm(dres) / np.linalg.norm(rhs)   # :263
     if tol_prev < tol:
         tol_prev = tol                                  # :264
-    mv = lambda v: bfun3(Phi1, A, Phi2, v)
+    if prec:
+        jacs = jac_gen(Phi1, A, Phi2, prec)
+        mv = lambda v: bfun3(Phi1, A, Phi2, jac_apply(jacs, prec, v, rx1, n, rx2))
+    else:
+        mv = lambda v: bfun3(Phi1, A, Phi2, v)
     dsol = dgmresr_hh(mv, dres, nrestart, tol / tol_prev, niters, stats)   # :267
+    if prec:
+        dsol = jac_apply(jacs, prec, dsol, rx1, n, rx2)                    # :272-274
     return dsol + sol_prev                              # :277-278
 
 
@@ -259,7 +319,10 @@ def assemble_local(Phi1, A1, Phi2):
 # ---------------------------------------------------------------------------
 
 DEFAULTS = dict(nswp=50, rmax=1000, max_full_size=50, local_restart=40, local_iters=2,
-                kickrank=4, resid_damp=2.0, tol_exit=None, verb=0)
+                kickrank=4, resid_damp=2.0, tol_exit=None, verb=0, local_prec="")
+
+# local_prec names -> the MEX prec code (solve/amen_solve2.m:205-207)
+LOCAL_PREC = {"": 0, "cjacobi": 1, "ljacobi": 2, "rjacobi": 3}
 
 
 def amen_solve2(A, y, tol, x0, z0=None, **opts):
@@ -282,6 +345,7 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
     kickrank, resid_damp = o["kickrank"], float(o["resid_damp"])
     tol_exit = tol if o["tol_exit"] is None else o["tol_exit"]       # :156-158
     verb = o["verb"]
+    prec = LOCAL_PREC[o["local_prec"]]                                 # :205-207
 
     if np.any(A.n != A.m):
         raise ValueError("AMEn does not know how to solve rectangular systems!")  # :216-218
@@ -392,7 +456,7 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
                 mv_count()
                 if norm_rhs > 0:                                       # :497
                     sol = solve3d_2(Phi1, A1, Phi2, rhs, real_tol, sol_prev,
-                                    local_restart, local_iters, st)    # :501
+                                    local_restart, local_iters, st, prec)  # :501
                     info["local_solves"] += 1
                     res_new = np.linalg.norm(bfun3(Phi1, A1, Phi2, sol) - rhs) / norm_rhs   # :504
                     mv_count()

@@ -199,3 +199,39 @@ def test_grad_oracle_vs_full_tensor_and_fd():
     assert v == pytest.approx(og.full_sampled(xs, idx, y), rel=1e-12)
     assert np.allclose(og.entries(xs, idx), og.full_tensor(xs)[tuple(idx.T)], rtol=1e-13)
     _fd_grad_check(lambda cs: og.full_sampled(cs, idx, y), xs, G, rng)
+
+
+@pytest.mark.parametrize("prec", [1, 2, 3])
+def test_jacobi_preconditioners_invert_their_blocks(prec):
+    """jac_gen/jac_apply (solve3d_2ml.m:21-70,120-146): P inverts the chosen
+    diagonal blocks of the dense local matrix B, and the preconditioned local
+    solve reaches the same solution as the plain one."""
+    from oracle.amen import assemble_local, jac_apply, jac_gen, solve3d_2
+    rng = np.random.default_rng(prec)
+    rx1, n, rx2, ra1, ra2 = 3, 4, 2, 2, 3
+    Phi1 = rng.standard_normal((rx1, rx1, ra1)) + 4 * np.eye(rx1)[:, :, None]
+    Phi2 = rng.standard_normal((rx2, ra2, rx2)) + 4 * np.eye(rx2)[:, None, :]
+    A = rng.standard_normal((ra1, n, n, ra2)) + 4 * np.eye(n)[None, :, :, None]
+    B = assemble_local(Phi1, A, Phi2)
+    N = rx1 * n * rx2
+    P = np.stack([jac_apply(jac_gen(Phi1, A, Phi2, prec), prec, e, rx1, n, rx2)
+                  for e in np.eye(N)], axis=1)
+    idx = np.arange(N).reshape(rx1, n, rx2, order="F")
+    if prec == 1:
+        groups = [idx[i, :, k] for i in range(rx1) for k in range(rx2)]
+    elif prec == 2:
+        groups = [idx[:, :, k].ravel(order="F") for k in range(rx2)]
+    else:
+        groups = [idx[i, :, :].ravel(order="F") for i in range(rx1)]
+    for g in groups:  # P restricted to a block is the inverse of B's block
+        np.testing.assert_allclose(P[np.ix_(g, g)] @ B[np.ix_(g, g)], np.eye(len(g)), atol=1e-10)
+    mask = np.zeros((N, N), bool)
+    for g in groups:
+        mask[np.ix_(g, g)] = True
+    assert not np.any(P[~mask])  # and zero elsewhere
+    rhs = rng.standard_normal(N)
+    x0 = np.zeros(N)
+    xs = np.linalg.solve(B, rhs)
+    for p in (0, prec):
+        x = solve3d_2(Phi1, A, Phi2, rhs, 1e-12, x0, nrestart=N, niters=2, prec=p)
+        assert np.linalg.norm(x - xs) <= 1e-9 * np.linalg.norm(xs)

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "amen.h"
+#include "jacobi.h"
 #include "linalg.h"
 #include "mixed.h"
 #include "round.h"
@@ -29,20 +30,39 @@ LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const do
                                            const double* rhs, const double* dres, double nres,
                                            double nrhs, double tol, const double* sol_prev,
                                            int64_t nrestart, int64_t niters, double* sol,
-                                           int precision, double* bsol_out = nullptr) {
-  if (precision == TTG_MIXED)
+                                           int precision, int prec = 0,
+                                           double* bsol_out = nullptr) {
+  TTG_REQUIRE(prec == 0 || prec == 1,
+              "local preconditioner %d is not implemented (only 0 and 1 = 'cjacobi')", prec);
+  if (precision == TTG_MIXED) {
+    TTG_REQUIRE(prec == 0, "the mixed-precision local solve has no local preconditioner");
     return local_solve_mixed(c, d, Phi1, A, Phi2, rhs, dres, nres, nrhs, tol, sol_prev, nrestart,
                              niters, sol, bsol_out);
+  }
   LocalSolveResult out;
   const int64_t sz = d.in_size();
   if (nrestart > sz) nrestart = sz;                                   // solve3d_2.c:184
-  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size());
+  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size()), J, pw;
+  if (prec == 1) {                                                    // solve3d_2.c:212-231
+    J.reset(c, d.rx1 * d.n * d.n * d.rx2);
+    pw.reset(c, sz);
+    jac_gen_c_f64(c, d.rx1, d.n, d.rx2, d.ra1, d.ra2, Phi1, A, Phi2, J.p());
+  }
   auto mv = [&](const double* x, double* y) {
-    local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
+    if (prec == 1) {  // right preconditioning: B P x
+      jac_apply_c_f64(c, d.rx1, d.n, d.rx2, J.p(), x, pw.p());
+      local_matvec_f64(c, d, Phi1, A, Phi2, pw.p(), y, t1.p(), t2.p());
+    } else {
+      local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
+    }
   };
   double tol_prev = nres / nrhs;                                      // :263
   if (tol_prev < tol) tol_prev = tol;                                 // :264
   GmresResult g = gmres_hh_f64(c, mv, dres, sz, nrestart, tol / tol_prev, niters, sol);  // :267
+  if (prec == 1) {                                                    // :272-274
+    jac_apply_c_f64(c, d.rx1, d.n, d.rx2, J.p(), sol, pw.p());
+    copy_f64(c, sz, pw.p(), sol);
+  }
   axpby_f64(c, sz, 1.0, sol_prev, 1.0, sol);                          // :277-278
   out.iters = g.iters;
   out.matvecs_fp64 += g.matvecs;
@@ -52,7 +72,7 @@ LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const do
 LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, const double* A,
                              const double* Phi2, const double* rhs, double tol,
                              const double* sol_prev, int64_t nrestart, int64_t niters,
-                             double* sol, int precision) {
+                             double* sol, int precision, int prec) {
   const int64_t sz = d.in_size();
   DBuf<double> dres(c, sz), s2(c, 2);
   local_matvec_f64(c, d, Phi1, A, Phi2, sol_prev, dres.p());          // solve3d_2.c:257
@@ -62,7 +82,8 @@ LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, co
   double h[2];
   read_scalars(c, s2.p(), h, 2);
   LocalSolveResult r = local_solve_from_residual(c, d, Phi1, A, Phi2, rhs, dres.p(), h[0], h[1],
-                                                 tol, sol_prev, nrestart, niters, sol, precision);
+                                                 tol, sol_prev, nrestart, niters, sol, precision,
+                                                 prec);
   r.matvecs_fp64 += 1;
   return r;
 }
@@ -201,7 +222,10 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   TTG_REQUIRE(Ah->r[0] == 1 && Ah->r[d] == 1 && yh->r[0] == 1 && yh->r[d] == 1,
               "border ranks must be 1");
   TTG_REQUIRE(o.trunc_norm == 1, "only trunc_norm 'residual' is implemented");
-  TTG_REQUIRE(o.local_prec == 0, "local preconditioners are not implemented");
+  TTG_REQUIRE(o.local_prec == 0 || o.local_prec == 1,
+              "local_prec %d is not implemented (0 = none, 1 = 'cjacobi')", o.local_prec);
+  TTG_REQUIRE(o.local_prec == 0 || o.precision == TTG_FP64,
+              "local_prec 'cjacobi' runs with precision TTG_FP64 only");
   TTG_REQUIRE(o.precision == TTG_FP64 || o.precision == TTG_MIXED, "unknown precision %d",
               o.precision);
   TTG_REQUIRE(o.nswp >= 1 && o.local_restart >= 1 && o.local_iters >= 1 && o.rmax >= 1 &&
@@ -412,7 +436,8 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
         if (norm_rhs > 0) {                                               // :497
           LocalSolveResult lr = local_solve_from_residual(
               c, md, Phi1, A1, Phi2, rhs.p(), dres.p(), nres, norm_rhs, real_tol, sol_prev,
-              o.local_restart, o.local_iters, sol.p(), o.precision, tmp.p());  // :501
+              o.local_restart, o.local_iters, sol.p(), o.precision, o.local_prec,
+              tmp.p());                                                   // :501
           local_solves++;
           gmres_iters += lr.iters;
           mv_fp64 += lr.matvecs_fp64;

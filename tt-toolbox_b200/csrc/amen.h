@@ -19,7 +19,7 @@ struct LocalSolveResult {
 LocalSolveResult local_solve(Context* c, const MvDims& d, const double* Phi1, const double* A,
                              const double* Phi2, const double* rhs, double tol,
                              const double* sol_prev, int64_t nrestart, int64_t niters,
-                             double* sol, int precision);
+                             double* sol, int precision, int prec = 0);
 
 // Solve on context c (its stream, allocator and solver handle); the inputs
 // may belong to another context of the same device.  The result handle

@@ -179,7 +179,8 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_
   TTG_REQUIRE(ctx && Phi1 && A && Phi2 && rhs && sol_prev && sol_out, "NULL argument");
   TTG_REQUIRE(rx1 >= 1 && n >= 1 && rx2 >= 1 && ra1 >= 1 && ra2 >= 1, "sizes must be >= 1");
   TTG_REQUIRE(trunc_norm == 1, "only the residual branch (trunc_norm = 1) is implemented");
-  TTG_REQUIRE(prec == 0, "local preconditioners are not implemented");
+  TTG_REQUIRE(prec == 0 || prec == 1,
+              "prec %d is not implemented (0 = none, 1 = 'cjacobi')", int(prec));
   TTG_REQUIRE(nrestart >= 1 && niters >= 1, "nrestart and niters must be >= 1");
   TTG_REQUIRE(std::isfinite(tol) && tol > 0, "tol must be > 0");
   Context* c = &ctx->c;
@@ -187,12 +188,14 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_
   MvDims d{rx1, rx1, ra1, n, n, rx2, ra2, rx2};
   TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 8 * sizeof(int), c->stream));
   LocalSolveResult r =
-      local_solve(c, d, Phi1, A, Phi2, rhs, tol, sol_prev, nrestart, niters, sol_out, precision);
+      local_solve(c, d, Phi1, A, Phi2, rhs, tol, sol_prev, nrestart, niters, sol_out, precision,
+                  prec);
   int herr[8];
   TTG_CUDA(cudaMemcpyAsync(herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost, c->stream));
   sync(c);
   if (herr[0] || herr[1] || herr[2])
     fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out in the local solve");
+  if (herr[4]) fail(TTG_ERR_SOLVER, "a singular preconditioner block or factorization");
   if (iters_out) *iters_out = r.iters;
   TTG_API_END
 }

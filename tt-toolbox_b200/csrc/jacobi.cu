@@ -1,0 +1,190 @@
+// Centre block-Jacobi local preconditioner ('cjacobi', MEX prec = 1).
+//
+// Restates solve/solve3d_2ml.m:50-67 (generation) and :138-146 (application),
+// the MATLAB twin of the MEX path's djac_gen/djac_apply (fmex/solve3d_2.c:
+// 212-231,272-274; readable C in fmex/solve3d.c:47-128): for every rank
+// pair (i, k) the n x n diagonal block of the local matrix
+//   J_ik = sum_{al,be} Phi1[i,i,al] A[al,:,:,be] Phi2[k,be,k]
+// is inverted, and P x applies the inverses block by block.
+//
+// Generation: two small GEMMs (diagonal of Phi1 against A, then against the
+// diagonal of Phi2) give all blocks at once; one CTA per block inverts it by
+// Gauss-Jordan elimination with partial (row) pivoting in shared memory --
+// the pivot is the first entry of largest magnitude, LAPACK's choice, and
+// the row interchanges are undone as column interchanges at the end.
+// Application is HBM-bound: every inverse entry is read once per apply.
+#include "jacobi.h"
+
+#include <cmath>
+
+namespace ttg {
+
+namespace {
+
+constexpr int GJ_THREADS = 256;
+
+__global__ void k_diag_phi1(int64_t rx1, int64_t ra1, const double* __restrict__ Phi1,
+                            double* __restrict__ d1) {
+  const int64_t total = rx1 * ra1;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e % rx1, a = e / rx1;
+    d1[e] = Phi1[i + rx1 * i + rx1 * rx1 * a];  // d1[i, a] = Phi1[i, i, a]
+  }
+}
+
+__global__ void k_diag_phi2(int64_t rx2, int64_t ra2, const double* __restrict__ Phi2,
+                            double* __restrict__ d2) {
+  const int64_t total = ra2 * rx2;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = e % ra2, k = e / ra2;
+    d2[e] = Phi2[k + rx2 * b + rx2 * ra2 * k];  // d2[b, k] = Phi2[k, b, k]
+  }
+}
+
+// One CTA per block (i, k), blockIdx.x = i + rx1 k; the block's entry (j, m)
+// lives at J[i + rx1 (j + n m) + rx1 n n k].  In place.
+__global__ void __launch_bounds__(GJ_THREADS) k_block_inv(int64_t rx1, int n,
+                                                          double* __restrict__ J,
+                                                          int* __restrict__ err) {
+  extern __shared__ double a[];  // n x n, a[r + n c]
+  __shared__ double f[JAC_MAX_N], g[JAC_MAX_N];
+  __shared__ int piv[JAC_MAX_N];
+  __shared__ int s_q;
+  __shared__ double s_max;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t b = blockIdx.x;
+  const int64_t i = b % rx1, k = b / rx1;
+  double* blk = J + i + rx1 * int64_t(n) * n * k;
+  for (int e = tid; e < n * n; e += GJ_THREADS) a[e] = blk[rx1 * int64_t(e)];
+  __syncthreads();
+  bool singular = false;
+  for (int p = 0; p < n; ++p) {
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = p;
+      for (int r = p + lane; r < n; r += 32) {
+        const double v = fabs(a[r + n * p]);
+        if (v > best) {
+          best = v;
+          bi = r;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        s_q = bi;
+        s_max = best;
+        piv[p] = bi;
+      }
+    }
+    __syncthreads();
+    if (!(s_max > 0.0)) {  // exactly singular (or NaN) block
+      singular = true;
+      break;
+    }
+    const int q = s_q;
+    if (q != p)
+      for (int col = tid; col < n; col += GJ_THREADS) {
+        const double t = a[p + n * col];
+        a[p + n * col] = a[q + n * col];
+        a[q + n * col] = t;
+      }
+    __syncthreads();
+    const double pinv = 1.0 / a[p + n * p];
+    for (int t = tid; t < n; t += GJ_THREADS) {
+      g[t] = (t == p ? 1.0 : a[p + n * t]) * pinv;  // scaled pivot row
+      f[t] = (t == p ? 0.0 : a[t + n * p]);         // multipliers of the other rows
+    }
+    __syncthreads();
+    for (int e = tid; e < n * n; e += GJ_THREADS) {
+      const int r = e % n, col = e / n;
+      if (r == p)
+        a[e] = g[col];
+      else
+        a[e] = (col == p ? 0.0 : a[e]) - f[r] * g[col];
+    }
+    __syncthreads();
+  }
+  if (singular) {
+    if (tid == 0) atomicOr(err, 1);
+    for (int e = tid; e < n * n; e += GJ_THREADS) blk[rx1 * int64_t(e)] = nan("");
+    return;
+  }
+  // inv(A) = inv(P A) P: undo the row interchanges as column interchanges
+  for (int p = n - 1; p >= 0; --p) {
+    const int q = piv[p];
+    if (q != p)
+      for (int r = tid; r < n; r += GJ_THREADS) {
+        const double t = a[r + n * p];
+        a[r + n * p] = a[r + n * q];
+        a[r + n * q] = t;
+      }
+    __syncthreads();
+  }
+  for (int e = tid; e < n * n; e += GJ_THREADS) blk[rx1 * int64_t(e)] = a[e];
+}
+
+// y[i, j, k] = sum_m J[i, j, m, k] x[i, m, k]; threads over (i, j, k), i fastest.
+__global__ void k_jac_apply_c(int64_t rx1, int64_t n, int64_t rx2, const double* __restrict__ J,
+                              const double* __restrict__ x, double* __restrict__ y) {
+  const int64_t total = rx1 * n * rx2;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e % rx1, j = (e / rx1) % n, k = e / (rx1 * n);
+    const double* Jr = J + i + rx1 * j + rx1 * n * n * k;
+    const double* xr = x + i + rx1 * n * k;
+    double s = 0.0;
+    for (int64_t m = 0; m < n; ++m) s += Jr[rx1 * n * m] * xr[rx1 * m];
+    y[e] = s;
+  }
+}
+
+int blocks_for(Context* c, int64_t n) {
+  int64_t b = (n + 255) / 256;
+  const int64_t cap = int64_t(c->num_sms) * 8;
+  if (b > cap) b = cap;
+  return int(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+void jac_gen_c_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1, int64_t ra2,
+                   const double* Phi1, const double* A, const double* Phi2, double* J) {
+  TTG_REQUIRE(n >= 1 && n <= JAC_MAX_N, "cjacobi: mode size %lld above %lld", (long long)n,
+              (long long)JAC_MAX_N);
+  TTG_REQUIRE(rx1 * rx2 <= int64_t(0x7fffffff), "cjacobi: too many blocks");
+  DBuf<double> d1(c, rx1 * ra1), d2(c, ra2 * rx2), G(c, rx1 * n * n * ra2);
+  k_diag_phi1<<<blocks_for(c, rx1 * ra1), 256, 0, c->stream>>>(rx1, ra1, Phi1, d1.p());
+  k_diag_phi2<<<blocks_for(c, ra2 * rx2), 256, 0, c->stream>>>(rx2, ra2, Phi2, d2.p());
+  c->launches += 2;
+  TTG_CHECK_LAUNCH();
+  // G[i, (j, m, be)] = sum_al d1[i, al] A[al, (j, m, be)]
+  gemm_f64(c, false, false, rx1, n * n * ra2, ra1, 1.0, d1.p(), rx1, 0, A, ra1, 0, 0.0, G.p(),
+           rx1, 0, 1);
+  // J[(i, j, m), k] = sum_be G[(i, j, m), be] d2[be, k]
+  gemm_f64(c, false, false, rx1 * n * n, rx2, ra2, 1.0, G.p(), rx1 * n * n, 0, d2.p(), ra2, 0,
+           0.0, J, rx1 * n * n, 0, 1);
+  const size_t smem = sizeof(double) * size_t(n) * size_t(n);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_block_inv), c->device, int(smem));
+  k_block_inv<<<unsigned(rx1 * rx2), GJ_THREADS, smem, c->stream>>>(rx1, int(n), J, c->d_err + 4);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void jac_apply_c_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, const double* J,
+                     const double* x, double* y) {
+  k_jac_apply_c<<<blocks_for(c, rx1 * n * rx2), 256, 0, c->stream>>>(rx1, n, rx2, J, x, y);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+}  // namespace ttg

@@ -387,6 +387,10 @@ def round(tt, eps, rmax=None, precision="fp64", ctx=None, stats=None):
     return host
 
 
+# local_prec names -> MEX prec codes (solve/amen_solve2.m:205-207); 'ljacobi'
+# and 'rjacobi' are not implemented on the device.
+_LOCAL_PREC = {"": 0, None: 0, 0: 0, "cjacobi": 1, 1: 1}
+
 _AMEN_KEYS = {"nswp", "rmax", "x0", "z0", "verb", "local_prec", "local_restart", "local_iters",
               "kickrank", "kicktype", "ismex", "max_full_size", "resid_damp", "trunc_norm",
               "tol_exit", "precision", "seed", "timing"}
@@ -402,8 +406,8 @@ def _check_amen_opts(opts):
     if opts.get("trunc_norm", "residual") not in ("residual", "resid", 1):
         raise TTGError(7, "trunc_norm %r is not implemented (only 'residual')" % opts["trunc_norm"])
     lp = opts.get("local_prec", "")
-    if lp not in ("", 0, None):
-        raise TTGError(7, "local_prec %r is not implemented" % (lp,))
+    if lp not in _LOCAL_PREC:
+        raise TTGError(7, "local_prec %r is not implemented ('' or 'cjacobi')" % (lp,))
     return opts
 
 
@@ -425,6 +429,7 @@ def _amen_opts(opts):
         o.seed = int(opts["seed"])
     if "timing" in opts:
         o.timing = 1 if opts["timing"] else 0
+    o.local_prec = _LOCAL_PREC[opts.get("local_prec", "")]
     o.precision = _PREC[opts.get("precision", "fp64")]
     return o
 
