@@ -119,7 +119,8 @@ def test_local_solve_rejects_bad_shapes(ctx):
 
 @pytest.mark.parametrize("cfg", [dict(d=6, n=4, r=3, terms=3, seed=7, eps=1e-12),
                                  dict(d=8, n=6, r=8, terms=2, seed=9, eps=1e-10),
-                                 dict(d=5, n=16, r=24, terms=4, seed=4, eps=1e-8)])
+                                 dict(d=5, n=16, r=24, terms=4, seed=4, eps=1e-8),
+                                 dict(d=4, n=64, r=24, terms=3, seed=6, eps=1e-9)])
 def test_round_parity(ctx, cfg):
     x = round_config(d=cfg["d"], n=cfg["n"], r=cfg["r"], terms=cfg["terms"], seed=cfg["seed"])
     ref, info = tt_round(x, cfg["eps"])

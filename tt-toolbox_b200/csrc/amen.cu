@@ -591,18 +591,45 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
           axpby_f64(c, M * rz[i + 1], -1.0, leftresid.p(), 1.0, uk.p());   // :707
           // [u, rv] = qr([u, uk]) ; v = [v, 0] * rv.'  (:713-716)
           const int64_t radd = rz[i + 1], wcols = r + radd;
-          DBuf<double> uu(c, M * wcols);
-          copy_f64(c, M * r, u.p(), uu.p());
-          copy_f64(c, M * radd, uk.p(), uu.p() + M * r);
           const int64_t kq = std::min(M, wcols);
-          DBuf<double> Q(c, M * kq), rv(c, kq * wcols);
-          qr_f64(c, M, wcols, uu.p(), Q.p(), rv.p());
-          // v_new (r2 x kq) = v (r2 x r) * rv(:, 1:r)^T  (the zero block drops out)
-          DBuf<double> vn(c, r2 * kq);
-          gemm_f64(c, false, true, r2, kq, r, 1.0, v.p(), r2, 0, rv.p(), kq, 0, 0.0, vn.p(), r2, 0,
-                   1);
-          u = std::move(Q);
-          v = std::move(vn);
+          if (M >= wcols) {
+            // u has orthonormal columns (left singular vectors), so a QR of
+            // [u, uk] is [u, Q2] with Q2 an orthonormal basis of uk's part
+            // orthogonal to u, and rv = [I, u'uk; 0, R2]: then v*rv(:,1:r)' =
+            // [v, 0].  This is the reference's factorization up to the column
+            // signs LAPACK would choose (a gauge of the TT representation).
+            // Two projection passes, QR, and a third projection + QR that
+            // keeps Q2 orthogonal to u even when uk lies (nearly) in span(u).
+            DBuf<double> w(c, M * radd), C(c, r * radd), Q2(c, M * radd), R2(c, radd * radd);
+            copy_f64(c, M * radd, uk.p(), w.p());
+            for (int pass = 0; pass < 3; ++pass) {
+              if (pass == 2) copy_f64(c, M * radd, Q2.p(), w.p());
+              gemm_f64(c, true, false, r, radd, M, 1.0, u.p(), M, 0, w.p(), M, 0, 0.0, C.p(), r,
+                       0, 1);
+              gemm_f64(c, false, false, M, radd, r, -1.0, u.p(), M, 0, C.p(), r, 0, 1.0, w.p(), M,
+                       0, 1);
+              if (pass >= 1) qr_f64(c, M, radd, w.p(), Q2.p(), R2.p());
+            }
+            DBuf<double> Q(c, M * kq), vn(c, r2 * kq);
+            copy_f64(c, M * r, u.p(), Q.p());
+            copy_f64(c, M * radd, Q2.p(), Q.p() + M * r);
+            fill_f64(c, r2 * kq, 0.0, vn.p());
+            copy_f64(c, r2 * r, v.p(), vn.p());
+            u = std::move(Q);
+            v = std::move(vn);
+          } else {
+            DBuf<double> uu(c, M * wcols);
+            copy_f64(c, M * r, u.p(), uu.p());
+            copy_f64(c, M * radd, uk.p(), uu.p() + M * r);
+            DBuf<double> Q(c, M * kq), rv(c, kq * wcols);
+            qr_f64(c, M, wcols, uu.p(), Q.p(), rv.p());
+            // v_new (r2 x kq) = v (r2 x r) * rv(:, 1:r)^T  (the zero block drops out)
+            DBuf<double> vn(c, r2 * kq);
+            gemm_f64(c, false, true, r2, kq, r, 1.0, v.p(), r2, 0, rv.p(), kq, 0, 0.0, vn.p(), r2,
+                     0, 1);
+            u = std::move(Q);
+            v = std::move(vn);
+          }
           r = kq;
         }
         // v = v.' * x_{i+1}  (:732-734)

@@ -23,6 +23,10 @@
     right-hand sides, tol 1e-8) through ``ttg_amen_solve_batch``, against
     the same systems solved one after another (the first ``--serial``).
 
+``python -m ttgpu.kernel_bench amen --precision fp64,mixed``
+    one solve of the anisotropic d=10, n=64 workload per precision (set
+    TTG_PROFILE=1 for the per-phase breakdown on stderr).
+
 ``python -m ttgpu.kernel_bench dgemm``
     cuBLAS FP64 GEMM throughput (torch.matmul, 8192^3) as the measured FP64
     tensor-core reference for the FP64 kernels.
@@ -185,6 +189,28 @@ def batch_bench(args):
     ctx.close()
 
 
+def amen_bench(args):
+    from . import amen_solve2
+    ctx = Context(args.device)
+    A, y, x0, z0 = workloads.aniso(d=args.d, n=args.n, seed=3)
+    dA, dy = DeviceTT.upload(ctx, A), DeviceTT.upload(ctx, y)
+    dx0, dz0 = DeviceTT.upload(ctx, x0), DeviceTT.upload(ctx, z0)
+    out = {"workload": "amen_solve2 aniso d=%d n=%d rmax %d tol %g" % (args.d, args.n, args.rmax,
+                                                                     args.tol)}
+    for prec in args.precision.split(","):
+        for rep in range(args.reps):
+            st = {}
+            x = amen_solve2(dA, dy, args.tol, x0=dx0, z0=dz0, ctx=ctx, stats=st, rmax=args.rmax,
+                            nswp=50, precision=prec)
+            x.free()
+        out[prec] = {k: st[k] for k in ("ms_total", "sweeps", "matvecs", "matvecs_fp64",
+                                        "gmres_iters", "launches", "max_rank")}
+    print(json.dumps(out))
+    for h in (dA, dy, dx0, dz0):
+        h.free()
+    ctx.close()
+
+
 def dgemm_bench(args):
     import torch
     n = args.size
@@ -248,15 +274,22 @@ def main():
     b.add_argument("--serial", type=int, default=64)
     b.add_argument("--tol", type=float, default=1e-8)
     b.add_argument("--precision", default="fp64,mixed")
+    am = sub.add_parser("amen")
+    am.add_argument("--d", type=int, default=10)
+    am.add_argument("--n", type=int, default=64)
+    am.add_argument("--rmax", type=int, default=128)
+    am.add_argument("--tol", type=float, default=1e-8)
+    am.add_argument("--reps", type=int, default=2)
+    am.add_argument("--precision", default="fp64,mixed")
     dg = sub.add_parser("dgemm")
     dg.add_argument("--size", type=int, default=8192)
     dg.add_argument("--reps", type=int, default=10)
-    for s in (m, r, g, b, dg):
+    for s in (m, r, g, b, am, dg):
         s.add_argument("--device", type=int, default=0)
         s.add_argument("--seed", type=int, default=5)
     args = p.parse_args()
     {"matvec": matvec, "round": round_bench, "grad": grad_bench, "batch": batch_bench,
-     "dgemm": dgemm_bench}[args.what](args)
+     "amen": amen_bench, "dgemm": dgemm_bench}[args.what](args)
 
 
 if __name__ == "__main__":
