@@ -117,7 +117,9 @@ struct Context {
   Allocator* alloc = nullptr;
   // Small pinned host buffer for scalar read-back.
   double* h_scal = nullptr;
-  int* d_err = nullptr;  // device error flag (bounded waits)
+  // Device int slots: 0-7 error flags of bounded waits and factorizations
+  // (cleared per solve), 63 the arrival counter of the one-launch reductions.
+  int* d_err = nullptr;
   // Counters (reset by the caller through ttg_stats).
   int64_t launches = 0;
   int64_t matvecs = 0;

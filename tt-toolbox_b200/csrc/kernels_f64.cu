@@ -170,11 +170,15 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;  // valid in thread 0
 }
 
-// mode 0: sum x*y ; mode 1: sum x^2 ; mode 2: sum (x-y)^2
-__global__ void k_reduce_partial(int64_t n, const double* __restrict__ x,
-                                 const double* __restrict__ y, int mode,
-                                 double* __restrict__ part) {
+// mode 0: sum x*y ; mode 1: sum x^2 ; mode 2: sum (x-y)^2.
+// Per-block partial sums; the last block to finish adds the partials in
+// block order (deterministic) and writes the result: one launch.  `counter` is a
+// device int that is zero between reductions (reset by the last block).
+__global__ void k_reduce_fused(int64_t n, const double* __restrict__ x,
+                               const double* __restrict__ y, int mode, double* __restrict__ part,
+                               unsigned* counter, double* out, int do_sqrt) {
   __shared__ double sh[32];
+  __shared__ bool last;
   double s = 0.0;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
@@ -189,16 +193,22 @@ __global__ void k_reduce_partial(int64_t n, const double* __restrict__ x,
     }
   }
   s = block_sum(s, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = s;
-}
-
-__global__ void k_reduce_final(int nparts, const double* __restrict__ part, double* out,
-                               int do_sqrt) {
-  __shared__ double sh[32];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[i];
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) *out = do_sqrt ? sqrt(s) : s;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s;
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int i = threadIdx.x; i < int(gridDim.x); i += blockDim.x)
+    t += reinterpret_cast<volatile const double*>(part)[i];
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) {
+    *out = do_sqrt ? sqrt(t) : t;
+    *counter = 0u;
+  }
 }
 
 void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int mode,
@@ -206,9 +216,10 @@ void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int 
   int nb = int(std::min<int64_t>((n + RED_THREADS * 4 - 1) / (RED_THREADS * 4), RED_MAX_BLOCKS));
   if (nb < 1) nb = 1;
   DBuf<double> part(c, nb);
-  k_reduce_partial<<<nb, RED_THREADS, 0, c->stream>>>(n, x, y, mode, part.p());
-  k_reduce_final<<<1, RED_THREADS, 0, c->stream>>>(nb, part.p(), out, do_sqrt ? 1 : 0);
-  c->launches += 2;
+  k_reduce_fused<<<nb, RED_THREADS, 0, c->stream>>>(n, x, y, mode, part.p(),
+                                                    reinterpret_cast<unsigned*>(c->d_err + 63),
+                                                    out, do_sqrt ? 1 : 0);
+  c->launches += 1;
   TTG_CHECK_LAUNCH();
 }
 

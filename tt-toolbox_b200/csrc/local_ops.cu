@@ -192,13 +192,16 @@ __global__ void __launch_bounds__(CN_THREADS) k_cumnorm(int64_t N, int cnt,
   }
 }
 
+// One warp per candidate: lanes stride over the block partials, then a fixed
+// shuffle tree (deterministic).
 __global__ void k_cumnorm_final(int nblk, int cnt, const double* __restrict__ part,
                                 double* __restrict__ out) {
-  const int b = threadIdx.x;
+  const int b = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (b >= cnt) return;
   double x = 0.0;
-  for (int k = 0; k < nblk; ++k) x += part[int64_t(k) * CUMNORM_MAXC + b];
-  out[b] = sqrt(x);
+  for (int k = lane; k < nblk; k += 32) x += part[int64_t(k) * CUMNORM_MAXC + b];
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  if (lane == 0) out[b] = sqrt(x);
 }
 
 }  // namespace
@@ -209,7 +212,7 @@ void cumulative_norms_f64(Context* c, int64_t N, int64_t cnt, double* R, const d
   int64_t nb = (N + CN_THREADS - 1) / CN_THREADS;
   nb = std::max<int64_t>(1, std::min<int64_t>(nb, int64_t(c->num_sms) * 4));
   k_cumnorm<<<unsigned(nb), CN_THREADS, 0, c->stream>>>(N, int(cnt), R, W, part);
-  k_cumnorm_final<<<1, 32, 0, c->stream>>>(int(nb), int(cnt), part, out);
+  k_cumnorm_final<<<1, 32 * CUMNORM_MAXC, 0, c->stream>>>(int(nb), int(cnt), part, out);
   c->launches += 2;
   TTG_CHECK_LAUNCH();
 }

@@ -313,7 +313,18 @@ void umma_gemm(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t
   }
 }
 
-int pick_bn(int64_t N) { return N <= 64 ? 64 : (N <= 128 ? 128 : 256); }
+// Tile width: the narrowest that keeps the grid within a few waves.  The
+// local matvec's GEMMs are small (tens of CTAs at the widest tile), so
+// narrower tiles mean more CTAs in flight, a shorter per-CTA epilogue and
+// less shared memory per CTA (several CTAs per SM).
+int pick_bn(Context* c, int64_t M, int64_t N, int64_t batch) {
+  const int64_t mt = (M + UM_BM - 1) / UM_BM;
+  for (int bn : {64, 128}) {
+    if (N <= bn) return bn;
+    if (mt * ((N + bn - 1) / bn) * batch <= 4 * int64_t(c->num_sms)) return bn;
+  }
+  return 256;
+}
 
 int64_t up8(int64_t v) { return (v + 7) / 8 * 8; }
 
@@ -340,9 +351,9 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
                                                                  phi1T.p());
   c->launches += 3;
   TTG_CHECK_LAUNCH();
-  bn1 = pick_bn(d.ra2 * d.ry2);
-  bn2 = pick_bn(d.ra1 * d.n);
-  bn3 = pick_bn(d.ry1);
+  bn1 = pick_bn(c, d.m * d.rx1, d.ra2 * d.ry2, 1);
+  bn2 = pick_bn(c, d.rx1, d.ra1 * d.n, d.ry2);
+  bn3 = pick_bn(c, d.ry2 * d.n, d.ry1, 1);
   make_map(&mapX, X.p(), d.rx2, d.m * d.rx1, ldx, UM_BM);
   make_map(&mapP2, phi2b.p(), d.rx2, d.ra2 * d.ry2, ldx, bn1);
   make_map(&mapT1, T1.p(), d.n * d.ra2, d.rx1 * d.ry2, ld1, UM_BM);
