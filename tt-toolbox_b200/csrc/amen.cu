@@ -598,17 +598,34 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
             // orthogonal to u, and rv = [I, u'uk; 0, R2]: then v*rv(:,1:r)' =
             // [v, 0].  This is the reference's factorization up to the column
             // signs LAPACK would choose (a gauge of the TT representation).
-            // Two projection passes, QR, and a third projection + QR that
-            // keeps Q2 orthogonal to u even when uk lies (nearly) in span(u).
-            DBuf<double> w(c, M * radd), C(c, r * radd), Q2(c, M * radd), R2(c, radd * radd);
+            // Two projection passes, then a QR of the M x radd block.  When a
+            // column of uk lies (numerically) in span(u), the QR of the
+            // projected block is not reliably orthogonal to u: a third
+            // projection and QR run, gated on the device by the columns' loss
+            // of norm (no host round trip).
+            DBuf<double> w(c, M * radd), C(c, r * radd), Q2(c, M * radd), R2(c, radd * radd),
+                G(c, 2 * radd * radd);
+            DBuf<int> keep(c, 1);
             copy_f64(c, M * radd, uk.p(), w.p());
-            for (int pass = 0; pass < 3; ++pass) {
-              if (pass == 2) copy_f64(c, M * radd, Q2.p(), w.p());
+            gemm_f64(c, true, false, radd, radd, M, 1.0, w.p(), M, 0, w.p(), M, 0, 0.0, G.p(),
+                     radd, 0, 1);
+            auto project = [&]() {
               gemm_f64(c, true, false, r, radd, M, 1.0, u.p(), M, 0, w.p(), M, 0, 0.0, C.p(), r,
                        0, 1);
               gemm_f64(c, false, false, M, radd, r, -1.0, u.p(), M, 0, C.p(), r, 0, 1.0, w.p(), M,
                        0, 1);
-              if (pass >= 1) qr_f64(c, M, radd, w.p(), Q2.p(), R2.p());
+            };
+            project();
+            project();
+            gemm_f64(c, true, false, radd, radd, M, 1.0, w.p(), M, 0, w.p(), M, 0, 0.0,
+                     G.p() + radd * radd, radd, 0, 1);
+            collapse_flag(c, radd, G.p(), radd, G.p() + radd * radd, radd, 1e-8, keep.p());
+            qr_f64(c, M, radd, w.p(), Q2.p(), R2.p());
+            {
+              SkipGuard guard(c, keep.p());  // runs only when a column collapsed
+              copy_f64(c, M * radd, Q2.p(), w.p());
+              project();
+              qr_f64(c, M, radd, w.p(), Q2.p(), R2.p());
             }
             DBuf<double> Q(c, M * kq), vn(c, r2 * kq);
             copy_f64(c, M * r, u.p(), Q.p());

@@ -148,7 +148,7 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
   TTG_REQUIRE(m >= 1 && n >= 1, "sizes must be >= 1");
   Context* c = &ctx->c;
   TTG_CUDA(cudaSetDevice(c->device));
-  qr_f64(c, m, n, A, Q, R, true);
+  qr_f64(c, m, n, A, Q, R);
   check_factorizations(c);
   TTG_API_END
 }

@@ -63,6 +63,10 @@ void scalar_op(Context* c, int op, double* out, const double* p0, const double* 
 // *out = first b < nb with cand[b] / *den > *thr, or -1 (one thread).
 void first_exceeding(Context* c, int64_t nb, const double* cand, const double* den,
                      const double* thr, double* out);
+// *keep = 1 when every column j of a projected block kept more than tau of
+// its norm (G1[j,j] > tau^2 G0[j,j]; G0, G1 Gram matrices before / after).
+void collapse_flag(Context* c, int64_t k, const double* G0, int64_t ld0, const double* G1,
+                   int64_t ld1, double tau, int* keep);
 // err_slot |= (*info != 0): LAPACK-style status accumulated without a host sync.
 void accumulate_info(Context* c, const int* info, int* err_slot);
 

@@ -27,6 +27,7 @@ struct GemmP {
   int64_t ldc, sC;
   double alpha, beta;
   const int* skip;  // optional: return at once when *skip != 0
+  int64_t kc;       // split-K: blockIdx.z owns k in [z kc, (z+1) kc); 0 = batched
 };
 
 template <bool TA, bool TB>
@@ -36,11 +37,21 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
   if (p.skip && *p.skip) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t bz = blockIdx.z;
-  const double* __restrict__ A = p.A + bz * p.sA;
-  const double* __restrict__ B = p.B + bz * p.sB;
+  const double* __restrict__ A;
+  const double* __restrict__ B;
   double* __restrict__ C = p.C + bz * p.sC;
+  int64_t K = p.K;
+  if (p.kc > 0) {  // one K slice of a split-K product; C is the slice's partial
+    const int64_t kb0 = bz * p.kc;
+    K = min(p.K - kb0, p.kc);
+    A = p.A + (TA ? kb0 : kb0 * p.lda);
+    B = p.B + (TB ? kb0 * p.ldb : kb0);
+  } else {
+    A = p.A + bz * p.sA;
+    B = p.B + bz * p.sB;
+  }
   const int64_t m0 = int64_t(blockIdx.x) * BM, n0 = int64_t(blockIdx.y) * BN;
-  const int64_t M = p.M, N = p.N, K = p.K;
+  const int64_t M = p.M, N = p.N;
 
   auto load_tile = [&](int64_t k0, int buf) {
     if (!TA) {  // m contiguous
@@ -342,6 +353,34 @@ __global__ void k_first_exceeding(int64_t nb, const double* cand, const double* 
   *out = r;
 }
 
+// C = alpha * sum_z part[z] + beta * C over the split-K slices, in slice
+// order (deterministic).  part: s slices of M x N (ld M).
+__global__ void k_splitk_reduce(int64_t M, int64_t N, int64_t s, const double* __restrict__ part,
+                                double alpha, double beta, double* __restrict__ C, int64_t ldc,
+                                const int* skip) {
+  if (skip && *skip) return;
+  const int64_t MN = M * N;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < MN;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    double acc = 0.0;
+    for (int64_t z = 0; z < s; ++z) acc += part[z * MN + e];
+    const int64_t m = e % M, n = e / M;
+    double* dst = C + m + n * ldc;
+    double v = alpha * acc;
+    if (beta != 0.0) v += beta * *dst;
+    *dst = v;
+  }
+}
+
+// *keep = 1 when every column j kept G1[j,j] > tau^2 G0[j,j] (one thread).
+__global__ void k_collapse_flag(int64_t k, const double* G0, int64_t ld0, const double* G1,
+                                int64_t ld1, double tau, int* keep) {
+  int ok = 1;
+  for (int64_t j = 0; j < k; ++j)
+    if (!(G1[j + j * ld1] > tau * tau * G0[j + j * ld0])) ok = 0;
+  *keep = ok;
+}
+
 __global__ void k_accumulate_info(const int* info, int* err_slot) {
   if (*info != 0) atomicOr(err_slot, 1);
 }
@@ -374,8 +413,28 @@ void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, dou
   TTG_REQUIRE(batch <= 65535, "gemm batch %lld too large", (long long)batch);
   const int64_t gx = (M + BM - 1) / BM, gy = (N + BN - 1) / BN;
   TTG_REQUIRE(gy <= 65535 && gx <= 0x7fffffff, "gemm too large");
-  GemmP p{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta, c->skip};
+  GemmP p{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta, c->skip, 0};
   dim3 grid{unsigned(gx), unsigned(gy), unsigned(batch)};
+  // Split-K for products with few output tiles and a long K (inner products
+  // of tall matrices: interface updates, projections): the K range is cut
+  // into slices computed by separate CTAs, then summed in slice order.
+  DBuf<double> part;
+  const int64_t tiles = gx * gy;
+  if (batch == 1 && K >= 512 && tiles * 2 < c->num_sms && M * N <= (int64_t(1) << 22)) {
+    int64_t s = std::min<int64_t>(K / 256, std::max<int64_t>(2, 2 * c->num_sms / tiles));
+    s = std::max<int64_t>(2, std::min<int64_t>(s, 64));
+    int64_t kc = (K + s - 1) / s;
+    kc = (kc + BK - 1) / BK * BK;
+    s = (K + kc - 1) / kc;
+    part.reset(c, s * M * N);
+    p.kc = kc;
+    p.C = part.p();
+    p.ldc = M;
+    p.sC = M * N;
+    p.alpha = 1.0;
+    p.beta = 0.0;
+    grid.z = unsigned(s);
+  }
   if (!tA && !tB)
     k_gemm_f64<false, false><<<grid, 128, 0, c->stream>>>(p);
   else if (!tA && tB)
@@ -386,6 +445,12 @@ void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, dou
     k_gemm_f64<true, true><<<grid, 128, 0, c->stream>>>(p);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
+  if (p.kc > 0) {
+    k_splitk_reduce<<<grid_for(c, M * N), 256, 0, c->stream>>>(M, N, int64_t(grid.z), part.p(),
+                                                               alpha, beta, C, ldc, c->skip);
+    c->launches += 1;
+    TTG_CHECK_LAUNCH();
+  }
 }
 
 void dot_f64(Context* c, int64_t n, const double* x, const double* y, double* out, bool do_sqrt) {
@@ -475,6 +540,13 @@ void scalar_op(Context* c, int op, double* out, const double* p0, const double* 
 void first_exceeding(Context* c, int64_t nb, const double* cand, const double* den,
                      const double* thr, double* out) {
   k_first_exceeding<<<1, 1, 0, c->stream>>>(nb, cand, den, thr, out);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void collapse_flag(Context* c, int64_t k, const double* G0, int64_t ld0, const double* G1,
+                   int64_t ld1, double tau, int* keep) {
+  k_collapse_flag<<<1, 1, 0, c->stream>>>(k, G0, ld0, G1, ld1, tau, keep);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
 }

@@ -50,98 +50,10 @@ void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t
   TTG_CHECK_LAUNCH();
 }
 
-namespace {
-
-// Row r of an m-row matrix -> row of the padded (p x Lr)-row layout in which
-// the first `rem` blocks hold Lr rows and the others Lr - 1 (zero-filled).
-__device__ __forceinline__ int64_t padded_row(int64_t r, int64_t Lr, int64_t rem) {
-  if (r < rem * Lr) return r;
-  const int64_t q = r - rem * Lr;
-  return (rem + q / (Lr - 1)) * Lr + q % (Lr - 1);
-}
-
-// dir 0: out[padded_row(r), c] = in[r, c];  dir 1: out[r, c] = in[padded_row(r), c].
-__global__ void k_pad_rows(int64_t m, int64_t n, int64_t Lr, int64_t rem, const double* in,
-                           int64_t ldi, double* out, int64_t ldo, int dir) {
-  const int64_t total = m * n;
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t r = e % m, col = e / m;
-    const int64_t pr = padded_row(r, Lr, rem);
-    if (dir == 0)
-      out[pr + col * ldo] = in[r + col * ldi];
-    else
-      out[r + col * ldo] = in[pr + col * ldi];
-  }
-}
-
-void pad_rows(Context* c, int64_t m, int64_t n, int64_t Lr, int64_t rem, const double* in,
-              int64_t ldi, double* out, int64_t ldo, int dir) {
-  int64_t blocks = (m * n + 255) / 256;
-  if (blocks > int64_t(c->num_sms) * 8) blocks = int64_t(c->num_sms) * 8;
-  k_pad_rows<<<unsigned(blocks), 256, 0, c->stream>>>(m, n, Lr, rem, in, ldi, out, ldo, dir);
-  c->launches += 1;
-  TTG_CHECK_LAUNCH();
-}
-
-// TSQR: one-CTA Householder QRs of row blocks (one batched launch), the
-// stacked n x n R factors factored again (recursively), and Q assembled as
-// Q_b = Q_leaf_b * Q_top[b] by one batched GEMM per level.  Blocks hold
-// Lr or Lr - 1 rows (>= n), stored Lr apart with zero rows at the end of the
-// short ones: zero rows leave the reflectors, and so R, unchanged and give
-// zero rows of Q.  Q: m x n (ld m), R: n x n (ld n); requires m >= 2n.
-void tsqr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
-              double* R) {
-  if (small_qr_fits(m, n)) {
-    small_qr_f64(c, m, n, A, lda, Q, R);
-    return;
-  }
-  const int64_t L = small_qr_max_rows(n);
-  const int64_t p = (m + L - 1) / L;
-  const int64_t Lr = (m + p - 1) / p;
-  const int64_t rem = m - p * (Lr - 1);  // blocks with Lr rows (1..p)
-  const int64_t P = p * Lr;
-  TTG_REQUIRE(Lr - 1 >= n, "tsqr: blocks of %lld rows for %lld columns", (long long)Lr,
-              (long long)n);
-  const double* Al = A;
-  int64_t ldl = lda;
-  DBuf<double> Apad, Qp;
-  if (P != m || lda != m) {
-    Apad.reset(c, P * n);
-    if (P != m) fill_f64(c, P * n, 0.0, Apad.p());
-    pad_rows(c, m, n, Lr, rem, A, lda, Apad.p(), P, 0);
-    Al = Apad.p();
-    ldl = P;
-  }
-  DBuf<double> Q0(c, P * n), S(c, p * n * n), Qt(c, p * n * n);
-  small_qr_batched_f64(c, p, Lr, n, Al, ldl, Lr, Q0.p(), Lr * n, S.p(), p * n, n);
-  tsqr_f64(c, p * n, n, S.p(), p * n, Qt.p(), R);
-  double* Qo = Q;
-  if (P != m) {
-    Qp.reset(c, P * n);
-    Qo = Qp.p();
-  }
-  gemm_f64(c, false, false, Lr, n, n, 1.0, Q0.p(), Lr, Lr * n, Qt.p(), p * n, n, 0.0, Qo, P, Lr,
-           p);
-  if (P != m) pad_rows(c, m, n, Lr, rem, Qp.p(), P, Q, m, 1);
-}
-
-bool tsqr_ok(int64_t m, int64_t n) {
-  return n >= 1 && n <= 96 && m >= 2 * n && small_qr_max_rows(n) >= 2 * n + 2 &&
-         m <= (int64_t(1) << 31);
-}
-
-}  // namespace
-
-int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R,
-               bool lapack_signs) {
+int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R) {
   const int64_t k = std::min(m, n);
   if (small_qr_fits(m, n)) {
     small_qr_f64(c, m, n, A, m, Q, R);
-    return k;
-  }
-  if (!lapack_signs && tsqr_ok(m, n)) {
-    tsqr_f64(c, m, n, A, m, Q, R);
     return k;
   }
   const int mi = as_int(m, "m"), ni = as_int(n, "n"), ki = as_int(k, "k");

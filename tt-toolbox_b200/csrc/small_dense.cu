@@ -150,12 +150,10 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
 // memory: Q (m x k, ld m), R (k x n, ld k), k = min(m, n).
 __global__ void __launch_bounds__(SD_THREADS) k_house_qr(int m, int n, const double* __restrict__ Ain,
                                                         int lda, double* __restrict__ Q,
-                                                        double* __restrict__ R, int ldr,
-                                                        int64_t sA, int64_t sQ, int64_t sR) {
-  // Batched over blockIdx.x: matrix b at Ain + b sA, Q + b sQ, R + b sR.
-  Ain += int64_t(blockIdx.x) * sA;
-  Q += int64_t(blockIdx.x) * sQ;
-  R += int64_t(blockIdx.x) * sR;
+                                                        double* __restrict__ R,
+                                                        const int* skip) {
+  if (skip && *skip) return;  // conditional factorization (Context::skip)
+  const int ldr = m < n ? m : n;
   extern __shared__ double sm[];
   double* A = sm;                 // m x n
   double* tau = sm + int64_t(m) * n;  // k
@@ -244,28 +242,11 @@ void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda
                   double* R) {
   const size_t smem = sizeof(double) * size_t(m * n + std::min(m, n));
   ensure_smem_attr(reinterpret_cast<const void*>(k_house_qr), c->device, int(SMEM_LIMIT + 1024));
-  k_house_qr<<<1, SD_THREADS, smem, c->stream>>>(int(m), int(n), A, int(lda), Q, R,
-                                                  int(std::min(m, n)), 0, 0, 0);
+  k_house_qr<<<1, SD_THREADS, smem, c->stream>>>(int(m), int(n), A, int(lda), Q, R, c->skip);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
 }
 
-void small_qr_batched_f64(Context* c, int64_t batch, int64_t m, int64_t n, const double* A,
-                          int64_t lda, int64_t sA, double* Q, int64_t sQ, double* R, int64_t ldr,
-                          int64_t sR) {
-  TTG_REQUIRE(small_qr_fits(m, n) && batch >= 1 && batch <= 0x7fffffff,
-              "batched QR: %lld x %lld does not fit one CTA", (long long)m, (long long)n);
-  const size_t smem = sizeof(double) * size_t(m * n + std::min(m, n));
-  ensure_smem_attr(reinterpret_cast<const void*>(k_house_qr), c->device, int(SMEM_LIMIT + 1024));
-  k_house_qr<<<unsigned(batch), SD_THREADS, smem, c->stream>>>(int(m), int(n), A, int(lda), Q, R,
-                                                               int(ldr), sA, sQ, sR);
-  c->launches += 1;
-  TTG_CHECK_LAUNCH();
-}
-
-int64_t small_qr_max_rows(int64_t n) {
-  return (int64_t(SMEM_LIMIT / sizeof(double)) - n) / n;
-}
 
 void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
                     double* VT) {
