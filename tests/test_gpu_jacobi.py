@@ -12,12 +12,15 @@ from oracle.tt import TT, tt_norm
 pytestmark = pytest.mark.gpu
 
 
-def _system(rng, rx1, n, rx2, ra1=3, ra2=2):
-    Phi1 = rng.standard_normal((rx1, rx1, ra1)) * 0.3
+def _system(rng, rx1, n, rx2, ra1=3, ra2=2, eps=0.05):
+    """Interfaces near 3 I and a Laplacian-like A core with small couplings:
+    unpreconditioned GMRES stalls on the 1/n^2 end of the spectrum, the
+    centre blocks carry it."""
+    Phi1 = rng.standard_normal((rx1, rx1, ra1)) * eps
     Phi1[:, :, 0] += 3 * np.eye(rx1)
-    A = rng.standard_normal((ra1, n, n, ra2)) * 0.3
+    A = rng.standard_normal((ra1, n, n, ra2)) * eps / n ** 2
     A[0, :, :, 0] += (n + 1) ** 2 * (2 * np.eye(n) - np.eye(n, k=1) - np.eye(n, k=-1)) / n ** 2
-    Phi2 = rng.standard_normal((rx2, ra2, rx2)) * 0.3
+    Phi2 = rng.standard_normal((rx2, ra2, rx2)) * eps
     Phi2[:, 0, :] += 3 * np.eye(rx2)
     return Phi1, A, Phi2
 
@@ -35,15 +38,13 @@ def test_cjacobi_local_solve_parity(ctx, rx1, n, rx2, tol):
     rhs = rng.standard_normal(sz)
     sol_prev = 0.01 * rng.standard_normal(sz)
     ref = oamen.solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, 40, 2, prec=1)
-    got = ttgpu.solve3d_2(Phi1, A, Phi2, rhs, tol, 1, sol_prev, 1, 40, 2, ctx=ctx)
+    info1, info0 = {}, {}
+    got = ttgpu.solve3d_2(Phi1, A, Phi2, rhs, tol, 1, sol_prev, 1, 40, 2, ctx=ctx, info=info1)
     assert rel(got, ref) < 1e-10
-    B = oamen.assemble_local(Phi1, A, Phi2) if sz <= 2000 else None
-    if B is not None:
-        # The stopping test is on the Householder GMRES estimate of the
-        # preconditioned residual; when P has large entries the true residual
-        # can sit above it by P's conditioning.  The solve must still be a
-        # good solve, and the oracle makes the same step (checked above).
-        assert np.linalg.norm(B @ got - rhs) <= 1e-6 * np.linalg.norm(rhs)
+    ttgpu.solve3d_2(Phi1, A, Phi2, rhs, tol, 1, sol_prev, 0, 40, 2, ctx=ctx, info=info0)
+    assert info1["iters"] < info0["iters"]
+    res = np.linalg.norm(oamen.bfun3(Phi1, A, Phi2, got) - rhs) / np.linalg.norm(rhs)
+    assert res <= 10 * tol
 
 
 def test_cjacobi_amen_parity(ctx):

@@ -107,6 +107,7 @@ struct PhaseProf {
     const char* e = getenv("TTG_PROFILE");
     on = e && e[0] == '1';
     c = cc;
+    fb0 = c->mixed_fallbacks;
   }
   void mark(const char* n) {
     if (!on) return;
@@ -116,9 +117,12 @@ struct PhaseProf {
     name = n;
     t0 = t;
   }
+  int64_t fb0 = 0;
   void report() {
     if (!on) return;
     mark("");
+    fprintf(stderr, "[ttg profile] mixed local solves finished in FP64: %lld\n",
+            (long long)(c->mixed_fallbacks - fb0));
     double tot = 0;
     for (auto& kv : ms) tot += kv.second;
     for (auto& kv : ms)

@@ -126,6 +126,8 @@ struct Context {
   int64_t matvec_flops = 0;
   // Per-kind local-matvec counters: [0] FP64 (DMMA), [1] BF16 (tcgen05).
   int64_t mv_count[2] = {0, 0};
+  // Mixed local solves that finished in FP64 (see local_solve_mixed).
+  int64_t mixed_fallbacks = 0;
   double mv_flops[2] = {0.0, 0.0};
   // Optional CUDA-event timing of every local matvec on the context stream.
   bool time_matvec = false;

@@ -388,6 +388,7 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
   const double target = tol * nrhs;
   copy_f64(c, sz, dres, r64.p());
   double nr = nres;
+  bool r64_valid = true;  // r64 = rhs - B sol for the current sol
   for (int outer = 0; outer < MAX_OUTER; ++outer) {
     if (!(nr > target)) break;
     nat_to_rev(c, d.rx1, d.n, d.rx2, r64.p(), rrev.p(), 1.0 / nr);
@@ -400,11 +401,31 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
     if (!(nr_new < nr)) {  // no progress: keep the better iterate and stop
       copy_f64(c, sz, prev.p(), sol);
       out.have_bsol = false;
+      r64_valid = false;
       break;
     }
     const bool stagnating = nr_new > 0.5 * nr;
     nr = nr_new;
     if (stagnating) break;
+  }
+  if (nr > target) {
+    // The low-precision corrections stopped paying (the local operator is
+    // too ill-conditioned for BF16 products): finish with the FP64
+    // Householder GMRES of the FP64 path on the remaining residual, so the
+    // local solve meets the same tolerance as there.
+    if (!r64_valid) nr = residual();
+    if (nr > target) {
+      DBuf<double> dsol(c, sz);
+      auto mv = [&](const double* x, double* y) {
+        local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
+      };
+      GmresResult g = gmres_hh_f64(c, mv, r64.p(), sz, nrestart, target / nr, niters, dsol.p());
+      axpby_f64(c, sz, 1.0, dsol.p(), 1.0, sol);
+      out.iters += g.iters;
+      out.matvecs_fp64 += g.matvecs;
+      out.have_bsol = false;
+      c->mixed_fallbacks += 1;
+    }
   }
   // Bounded-wait timeouts are reported through the context error slots 1-2,
   // checked by the caller once its sequence is done.
