@@ -87,3 +87,7 @@ def test_preconditioner_errors(ctx):
     A0[:] = 0.0  # every Jacobi block singular: the factorization error surfaces
     with pytest.raises(ttgpu.TTGError):
         ttgpu.solve3d_2(Phi1, A0, Phi2, rhs, 1e-8, 1, np.zeros(36), 1, ctx=ctx)
+    # the failure does not leak into the next call on the context
+    M = rng.standard_normal((8, 8))
+    U, s, VT = ttgpu.dense_svd(M, ctx=ctx)
+    assert np.allclose(U * s @ VT, M)

@@ -21,6 +21,12 @@ ttg::Context* grad_ctx(ttg_tt x, ttg_tt other, double* grad) {
   return x->ctx;
 }
 
+// Error slots start clear for every call that reads them at its end, so a
+// failed call cannot leak its flags into the next one.
+void clear_error_slots(ttg::Context* c) {
+  TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 8 * sizeof(int), c->stream));
+}
+
 void grad_value_out(ttg::Context* c, const double* dval, double* value) {
   if (value) ttg::read_scalars(c, dval, value, 1);
 }
@@ -56,6 +62,7 @@ int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax, int32_t
   TTG_REQUIRE(rmax == nullptr || nrmax == 1 || nrmax == in->d + 1,
               "rmax must have 1 or d+1 entries");
   TTG_CUDA(cudaSetDevice(in->ctx->device));
+  clear_error_slots(in->ctx);
   std::vector<int64_t> rm;
   if (rmax) {
     rm.assign(rmax, rmax + nrmax);
@@ -148,6 +155,7 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
   TTG_REQUIRE(m >= 1 && n >= 1, "sizes must be >= 1");
   Context* c = &ctx->c;
   TTG_CUDA(cudaSetDevice(c->device));
+  clear_error_slots(c);
   qr_f64(c, m, n, A, Q, R);
   check_factorizations(c);
   TTG_API_END
@@ -160,6 +168,7 @@ int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double
   TTG_REQUIRE(m >= 1 && n >= 1, "sizes must be >= 1");
   Context* c = &ctx->c;
   TTG_CUDA(cudaSetDevice(c->device));
+  clear_error_slots(c);
   TTG_CUDA(cudaMemsetAsync(c->d_err + 3, 0, sizeof(int), c->stream));
   svd_f64(c, m, n, A, U, S, VT);
   int herr = 0;
@@ -193,6 +202,7 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_
   int herr[8];
   TTG_CUDA(cudaMemcpyAsync(herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost, c->stream));
   sync(c);
+  if (herr[0] || herr[1] || herr[2] || herr[4]) clear_error_slots(c);
   if (herr[0] || herr[1] || herr[2])
     fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out in the local solve");
   if (herr[4]) fail(TTG_ERR_SOLVER, "a singular preconditioner block or factorization");
