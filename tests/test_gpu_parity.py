@@ -225,3 +225,16 @@ def test_amen_errors(ctx):
     with pytest.raises(ttgpu.TTGError) as e:
         ttgpu.amen_solve2(host_mat(A), host_tt(y), 1e-6, kicktype="svd", ctx=ctx)
     assert e.value.code == 7
+
+
+def test_round_rank_deficient_concatenation(ctx):
+    """x + x has exactly half the concatenated ranks: the QR sweep factors
+    exactly rank-deficient tall cores (rows 1024, 32 columns, the shifted
+    Cholesky QR path); ranks and the result must match the oracle."""
+    rng = np.random.default_rng(17)
+    x = tt_randn(64, 4, 16, rng, scale=lambda r1, nn, r2: 1.0 / np.sqrt(r1 * nn))
+    xx = x + x
+    ref, _ = tt_round(xx, 1e-10)
+    got = back(ttgpu.round(host_tt(xx), 1e-10, ctx=ctx))
+    assert list(got.r) == list(ref.r) == [1, 16, 16, 16, 1]
+    assert tt_rel(got, ref) < SOLVE_TOL

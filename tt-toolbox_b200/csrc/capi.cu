@@ -156,7 +156,7 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
   Context* c = &ctx->c;
   TTG_CUDA(cudaSetDevice(c->device));
   clear_error_slots(c);
-  qr_f64(c, m, n, A, Q, R);
+  qr_f64(c, m, n, A, Q, R, true);
   check_factorizations(c);
   TTG_API_END
 }

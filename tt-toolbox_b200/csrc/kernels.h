@@ -67,6 +67,8 @@ void first_exceeding(Context* c, int64_t nb, const double* cand, const double* d
 // its norm (G1[j,j] > tau^2 G0[j,j]; G0, G1 Gram matrices before / after).
 void collapse_flag(Context* c, int64_t k, const double* G0, int64_t ld0, const double* G1,
                    int64_t ld1, double tau, int* keep);
+// *flag |= 1 when max |G - I| > tol (G: n x n, ld n) or G has a NaN.
+void orth_check(Context* c, int64_t n, const double* G, double tol, int* flag);
 // err_slot |= (*info != 0): LAPACK-style status accumulated without a host sync.
 void accumulate_info(Context* c, const int* info, int* err_slot);
 

@@ -381,6 +381,16 @@ __global__ void k_collapse_flag(int64_t k, const double* G0, int64_t ld0, const 
   *keep = ok;
 }
 
+// *flag |= 1 when max |G - I| > tol (G: n x n Gram matrix of a basis).
+__global__ void k_orth_check(int64_t n, const double* G, double tol, int* flag) {
+  int bad = 0;
+  for (int64_t e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const double v = G[e] - ((e % n) == (e / n) ? 1.0 : 0.0);
+    if (!(fabs(v) <= tol)) bad = 1;
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
 __global__ void k_accumulate_info(const int* info, int* err_slot) {
   if (*info != 0) atomicOr(err_slot, 1);
 }
@@ -547,6 +557,12 @@ void first_exceeding(Context* c, int64_t nb, const double* cand, const double* d
 void collapse_flag(Context* c, int64_t k, const double* G0, int64_t ld0, const double* G1,
                    int64_t ld1, double tau, int* keep) {
   k_collapse_flag<<<1, 1, 0, c->stream>>>(k, G0, ld0, G1, ld1, tau, keep);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
+
+void orth_check(Context* c, int64_t n, const double* G, double tol, int* flag) {
+  k_orth_check<<<1, 256, 0, c->stream>>>(n, G, tol, flag);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
 }

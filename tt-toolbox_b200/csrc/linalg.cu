@@ -50,12 +50,65 @@ void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t
   TTG_CHECK_LAUNCH();
 }
 
-int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R) {
+namespace {
+
+// Shifted Cholesky QR, three passes (sCholeskyQR3: Fukaya, Kannan,
+// Nakatsukasa, Yamamoto, Yanagisawa, SIAM J. Sci. Comput. 42 (2020)
+// A477-A503).  Pass 1 factors the Gram matrix shifted by
+// s = 11 (m n + n (n + 1)) u ||A||_F^2, which keeps it positive definite for
+// any A (rank-deficient included) and leaves Q1 = A R1^{-1} with condition
+// number O(u^{-1/2}); two plain Cholesky QR passes then restore
+// orthogonality to O(u).  R = R3 R2 R1 (positive diagonal).  Every step is a
+// GEMM (split-K for the m-long Gram products) or one small one-CTA kernel.
+// Returns false (outputs unusable) when the input was too close to rank
+// deficient for the unshifted passes.
+bool scholqr3_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R) {
+  DBuf<double> G(c, n * n), Ri(c, n * n), Rinv(c, n * n), Racc(c, n * n), T(c, n * n),
+      W(c, m * n);
+  DBuf<int> flag(c, 1);
+  TTG_CUDA(cudaMemsetAsync(flag.p(), 0, sizeof(int), c->stream));
+  const double u = 1.1102230246251565e-16;
+  const double shift = 11.0 * (double(m) * n + double(n) * (n + 1)) * u;
+  const double* src = A;
+  for (int pass = 0; pass < 3; ++pass) {
+    double* dst = (pass == 1) ? W.p() : Q;  // Q1 -> Q, Q2 -> W, Q3 -> Q
+    gemm_f64(c, true, false, n, n, m, 1.0, src, m, 0, src, m, 0, 0.0, G.p(), n, 0, 1);
+    chol_inv_f64(c, n, G.p(), n, pass == 0 ? shift : 0.0, Ri.p(), Rinv.p(), flag.p());
+    gemm_f64(c, false, false, m, n, n, 1.0, src, m, 0, Rinv.p(), n, 0, 0.0, dst, m, 0, 1);
+    if (pass == 0) {
+      copy_f64(c, n * n, Ri.p(), Racc.p());
+    } else {  // Racc = Ri * Racc
+      gemm_f64(c, false, false, n, n, n, 1.0, Ri.p(), n, 0, Racc.p(), n, 0, 0.0, T.p(), n, 0, 1);
+      copy_f64(c, n * n, T.p(), Racc.p());
+    }
+    src = dst;
+  }
+  copy_f64(c, n * n, Racc.p(), R);
+  // Exactly rank-deficient inputs break the unshifted passes (singular Gram
+  // matrices): check Q's orthogonality and report; the caller then takes
+  // the Householder path.  One host read per factorization.
+  gemm_f64(c, true, false, n, n, m, 1.0, Q, m, 0, Q, m, 0, 0.0, G.p(), n, 0, 1);
+  orth_check(c, n, G.p(), 1e-12, flag.p());
+  int h = 0;
+  TTG_CUDA(cudaMemcpyAsync(&h, flag.p(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  return h == 0;
+}
+
+bool scholqr_ok(int64_t m, int64_t n) {
+  return n >= 8 && n <= 96 && m >= 4 * n && chol_inv_fits(n);
+}
+
+}  // namespace
+
+int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R,
+               bool lapack_signs) {
   const int64_t k = std::min(m, n);
   if (small_qr_fits(m, n)) {
     small_qr_f64(c, m, n, A, m, Q, R);
     return k;
   }
+  if (!lapack_signs && scholqr_ok(m, n) && scholqr3_f64(c, m, n, A, Q, R)) return k;
   const int mi = as_int(m, "m"), ni = as_int(n, "n"), ki = as_int(k, "k");
   DBuf<double> work(c, m * n), tau(c, k > 0 ? k : 1);
   DBuf<int> info(c, 1);

@@ -12,7 +12,12 @@ void check_factorizations(Context* c);
 // Thin QR of the m x n column-major A (lda = m): Q (m x k, ld m) and
 // R (k x n, ld k), k = min(m, n).  A is not modified.  Householder QR with
 // LAPACK's sign convention (geqrf/orgqr), as MATLAB's qr(A,0).
-int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R);
+// lapack_signs = false lets tall inputs (m >= 4n, 8 <= n <= 96) take a
+// shifted Cholesky QR (linalg.cu): the same factorization up to the signs of
+// Q's columns and R's rows, which the TT sweeps treat as a gauge; inputs too
+// close to rank deficiency for it fall back to the Householder QR.
+int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R,
+               bool lapack_signs = false);
 
 // Economy SVD A = U diag(S) VT of the m x n column-major A:
 // U (m x k, ld m), S (k) on the device, VT (k x n, ld k), k = min(m, n).

@@ -232,7 +232,88 @@ __global__ void __launch_bounds__(SD_THREADS) k_house_qr(int m, int n, const dou
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Cholesky factor and its inverse for shifted Cholesky QR
+// ---------------------------------------------------------------------------
+
+// G (n x n SPD Gram matrix, ldg) -> R = chol(G + shift I) upper (R' R = G +
+// shift I) and Rinv = R^{-1}, both n x n with leading dimension n.  shift =
+// shift_factor * trace(G).  err_slot |= 1 if a pivot is not positive.
+__global__ void __launch_bounds__(SD_THREADS) k_chol_inv(int n, const double* __restrict__ G,
+                                                        int ldg, double shift_factor,
+                                                        double* __restrict__ R,
+                                                        double* __restrict__ Rinv, int* err) {
+  extern __shared__ double sm[];
+  double* L = sm;                  // n x n, lower triangle = Cholesky factor
+  double* X = sm + int64_t(n) * n; // n x n, L^{-1}
+  __shared__ double s_shift;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < n * n; e += SD_THREADS) L[e] = G[(e % n) + int64_t(e / n) * ldg];
+  __syncthreads();
+  if (tid == 0) {
+    double tr = 0.0;
+    for (int i = 0; i < n; ++i) tr += L[i + n * i];
+    s_shift = shift_factor * tr;
+    s_bad = 0;
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += SD_THREADS) L[i + n * i] += s_shift;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (tid == 0) {
+      const double d = L[j + n * j];
+      if (!(d > 0.0)) s_bad = 1;
+      L[j + n * j] = d > 0.0 ? sqrt(d) : 1.0;
+    }
+    __syncthreads();
+    const double dj = L[j + n * j];
+    for (int i = j + 1 + tid; i < n; i += SD_THREADS) L[i + n * j] /= dj;
+    __syncthreads();
+    const int m = n - j - 1;
+    for (int e = tid; e < m * m; e += SD_THREADS) {
+      const int i = j + 1 + e % m, k = j + 1 + e / m;
+      if (k <= i) L[i + n * k] -= L[i + n * j] * L[k + n * j];
+    }
+    __syncthreads();
+  }
+  // X = L^{-1}: column c by forward substitution (one thread per column)
+  for (int c = tid; c < n; c += SD_THREADS) {
+    for (int i = 0; i < n; ++i) {
+      if (i < c) {
+        X[i + n * c] = 0.0;
+        continue;
+      }
+      double v = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) v -= L[i + n * k] * X[k + n * c];
+      X[i + n * c] = v / L[i + n * i];
+    }
+  }
+  __syncthreads();
+  // R = L', Rinv = X' (both upper triangular)
+  for (int e = tid; e < n * n; e += SD_THREADS) {
+    const int r = e % n, c = e / n;
+    R[e] = r <= c ? L[c + n * r] : 0.0;
+    Rinv[e] = r <= c ? X[c + n * r] : 0.0;
+  }
+  if (tid == 0 && s_bad) atomicOr(err, 1);
+}
+
 }  // namespace
+
+bool chol_inv_fits(int64_t n) { return 2 * n * n * int64_t(sizeof(double)) <= int64_t(SMEM_LIMIT); }
+
+void chol_inv_f64(Context* c, int64_t n, const double* G, int64_t ldg, double shift_factor,
+                  double* R, double* Rinv, int* flag) {
+  TTG_REQUIRE(chol_inv_fits(n), "chol_inv: n = %lld too large", (long long)n);
+  const size_t smem = 2 * sizeof(double) * size_t(n * n);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_chol_inv), c->device, int(SMEM_LIMIT + 1024));
+  k_chol_inv<<<1, SD_THREADS, smem, c->stream>>>(int(n), G, int(ldg), shift_factor, R, Rinv,
+                                                 flag ? flag : c->d_err + 4);
+  c->launches += 1;
+  TTG_CHECK_LAUNCH();
+}
 
 bool small_qr_fits(int64_t m, int64_t n) {
   return m * n + std::min(m, n) <= int64_t(SMEM_LIMIT / sizeof(double)) && m <= 0x7fffffff;

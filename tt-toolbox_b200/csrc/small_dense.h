@@ -9,6 +9,13 @@ bool small_qr_fits(int64_t m, int64_t n);
 // Thin Householder QR in one CTA: Q (m x k, ld m), R (k x n, ld k).
 void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
                   double* R);
+// Cholesky factor of a shifted Gram matrix and its inverse, one CTA:
+// R' R = G + shift_factor * trace(G) * I, Rinv = R^{-1} (n x n, ld n, upper).
+// A non-positive pivot sets *flag (nullptr: the context's factorization
+// error slot).
+bool chol_inv_fits(int64_t n);
+void chol_inv_f64(Context* c, int64_t n, const double* G, int64_t ldg, double shift_factor,
+                  double* R, double* Rinv, int* flag = nullptr);
 // One-sided Jacobi SVD of a square n x n matrix: U (n x n), S (n, descending),
 // VT (n x n), all with leading dimension n.
 void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
