@@ -8,7 +8,7 @@ import ttgpu
 pytestmark = pytest.mark.gpu
 
 SHAPES = [(64, 64), (132, 132), (4096, 64), (256, 4), (4, 256), (37, 53), (1, 5), (5, 1),
-          (8448, 132), (160, 150)]
+          (8448, 132), (160, 150), (256, 256), (1000, 201)]
 
 
 @pytest.mark.parametrize("m,n", SHAPES)
@@ -25,10 +25,11 @@ def test_dense_svd_matches_lapack(ctx, m, n):
     assert np.all(np.diff(s) <= 0)
 
 
-def test_dense_svd_graded_spectrum(ctx):
-    """Singular values spanning 14 decades (the truncation regime of AMEn)."""
+@pytest.mark.parametrize("n", [96, 180])
+def test_dense_svd_graded_spectrum(ctx, n):
+    """Singular values spanning 14 decades (the truncation regime of AMEn);
+    n = 180 runs the grid-wide Jacobi rounds."""
     rng = np.random.default_rng(3)
-    n = 96
     Q1, _ = np.linalg.qr(rng.standard_normal((512, n)))
     Q2, _ = np.linalg.qr(rng.standard_normal((n, n)))
     sv = 10.0 ** (-np.linspace(0, 14, n))

@@ -32,11 +32,13 @@ int as_int(int64_t v, const char* what) {
 }  // namespace
 
 void check_factorizations(Context* c) {
-  int h = 0;
-  TTG_CUDA(cudaMemcpyAsync(&h, c->d_err + 4, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  int h[5] = {0, 0, 0, 0, 0};
+  TTG_CUDA(cudaMemcpyAsync(h, c->d_err, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   sync(c);
-  if (h) {
-    TTG_CUDA(cudaMemsetAsync(c->d_err + 4, 0, sizeof(int), c->stream));
+  if (h[0] || h[1] || h[2] || h[4]) {
+    TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 5 * sizeof(int), c->stream));
+    if (h[0] || h[1] || h[2])
+      fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out in a factorization");
     fail(TTG_ERR_SOLVER, "a device factorization reported a non-zero LAPACK info");
   }
 }

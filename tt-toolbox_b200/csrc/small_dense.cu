@@ -36,6 +36,40 @@ __device__ __forceinline__ int rr_player(int k, int r, int ne) {
   return k == 0 ? 0 : 1 + ((k - 1 + r) % (ne - 1));
 }
 
+// Singular values = column norms of the rotated A, ranked descending
+// (stable on index); U = A diag(1/s), VT = V^T in that order.  One CTA of
+// SD_THREADS; sig: 2n doubles of scratch.
+__device__ void jacobi_finish(int n, const double* A, const double* V, double* __restrict__ U,
+                              double* __restrict__ S, double* __restrict__ VT, double* sig) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j = warp; j < n; j += SD_WARPS) {
+    const double* aj = A + int64_t(j) * n;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += aj[i] * aj[i];
+    s = wsum(s);
+    if (lane == 0) sig[j] = sqrt(s);
+  }
+  __syncthreads();
+  for (int j = tid; j < n; j += SD_THREADS) {
+    const double sj = sig[j];
+    int pos = 0;
+    for (int k = 0; k < n; ++k) {
+      const double sk = sig[k];
+      pos += (sk > sj) || (sk == sj && k < j);
+    }
+    S[pos] = sj;
+    sig[n + j] = double(pos);
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += SD_THREADS) {
+    const int i = e % n, j = e / n;
+    const int pos = int(sig[n + j]);
+    const double sj = sig[j];
+    U[i + int64_t(pos) * n] = sj > 0.0 ? A[e] / sj : (i == pos ? 1.0 : 0.0);
+    VT[pos + int64_t(i) * n] = V[e];
+  }
+}
+
 // A: n x n (column-major, lda) input; U (n x n, ld n), S (n), VT (n x n, ld n)
 // outputs.  work: n*n doubles of global scratch used when A does not fit in
 // shared memory.  Status: *err = 5 if the sweep limit is reached.
@@ -116,34 +150,154 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
     if (s_done) break;
   }
   if (tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(err, 5);
-  // Column norms -> singular values; rank by value (descending, stable on index).
-  double* sig = work + int64_t(n) * n;  // n scratch
-  for (int j = warp; j < n; j += SD_WARPS) {
-    const double* aj = A + int64_t(j) * n;
-    double s = 0.0;
-    for (int i = lane; i < n; i += 32) s += aj[i] * aj[i];
-    s = wsum(s);
-    if (lane == 0) sig[j] = sqrt(s);
-  }
+  jacobi_finish(n, A, V, U, S, VT, work + int64_t(n) * n);
+}
+
+
+// ---------------------------------------------------------------------------
+// Grid-wide one-sided Jacobi SVD for matrices too large for one CTA's shared
+// memory: one CTA per column pair of a round-robin round, a bounded grid
+// barrier between rounds (cooperative launch), the same rotation and
+// stopping rule as k_jacobi_svd.
+// ---------------------------------------------------------------------------
+
+constexpr int JC_THREADS = 256;
+constexpr long long JC_SPIN_LIMIT = 1LL << 24;
+
+__device__ void jc_barrier(unsigned* bar, int* err) {
   __syncthreads();
-  for (int j = tid; j < n; j += SD_THREADS) {
-    const double sj = sig[j];
-    int pos = 0;
-    for (int k = 0; k < n; ++k) {
-      const double sk = sig[k];
-      pos += (sk > sj) || (sk == sj && k < j);
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = bar + 1;
+    volatile int* verr = err;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == gen) {
+        if (*verr) break;
+        if (++spins > JC_SPIN_LIMIT) {
+          atomicExch(err, 6);
+          break;
+        }
+        __nanosleep(64);
+      }
     }
-    S[pos] = sj;
-    sig[n + j] = double(pos);
+    __threadfence();
   }
   __syncthreads();
-  for (int e = tid; e < n * n; e += SD_THREADS) {
-    const int i = e % n, j = e / n;
-    const int pos = int(sig[n + j]);
-    const double sj = sig[j];
-    U[i + int64_t(pos) * n] = sj > 0.0 ? A[e] / sj : (i == pos ? 1.0 : 0.0);
-    VT[pos + int64_t(i) * n] = V[e];
+}
+
+// A (n x n work copy, ld n) and V (n x n) in global memory; offmax: three
+// u64 slots holding the per-sweep maximum off-diagonal measure (bit pattern
+// of a non-negative double).  *sweeps_out = sweeps run.
+__global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double* __restrict__ Ain,
+                                                           int lda, double* A, double* V,
+                                                           unsigned* bar,
+                                                           unsigned long long* offmax, int* err,
+                                                           int* sweep_err) {
+  __shared__ double red[3][JC_THREADS / 32];
+  __shared__ double s_rot[2];
+  __shared__ int s_skip;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t nn = int64_t(n) * n;
+  for (int64_t e = blockIdx.x * int64_t(JC_THREADS) + tid; e < nn;
+       e += int64_t(gridDim.x) * JC_THREADS) {
+    const int64_t i = e % n, j = e / n;
+    A[e] = Ain[i + j * lda];
+    V[e] = (i == j) ? 1.0 : 0.0;
   }
+  if (blockIdx.x == 0 && tid < 3) offmax[tid] = 0ull;
+  jc_barrier(bar, err);
+  const int ne = (n + 1) & ~1;
+  const double tol = 4.0 * 2.220446049250313e-16;
+  int sweep = 0;
+  for (sweep = 0; sweep < JAC_MAX_SWEEPS; ++sweep) {
+    const int slot = sweep % 3;
+    if (blockIdx.x == 0 && tid == 0) offmax[(sweep + 1) % 3] = 0ull;
+    double off = 0.0;
+    for (int r = 0; r < ne - 1; ++r) {
+      for (int pr = blockIdx.x; pr < ne / 2; pr += gridDim.x) {
+        int p = rr_player(pr, r, ne), q = rr_player(ne - 1 - pr, r, ne);
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        if (q >= n) continue;  // dummy player (uniform in the CTA)
+        double* ap = A + int64_t(p) * n;
+        double* aq = A + int64_t(q) * n;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int i = tid; i < n; i += JC_THREADS) {
+          const double x = ap[i], y = aq[i];
+          al += x * x;
+          be += y * y;
+          ga += x * y;
+        }
+        al = wsum(al);
+        be = wsum(be);
+        ga = wsum(ga);
+        if (lane == 0) {
+          red[0][warp] = al;
+          red[1][warp] = be;
+          red[2][warp] = ga;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          double a2 = 0.0, b2 = 0.0, g2 = 0.0;
+          for (int w = 0; w < JC_THREADS / 32; ++w) {
+            a2 += red[0][w];
+            b2 += red[1][w];
+            g2 += red[2][w];
+          }
+          const double nrm = sqrt(a2 * b2);
+          if (nrm == 0.0 || fabs(g2) <= tol * nrm) {
+            s_skip = 1;
+          } else {
+            s_skip = 0;
+            off = fmax(off, fabs(g2) / nrm);
+            const double zeta = (b2 - a2) / (2.0 * g2);
+            const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            const double cc = 1.0 / sqrt(1.0 + t * t);
+            s_rot[0] = cc;
+            s_rot[1] = cc * t;
+          }
+        }
+        __syncthreads();
+        if (!s_skip) {
+          const double cc = s_rot[0], sn = s_rot[1];
+          double* vp = V + int64_t(p) * n;
+          double* vq = V + int64_t(q) * n;
+          for (int i = tid; i < n; i += JC_THREADS) {
+            const double x = ap[i], y = aq[i];
+            ap[i] = cc * x - sn * y;
+            aq[i] = sn * x + cc * y;
+            const double vx = vp[i], vy = vq[i];
+            vp[i] = cc * vx - sn * vy;
+            vq[i] = sn * vx + cc * vy;
+          }
+        }
+        __syncthreads();
+      }
+      jc_barrier(bar, err);
+    }
+    if (tid == 0) atomicMax(offmax + slot, (unsigned long long)__double_as_longlong(off));
+    jc_barrier(bar, err);
+    const double m = __longlong_as_double((long long)(*(volatile unsigned long long*)(offmax + slot)));
+    if (m <= tol) break;
+    if (*(volatile int*)err) break;
+  }
+  if (blockIdx.x == 0 && tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(sweep_err, 5);
+}
+
+__global__ void __launch_bounds__(SD_THREADS) k_jacobi_finish(int n, const double* A,
+                                                             const double* V, double* U,
+                                                             double* S, double* VT, double* sig) {
+  jacobi_finish(n, A, V, U, S, VT, sig);
 }
 
 // Householder QR of the m x n matrix A (column-major, lda) held in shared
@@ -335,6 +489,32 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
   const size_t mat = size_t(n * n) * sizeof(double);
   const int mode = 2 * mat <= SMEM_LIMIT ? 2 : (mat <= SMEM_LIMIT ? 1 : 0);
   DBuf<double> V(c, n * n), work(c, n * n + 2 * n);
+  if (mode != 2) {
+    // Grid-wide rounds: one CTA per column pair (up to what fits at once).
+    int occ = 0;
+    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_coop, JC_THREADS, 0));
+    const int64_t pairs = (n + 1) / 2;
+    const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(pairs,
+                                                                  int64_t(c->num_sms) * occ)));
+    DBuf<unsigned> bar(c, 2);
+    DBuf<unsigned long long> offmax(c, 3);
+    TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 2 * sizeof(unsigned), c->stream));
+    int ni = int(n), ldi = int(lda);
+    double* Aw = work.p();
+    double* Vp = V.p();
+    unsigned* barp = bar.p();
+    unsigned long long* offp = offmax.p();
+    int* errp = c->d_err + 0;
+    int* swp = c->d_err + 3;
+    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp};
+    TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_jacobi_coop, dim3(blocks),
+                                         dim3(JC_THREADS), args, 0, c->stream));
+    k_jacobi_finish<<<1, SD_THREADS, 0, c->stream>>>(int(n), work.p(), V.p(), U, S, VT,
+                                                     work.p() + int64_t(n) * n);
+    c->launches += 2;
+    TTG_CHECK_LAUNCH();
+    return;
+  }
   ensure_smem_attr(reinterpret_cast<const void*>(k_jacobi_svd), c->device,
                    int(SMEM_LIMIT + 1024));
   const size_t smem = size_t(mode) * mat;
