@@ -213,6 +213,15 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
 int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double* U, double* S,
                   double* VT);
 
+/* SDV TT files (the toolbox's binary format: fmex/tt_read.c:13-100,
+ * fmex/tt_write.c:21-80; read by tt_tensor(filename),
+ * @tt_tensor/tt_tensor.m:150).  Reading gives a TT tensor handle of ctx
+ * (float files are widened to double; complex files fail with
+ * TTG_ERR_UNSUPPORTED).  Writing stores a tensor, or a TT matrix as the tensor
+ * of its cores with mode sizes n_k m_k; precision 0 = double, 1 = float. */
+int ttg_tt_read_sdv(ttg_context ctx, const char* path, ttg_tt* out);
+int ttg_tt_write_sdv(ttg_tt tt, const char* path, int32_t precision);
+
 /* Batched amen_solve2: `count` independent systems A[i] x = y[i] solved
  * concurrently on the context's device.  No single reference counterpart:
  * each system is amen_solve2(A{i}, y{i}, tol(i), opts{i}) (solve/amen_solve2.m:1);

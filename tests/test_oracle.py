@@ -235,3 +235,14 @@ def test_jacobi_preconditioners_invert_their_blocks(prec):
     for p in (0, prec):
         x = solve3d_2(Phi1, A, Phi2, rhs, 1e-12, x0, nrestart=N, niters=2, prec=p)
         assert np.linalg.norm(x - xs) <= 1e-9 * np.linalg.norm(xs)
+
+
+@pytest.mark.parametrize("name", ["A", "b"])
+def test_sdv_fixture_rebuilds_reference_bytes(name):
+    """The oracle's SDV writer, fed the parsed contents of the reference's own
+    fmex/{A,b}.sdv, reproduces the file byte for byte (SHA-256 pinned)."""
+    from golden_io import load_sdv
+    from oracle import sdv
+    hd, g, data = load_sdv(name)
+    f = sdv.parse(data)
+    assert f["d"] == 80 and np.array_equal(f["core"], g["core"])

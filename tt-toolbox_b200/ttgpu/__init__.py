@@ -120,6 +120,8 @@ def lib():
     sigs["ttg_dense_qr"] = [_vp, _i64, _i64, _vp, _vp, _vp]
     sigs["ttg_dense_svd"] = [_vp, _i64, _i64, _vp, _vp, _vp, _vp]
     sigs["ttg_grad_xAx"] = [_vp, _vp, _vp, _pd]
+    sigs["ttg_tt_read_sdv"] = [_vp, C.c_char_p, C.POINTER(_vp)]
+    sigs["ttg_tt_write_sdv"] = [_vp, C.c_char_p, C.c_int32]
     sigs["ttg_amen_solve_batch"] = [_vp, _i64, C.POINTER(_vp), C.POINTER(_vp), _pd,
                                     C.POINTER(AmenOpts), C.POINTER(_vp), C.POINTER(_vp),
                                     C.c_int32, C.POINTER(_vp), C.POINTER(AmenStats),
@@ -768,3 +770,45 @@ def grad_sampled(x, idx, y=None, ctx=None, out=None):
     finally:
         if own:
             ss.free()
+
+
+# ---------------------------------------------------------------------------
+# SDV TT files (fmex/tt_read.c, fmex/tt_write.c)
+# ---------------------------------------------------------------------------
+
+def read_sdv(path, ctx=None, device=False):
+    """``tt_tensor(filename)``: a host ``TensorTrain`` (``DeviceTT`` with
+    ``device=True``) read from a SDV file."""
+    ctx = ctx or default_context()
+    h = _vp()
+    _check(lib().ttg_tt_read_sdv(ctx.h, os.fsencode(path), C.byref(h)))
+    t = DeviceTT(ctx, h)
+    if device:
+        return t
+    host = t.download()
+    t.free()
+    return host
+
+
+def write_sdv(path, tt, precision="double", ctx=None):
+    """Write a TT tensor or matrix (host or device) as a SDV file;
+    ``precision`` 'double' or 'float'."""
+    ctx = ctx or (tt.ctx if isinstance(tt, DeviceTT) else default_context())
+    prec = {"double": 0, "float": 1}[precision]
+    dev = tt if isinstance(tt, DeviceTT) else DeviceTT.upload(ctx, tt)
+    try:
+        _check(lib().ttg_tt_write_sdv(dev.h, os.fsencode(path), prec))
+    finally:
+        if dev is not tt:
+            dev.free()
+
+
+def as_matrix(tt, n, m):
+    """Reinterpret a TT tensor whose mode sizes are n_k m_k as a TT matrix
+    (row index fastest), as ``tt_matrix(tt, n, m)``."""
+    n = np.asarray(n, np.int64)
+    m = np.asarray(m, np.int64)
+    if not np.array_equal(np.asarray(tt.n, np.int64), n * m):
+        raise ValueError("mode sizes are not n .* m")
+    return TTMatrix(n, m, tt.r, tt.core)
+
