@@ -231,17 +231,34 @@ def dgemm_bench(args):
 
 
 def _rel_diff(X, Y):
-    """||Y - X|| / ||X|| by TT inner products in FP64 on the host."""
+    """||Y - X|| / ||X|| in FP64 on the host: the difference as one TT (rank
+    concatenation) orthogonalised left to right; the norm is that of the last
+    core.  (An inner-product formula would lose everything below 1e-8 to
+    cancellation.)"""
     xs, ys = X.cores(), Y.cores()
+    d = len(xs)
 
-    def gram(a, b):
-        G = np.ones((1, 1))
-        for ca, cb in zip(a, b):
-            t = np.tensordot(G, ca, axes=([0], [0]))          # [j, n, k]
-            G = np.tensordot(t, cb, axes=([0, 1], [0, 1]))    # [k, l]
-        return G[0, 0]
-    xx, yy, xy = gram(xs, xs), gram(ys, ys), gram(xs, ys)
-    return float(np.sqrt(max(xx + yy - 2 * xy, 0.0) / xx))
+    def norm(cores):
+        R = np.ones((1, 1))
+        for k, c in enumerate(cores):
+            r1, n, r2 = c.shape
+            c = np.tensordot(R, c, axes=([1], [0])).reshape(-1, r2, order="F")
+            if k == d - 1:
+                return float(np.linalg.norm(c))
+            q, R = np.linalg.qr(c)
+
+    diff = []
+    for k, (a, b) in enumerate(zip(xs, ys)):
+        if k == 0:
+            diff.append(np.concatenate([a, -b], axis=2))
+        elif k == d - 1:
+            diff.append(np.concatenate([a, b], axis=0))
+        else:
+            c = np.zeros((a.shape[0] + b.shape[0], a.shape[1], a.shape[2] + b.shape[2]))
+            c[:a.shape[0], :, :a.shape[2]] = a
+            c[a.shape[0]:, :, a.shape[2]:] = b
+            diff.append(c)
+    return norm(diff) / norm(xs)
 
 
 def main():
