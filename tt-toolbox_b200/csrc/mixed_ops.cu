@@ -24,6 +24,8 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <cstdlib>
+#include <map>
 #include <mutex>
 
 #include "mixed_ops.h"
@@ -351,15 +353,121 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
                                                                  phi1T.p());
   c->launches += 3;
   TTG_CHECK_LAUNCH();
-  bn1 = pick_bn(c, d.m * d.rx1, d.ra2 * d.ry2, 1);
-  bn2 = pick_bn(c, d.rx1, d.ra1 * d.n, d.ry2);
-  bn3 = pick_bn(c, d.ry2 * d.n, d.ry1, 1);
   make_map(&mapX, X.p(), d.rx2, d.m * d.rx1, ldx, UM_BM);
-  make_map(&mapP2, phi2b.p(), d.rx2, d.ra2 * d.ry2, ldx, bn1);
   make_map(&mapT1, T1.p(), d.n * d.ra2, d.rx1 * d.ry2, ld1, UM_BM);
-  make_map(&mapAT, AT.p(), d.n * d.ra2, d.ra1 * d.n, ld1, bn2);
   make_map(&mapT2, T2.p(), d.rx1 * d.ra1, d.ry2 * d.n, ld2, UM_BM);
+  bn1 = tuned_bn(c, 1);
+  bn2 = tuned_bn(c, 2);
+  bn3 = tuned_bn(c, 3);
+  make_map(&mapP2, phi2b.p(), d.rx2, d.ra2 * d.ry2, ldx, bn1);
+  make_map(&mapAT, AT.p(), d.n * d.ra2, d.ra1 * d.n, ld1, bn2);
   make_map(&mapP1, phi1T.p(), d.rx1 * d.ra1, d.ry1, ld2, bn3);
+}
+
+// ---------------------------------------------------------------------------
+// Tile-width autotuner
+//
+// The first time a stage shape (M, N, K, batch) is met on a device, each
+// admissible tile width is timed with CUDA events on the context stream
+// (one warm-up and three timed launches, on the operands just converted and
+// whatever the intermediates hold -- the values do not change the work) and
+// the fastest is kept for the life of the process.  The width only decides
+// which CTA computes which output columns; every output element is still
+// the same K-ordered sequence of MMA steps.  TTG_AUTOTUNE=0 turns tuning off
+// (the CTA-count heuristic pick_bn is used instead), e.g. for runs that must
+// repeat the same launch configuration.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct TuneKey {
+  int device, stage;
+  int64_t M, N, K, batch;
+  bool operator<(const TuneKey& o) const {
+    if (device != o.device) return device < o.device;
+    if (stage != o.stage) return stage < o.stage;
+    if (M != o.M) return M < o.M;
+    if (N != o.N) return N < o.N;
+    if (K != o.K) return K < o.K;
+    return batch < o.batch;
+  }
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tuned;
+
+bool autotune_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("TTG_AUTOTUNE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+}  // namespace
+
+void MixedOp::run_stage(Context* c, int stage, int bn, const CUtensorMap& mapB, float* y) {
+  const int64_t rows = d.m * d.rx1;
+  if (stage == 1) {
+    OutMap o1{T1.p(), rows, d.ra2 * d.ry2, d.m, 1, ld1, d.ra2, d.m, ld1 * d.rx1, 0};
+    umma_gemm(c, mapX, mapB, d.rx2, 0, 0, rows, d.ra2 * d.ry2, 1, o1, true, bn);
+  } else if (stage == 2) {
+    OutMap o2{T2.p(), d.rx1, d.ra1 * d.n, d.rx1, 1, 0, d.ra1, d.rx1, ld2 * d.ry2, ld2};
+    umma_gemm(c, mapT1, mapB, d.n * d.ra2, d.rx1, 0, d.rx1, d.ra1 * d.n, d.ry2, o2, true, bn);
+  } else {
+    const int64_t rows3 = d.ry2 * d.n;
+    OutMap o3{y, rows3, d.ry1, rows3, 1, 0, d.ry1, rows3, 0, 0};
+    umma_gemm(c, mapT2, mapB, d.rx1 * d.ra1, 0, 0, rows3, d.ry1, 1, o3, false, bn);
+  }
+}
+
+int MixedOp::tuned_bn(Context* c, int stage) {
+  int64_t M, N, K, batch = 1;
+  if (stage == 1) {
+    M = d.m * d.rx1; N = d.ra2 * d.ry2; K = d.rx2;
+  } else if (stage == 2) {
+    M = d.rx1; N = d.ra1 * d.n; K = d.n * d.ra2; batch = d.ry2;
+  } else {
+    M = d.ry2 * d.n; N = d.ry1; K = d.rx1 * d.ra1;
+  }
+  const int fallback = pick_bn(c, M, N, batch);
+  if (!autotune_enabled() || c->skip) return fallback;
+  const TuneKey key{c->device, stage, M, N, K, batch};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return it->second;
+  }
+  DBuf<float> ysc;
+  if (stage == 3) ysc.reset(c, d.ry2 * d.n * d.ry1);
+  float best_ms = 1e30f;
+  int best = fallback;
+  cudaEvent_t e0, e1;
+  TTG_CUDA(cudaEventCreate(&e0));
+  TTG_CUDA(cudaEventCreate(&e1));
+  for (int bn : {64, 128, 256}) {
+    if (bn > 64 && bn / 2 >= N) break;  // wider tiles than N only waste columns
+    CUtensorMap mb;
+    if (stage == 1) make_map(&mb, phi2b.p(), d.rx2, N, ldx, bn);
+    else if (stage == 2) make_map(&mb, AT.p(), K, N, ld1, bn);
+    else make_map(&mb, phi1T.p(), K, N, ld2, bn);
+    run_stage(c, stage, bn, mb, ysc.p());
+    TTG_CUDA(cudaEventRecord(e0, c->stream));
+    for (int rep = 0; rep < 3; ++rep) run_stage(c, stage, bn, mb, ysc.p());
+    TTG_CUDA(cudaEventRecord(e1, c->stream));
+    TTG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    TTG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = bn;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tuned[key] = best;
+  return best;
 }
 
 void MixedOp::apply(Context* c, const float* v, float* y) {
@@ -368,16 +476,9 @@ void MixedOp::apply(Context* c, const float* v, float* y) {
   k_cvt_x<<<blocks_for(c, ldx * rows), 256, 0, c->stream>>>(d.rx2, rows, ldx, v, X.p(), c->skip);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
-  // stage 1: T1[(m,a),(be,k)]
-  OutMap o1{T1.p(), rows, d.ra2 * d.ry2, d.m, 1, ld1, d.ra2, d.m, ld1 * d.rx1, 0};
-  umma_gemm(c, mapX, mapP2, d.rx2, 0, 0, rows, d.ra2 * d.ry2, 1, o1, true, bn1);
-  // stage 2: per k, T2_k[a,(al,j)]
-  OutMap o2{T2.p(), d.rx1, d.ra1 * d.n, d.rx1, 1, 0, d.ra1, d.rx1, ld2 * d.ry2, ld2};
-  umma_gemm(c, mapT1, mapAT, d.n * d.ra2, d.rx1, 0, d.rx1, d.ra1 * d.n, d.ry2, o2, true, bn2);
-  // stage 3: y[(k,j), i] in the reversed vector layout
-  const int64_t rows3 = d.ry2 * d.n;
-  OutMap o3{y, rows3, d.ry1, rows3, 1, 0, d.ry1, rows3, 0, 0};
-  umma_gemm(c, mapT2, mapP1, d.rx1 * d.ra1, 0, 0, rows3, d.ry1, 1, o3, false, bn3);
+  run_stage(c, 1, bn1, mapP2, y);  // T1[(m,a),(be,k)]
+  run_stage(c, 2, bn2, mapAT, y);  // per k, T2_k[a,(al,j)]
+  run_stage(c, 3, bn3, mapP1, y);  // y[(k,j), i] in the reversed vector layout
   c->matvecs += 1;
   c->matvec_flops += int64_t(d.flops());
   c->mv_count[1] += 1;
