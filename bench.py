@@ -134,60 +134,6 @@ class Clocks:
 # correctness check of the measured run (host numpy, outside the timed region)
 # ---------------------------------------------------------------------------
 
-def true_residual(A, x, y):
-    """||A x - y|| / ||y|| for host TT objects (matvec by core products, norm
-    by a left-to-right QR sweep)."""
-    import numpy as np
-
-    def cores_of(t):
-        return t.cores()
-
-    def mat_cores(M):
-        out, pos = [], 0
-        for k in range(M.d):
-            sz = int(M.r[k] * M.n[k] * M.m[k] * M.r[k + 1])
-            out.append(M.core[pos:pos + sz].reshape(
-                (int(M.r[k]), int(M.n[k]), int(M.m[k]), int(M.r[k + 1])), order="F"))
-            pos += sz
-        return out
-
-    Ac, xc, yc = mat_cores(A), cores_of(x), cores_of(y)
-    d = len(xc)
-    res = []
-    for k in range(d):
-        ax = np.einsum("anmb,cmd->acnbd", Ac[k], xc[k])
-        ra1, rx1, n, ra2, rx2 = ax.shape
-        ax = ax.reshape(ra1 * rx1, n, ra2 * rx2, order="F")
-        yk = -yc[k] if k == 0 else yc[k]
-        r1a, _, r2a = ax.shape
-        r1b, _, r2b = yk.shape
-        if k == 0:
-            c = np.concatenate([ax, yk], axis=2)
-        elif k == d - 1:
-            c = np.concatenate([ax, yk], axis=0)
-        else:
-            c = np.zeros((r1a + r1b, n, r2a + r2b))
-            c[:r1a, :, :r2a] = ax
-            c[r1a:, :, r2a:] = yk
-        res.append(c)
-
-    def norm(cs):
-        nrm = 1.0
-        core = cs[0]
-        for k in range(len(cs) - 1):
-            r1, n, r2 = core.shape
-            q, rr = np.linalg.qr(core.reshape(r1 * n, r2, order="F"))
-            s = np.linalg.norm(rr)
-            nrm *= s
-            rr = rr / s
-            nxt = cs[k + 1]
-            core = (rr @ nxt.reshape(nxt.shape[0], -1, order="F")).reshape(
-                rr.shape[0], nxt.shape[1], nxt.shape[2], order="F")
-        return nrm * np.linalg.norm(core)
-
-    return norm(res) / norm(yc)
-
-
 # ---------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------
@@ -308,7 +254,7 @@ def run_ours(args, dist):
     ms_step_max = dist.max(ms_step)
     x = xdev.download()
     xdev.free()
-    res = true_residual(A, x, y)
+    res = ttgpu.true_residual(A, x, y, ctx=ctx)
 
     # end to end through the C ABI with host buffers
     e2e_t = []
@@ -332,7 +278,7 @@ def run_ours(args, dist):
             ox.free()
             a = agg[op]
             other = {"precision": op, "ms_per_step": statistics.mean(oms), "sweeps": osw,
-                     "true_residual": true_residual(A, xo, y),
+                     "true_residual": ttgpu.true_residual(A, xo, y, ctx=ctx),
                      "speedup_of_headline": statistics.mean(oms) / ms_step}
             if a["ms_fp64"] > 0:
                 other["fp64_matvec_tflops"] = a["gflop_fp64"] / a["ms_fp64"]

@@ -213,6 +213,18 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
 int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double* U, double* S,
                   double* VT);
 
+/* TT algebra on device-resident handles (the caller side of the path: the
+ * true residual ||A x - y|| / ||y||, round's inputs).  Results are new
+ * handles of the operands' context; tensors need boundary ranks 1 for dot.
+ *   ttg_tt_matvec : exact A x, ranks multiply   (@tt_matrix/mtimes.m:38-65)
+ *   ttg_tt_axpby  : a x + b y, ranks add         (@tt_tensor/plus.m:40-86)
+ *   ttg_tt_norm   : QR-based Frobenius norm      (@tt_tensor/norm.m:16-42)
+ *   ttg_tt_dot    : <x, y>                       (@tt_tensor/dot.m:92-111) */
+int ttg_tt_matvec(ttg_tt A, ttg_tt x, ttg_tt* out);
+int ttg_tt_axpby(double a, ttg_tt x, double b, ttg_tt y, ttg_tt* out);
+int ttg_tt_norm(ttg_tt x, double* nrm);
+int ttg_tt_dot(ttg_tt x, ttg_tt y, double* val);
+
 /* SDV TT files (the toolbox's binary format: fmex/tt_read.c:13-100,
  * fmex/tt_write.c:21-80; read by tt_tensor(filename),
  * @tt_tensor/tt_tensor.m:150).  Reading gives a TT tensor handle of ctx

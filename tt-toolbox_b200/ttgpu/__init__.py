@@ -121,6 +121,10 @@ def lib():
     sigs["ttg_dense_svd"] = [_vp, _i64, _i64, _vp, _vp, _vp, _vp]
     sigs["ttg_grad_xAx"] = [_vp, _vp, _vp, _pd]
     sigs["ttg_tt_read_sdv"] = [_vp, C.c_char_p, C.POINTER(_vp)]
+    sigs["ttg_tt_matvec"] = [_vp, _vp, C.POINTER(_vp)]
+    sigs["ttg_tt_axpby"] = [C.c_double, _vp, C.c_double, _vp, C.POINTER(_vp)]
+    sigs["ttg_tt_norm"] = [_vp, _pd]
+    sigs["ttg_tt_dot"] = [_vp, _vp, _pd]
     sigs["ttg_tt_write_sdv"] = [_vp, C.c_char_p, C.c_int32]
     sigs["ttg_amen_solve_batch"] = [_vp, _i64, C.POINTER(_vp), C.POINTER(_vp), _pd,
                                     C.POINTER(AmenOpts), C.POINTER(_vp), C.POINTER(_vp),
@@ -811,4 +815,104 @@ def as_matrix(tt, n, m):
     if not np.array_equal(np.asarray(tt.n, np.int64), n * m):
         raise ValueError("mode sizes are not n .* m")
     return TTMatrix(n, m, tt.r, tt.core)
+
+
+# ---------------------------------------------------------------------------
+# TT algebra on the device (@tt_matrix/mtimes.m, @tt_tensor/plus.m,
+# @tt_tensor/norm.m, @tt_tensor/dot.m)
+# ---------------------------------------------------------------------------
+
+def _dev_args(ctx, *ts):
+    owned, hs = [], []
+    for t in ts:
+        if isinstance(t, DeviceTT):
+            hs.append(t)
+        else:
+            h = DeviceTT.upload(ctx, t)
+            owned.append(h)
+            hs.append(h)
+    return owned, hs
+
+
+def _ctx_of(ctx, *ts):
+    for t in ts:
+        if isinstance(t, DeviceTT):
+            return ctx or t.ctx
+    return ctx or default_context()
+
+
+def _result(ctx, h, device):
+    t = DeviceTT(ctx, h)
+    if device:
+        return t
+    host = t.download()
+    t.free()
+    return host
+
+
+def tt_matvec(A, x, ctx=None):
+    """``A * x`` exactly (ranks multiply); a ``DeviceTT`` when ``x`` is one."""
+    ctx = _ctx_of(ctx, A, x)
+    owned, (dA, dx) = _dev_args(ctx, A, x)
+    try:
+        h = _vp()
+        _check(lib().ttg_tt_matvec(dA.h, dx.h, C.byref(h)))
+        return _result(ctx, h, isinstance(x, DeviceTT))
+    finally:
+        for t in owned:
+            t.free()
+
+
+def tt_axpby(a, x, b, y, ctx=None):
+    """``a*x + b*y`` (ranks add); a ``DeviceTT`` when ``x`` is one."""
+    ctx = _ctx_of(ctx, x, y)
+    owned, (dx, dy) = _dev_args(ctx, x, y)
+    try:
+        h = _vp()
+        _check(lib().ttg_tt_axpby(float(a), dx.h, float(b), dy.h, C.byref(h)))
+        return _result(ctx, h, isinstance(x, DeviceTT))
+    finally:
+        for t in owned:
+            t.free()
+
+
+def tt_norm(x, ctx=None):
+    """``norm(x)`` by the QR sweep of ``@tt_tensor/norm.m``."""
+    ctx = _ctx_of(ctx, x)
+    owned, (dx,) = _dev_args(ctx, x)
+    try:
+        v = C.c_double(0.0)
+        _check(lib().ttg_tt_norm(dx.h, C.byref(v)))
+        return v.value
+    finally:
+        for t in owned:
+            t.free()
+
+
+def tt_dot(x, y, ctx=None):
+    """``dot(x, y)``."""
+    ctx = _ctx_of(ctx, x, y)
+    owned, (dx, dy) = _dev_args(ctx, x, y)
+    try:
+        v = C.c_double(0.0)
+        _check(lib().ttg_tt_dot(dx.h, dy.h, C.byref(v)))
+        return v.value
+    finally:
+        for t in owned:
+            t.free()
+
+
+def true_residual(A, x, y, ctx=None):
+    """``norm(A*x - y) / norm(y)`` on the device."""
+    ctx = _ctx_of(ctx, A, x, y)
+    owned, (dA, dx, dy) = _dev_args(ctx, A, x, y)
+    ax = r = None
+    try:
+        ax = tt_matvec(dA, dx, ctx)
+        r = tt_axpby(1.0, ax, -1.0, dy, ctx)
+        return tt_norm(r, ctx) / tt_norm(dy, ctx)
+    finally:
+        for t in owned + [ax, r]:
+            if t is not None:
+                t.free()
 
