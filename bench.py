@@ -40,6 +40,13 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision")
+    p.add_argument("--workload", default="amen", choices=["amen", "batch"],
+                   help="amen: the headline single solve; batch: 512 independent systems "
+                        "(one timed batch; --steps/--warmup do not apply)")
+    p.add_argument("--batch-count", type=int, default=512)
+    p.add_argument("--batch-workers", type=int, default=8)
+    p.add_argument("--batch-sample", type=int, default=32,
+                   help="systems solved one by one (GPU FP64) and by the CPU oracle")
     return p.parse_args()
 
 
@@ -343,6 +350,90 @@ def run_ours(args, dist):
     return line
 
 
+BATCH_METRIC = "batched AMEn: independent Laplacian systems to tol 1e-8, total time"
+
+
+def run_batch(args, dist):
+    """Config 4: ``count`` independent seeded Laplacian systems (d U{6..14},
+    n in {8,16,32,64}, rmax U{8..64}, all-ones right-hand sides, tol 1e-8)
+    through ``ttg_amen_solve_batch`` (worker streams), mixed precision,
+    against the same systems solved one after another in FP64 on the GPU and
+    by the CPU oracle (both on the first ``batch_sample`` systems, scaled to
+    the whole batch by count)."""
+    if dist.rank != 0:
+        return None
+    import numpy as np
+    import ttgpu
+    from ttgpu import workloads
+    ctx = ttgpu.Context(int(os.environ.get("TTG_DEVICE", "0")))
+    As, ys, rmaxs, shapes = workloads.batch_systems(count=args.batch_count, seed=4)
+    dAs = [ttgpu.DeviceTT.upload(ctx, a) for a in As]
+    dys = [ttgpu.DeviceTT.upload(ctx, y) for y in ys]
+    per = [dict(rmax=r) for r in rmaxs]
+    k = min(args.batch_sample, args.batch_count)
+    # warm-up: kernels loaded and tile widths tuned on a small batch
+    for x in ttgpu.amen_solve2_batch(dAs[:16], dys[:16], 1e-8, workers=args.batch_workers,
+                                     ctx=ctx, per_system=per[:16], precision="mixed"):
+        x.free()
+    ctx.sync()
+    clocks = Clocks(0)
+    clocks.start()
+    st = []
+    t0 = time.perf_counter()
+    xs = ttgpu.amen_solve2_batch(dAs, dys, 1e-8, workers=args.batch_workers, ctx=ctx,
+                                 stats=st, per_system=per, precision="mixed")
+    ctx.sync()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    conv = sum(1 for q in st if q["sweeps"] and q["max_res"][q["sweeps"] - 1] < 1e-8)
+    res = [ttgpu.true_residual(dAs[i], xs[i], dys[i], ctx=ctx) for i in range(k)]
+    for x in xs:
+        x.free()
+    gflop = sum(q["matvec_gflop"] for q in st)
+    launches = sum(q["launches"] for q in st)
+    t0 = time.perf_counter()
+    for i in range(k):
+        ttgpu.amen_solve2(dAs[i], dys[i], 1e-8, ctx=ctx, rmax=rmaxs[i], precision="fp64").free()
+    ctx.sync()
+    serial = (time.perf_counter() - t0) / k * args.batch_count
+    line = {
+        "metric": BATCH_METRIC, "value": wall, "unit": "s", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16/f32 matvec + f64 refinement",
+        "data": "synthetic (seeded PCG64)",
+        "config": {"workload": "%d Laplacian systems, d U{6..14}, n in {8,16,32,64}, rmax "
+                               "U{8..64}, ones rhs, tol 1e-8" % args.batch_count,
+                   "workers": args.batch_workers, "converged": conv,
+                   "true_residual_max_of_sample": max(res)},
+        "gpu_launches": launches, "matvec_tflops": gflop / wall * 1e-3, "clocks": clk,
+        "compare": {"serial_fp64_gpu_s": serial,
+                    "speedup_vs_serial_fp64_gpu": serial / wall,
+                    "sample": "first %d systems one by one, scaled by count" % k},
+    }
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, ROOT)
+        from oracle.amen import amen_solve2 as ref_solve
+        from oracle.tt import TT, TTMatrix, tt_randn
+        t0 = time.perf_counter()
+        kc = max(1, k // 4)
+        for i in range(kc):
+            A, y = As[i], ys[i]
+            Ao = TTMatrix.from_flat(A.n, A.m, A.r, A.core)
+            yo = TT.from_flat(y.n, y.r, y.core)
+            rng = np.random.default_rng(i)
+            x0 = tt_randn([int(v) for v in A.n], A.d, 2, rng)
+            ref_solve(Ao, yo, 1e-8, x0, None, rmax=rmaxs[i], nswp=20)
+        cpu = (time.perf_counter() - t0) / kc * args.batch_count
+        line["cpu_baseline"] = {"value": cpu, "unit": "s", "cores": os.cpu_count(),
+                                "kind": "port",
+                                "sample": "FP64 oracle on the first %d systems, scaled by count"
+                                          % kc}
+    for h in dAs + dys:
+        h.free()
+    ctx.close()
+    return line
+
+
 def main():
     args = parse()
     if args.impl == "ours":
@@ -350,7 +441,10 @@ def main():
         ttgpu.lib()  # before torch (see Dist)
     dist = Dist()
     try:
-        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if args.workload == "batch":
+            line = run_batch(args, dist) if args.impl == "ours" else None
+        else:
+            line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
         if dist.rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:
