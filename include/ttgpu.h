@@ -213,6 +213,26 @@ int ttg_dense_qr(ttg_context ctx, int64_t m, int64_t n, const double* A, double*
 int ttg_dense_svd(ttg_context ctx, int64_t m, int64_t n, const double* A, double* U, double* S,
                   double* VT);
 
+/* AMEn approximate matrix-by-vector product y ~ A x
+ * ([y, z] = amen_mv(A, x, tol, ...), core/amen_mv.m:1-419, default path:
+ * renorm 'direct', fkick false, kickrank2 0).  A: TT matrix with square
+ * cores matching x.  y0 / z0 (nullable: right-orthogonal random TTs of
+ * ranks 2 / kickrank drawn from opts->seed) as the options 'y0', 'z0'.
+ * y_out receives the approximation; z_out (nullable) the error TT;
+ * sweeps_out (nullable) the sweeps run. */
+typedef struct {
+  int64_t nswp;      /* 20 (amen_mv.m:55)            */
+  int64_t kickrank;  /* 4  (:56); 0 disables z        */
+  int32_t init_qr;   /* 1  (:61)                      */
+  int32_t verb;      /* 0                             */
+  uint64_t seed;     /* random y0 / z0 when NULL      */
+  int64_t reserved[4];
+} ttg_amen_mv_opts;
+
+int ttg_amen_mv_opts_default(ttg_amen_mv_opts* opts);
+int ttg_amen_mv(ttg_tt A, ttg_tt x, double tol, const ttg_amen_mv_opts* opts, ttg_tt y0,
+                ttg_tt z0, ttg_tt* y_out, ttg_tt* z_out, int64_t* sweeps_out);
+
 /* TT algebra on device-resident handles (the caller side of the path: the
  * true residual ||A x - y|| / ||y||, round's inputs).  Results are new
  * handles of the operands' context; tensors need boundary ranks 1 for dot.

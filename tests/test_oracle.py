@@ -246,3 +246,19 @@ def test_sdv_fixture_rebuilds_reference_bytes(name):
     hd, g, data = load_sdv(name)
     f = sdv.parse(data)
     assert f["d"] == 80 and np.array_equal(f["core"], g["core"])
+
+
+def test_amen_mv_oracle_reaches_exact_product():
+    """oracle.amen_mv (core/amen_mv.m default path) at tight tolerance gives the
+    exact TT matvec; at loose tolerance an error near tol."""
+    from oracle.amen_mv import amen_mv
+    A, _, _, _ = aniso_config(d=5, n=6)
+    rng = np.random.default_rng(8)
+    x = tt_randn(6, 5, 4, rng)
+    ex = tt_matvec(A, x)
+    y0 = tt_rand(6, 5, 2, np.random.default_rng(1))
+    z0 = tt_rand(6, 5, 4, np.random.default_rng(2))
+    y, z, info = amen_mv(A, x, 1e-12, y0, z0)
+    assert tt_norm(y - ex) <= 1e-11 * tt_norm(ex)
+    y, z, info = amen_mv(A, x, 1e-3, y0, z0)
+    assert tt_norm(y - ex) <= 1e-2 * tt_norm(ex)

@@ -71,6 +71,11 @@ class AmenStats(C.Structure):
                     gflop_fp64=float(self.gflop_fp64), ms_fp64=float(self.ms_fp64))
 
 
+class AmenMvOpts(C.Structure):
+    _fields_ = [("nswp", _i64), ("kickrank", _i64), ("init_qr", C.c_int32),
+                ("verb", C.c_int32), ("seed", C.c_uint64), ("reserved", _i64 * 4)]
+
+
 class RoundStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_qr_sweep", C.c_double),
                 ("ms_svd_sweep", C.c_double), ("max_rank", _i64)]
@@ -122,6 +127,8 @@ def lib():
     sigs["ttg_grad_xAx"] = [_vp, _vp, _vp, _pd]
     sigs["ttg_tt_read_sdv"] = [_vp, C.c_char_p, C.POINTER(_vp)]
     sigs["ttg_tt_matvec"] = [_vp, _vp, C.POINTER(_vp)]
+    sigs["ttg_amen_mv"] = [_vp, _vp, C.c_double, C.POINTER(AmenMvOpts), _vp, _vp,
+                           C.POINTER(_vp), C.POINTER(_vp), _p64]
     sigs["ttg_tt_axpby"] = [C.c_double, _vp, C.c_double, _vp, C.POINTER(_vp)]
     sigs["ttg_tt_norm"] = [_vp, _pd]
     sigs["ttg_tt_dot"] = [_vp, _vp, _pd]
@@ -136,6 +143,8 @@ def lib():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = C.c_int
+    L.ttg_amen_mv_opts_default.argtypes = [C.POINTER(AmenMvOpts)]
+    L.ttg_amen_mv_opts_default.restype = C.c_int
     L.ttg_amen_opts_default.argtypes = [C.POINTER(AmenOpts)]
     L.ttg_amen_opts_default.restype = None
     _lib = L
@@ -915,4 +924,35 @@ def true_residual(A, x, y, ctx=None):
         for t in owned + [ax, r]:
             if t is not None:
                 t.free()
+
+
+def amen_mv(A, x, tol, y0=None, z0=None, ctx=None, nswp=20, kickrank=4, init_qr=True, verb=0,
+            seed=None):
+    """``[y, z] = amen_mv(A, x, tol, 'y0', y0, 'z0', z0, ...)``
+    (``core/amen_mv.m``): returns ``(y, z, sweeps)``, host TTs unless ``x``
+    is a ``DeviceTT`` (``z`` is None when ``kickrank`` is 0)."""
+    ctx = _ctx_of(ctx, A, x)
+    o = AmenMvOpts()
+    lib().ttg_amen_mv_opts_default(C.byref(o))
+    o.nswp, o.kickrank, o.init_qr, o.verb = int(nswp), int(kickrank), int(bool(init_qr)), int(verb)
+    if seed is not None:
+        o.seed = int(seed)
+    owned, hs = _dev_args(ctx, *[t for t in (A, x, y0, z0) if t is not None])
+    it = iter(hs)
+    dA, dx = next(it), next(it)
+    dy0 = next(it) if y0 is not None else None
+    dz0 = next(it) if z0 is not None else None
+    yh, zh, sw = _vp(), _vp(), _i64(0)
+    try:
+        _check(lib().ttg_amen_mv(dA.h, dx.h, float(tol), C.byref(o),
+                                 dy0.h if dy0 is not None else None,
+                                 dz0.h if dz0 is not None else None,
+                                 C.byref(yh), C.byref(zh), C.byref(sw)))
+        dev = isinstance(x, DeviceTT)
+        y = _result(ctx, yh, dev)
+        z = _result(ctx, zh, dev) if zh.value else None
+        return y, z, sw.value
+    finally:
+        for t in owned:
+            t.free()
 
