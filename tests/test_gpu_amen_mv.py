@@ -27,8 +27,10 @@ def back(t):
 @pytest.mark.parametrize("cfg", [dict(d=6, n=8, rx=5, kick=4), dict(d=5, n=16, rx=9, kick=4),
                                  dict(d=4, n=6, rx=3, kick=0)])
 def test_amen_mv_tight_tolerance_parity(ctx, cfg):
-    """Tight tolerance: y reaches the exact (rank ra*rx) product, so both
-    implementations agree with it and with each other to 1e-10."""
+    """Tight tolerance: both implementations agree to 1e-10; with enrichment
+    (kickrank > 0) y reaches the exact (rank ra*rx) product, without it the
+    ranks stay those of y0 (plain ALS, as in the reference) and y is the
+    converged rank-2 approximation."""
     A, _, _, _ = aniso_config(d=cfg["d"], n=cfg["n"])
     rng = np.random.default_rng(cfg["d"] * 10 + cfg["n"])
     x = tt_randn(cfg["n"], cfg["d"], cfg["rx"], rng)
@@ -42,9 +44,11 @@ def test_amen_mv_tight_tolerance_parity(ctx, cfg):
     assert sweeps == info["sweeps"]
     assert list(got.r) == list(ref.r)
     assert tt_norm(got - ref) <= 1e-10 * tt_norm(ref)
-    assert tt_norm(got - ex) <= 1e-10 * tt_norm(ex)
     if cfg["kick"]:
+        assert tt_norm(got - ex) <= 1e-10 * tt_norm(ex)
         assert z is not None and z.d == cfg["d"]
+    else:
+        assert max(got.r) == 2 and z is None
 
 
 def test_amen_mv_loose_tolerance(ctx):
