@@ -10,6 +10,8 @@
 // Gram-Schmidt applied twice (CGS2): one cooperative kernel per Arnoldi step
 // performs both projections, the normalisation and the Givens update of the
 // least-squares residual; partial sums are reduced in a fixed order.
+#include <cuda_bf16.h>
+
 #include <cmath>
 #include <cstring>
 
@@ -41,7 +43,18 @@ struct ArArgs {
   int* err;
   int* stop;       // [0] converged flag, [1] step at which it converged
   double thresh;   // absolute residual threshold of the current solve
+  // BF16 operand of the next local matvec, written with each new basis
+  // vector: X[b + ldx * row] = bf16(V[b + rx2 * row]) (padding b >= rx2 stays
+  // zero), so the matvec needs no conversion launch.
+  __nv_bfloat16* X;
+  int rx2;
+  int ldx;
 };
+
+__device__ __forceinline__ void put_x(const ArArgs& a, int64_t i, float v) {
+  const int64_t row = i / a.rx2, b = i - row * a.rx2;
+  a.X[b + int64_t(a.ldx) * row] = __float2bfloat16_rn(v);
+}
 
 __device__ __forceinline__ float warp_sumf(float v) {
 #pragma unroll
@@ -161,7 +174,11 @@ __global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
   const double nrm = sqrt(hp[0]);
   float* Vn = a.V + int64_t(j + 1) * a.sz;
   const float inv = nrm > 0.0 ? float(1.0 / nrm) : 0.f;
-  AR_LOOP(i, a.sz) Vn[i] = a.w[i] * inv;
+  AR_LOOP(i, a.sz) {
+    const float v = a.w[i] * inv;
+    Vn[i] = v;
+    put_x(a, i, v);
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     double* Hj = a.H + int64_t(a.m + 1) * j;
     for (int c = 0; c < ncol; ++c) Hj[c] = ht[c];
@@ -209,7 +226,11 @@ __global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r
   reduce_parts(a.part, 1, tot);
   const double beta = sqrt(tot[0]);
   const float inv = beta > 0.0 ? float(1.0 / beta) : 0.f;
-  AR_LOOP(i, a.sz) a.V[i] = r[i] * inv;
+  AR_LOOP(i, a.sz) {
+    const float v = r[i] * inv;
+    a.V[i] = v;
+    put_x(a, i, v);
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     for (int k = 0; k <= a.m; ++k) a.g[k] = 0.0;
     a.g[0] = beta;
@@ -283,6 +304,7 @@ struct Gmres32 {
     stop.reset(c, 4);
     a.stop = stop.p();
     a.thresh = 0.0;
+    a.X = nullptr;
   }
 
   size_t arnoldi_smem() const {
@@ -298,6 +320,9 @@ struct Gmres32 {
   // Solve B x = b approximately; x (FP32, zeroed here); returns Krylov steps.
   int64_t solve(MixedOp& op, const float* b, float* x, double reltol, int64_t max_restarts) {
     int64_t steps = 0;
+    a.X = op.X.p();
+    a.rx2 = int(op.d.rx2);
+    a.ldx = int(op.ldx);
     TTG_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * sz, c->stream));
     double bnorm = -1.0;
     for (int64_t it = 0; it < max_restarts; ++it) {
@@ -325,7 +350,7 @@ struct Gmres32 {
         const int jend = std::min(m, j + chunk);
         for (int jj = j; jj < jend; ++jj) {
           int jv = jj;
-          op.apply(c, a.V + int64_t(jv) * sz, w.p());
+          op.apply_converted(c, w.p());  // X holds V(:, jv) (k_ar_init / k_arnoldi)
           void* aa[] = {&a, &jv};
           coop((const void*)k_arnoldi, aa, arnoldi_smem());
         }

@@ -344,6 +344,10 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
   AT.reset(c, ld1 * d.ra1 * d.n);
   phi1T.reset(c, ld2 * d.ry1);
   X.reset(c, ldx * d.m * d.rx1);
+  // Padding columns (b >= rx2) must read as zero: the Krylov kernels write
+  // only the valid part of X.
+  if (ldx != d.rx2)
+    TTG_CUDA(cudaMemsetAsync(X.p(), 0, sizeof(__nv_bfloat16) * X.size(), c->stream));
   T1.reset(c, ld1 * d.rx1 * d.ry2);
   T2.reset(c, ld2 * d.ry2 * d.n);
   k_cvt_phi2<<<blocks_for(c, phi2b.size()), 256, 0, c->stream>>>(d.rx2, d.ra2 * d.ry2, ldx, Phi2,
@@ -476,6 +480,15 @@ void MixedOp::apply(Context* c, const float* v, float* y) {
   k_cvt_x<<<blocks_for(c, ldx * rows), 256, 0, c->stream>>>(d.rx2, rows, ldx, v, X.p(), c->skip);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
+  stages(c, y);
+}
+
+void MixedOp::apply_converted(Context* c, float* y) {
+  MvTiming timing(c, 1);
+  stages(c, y);
+}
+
+void MixedOp::stages(Context* c, float* y) {
   run_stage(c, 1, bn1, mapP2, y);  // T1[(m,a),(be,k)]
   run_stage(c, 2, bn2, mapAT, y);  // per k, T2_k[a,(al,j)]
   run_stage(c, 3, bn3, mapP1, y);  // y[(k,j), i] in the reversed vector layout

@@ -19,11 +19,16 @@ struct MixedOp {
   void prepare(Context* c, const MvDims& d, const double* Phi1, const double* A,
                const double* Phi2);
   void apply(Context* c, const float* v, float* y);
+  // Same with X already holding the BF16 operand (written by the Arnoldi
+  // kernels of the Krylov solver).
+  void apply_converted(Context* c, float* y);
   // One GEMM stage (1, 2, 3) with tile width bn and B-operand map mapB;
   // stage 3 writes y.
   void run_stage(Context* c, int stage, int bn, const CUtensorMap& mapB, float* y);
   // Tile width of a stage: autotuned once per shape and device (mixed_ops.cu).
   int tuned_bn(Context* c, int stage);
+  // The three GEMM stages from X to y, with the matvec counters.
+  void stages(Context* c, float* y);
 };
 
 // Natural [i, j, k] FP64 <-> reversed [k, j, i] FP32 vector layouts.
