@@ -7,8 +7,8 @@
 // the local residuals and the per-sweep maxima): small device kernels update
 // it in stream order.  The host reads device values only where the
 // algorithm branches on them: the local-solve tolerance (one read per core),
-// the candidate ranks of the residual-based truncation (batched reads), the
-// Krylov stopping test, and the per-sweep stopping test.
+// the rank of the residual-based truncation (one read per chunk of 16
+// candidates), the Krylov stopping test, and the per-sweep stopping test.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -478,9 +478,11 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
         // thr = max(real_tol*resid_damp, res_new) (:547)
         scalar_op(c, SC_MAX_CONST, S.p(Scalars::THR), S.p(Scalars::RES_NEW), nullptr, nullptr,
                   real_tol * resid_damp);
-        // Candidate ranks rr = K-1, K-2, ..., 1 (:539-550): residuals are
-        // evaluated in growing batches and read back once per batch; the rank
-        // is the first candidate whose residual exceeds thr, as in the loop.
+        // Candidate ranks rr = K-1, K-2, ..., 1 (:539-550): the rank is the
+        // first candidate whose residual exceeds thr, as in the loop.  The
+        // residuals come from rank-one images of the SVD terms when B sol is
+        // at hand; otherwise (zero rhs, dense branch) one local residual per
+        // candidate, evaluated in growing batches with one read per batch.
         int64_t found = -1, next = K - 1, batch = 1;
         if (have_bsol && next >= 1) {
           // rhs - B(U_rr S_rr V_rr^T) = (rhs - B sol) + sum_{k >= rr} s_k B(u_k v_k^T):

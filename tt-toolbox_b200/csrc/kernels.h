@@ -13,7 +13,8 @@ void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, dou
               int64_t sB, double beta, double* C, int64_t ldc, int64_t sC, int64_t batch = 1);
 
 // out = sum(x.*y) (or sum(x.^2) when y == nullptr) into a device scalar;
-// deterministic two-stage reduction.  If do_sqrt, stores sqrt of the sum.
+// deterministic one-launch reduction (block partials summed in block order
+// by the last block).  If do_sqrt, stores sqrt of the sum.
 void dot_f64(Context* c, int64_t n, const double* x, const double* y, double* out,
              bool do_sqrt = false);
 // Frobenius norm to host (synchronises).

@@ -59,7 +59,7 @@ int64_t rank1_scratch_size(const MvDims& d, int64_t cnt);
 
 // Running sums of candidate residuals: for b = 0..cnt-1,
 //   R += W[:, cnt-1-b];  out[b] = ||R||      (R updated in place)
-// deterministic two-stage reduction.  part: cumulative_norms_part_size(c).
+// deterministic two-kernel reduction.  part: cumulative_norms_part_size(c).
 constexpr int CUMNORM_MAXC = 16;
 void cumulative_norms_f64(Context* c, int64_t N, int64_t cnt, double* R, const double* W,
                           double* part, double* out);
