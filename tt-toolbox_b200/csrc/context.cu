@@ -96,6 +96,8 @@ void context_init(Context& c, int device) {
   TTG_CUDA(cudaMallocHost(&c.h_scal, 4096 * sizeof(double)));
   TTG_CUDA(cudaMalloc(&c.d_err, 64 * sizeof(int)));
   TTG_CUDA(cudaMemset(c.d_err, 0, 64 * sizeof(int)));
+  TTG_CUDA(cudaMalloc(&c.d_tile_cnt, GEMM_TILE_COUNTERS * sizeof(unsigned)));
+  TTG_CUDA(cudaMemset(c.d_tile_cnt, 0, GEMM_TILE_COUNTERS * sizeof(unsigned)));
   TTG_CUDA(cudaEventCreate(&c.ev0));
   TTG_CUDA(cudaEventCreate(&c.ev1));
 }
@@ -107,6 +109,7 @@ void context_release(Context& c) {
   if (c.solver) cusolverDnDestroy(c.solver);
   if (c.h_scal) cudaFreeHost(c.h_scal);
   if (c.d_err) cudaFree(c.d_err);
+  if (c.d_tile_cnt) cudaFree(c.d_tile_cnt);
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
   for (auto& e : c.ev_pool) {
@@ -118,6 +121,7 @@ void context_release(Context& c) {
   c.solver = nullptr;
   c.h_scal = nullptr;
   c.d_err = nullptr;
+  c.d_tile_cnt = nullptr;
   c.ev0 = c.ev1 = nullptr;
   c.stream = nullptr;
 }

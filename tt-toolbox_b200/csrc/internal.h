@@ -51,6 +51,9 @@ struct Error {
     if (!(cond)) ::ttg::fail(TTG_ERR_INVALID, __VA_ARGS__);                         \
   } while (0)
 
+// Number of per-tile arrival counters a context holds for split-K GEMMs.
+constexpr int64_t GEMM_TILE_COUNTERS = int64_t(1) << 16;
+
 // Caching device allocator: blocks are rounded up to a size class and kept
 // on per-class free lists, so a solve that reaches steady state performs no
 // cudaMalloc.  get/put are serialised by a mutex: the batched solve draws its
@@ -120,6 +123,9 @@ struct Context {
   // Device int slots: 0-7 error flags of bounded waits and factorizations
   // (cleared per solve), 63 the arrival counter of the one-launch reductions.
   int* d_err = nullptr;
+  // Per-output-tile arrival counters of split-K GEMMs (GEMM_TILE_COUNTERS,
+  // zero between launches: the last slice of a tile resets its counter).
+  unsigned* d_tile_cnt = nullptr;
   // Counters (reset by the caller through ttg_stats).
   int64_t launches = 0;
   int64_t matvecs = 0;

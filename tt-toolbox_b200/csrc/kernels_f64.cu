@@ -16,6 +16,8 @@ namespace ttg {
 namespace {
 
 constexpr int BM = 64, BN = 64, BK = 16, PADS = 8;
+// Split-K partial values one CTA may sum in the GEMM kernel itself.
+constexpr int64_t SPLITK_INKERNEL_MAX = 4096;
 
 struct GemmP {
   int64_t M, N, K;
@@ -27,7 +29,15 @@ struct GemmP {
   int64_t ldc, sC;
   double alpha, beta;
   const int* skip;  // optional: return at once when *skip != 0
-  int64_t kc;       // split-K: blockIdx.z owns k in [z kc, (z+1) kc); 0 = batched
+  // Split-K: nsplit > 1 slices of kc columns of K per batch item, blockIdx.z =
+  // item * nsplit + slice.  Each slice writes its partial tile to `part`
+  // ([item][slice] blocks of M x N, ld M).  With `cnt` (one arrival counter
+  // per tile and item) the slice that arrives last at its tile adds the
+  // partials in slice order (deterministic), applies alpha/beta, writes C and
+  // resets the counter; without it k_splitk_reduce does the same afterwards.
+  int64_t nsplit, kc;
+  double* part;
+  unsigned* cnt;
 };
 
 template <bool TA, bool TB>
@@ -36,20 +46,13 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
   __shared__ double Bs[2][BK][BN + PADS];
   if (p.skip && *p.skip) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t bz = blockIdx.z;
-  const double* __restrict__ A;
-  const double* __restrict__ B;
-  double* __restrict__ C = p.C + bz * p.sC;
-  int64_t K = p.K;
-  if (p.kc > 0) {  // one K slice of a split-K product; C is the slice's partial
-    const int64_t kb0 = bz * p.kc;
-    K = min(p.K - kb0, p.kc);
-    A = p.A + (TA ? kb0 : kb0 * p.lda);
-    B = p.B + (TB ? kb0 * p.ldb : kb0);
-  } else {
-    A = p.A + bz * p.sA;
-    B = p.B + bz * p.sB;
-  }
+  const bool split = p.nsplit > 1;
+  const int64_t item = split ? blockIdx.z / p.nsplit : blockIdx.z;
+  const int64_t slice = split ? blockIdx.z % p.nsplit : 0;
+  const int64_t kb0 = slice * p.kc;
+  const double* __restrict__ A = p.A + item * p.sA + (TA ? kb0 : kb0 * p.lda);
+  const double* __restrict__ B = p.B + item * p.sB + (TB ? kb0 * p.ldb : kb0);
+  const int64_t K = split ? min(p.K - kb0, p.kc) : p.K;
   const int64_t m0 = int64_t(blockIdx.x) * BM, n0 = int64_t(blockIdx.y) * BN;
   const int64_t M = p.M, N = p.N;
 
@@ -133,6 +136,33 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
     __syncthreads();
   }
 
+  double* __restrict__ C = p.C + item * p.sC;
+  if (!split) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t row = m0 + wm + i * 8 + g;
+      if (row >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int64_t col = n0 + wn + j * 8 + 2 * t + e;
+          if (col < N) {
+            double* dst = C + row + col * p.ldc;
+            double v = p.alpha * acc[i][j][e];
+            if (p.beta != 0.0) v += p.beta * *dst;
+            *dst = v;
+          }
+        }
+      }
+    }
+    return;
+  }
+
+  // Split-K: publish this slice's partial tile, then the last slice to
+  // arrive reduces the tile.
+  const int64_t MN = M * N;
+  double* Pme = p.part + blockIdx.z * MN;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int64_t row = m0 + wm + i * 8 + g;
@@ -142,14 +172,35 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int64_t col = n0 + wn + j * 8 + 2 * t + e;
-        if (col < N) {
-          double* dst = C + row + col * p.ldc;
-          double v = p.alpha * acc[i][j][e];
-          if (p.beta != 0.0) v += p.beta * *dst;
-          *dst = v;
-        }
+        if (col < N) Pme[row + col * M] = acc[i][j][e];
       }
     }
+  }
+  if (!p.cnt) return;
+  __threadfence();
+  __syncthreads();
+  __shared__ int s_last;
+  if (tid == 0) {
+    unsigned* ctr = p.cnt + item * (int64_t(gridDim.x) * gridDim.y) + blockIdx.x +
+                    int64_t(gridDim.x) * blockIdx.y;
+    const unsigned prev = atomicAdd(ctr, 1u);
+    s_last = prev == unsigned(p.nsplit - 1);
+    if (s_last) *ctr = 0u;  // every slice has arrived: ready for the next launch
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const double* P0 = p.part + item * p.nsplit * MN;
+  for (int e = tid; e < BM * BN; e += 128) {
+    const int64_t row = m0 + (e % BM), col = n0 + (e / BM);
+    if (row >= M || col >= N) continue;
+    const int64_t off = row + col * M;
+    double acc2 = 0.0;
+    for (int64_t z = 0; z < p.nsplit; ++z) acc2 += __ldcg(P0 + z * MN + off);
+    double* dst = C + row + col * p.ldc;
+    double v = p.alpha * acc2;
+    if (p.beta != 0.0) v += p.beta * *dst;
+    *dst = v;
   }
 }
 
@@ -353,19 +404,22 @@ __global__ void k_first_exceeding(int64_t nb, const double* cand, const double* 
   *out = r;
 }
 
-// C = alpha * sum_z part[z] + beta * C over the split-K slices, in slice
-// order (deterministic).  part: s slices of M x N (ld M).
-__global__ void k_splitk_reduce(int64_t M, int64_t N, int64_t s, const double* __restrict__ part,
-                                double alpha, double beta, double* __restrict__ C, int64_t ldc,
+// C_b = alpha * sum_z part[b][z] + beta * C_b over the split-K slices, in
+// slice order (deterministic).  part: batch x s blocks of M x N (ld M).
+__global__ void k_splitk_reduce(int64_t M, int64_t N, int64_t s, int64_t batch,
+                                const double* __restrict__ part, double alpha, double beta,
+                                double* __restrict__ C, int64_t ldc, int64_t sC,
                                 const int* skip) {
   if (skip && *skip) return;
   const int64_t MN = M * N;
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < MN;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < MN * batch;
        e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = e / MN, r = e % MN;
+    const double* src = part + b * s * MN + r;
     double acc = 0.0;
-    for (int64_t z = 0; z < s; ++z) acc += part[z * MN + e];
-    const int64_t m = e % M, n = e / M;
-    double* dst = C + m + n * ldc;
+    for (int64_t z = 0; z < s; ++z) acc += src[z * MN];
+    const int64_t m = r % M, n = r / M;
+    double* dst = C + b * sC + m + n * ldc;
     double v = alpha * acc;
     if (beta != 0.0) v += beta * *dst;
     *dst = v;
@@ -423,27 +477,39 @@ void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, dou
   TTG_REQUIRE(batch <= 65535, "gemm batch %lld too large", (long long)batch);
   const int64_t gx = (M + BM - 1) / BM, gy = (N + BN - 1) / BN;
   TTG_REQUIRE(gy <= 65535 && gx <= 0x7fffffff, "gemm too large");
-  GemmP p{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta, c->skip, 0};
+  GemmP p{M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, alpha, beta, c->skip, 1, 0, nullptr,
+          nullptr};
   dim3 grid{unsigned(gx), unsigned(gy), unsigned(batch)};
-  // Split-K for products with few output tiles and a long K (inner products
-  // of tall matrices: interface updates, projections): the K range is cut
-  // into slices computed by separate CTAs, then summed in slice order.
+  // Split-K when the output tiles (times the batch) cannot fill the SMs and
+  // K is long: one CTA's FP64 DMMA rate is a small share of the device's, so
+  // a few long-K CTAs (inner products of tall matrices: interface updates,
+  // Gram matrices, projections) would run for about K x 30 ns each.  K is cut
+  // into slices of at least 4 k-tiles so that about two CTAs per SM run.  The
+  // slices of a tile are summed in slice order: by the last slice to finish
+  // when the partials are few (no second launch), else by a reduction kernel
+  // spread over the device (one CTA reading many partials is latency-bound).
   DBuf<double> part;
-  const int64_t tiles = gx * gy;
-  if (batch == 1 && K >= 512 && tiles * 2 < c->num_sms && M * N <= (int64_t(1) << 22)) {
-    int64_t s = std::min<int64_t>(K / 256, std::max<int64_t>(2, 2 * c->num_sms / tiles));
-    s = std::max<int64_t>(2, std::min<int64_t>(s, 64));
-    int64_t kc = (K + s - 1) / s;
-    kc = (kc + BK - 1) / BK * BK;
-    s = (K + kc - 1) / kc;
-    part.reset(c, s * M * N);
-    p.kc = kc;
-    p.C = part.p();
-    p.ldc = M;
-    p.sC = M * N;
-    p.alpha = 1.0;
-    p.beta = 0.0;
-    grid.z = unsigned(s);
+  const int64_t ctas = gx * gy * batch;
+  const int64_t ktiles = (K + BK - 1) / BK;
+  // (A context without an allocator -- the caller-scratch entry point -- runs
+  // every product unsplit.)
+  if (c->alloc && c->d_tile_cnt && ctas < c->num_sms && ktiles >= 8 &&
+      ctas <= GEMM_TILE_COUNTERS) {
+    int64_t s = std::min<int64_t>((2 * c->num_sms + ctas - 1) / ctas, ktiles / 4);
+    if (s * batch > 65535) s = 65535 / batch;
+    if (s >= 2) {
+      const int64_t kc = (ktiles + s - 1) / s * BK;
+      s = (K + kc - 1) / kc;
+      if (s >= 2) {
+        part.reset(c, batch * s * M * N);
+        p.nsplit = s;
+        p.kc = kc;
+        p.part = part.p();
+        const int64_t tile_elems = std::min<int64_t>(M, BM) * std::min<int64_t>(N, BN);
+        if (s * tile_elems <= SPLITK_INKERNEL_MAX) p.cnt = c->d_tile_cnt;
+        grid.z = unsigned(batch * s);
+      }
+    }
   }
   if (!tA && !tB)
     k_gemm_f64<false, false><<<grid, 128, 0, c->stream>>>(p);
@@ -455,9 +521,9 @@ void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, dou
     k_gemm_f64<true, true><<<grid, 128, 0, c->stream>>>(p);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
-  if (p.kc > 0) {
-    k_splitk_reduce<<<grid_for(c, M * N), 256, 0, c->stream>>>(M, N, int64_t(grid.z), part.p(),
-                                                               alpha, beta, C, ldc, c->skip);
+  if (p.nsplit > 1 && !p.cnt) {
+    k_splitk_reduce<<<grid_for(c, M * N * batch), 256, 0, c->stream>>>(
+        M, N, p.nsplit, batch, part.p(), alpha, beta, C, ldc, sC, c->skip);
     c->launches += 1;
     TTG_CHECK_LAUNCH();
   }

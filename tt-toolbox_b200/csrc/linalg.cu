@@ -129,7 +129,8 @@ int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, dou
 
 namespace {
 // Economy SVD of a tall m x n (m >= n) matrix: QR, then one-sided Jacobi SVD
-// of the n x n triangular factor (small_dense.cu), U = Q Ur.
+// of the n x n triangular factor R (small_dense.cu) run on the rows of R
+// (the columns of R^T), U = Q Ur.
 void svd_tall(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
               double* VT) {
   if (m == n) {
@@ -138,7 +139,7 @@ void svd_tall(Context* c, int64_t m, int64_t n, const double* A, double* U, doub
   }
   DBuf<double> Q(c, m * n), R(c, n * n), Ur(c, n * n);
   qr_f64(c, m, n, A, Q.p(), R.p());
-  jacobi_svd_f64(c, n, R.p(), n, Ur.p(), S, VT);
+  jacobi_svd_f64(c, n, R.p(), n, Ur.p(), S, VT, true);
   gemm_f64(c, false, false, m, n, n, 1.0, Q.p(), m, 0, Ur.p(), n, 0, 0.0, U, m, 0, 1);
 }
 }  // namespace

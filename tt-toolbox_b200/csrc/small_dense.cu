@@ -37,10 +37,13 @@ __device__ __forceinline__ int rr_player(int k, int r, int ne) {
 }
 
 // Singular values = column norms of the rotated A, ranked descending
-// (stable on index); U = A diag(1/s), VT = V^T in that order.  One CTA of
-// SD_THREADS; sig: 2n doubles of scratch.
+// (stable on index); U = A diag(1/s), VT = V^T in that order.  With trans the
+// rotated matrix is the transpose of the input (X = In^T = Ux S Vx^T), so the
+// input's factors swap: U = Vx, VT = Ux^T.  One CTA of SD_THREADS; sig: 2n
+// doubles of scratch.
 __device__ void jacobi_finish(int n, const double* A, const double* V, double* __restrict__ U,
-                              double* __restrict__ S, double* __restrict__ VT, double* sig) {
+                              double* __restrict__ S, double* __restrict__ VT, double* sig,
+                              int trans) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int j = warp; j < n; j += SD_WARPS) {
     const double* aj = A + int64_t(j) * n;
@@ -65,8 +68,14 @@ __device__ void jacobi_finish(int n, const double* A, const double* V, double* _
     const int i = e % n, j = e / n;
     const int pos = int(sig[n + j]);
     const double sj = sig[j];
-    U[i + int64_t(pos) * n] = sj > 0.0 ? A[e] / sj : (i == pos ? 1.0 : 0.0);
-    VT[pos + int64_t(i) * n] = V[e];
+    const double ua = sj > 0.0 ? A[e] / sj : (i == pos ? 1.0 : 0.0);
+    if (!trans) {
+      U[i + int64_t(pos) * n] = ua;
+      VT[pos + int64_t(i) * n] = V[e];
+    } else {
+      U[i + int64_t(pos) * n] = V[e];
+      VT[pos + int64_t(i) * n] = ua;
+    }
   }
 }
 
@@ -79,7 +88,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
                                                           double* __restrict__ VT,
                                                           double* __restrict__ Vg,
                                                           double* __restrict__ work, int in_smem,
-                                                          int* err) {
+                                                          int trans, int* err) {
   extern __shared__ double sm[];
   __shared__ double s_off[SD_WARPS];
   __shared__ int s_done;
@@ -90,12 +99,12 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int e = tid; e < n * n; e += SD_THREADS) {
     const int i = e % n, j = e / n;
-    A[e] = Ain[i + int64_t(j) * lda];
+    A[e] = trans ? Ain[j + int64_t(i) * lda] : Ain[i + int64_t(j) * lda];
     V[e] = (i == j) ? 1.0 : 0.0;
   }
   __syncthreads();
   const int ne = (n + 1) & ~1;  // even number of players (dummy column n if odd)
-  const double tol = 4.0 * 2.220446049250313e-16;
+  const double tol = 4.0 * 2.220446049250313e-16, tol2 = tol * tol;
   int sweep = 0;
   for (sweep = 0; sweep < JAC_MAX_SWEEPS; ++sweep) {
     double off = 0.0;
@@ -120,12 +129,14 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
         al = wsum(al);
         be = wsum(be);
         ga = wsum(ga);
-        const double nrm = sqrt(al * be);
-        if (nrm == 0.0 || fabs(ga) <= tol * nrm) continue;
-        off = fmax(off, fabs(ga) / nrm);
+        // |ga| <= tol sqrt(al be), compared in squares (no square root on
+        // the path of a pair that needs no rotation)
+        const double ab = al * be, g2 = ga * ga;
+        if (ab == 0.0 || g2 <= tol2 * ab) continue;
+        off = fmax(off, g2 / ab);
         const double zeta = (be - al) / (2.0 * ga);
         const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        const double c = rsqrt(1.0 + t * t), s = c * t;
         double* vp = V + int64_t(p) * n;
         double* vq = V + int64_t(q) * n;
         for (int i = lane; i < n; i += 32) {
@@ -144,13 +155,13 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
     if (tid == 0) {
       double m = 0.0;
       for (int w = 0; w < SD_WARPS; ++w) m = fmax(m, s_off[w]);
-      s_done = (m <= tol) ? 1 : 0;
+      s_done = (m <= tol2) ? 1 : 0;
     }
     __syncthreads();
     if (s_done) break;
   }
   if (tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(err, 5);
-  jacobi_finish(n, A, V, U, S, VT, work + int64_t(n) * n);
+  jacobi_finish(n, A, V, U, S, VT, work + int64_t(n) * n, trans);
 }
 
 
@@ -199,7 +210,7 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
                                                            int lda, double* A, double* V,
                                                            unsigned* bar,
                                                            unsigned long long* offmax, int* err,
-                                                           int* sweep_err) {
+                                                           int* sweep_err, int trans) {
   __shared__ double red[3][JC_THREADS / 32];
   __shared__ double s_rot[2];
   __shared__ int s_skip;
@@ -208,7 +219,7 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
   for (int64_t e = blockIdx.x * int64_t(JC_THREADS) + tid; e < nn;
        e += int64_t(gridDim.x) * JC_THREADS) {
     const int64_t i = e % n, j = e / n;
-    A[e] = Ain[i + j * lda];
+    A[e] = trans ? Ain[j + i * lda] : Ain[i + j * lda];
     V[e] = (i == j) ? 1.0 : 0.0;
   }
   if (blockIdx.x == 0 && tid < 3) offmax[tid] = 0ull;
@@ -296,8 +307,9 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
 
 __global__ void __launch_bounds__(SD_THREADS) k_jacobi_finish(int n, const double* A,
                                                              const double* V, double* U,
-                                                             double* S, double* VT, double* sig) {
-  jacobi_finish(n, A, V, U, S, VT, sig);
+                                                             double* S, double* VT, double* sig,
+                                                             int trans) {
+  jacobi_finish(n, A, V, U, S, VT, sig, trans);
 }
 
 // Householder QR of the m x n matrix A (column-major, lda) held in shared
@@ -414,37 +426,32 @@ __global__ void __launch_bounds__(SD_THREADS) k_chol_inv(int n, const double* __
   }
   __syncthreads();
   for (int i = tid; i < n; i += SD_THREADS) L[i + n * i] += s_shift;
+  for (int e = tid; e < n * n; e += SD_THREADS) X[e] = (e % n == e / n) ? 1.0 : 0.0;
   __syncthreads();
+  // Right-looking Cholesky G = L L', with the row operations of the forward
+  // elimination L X = I applied to X = I in the same steps (X = L^{-1} at
+  // the end): step j scales column j of L and row j of X by the pivot, then
+  // removes column j from the trailing lower triangle and row j from the rows
+  // of X below it.  Two barriers per column.
   for (int j = 0; j < n; ++j) {
-    if (tid == 0) {
-      const double d = L[j + n * j];
-      if (!(d > 0.0)) s_bad = 1;
-      L[j + n * j] = d > 0.0 ? sqrt(d) : 1.0;
-    }
-    __syncthreads();
-    const double dj = L[j + n * j];
+    const double d = L[j + n * j];
+    const double dj = d > 0.0 ? sqrt(d) : 1.0;
+    if (tid == 0 && !(d > 0.0)) s_bad = 1;
     for (int i = j + 1 + tid; i < n; i += SD_THREADS) L[i + n * j] /= dj;
+    for (int cc = tid; cc <= j; cc += SD_THREADS) X[j + n * cc] /= dj;
     __syncthreads();
     const int m = n - j - 1;
     for (int e = tid; e < m * m; e += SD_THREADS) {
       const int i = j + 1 + e % m, k = j + 1 + e / m;
       if (k <= i) L[i + n * k] -= L[i + n * j] * L[k + n * j];
     }
+    for (int e = tid; e < m * (j + 1); e += SD_THREADS) {
+      const int i = j + 1 + e % m, cc = e / m;
+      X[i + n * cc] -= L[i + n * j] * X[j + n * cc];
+    }
+    if (tid == 0) L[j + n * j] = dj;
     __syncthreads();
   }
-  // X = L^{-1}: column c by forward substitution (one thread per column)
-  for (int c = tid; c < n; c += SD_THREADS) {
-    for (int i = 0; i < n; ++i) {
-      if (i < c) {
-        X[i + n * c] = 0.0;
-        continue;
-      }
-      double v = (i == c) ? 1.0 : 0.0;
-      for (int k = c; k < i; ++k) v -= L[i + n * k] * X[k + n * c];
-      X[i + n * c] = v / L[i + n * i];
-    }
-  }
-  __syncthreads();
   // R = L', Rinv = X' (both upper triangular)
   for (int e = tid; e < n * n; e += SD_THREADS) {
     const int r = e % n, c = e / n;
@@ -484,7 +491,8 @@ void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda
 
 
 void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
-                    double* VT) {
+                    double* VT, bool via_transpose) {
+  int trans = via_transpose ? 1 : 0;
   TTG_REQUIRE(n >= 1 && n <= 4096, "jacobi_svd: n = %lld out of range", (long long)n);
   const size_t mat = size_t(n * n) * sizeof(double);
   const int mode = 2 * mat <= SMEM_LIMIT ? 2 : (mat <= SMEM_LIMIT ? 1 : 0);
@@ -506,11 +514,11 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
     unsigned long long* offp = offmax.p();
     int* errp = c->d_err + 0;
     int* swp = c->d_err + 3;
-    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp};
+    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp, &trans};
     TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_jacobi_coop, dim3(blocks),
                                          dim3(JC_THREADS), args, 0, c->stream));
     k_jacobi_finish<<<1, SD_THREADS, 0, c->stream>>>(int(n), work.p(), V.p(), U, S, VT,
-                                                     work.p() + int64_t(n) * n);
+                                                     work.p() + int64_t(n) * n, trans);
     c->launches += 2;
     TTG_CHECK_LAUNCH();
     return;
@@ -519,7 +527,7 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
                    int(SMEM_LIMIT + 1024));
   const size_t smem = size_t(mode) * mat;
   k_jacobi_svd<<<1, SD_THREADS, smem, c->stream>>>(int(n), A, int(lda), U, S, VT, V.p(),
-                                                    work.p(), mode, c->d_err + 3);
+                                                    work.p(), mode, trans, c->d_err + 3);
   c->launches += 1;
   TTG_CHECK_LAUNCH();
 }
