@@ -433,10 +433,10 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
         axpby_f64(c, N, 1.0, rhs.p(), -1.0, dres.p());
         dot_f64(c, N, dres.p(), nullptr, S.p(Scalars::T0), true);
         scalar_op(c, SC_DIV, S.p(Scalars::RES_PREV), S.p(Scalars::T0), S.p(Scalars::NRHS));
-        double h[2];
-        read_scalars(c, S.p(Scalars::NRHS), h, 1);
-        read_scalars(c, S.p(Scalars::T0), h + 1, 1);
-        const double norm_rhs = h[0], nres = h[1];
+        // one read of the slots NRHS .. T0
+        double h[Scalars::T0 - Scalars::NRHS + 1];
+        read_scalars(c, S.p(Scalars::NRHS), h, int(Scalars::T0 - Scalars::NRHS + 1));
+        const double norm_rhs = h[0], nres = h[Scalars::T0 - Scalars::NRHS];
         if (norm_rhs > 0) {                                               // :497
           LocalSolveResult lr = local_solve_from_residual(
               c, md, Phi1, A1, Phi2, rhs.p(), dres.p(), nres, norm_rhs, real_tol, sol_prev,

@@ -1,4 +1,5 @@
 // Context, caching allocator, error reporting and TT handles of libttgpu.
+#include <cstdlib>
 #include <cstdarg>
 #include <cstring>
 #include <mutex>
@@ -100,6 +101,8 @@ void context_init(Context& c, int device) {
   TTG_CUDA(cudaMemset(c.d_tile_cnt, 0, GEMM_TILE_COUNTERS * sizeof(unsigned)));
   TTG_CUDA(cudaEventCreate(&c.ev0));
   TTG_CUDA(cudaEventCreate(&c.ev1));
+  const char* pdl = getenv("TTG_PDL");  // TTG_PDL=0: plain stream-ordered launches
+  c.pdl = !(pdl && pdl[0] == '0');
 }
 
 void context_release(Context& c) {

@@ -15,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/ttgpu.h"
@@ -137,6 +138,9 @@ struct Context {
   double mv_flops[2] = {0.0, 0.0};
   // Optional CUDA-event timing of every local matvec on the context stream.
   bool time_matvec = false;
+  // Launch the library's stream-ordered kernels as programmatic dependent
+  // launches (see launch()); off for contexts on a caller's stream.
+  bool pdl = false;
   struct EvPair {
     cudaEvent_t a, b;
     int kind;
@@ -217,6 +221,40 @@ void DBuf<T>::release() {
 }
 
 void set_last_error(const char* msg);
+
+// Programmatic dependent launch.  A kernel launched by launch() may be
+// scheduled while its predecessor on the stream is still running: the
+// predecessor lets it start with pdl_trigger() once all of its own CTAs
+// run, and the kernel itself must call pdl_wait() before its first access
+// to global memory (pdl_wait returns when the predecessor grid has
+// completed and its writes are visible; it is a no-op for a kernel launched
+// without the attribute).  Every kernel launched through launch() therefore
+// starts with pdl_begin(): it waits, then lets its own successor be
+// scheduled.  This hides the kernel-to-kernel launch latency of the long
+// chains of short kernels in a sweep.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#endif
+
+template <typename... KArgs, typename... Args>
+void launch(Context* c, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+            Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = c->pdl ? 1 : 0;
+  TTG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+  c->launches += 1;
+}
 
 #define TTG_API_BEGIN try {
 #define TTG_API_END                                    \

@@ -25,6 +25,7 @@ constexpr int GJ_THREADS = 256;
 
 __global__ void k_diag_phi1(int64_t rx1, int64_t ra1, const double* __restrict__ Phi1,
                             double* __restrict__ d1) {
+  pdl_begin();
   const int64_t total = rx1 * ra1;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -35,6 +36,7 @@ __global__ void k_diag_phi1(int64_t rx1, int64_t ra1, const double* __restrict__
 
 __global__ void k_diag_phi2(int64_t rx2, int64_t ra2, const double* __restrict__ Phi2,
                             double* __restrict__ d2) {
+  pdl_begin();
   const int64_t total = ra2 * rx2;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -48,6 +50,7 @@ __global__ void k_diag_phi2(int64_t rx2, int64_t ra2, const double* __restrict__
 __global__ void __launch_bounds__(GJ_THREADS) k_block_inv(int64_t rx1, int n,
                                                           double* __restrict__ J,
                                                           int* __restrict__ err) {
+  pdl_begin();
   extern __shared__ double a[];  // n x n, a[r + n c]
   __shared__ double f[JAC_MAX_N], g[JAC_MAX_N];
   __shared__ int piv[JAC_MAX_N];
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(GJ_THREADS) k_block_inv(int64_t rx1, int n,
 // y[i, j, k] = sum_m J[i, j, m, k] x[i, m, k]; threads over (i, j, k), i fastest.
 __global__ void k_jac_apply_c(int64_t rx1, int64_t n, int64_t rx2, const double* __restrict__ J,
                               const double* __restrict__ x, double* __restrict__ y) {
+  pdl_begin();
   const int64_t total = rx1 * n * rx2;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -163,9 +167,8 @@ void jac_gen_c_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
               (long long)JAC_MAX_N);
   TTG_REQUIRE(rx1 * rx2 <= int64_t(0x7fffffff), "cjacobi: too many blocks");
   DBuf<double> d1(c, rx1 * ra1), d2(c, ra2 * rx2), G(c, rx1 * n * n * ra2);
-  k_diag_phi1<<<blocks_for(c, rx1 * ra1), 256, 0, c->stream>>>(rx1, ra1, Phi1, d1.p());
-  k_diag_phi2<<<blocks_for(c, ra2 * rx2), 256, 0, c->stream>>>(rx2, ra2, Phi2, d2.p());
-  c->launches += 2;
+  launch(c, k_diag_phi1, blocks_for(c, rx1 * ra1), 256, 0, rx1, ra1, Phi1, d1.p());
+  launch(c, k_diag_phi2, blocks_for(c, ra2 * rx2), 256, 0, rx2, ra2, Phi2, d2.p());
   TTG_CHECK_LAUNCH();
   // G[i, (j, m, be)] = sum_al d1[i, al] A[al, (j, m, be)]
   gemm_f64(c, false, false, rx1, n * n * ra2, ra1, 1.0, d1.p(), rx1, 0, A, ra1, 0, 0.0, G.p(),
@@ -175,15 +178,13 @@ void jac_gen_c_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
            0.0, J, rx1 * n * n, 0, 1);
   const size_t smem = sizeof(double) * size_t(n) * size_t(n);
   ensure_smem_attr(reinterpret_cast<const void*>(k_block_inv), c->device, int(smem));
-  k_block_inv<<<unsigned(rx1 * rx2), GJ_THREADS, smem, c->stream>>>(rx1, int(n), J, c->d_err + 4);
-  c->launches += 1;
+  launch(c, k_block_inv, unsigned(rx1 * rx2), GJ_THREADS, smem, rx1, int(n), J, c->d_err + 4);
   TTG_CHECK_LAUNCH();
 }
 
 void jac_apply_c_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, const double* J,
                      const double* x, double* y) {
-  k_jac_apply_c<<<blocks_for(c, rx1 * n * rx2), 256, 0, c->stream>>>(rx1, n, rx2, J, x, y);
-  c->launches += 1;
+  launch(c, k_jac_apply_c, blocks_for(c, rx1 * n * rx2), 256, 0, rx1, n, rx2, J, x, y);
   TTG_CHECK_LAUNCH();
 }
 

@@ -42,6 +42,7 @@ struct GemmP {
 
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
+  pdl_begin();
   __shared__ double As[2][BK][BM + PADS];
   __shared__ double Bs[2][BK][BN + PADS];
   if (p.skip && *p.skip) return;
@@ -239,6 +240,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 __global__ void k_reduce_fused(int64_t n, const double* __restrict__ x,
                                const double* __restrict__ y, int mode, double* __restrict__ part,
                                unsigned* counter, double* out, int do_sqrt) {
+  pdl_begin();
   __shared__ double sh[32];
   __shared__ bool last;
   double s = 0.0;
@@ -278,10 +280,8 @@ void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int 
   int nb = int(std::min<int64_t>((n + RED_THREADS * 4 - 1) / (RED_THREADS * 4), RED_MAX_BLOCKS));
   if (nb < 1) nb = 1;
   DBuf<double> part(c, nb);
-  k_reduce_fused<<<nb, RED_THREADS, 0, c->stream>>>(n, x, y, mode, part.p(),
-                                                    reinterpret_cast<unsigned*>(c->d_err + 63),
-                                                    out, do_sqrt ? 1 : 0);
-  c->launches += 1;
+  launch(c, k_reduce_fused, nb, RED_THREADS, 0, n, x, y, mode, part.p(),
+         reinterpret_cast<unsigned*>(c->d_err + 63), out, do_sqrt ? 1 : 0);
   TTG_CHECK_LAUNCH();
 }
 
@@ -291,6 +291,7 @@ void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int 
 
 __global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b,
                         double* __restrict__ y) {
+  pdl_begin();
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = (b == 0.0 ? 0.0 : b * y[i]) + a * x[i];
@@ -298,13 +299,22 @@ __global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, doubl
 
 __global__ void k_scale_dev(int64_t n, const double* __restrict__ x, double* __restrict__ y,
                             const double* num, const double* den) {
+  pdl_begin();
   const double s = (num ? *num : 1.0) / (den ? *den : 1.0);
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = x[i] * s;
 }
 
+__global__ void k_copy(int64_t n, const double* __restrict__ x, double* __restrict__ y) {
+  pdl_begin();
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = x[i];
+}
+
 __global__ void k_fill(int64_t n, double v, double* y) {
+  pdl_begin();
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = v;
@@ -313,6 +323,7 @@ __global__ void k_fill(int64_t n, double v, double* y) {
 __global__ void k_transpose(int64_t rows, int64_t cols, const double* __restrict__ in,
                             int64_t ldi, int64_t si, double* __restrict__ out, int64_t ldo,
                             int64_t so) {
+  pdl_begin();
   __shared__ double tile[32][33];
   const int64_t b = blockIdx.z;
   in += b * si;
@@ -331,6 +342,7 @@ __global__ void k_transpose(int64_t rows, int64_t cols, const double* __restrict
 
 __global__ void k_copy2d(int64_t rows, int64_t cols, const double* __restrict__ in, int64_t ldi,
                          double* __restrict__ out, int64_t ldo, const double* scale_col) {
+  pdl_begin();
   const int64_t total = rows * cols;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
        i += int64_t(gridDim.x) * blockDim.x) {
@@ -350,6 +362,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 }
 
 __global__ void k_randn(int64_t n, uint64_t seed, uint64_t offset, double* y) {
+  pdl_begin();
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
     const uint64_t h1 = mix64(seed ^ mix64(2 * (offset + i)));
@@ -361,6 +374,7 @@ __global__ void k_randn(int64_t n, uint64_t seed, uint64_t offset, double* y) {
 }
 
 __global__ void k_normalize_by(int64_t n, double* __restrict__ x, double* nrm) {
+  pdl_begin();
   const double v = *nrm;
   const double s = v > 0.0 ? 1.0 / v : 1.0;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
@@ -372,6 +386,7 @@ __global__ void k_normalize_by(int64_t n, double* __restrict__ x, double* nrm) {
 
 __global__ void k_axpby_dev(int64_t n, double a, const double* __restrict__ x,
                             const double* __restrict__ b, double* __restrict__ y) {
+  pdl_begin();
   const double bv = *b;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
@@ -380,6 +395,7 @@ __global__ void k_axpby_dev(int64_t n, double a, const double* __restrict__ x,
 
 __global__ void k_scalar_op(int op, double* out, const double* p0, const double* p1,
                             const double* p2, double k) {
+  pdl_begin();
   switch (op) {
     case 0: *out = *p0 / *p1; break;
     case 1: *out = fmax(*out, *p0); break;
@@ -394,6 +410,7 @@ __global__ void k_scalar_op(int op, double* out, const double* p0, const double*
 
 __global__ void k_first_exceeding(int64_t nb, const double* cand, const double* den,
                                   const double* thr, double* out) {
+  pdl_begin();
   double r = -1.0;
   for (int64_t b = 0; b < nb; ++b) {
     if (cand[b] / *den > *thr) {
@@ -410,6 +427,7 @@ __global__ void k_splitk_reduce(int64_t M, int64_t N, int64_t s, int64_t batch,
                                 const double* __restrict__ part, double alpha, double beta,
                                 double* __restrict__ C, int64_t ldc, int64_t sC,
                                 const int* skip) {
+  pdl_begin();
   if (skip && *skip) return;
   const int64_t MN = M * N;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < MN * batch;
@@ -429,6 +447,7 @@ __global__ void k_splitk_reduce(int64_t M, int64_t N, int64_t s, int64_t batch,
 // *keep = 1 when every column j kept G1[j,j] > tau^2 G0[j,j] (one thread).
 __global__ void k_collapse_flag(int64_t k, const double* G0, int64_t ld0, const double* G1,
                                 int64_t ld1, double tau, int* keep) {
+  pdl_begin();
   int ok = 1;
   for (int64_t j = 0; j < k; ++j)
     if (!(G1[j + j * ld1] > tau * tau * G0[j + j * ld0])) ok = 0;
@@ -437,6 +456,7 @@ __global__ void k_collapse_flag(int64_t k, const double* G0, int64_t ld0, const 
 
 // *flag |= 1 when max |G - I| > tol (G: n x n Gram matrix of a basis).
 __global__ void k_orth_check(int64_t n, const double* G, double tol, int* flag) {
+  pdl_begin();
   int bad = 0;
   for (int64_t e = threadIdx.x; e < n * n; e += blockDim.x) {
     const double v = G[e] - ((e % n) == (e / n) ? 1.0 : 0.0);
@@ -446,6 +466,7 @@ __global__ void k_orth_check(int64_t n, const double* G, double tol, int* flag) 
 }
 
 __global__ void k_accumulate_info(const int* info, int* err_slot) {
+  pdl_begin();
   if (*info != 0) atomicOr(err_slot, 1);
 }
 
@@ -512,19 +533,17 @@ void gemm_f64(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, dou
     }
   }
   if (!tA && !tB)
-    k_gemm_f64<false, false><<<grid, 128, 0, c->stream>>>(p);
+    launch(c, k_gemm_f64<false, false>, grid, 128, 0, p);
   else if (!tA && tB)
-    k_gemm_f64<false, true><<<grid, 128, 0, c->stream>>>(p);
+    launch(c, k_gemm_f64<false, true>, grid, 128, 0, p);
   else if (tA && !tB)
-    k_gemm_f64<true, false><<<grid, 128, 0, c->stream>>>(p);
+    launch(c, k_gemm_f64<true, false>, grid, 128, 0, p);
   else
-    k_gemm_f64<true, true><<<grid, 128, 0, c->stream>>>(p);
-  c->launches += 1;
+    launch(c, k_gemm_f64<true, true>, grid, 128, 0, p);
   TTG_CHECK_LAUNCH();
   if (p.nsplit > 1 && !p.cnt) {
-    k_splitk_reduce<<<grid_for(c, M * N * batch), 256, 0, c->stream>>>(
-        M, N, p.nsplit, batch, part.p(), alpha, beta, C, ldc, sC, c->skip);
-    c->launches += 1;
+    launch(c, k_splitk_reduce, grid_for(c, M * N * batch), 256, 0, M, N, p.nsplit, batch,
+           part.p(), alpha, beta, C, ldc, sC, c->skip);
     TTG_CHECK_LAUNCH();
   }
 }
@@ -548,29 +567,29 @@ double nrm2_host(Context* c, int64_t n, const double* x) {
 
 void axpby_f64(Context* c, int64_t n, double a, const double* x, double b, double* y) {
   if (n <= 0) return;
-  k_axpby<<<grid_for(c, n), 256, 0, c->stream>>>(n, a, x, b, y);
-  c->launches += 1;
+  launch(c, k_axpby, grid_for(c, n), 256, 0, n, a, x, b, y);
   TTG_CHECK_LAUNCH();
 }
 
 void scale_dev_f64(Context* c, int64_t n, const double* x, double* y, const double* num,
                    const double* den) {
   if (n <= 0) return;
-  k_scale_dev<<<grid_for(c, n), 256, 0, c->stream>>>(n, x, y, num, den);
-  c->launches += 1;
+  launch(c, k_scale_dev, grid_for(c, n), 256, 0, n, x, y, num, den);
   TTG_CHECK_LAUNCH();
 }
 
 void fill_f64(Context* c, int64_t n, double v, double* y) {
   if (n <= 0) return;
-  k_fill<<<grid_for(c, n), 256, 0, c->stream>>>(n, v, y);
-  c->launches += 1;
+  launch(c, k_fill, grid_for(c, n), 256, 0, n, v, y);
   TTG_CHECK_LAUNCH();
 }
 
 void copy_f64(Context* c, int64_t n, const double* x, double* y) {
   if (n <= 0 || x == y) return;
-  TTG_CUDA(cudaMemcpyAsync(y, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  // a kernel rather than a memcpy node, so that it chains with its
+  // neighbours as a programmatic dependent launch
+  launch(c, k_copy, grid_for(c, n), 256, 0, n, x, y);
+  TTG_CHECK_LAUNCH();
 }
 
 void transpose_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_t ldi,
@@ -578,71 +597,61 @@ void transpose_f64(Context* c, int64_t rows, int64_t cols, const double* in, int
   if (rows <= 0 || cols <= 0 || batch <= 0) return;
   TTG_REQUIRE((cols + 31) / 32 <= 65535 && batch <= 65535, "transpose too large");
   dim3 grid{unsigned((rows + 31) / 32), unsigned((cols + 31) / 32), unsigned(batch)};
-  k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(rows, cols, in, ldi, si, out, ldo, so);
-  c->launches += 1;
+  launch(c, k_transpose, grid, dim3(32, 8), 0, rows, cols, in, ldi, si, out, ldo, so);
   TTG_CHECK_LAUNCH();
 }
 
 void copy2d_f64(Context* c, int64_t rows, int64_t cols, const double* in, int64_t ldi,
                 double* out, int64_t ldo, const double* scale_col) {
   if (rows <= 0 || cols <= 0) return;
-  k_copy2d<<<grid_for(c, rows * cols), 256, 0, c->stream>>>(rows, cols, in, ldi, out, ldo,
-                                                            scale_col);
-  c->launches += 1;
+  launch(c, k_copy2d, grid_for(c, rows * cols), 256, 0, rows, cols, in, ldi, out, ldo,
+         scale_col);
   TTG_CHECK_LAUNCH();
 }
 
 void normalize_by_dev(Context* c, int64_t n, double* x, double* nrm) {
   if (n <= 0) return;
-  k_normalize_by<<<grid_for(c, n), 256, 0, c->stream>>>(n, x, nrm);
-  c->launches += 1;
+  launch(c, k_normalize_by, grid_for(c, n), 256, 0, n, x, nrm);
   TTG_CHECK_LAUNCH();
 }
 
 void axpby_dev(Context* c, int64_t n, double a, const double* x, const double* b, double* y) {
   if (n <= 0) return;
-  k_axpby_dev<<<grid_for(c, n), 256, 0, c->stream>>>(n, a, x, b, y);
-  c->launches += 1;
+  launch(c, k_axpby_dev, grid_for(c, n), 256, 0, n, a, x, b, y);
   TTG_CHECK_LAUNCH();
 }
 
 void scalar_op(Context* c, int op, double* out, const double* p0, const double* p1,
                const double* p2, double k) {
-  k_scalar_op<<<1, 1, 0, c->stream>>>(op, out, p0, p1, p2, k);
-  c->launches += 1;
+  launch(c, k_scalar_op, 1, 1, 0, op, out, p0, p1, p2, k);
   TTG_CHECK_LAUNCH();
 }
 
 void first_exceeding(Context* c, int64_t nb, const double* cand, const double* den,
                      const double* thr, double* out) {
-  k_first_exceeding<<<1, 1, 0, c->stream>>>(nb, cand, den, thr, out);
-  c->launches += 1;
+  launch(c, k_first_exceeding, 1, 1, 0, nb, cand, den, thr, out);
   TTG_CHECK_LAUNCH();
 }
 
 void collapse_flag(Context* c, int64_t k, const double* G0, int64_t ld0, const double* G1,
                    int64_t ld1, double tau, int* keep) {
-  k_collapse_flag<<<1, 1, 0, c->stream>>>(k, G0, ld0, G1, ld1, tau, keep);
-  c->launches += 1;
+  launch(c, k_collapse_flag, 1, 1, 0, k, G0, ld0, G1, ld1, tau, keep);
   TTG_CHECK_LAUNCH();
 }
 
 void orth_check(Context* c, int64_t n, const double* G, double tol, int* flag) {
-  k_orth_check<<<1, 256, 0, c->stream>>>(n, G, tol, flag);
-  c->launches += 1;
+  launch(c, k_orth_check, 1, 256, 0, n, G, tol, flag);
   TTG_CHECK_LAUNCH();
 }
 
 void accumulate_info(Context* c, const int* info, int* err_slot) {
-  k_accumulate_info<<<1, 1, 0, c->stream>>>(info, err_slot);
-  c->launches += 1;
+  launch(c, k_accumulate_info, 1, 1, 0, info, err_slot);
   TTG_CHECK_LAUNCH();
 }
 
 void randn_f64(Context* c, int64_t n, uint64_t seed, uint64_t offset, double* y) {
   if (n <= 0) return;
-  k_randn<<<grid_for(c, n), 256, 0, c->stream>>>(n, seed, offset, y);
-  c->launches += 1;
+  launch(c, k_randn, grid_for(c, n), 256, 0, n, seed, offset, y);
   TTG_CHECK_LAUNCH();
 }
 

@@ -9,6 +9,7 @@ namespace {
 
 __global__ void k_triu(int64_t k, int64_t n, const double* __restrict__ A, int64_t lda,
                        double* __restrict__ R) {
+  pdl_begin();
   const int64_t total = k * n;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -47,8 +48,7 @@ void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t
   if (k <= 0 || n <= 0) return;
   int64_t blocks = (k * n + 255) / 256;
   if (blocks > int64_t(c->num_sms) * 8) blocks = int64_t(c->num_sms) * 8;
-  k_triu<<<unsigned(blocks), 256, 0, c->stream>>>(k, n, A, lda, R);
-  c->launches += 1;
+  launch(c, k_triu, unsigned(blocks), 256, 0, k, n, A, lda, R);
   TTG_CHECK_LAUNCH();
 }
 

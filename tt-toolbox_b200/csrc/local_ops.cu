@@ -86,6 +86,7 @@ namespace {
 __global__ void k_assemble(int64_t rx1, int64_t n, int64_t rx2, int64_t ra1, int64_t ra2,
                            const double* __restrict__ Phi1, const double* __restrict__ A,
                            const double* __restrict__ Phi2, double* __restrict__ B) {
+  pdl_begin();
   const int64_t N = rx1 * n * rx2;
   const int64_t total = N * N;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
@@ -113,8 +114,7 @@ void assemble_local_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t
   int64_t blocks = (N * N + 255) / 256;
   if (blocks > int64_t(c->num_sms) * 8) blocks = int64_t(c->num_sms) * 8;
   if (blocks < 1) blocks = 1;
-  k_assemble<<<unsigned(blocks), 256, 0, c->stream>>>(rx1, n, rx2, ra1, ra2, Phi1, A, Phi2, B);
-  c->launches += 1;
+  launch(c, k_assemble, unsigned(blocks), 256, 0, rx1, n, rx2, ra1, ra2, Phi1, A, Phi2, B);
   TTG_CHECK_LAUNCH();
 }
 
@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(CN_THREADS) k_cumnorm(int64_t N, int cnt,
                                                          double* __restrict__ R,
                                                          const double* __restrict__ W,
                                                          double* __restrict__ part) {
+  pdl_begin();
   double acc2[CUMNORM_MAXC];
 #pragma unroll
   for (int b = 0; b < CUMNORM_MAXC; ++b) acc2[b] = 0.0;
@@ -196,6 +197,7 @@ __global__ void __launch_bounds__(CN_THREADS) k_cumnorm(int64_t N, int cnt,
 // shuffle tree (deterministic).
 __global__ void k_cumnorm_final(int nblk, int cnt, const double* __restrict__ part,
                                 double* __restrict__ out) {
+  pdl_begin();
   const int b = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (b >= cnt) return;
   double x = 0.0;
@@ -211,9 +213,8 @@ void cumulative_norms_f64(Context* c, int64_t N, int64_t cnt, double* R, const d
   TTG_REQUIRE(cnt >= 1 && cnt <= CUMNORM_MAXC, "cumulative_norms: cnt %lld", (long long)cnt);
   int64_t nb = (N + CN_THREADS - 1) / CN_THREADS;
   nb = std::max<int64_t>(1, std::min<int64_t>(nb, int64_t(c->num_sms) * 4));
-  k_cumnorm<<<unsigned(nb), CN_THREADS, 0, c->stream>>>(N, int(cnt), R, W, part);
-  k_cumnorm_final<<<1, 32 * CUMNORM_MAXC, 0, c->stream>>>(int(nb), int(cnt), part, out);
-  c->launches += 2;
+  launch(c, k_cumnorm, unsigned(nb), CN_THREADS, 0, N, int(cnt), R, W, part);
+  launch(c, k_cumnorm_final, 1, 32 * CUMNORM_MAXC, 0, int(nb), int(cnt), part, out);
   TTG_CHECK_LAUNCH();
 }
 

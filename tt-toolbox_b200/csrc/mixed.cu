@@ -241,6 +241,7 @@ __global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r
 
 // x += V(:, 0:k) y with H(0:k,0:k) y = g(0:k) (upper triangular after Givens).
 __global__ void k_ar_update(ArArgs a, int k, float* x) {
+  pdl_begin();
   extern __shared__ double y[];
   if (threadIdx.x == 0) {
     for (int row = k - 1; row >= 0; --row) {
@@ -260,6 +261,7 @@ __global__ void k_ar_update(ArArgs a, int k, float* x) {
 
 // r = b - y (FP32)
 __global__ void k_sub_f32(int64_t n, const float* b, const float* y, float* r) {
+  pdl_begin();
   AR_LOOP(i, n) r[i] = b[i] - y[i];
 }
 
@@ -329,8 +331,7 @@ struct Gmres32 {
       const float* rr = b;
       if (it > 0) {
         op.apply(c, x, w.p());
-        k_sub_f32<<<blocks, AR_THREADS, 0, c->stream>>>(sz, b, w.p(), r.p());
-        c->launches += 1;
+        launch(c, k_sub_f32, blocks, AR_THREADS, 0, sz, b, w.p(), r.p());
         rr = r.p();
       }
       void* ai[] = {&a, &rr};
@@ -370,8 +371,7 @@ struct Gmres32 {
       guard.release();
       steps += conv ? j + 1 : m;
       const int k = conv ? j + 1 : m;
-      k_ar_update<<<blocks, AR_THREADS, sizeof(double) * (m + 1), c->stream>>>(a, k, x);
-      c->launches += 1;
+      launch(c, k_ar_update, blocks, AR_THREADS, sizeof(double) * (m + 1), a, k, x);
       TTG_CHECK_LAUNCH();
       if (conv) break;
     }

@@ -61,6 +61,7 @@ template <int BN, bool OUT_BF16>
 __global__ void __launch_bounds__(128, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 int K, int a_rows_pb, int b_rows_pb, OutMap om, int* err, const int* skip) {
+  pdl_begin();
   using namespace umma;
   if (skip && *skip) return;  // queued Krylov step after convergence
   constexpr int B_BYTES = BN * UM_BK * 2;
@@ -180,6 +181,7 @@ __global__ void __launch_bounds__(128, 1)
 // Phi2b[b + ldp*col] = Phi2[b, col], col = (be, k)  (zero padding b >= rx2)
 __global__ void k_cvt_phi2(int64_t rx2, int64_t ncols, int64_t ldp, const double* __restrict__ P,
                            __nv_bfloat16* __restrict__ out) {
+  pdl_begin();
   const int64_t total = ldp * ncols;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -191,6 +193,7 @@ __global__ void k_cvt_phi2(int64_t rx2, int64_t ncols, int64_t ldp, const double
 // AT[(m + n*be) + ld1*(al + ra1*j)] = A[al, j, m, be]
 __global__ void k_cvt_AT(int64_t ra1, int64_t n, int64_t ra2, int64_t ld1,
                          const double* __restrict__ A, __nv_bfloat16* __restrict__ out) {
+  pdl_begin();
   const int64_t total = ld1 * ra1 * n;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -207,6 +210,7 @@ __global__ void k_cvt_AT(int64_t ra1, int64_t n, int64_t ra2, int64_t ld1,
 // Phi1T[(a + rx1*al) + ld2*i] = Phi1[i, a, al]
 __global__ void k_cvt_phi1(int64_t ry1, int64_t rx1, int64_t ra1, int64_t ld2,
                            const double* __restrict__ P, __nv_bfloat16* __restrict__ out) {
+  pdl_begin();
   const int64_t total = ld2 * ry1;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -223,6 +227,7 @@ __global__ void k_cvt_phi1(int64_t ry1, int64_t rx1, int64_t ra1, int64_t ld2,
 // X[b + ldx*row] = v[b + rx2*row]  (row = m + n*a; zero padding)
 __global__ void k_cvt_x(int64_t rx2, int64_t rows, int64_t ldx, const float* __restrict__ v,
                         __nv_bfloat16* __restrict__ out, const int* skip) {
+  pdl_begin();
   if (skip && *skip) return;
   const int64_t total = ldx * rows;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
@@ -235,6 +240,7 @@ __global__ void k_cvt_x(int64_t rx2, int64_t rows, int64_t ldx, const float* __r
 // Natural [i, j, k] (FP64) <-> reversed [k, j, i] (FP32) vector layouts.
 __global__ void k_nat_to_rev(int64_t r1, int64_t n, int64_t r2, const double* __restrict__ x,
                              float* __restrict__ y, double scale) {
+  pdl_begin();
   const int64_t total = r1 * n * r2;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -245,6 +251,7 @@ __global__ void k_nat_to_rev(int64_t r1, int64_t n, int64_t r2, const double* __
 
 __global__ void k_rev_to_nat_add(int64_t r1, int64_t n, int64_t r2, const float* __restrict__ y,
                                  double* __restrict__ x, double scale) {
+  pdl_begin();
   const int64_t total = r1 * n * r2;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
@@ -294,9 +301,8 @@ void launch_bn(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t
   const size_t smem = umma_smem_bytes<BN>();
   ensure_smem_attr(reinterpret_cast<const void*>(k_umma_gemm<BN, OB>), c->device, int(smem));
   dim3 grid{unsigned((M + UM_BM - 1) / UM_BM), unsigned((N + BN - 1) / BN), unsigned(batch)};
-  k_umma_gemm<BN, OB><<<grid, 128, smem, c->stream>>>(ta, tb, int(K), int(a_rows_pb),
-                                                      int(b_rows_pb), om, c->d_err + 1, c->skip);
-  c->launches += 1;
+  launch(c, k_umma_gemm<BN, OB>, grid, 128, smem, ta, tb, int(K), int(a_rows_pb),
+         int(b_rows_pb), om, c->d_err + 1, c->skip);
   TTG_CHECK_LAUNCH();
 }
 
@@ -350,12 +356,11 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
     TTG_CUDA(cudaMemsetAsync(X.p(), 0, sizeof(__nv_bfloat16) * X.size(), c->stream));
   T1.reset(c, ld1 * d.rx1 * d.ry2);
   T2.reset(c, ld2 * d.ry2 * d.n);
-  k_cvt_phi2<<<blocks_for(c, phi2b.size()), 256, 0, c->stream>>>(d.rx2, d.ra2 * d.ry2, ldx, Phi2,
-                                                                 phi2b.p());
-  k_cvt_AT<<<blocks_for(c, AT.size()), 256, 0, c->stream>>>(d.ra1, d.n, d.ra2, ld1, A, AT.p());
-  k_cvt_phi1<<<blocks_for(c, phi1T.size()), 256, 0, c->stream>>>(d.ry1, d.rx1, d.ra1, ld2, Phi1,
-                                                                 phi1T.p());
-  c->launches += 3;
+  launch(c, k_cvt_phi2, blocks_for(c, phi2b.size()), 256, 0, d.rx2, d.ra2 * d.ry2, ldx, Phi2,
+         phi2b.p());
+  launch(c, k_cvt_AT, blocks_for(c, AT.size()), 256, 0, d.ra1, d.n, d.ra2, ld1, A, AT.p());
+  launch(c, k_cvt_phi1, blocks_for(c, phi1T.size()), 256, 0, d.ry1, d.rx1, d.ra1, ld2, Phi1,
+         phi1T.p());
   TTG_CHECK_LAUNCH();
   make_map(&mapX, X.p(), d.rx2, d.m * d.rx1, ldx, UM_BM);
   make_map(&mapT1, T1.p(), d.n * d.ra2, d.rx1 * d.ry2, ld1, UM_BM);
@@ -477,8 +482,7 @@ int MixedOp::tuned_bn(Context* c, int stage) {
 void MixedOp::apply(Context* c, const float* v, float* y) {
   MvTiming timing(c, 1);
   const int64_t rows = d.m * d.rx1;
-  k_cvt_x<<<blocks_for(c, ldx * rows), 256, 0, c->stream>>>(d.rx2, rows, ldx, v, X.p(), c->skip);
-  c->launches += 1;
+  launch(c, k_cvt_x, blocks_for(c, ldx * rows), 256, 0, d.rx2, rows, ldx, v, X.p(), c->skip);
   TTG_CHECK_LAUNCH();
   stages(c, y);
 }
@@ -500,15 +504,13 @@ void MixedOp::stages(Context* c, float* y) {
 
 void nat_to_rev(Context* c, int64_t r1, int64_t n, int64_t r2, const double* x, float* y,
                 double scale) {
-  k_nat_to_rev<<<blocks_for(c, r1 * n * r2), 256, 0, c->stream>>>(r1, n, r2, x, y, scale);
-  c->launches += 1;
+  launch(c, k_nat_to_rev, blocks_for(c, r1 * n * r2), 256, 0, r1, n, r2, x, y, scale);
   TTG_CHECK_LAUNCH();
 }
 
 void rev_to_nat_add(Context* c, int64_t r1, int64_t n, int64_t r2, const float* y, double* x,
                     double scale) {
-  k_rev_to_nat_add<<<blocks_for(c, r1 * n * r2), 256, 0, c->stream>>>(r1, n, r2, y, x, scale);
-  c->launches += 1;
+  launch(c, k_rev_to_nat_add, blocks_for(c, r1 * n * r2), 256, 0, r1, n, r2, y, x, scale);
   TTG_CHECK_LAUNCH();
 }
 

@@ -31,9 +31,12 @@ __device__ __forceinline__ double wsum(double v) {
 }
 
 // Column index of slot k in round r of a round-robin tournament on ne (even)
-// players: slot 0 is fixed, the others rotate.
+// players: slot 0 is fixed, the others rotate.  k - 1 + r < 2 (ne - 1), so a
+// conditional subtraction replaces the modulo.
 __device__ __forceinline__ int rr_player(int k, int r, int ne) {
-  return k == 0 ? 0 : 1 + ((k - 1 + r) % (ne - 1));
+  int x = k - 1 + r;
+  if (x >= ne - 1) x -= ne - 1;
+  return k == 0 ? 0 : 1 + x;
 }
 
 // Singular values = column norms of the rotated A, ranked descending
@@ -89,6 +92,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
                                                           double* __restrict__ Vg,
                                                           double* __restrict__ work, int in_smem,
                                                           int trans, int* err) {
+  pdl_begin();
   extern __shared__ double sm[];
   __shared__ double s_off[SD_WARPS];
   __shared__ int s_done;
@@ -134,8 +138,12 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
         const double ab = al * be, g2 = ga * ga;
         if (ab == 0.0 || g2 <= tol2 * ab) continue;
         off = fmax(off, g2 / ab);
-        const double zeta = (be - al) / (2.0 * ga);
-        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = (be - al) / (2 ga),
+        // written with one division: t = sign(zeta) |g| / (|dd| + hypot(dd, g))
+        // for dd = be - al, g = 2 ga (sign(zeta) = +1 when dd = 0).
+        const double dd = be - al, gg = 2.0 * ga;
+        const double sg = ((dd >= 0.0) == (gg > 0.0) || dd == 0.0) ? 1.0 : -1.0;
+        const double t = sg * fabs(gg) / (fabs(dd) + sqrt(dd * dd + gg * gg));
         const double c = rsqrt(1.0 + t * t), s = c * t;
         double* vp = V + int64_t(p) * n;
         double* vq = V + int64_t(q) * n;
@@ -309,6 +317,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_finish(int n, const doubl
                                                              const double* V, double* U,
                                                              double* S, double* VT, double* sig,
                                                              int trans) {
+  pdl_begin();
   jacobi_finish(n, A, V, U, S, VT, sig, trans);
 }
 
@@ -318,6 +327,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_house_qr(int m, int n, const dou
                                                         int lda, double* __restrict__ Q,
                                                         double* __restrict__ R,
                                                         const int* skip) {
+  pdl_begin();
   if (skip && *skip) return;  // conditional factorization (Context::skip)
   const int ldr = m < n ? m : n;
   extern __shared__ double sm[];
@@ -410,6 +420,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_chol_inv(int n, const double* __
                                                         int ldg, double shift_factor,
                                                         double* __restrict__ R,
                                                         double* __restrict__ Rinv, int* err) {
+  pdl_begin();
   extern __shared__ double sm[];
   double* L = sm;                  // n x n, lower triangle = Cholesky factor
   double* X = sm + int64_t(n) * n; // n x n, L^{-1}
@@ -470,9 +481,8 @@ void chol_inv_f64(Context* c, int64_t n, const double* G, int64_t ldg, double sh
   TTG_REQUIRE(chol_inv_fits(n), "chol_inv: n = %lld too large", (long long)n);
   const size_t smem = 2 * sizeof(double) * size_t(n * n);
   ensure_smem_attr(reinterpret_cast<const void*>(k_chol_inv), c->device, int(SMEM_LIMIT + 1024));
-  k_chol_inv<<<1, SD_THREADS, smem, c->stream>>>(int(n), G, int(ldg), shift_factor, R, Rinv,
-                                                 flag ? flag : c->d_err + 4);
-  c->launches += 1;
+  launch(c, k_chol_inv, 1, SD_THREADS, smem, int(n), G, int(ldg), shift_factor, R, Rinv,
+         flag ? flag : c->d_err + 4);
   TTG_CHECK_LAUNCH();
 }
 
@@ -484,8 +494,7 @@ void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda
                   double* R) {
   const size_t smem = sizeof(double) * size_t(m * n + std::min(m, n));
   ensure_smem_attr(reinterpret_cast<const void*>(k_house_qr), c->device, int(SMEM_LIMIT + 1024));
-  k_house_qr<<<1, SD_THREADS, smem, c->stream>>>(int(m), int(n), A, int(lda), Q, R, c->skip);
-  c->launches += 1;
+  launch(c, k_house_qr, 1, SD_THREADS, smem, int(m), int(n), A, int(lda), Q, R, c->skip);
   TTG_CHECK_LAUNCH();
 }
 
@@ -517,18 +526,17 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
     void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp, &trans};
     TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_jacobi_coop, dim3(blocks),
                                          dim3(JC_THREADS), args, 0, c->stream));
-    k_jacobi_finish<<<1, SD_THREADS, 0, c->stream>>>(int(n), work.p(), V.p(), U, S, VT,
-                                                     work.p() + int64_t(n) * n, trans);
-    c->launches += 2;
+    launch(c, k_jacobi_finish, 1, SD_THREADS, 0, int(n), work.p(), V.p(), U, S, VT,
+           work.p() + int64_t(n) * n, trans);
+    c->launches += 1;  // the cooperative sweep kernel
     TTG_CHECK_LAUNCH();
     return;
   }
   ensure_smem_attr(reinterpret_cast<const void*>(k_jacobi_svd), c->device,
                    int(SMEM_LIMIT + 1024));
   const size_t smem = size_t(mode) * mat;
-  k_jacobi_svd<<<1, SD_THREADS, smem, c->stream>>>(int(n), A, int(lda), U, S, VT, V.p(),
-                                                    work.p(), mode, trans, c->d_err + 3);
-  c->launches += 1;
+  launch(c, k_jacobi_svd, 1, SD_THREADS, smem, int(n), A, int(lda), U, S, VT, V.p(), work.p(),
+         mode, trans, c->d_err + 3);
   TTG_CHECK_LAUNCH();
 }
 

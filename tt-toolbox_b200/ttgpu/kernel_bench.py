@@ -25,7 +25,11 @@
 
 ``python -m ttgpu.kernel_bench amen --precision fp64,mixed``
     one solve of the anisotropic d=10, n=64 workload per precision (set
-    TTG_PROFILE=1 for the per-phase breakdown on stderr).
+    TTG_PROFILE=1 for the per-phase breakdown on stderr).  With
+    ``--kernel-table`` the last repetition runs under the CUDA activity
+    tracer (CUPTI through ``torch.profiler``): per kernel its launches and
+    device time in that warm solve, the idle gaps between consecutive
+    kernels, and the top launch shapes (grid, block, shared memory).
 
 ``python -m ttgpu.kernel_bench dgemm``
     cuBLAS FP64 GEMM throughput (torch.matmul, 8192^3) as the measured FP64
@@ -196,18 +200,90 @@ def amen_bench(args):
     dx0, dz0 = DeviceTT.upload(ctx, x0), DeviceTT.upload(ctx, z0)
     out = {"workload": "amen_solve2 aniso d=%d n=%d rmax %d tol %g" % (args.d, args.n, args.rmax,
                                                                      args.tol)}
+    tables = {}
     for prec in args.precision.split(","):
         for rep in range(args.reps):
             st = {}
-            x = amen_solve2(dA, dy, args.tol, x0=dx0, z0=dz0, ctx=ctx, stats=st, rmax=args.rmax,
-                            nswp=50, precision=prec)
-            x.free()
+
+            def solve():
+                x = amen_solve2(dA, dy, args.tol, x0=dx0, z0=dz0, ctx=ctx, stats=st,
+                                rmax=args.rmax, nswp=50, precision=prec)
+                ctx.sync()
+                x.free()
+
+            if args.kernel_table and rep == args.reps - 1:
+                tables[prec] = _kernel_table(solve)
+            else:
+                solve()
         out[prec] = {k: st[k] for k in ("ms_total", "sweeps", "matvecs", "matvecs_fp64",
                                         "gmres_iters", "launches", "max_rank")}
     print(json.dumps(out))
+    for prec, tab in tables.items():
+        print("\n# kernels of one warm solve, precision %s\n%s" % (prec, tab))
     for h in (dA, dy, dx0, dz0):
         h.free()
     ctx.close()
+
+
+def _kernel_table(run, top=30, top_shapes=25):
+    """Run ``run()`` under the CUDA activity tracer and summarise its kernels."""
+    import collections
+    import os
+    import re
+    import tempfile
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        run()
+        torch.cuda.synchronize()
+    fd, path = tempfile.mkstemp(suffix=".json")
+    os.close(fd)
+    try:
+        prof.export_chrome_trace(path)
+        with open(path) as f:
+            events = [e for e in json.load(f)["traceEvents"] if e.get("cat") == "kernel"]
+    finally:
+        os.remove(path)
+
+    def short(name):
+        name = name.replace("(anonymous namespace)::", "").replace("ttg::", "")
+        return re.sub(r"^void ", "", name.split("(")[0])
+
+    tot, cnt = collections.defaultdict(float), collections.Counter()
+    shp, shc = collections.defaultdict(float), collections.Counter()
+    for e in events:
+        k = short(e["name"])
+        tot[k] += e["dur"]
+        cnt[k] += 1
+        a = e.get("args", {})
+        key = "%s grid=%s block=%s smem=%s" % (k, a.get("grid"), a.get("block"),
+                                               a.get("shared memory"))
+        shp[key] += e["dur"]
+        shc[key] += 1
+    spans = sorted((e["ts"], e["ts"] + e["dur"]) for e in events)
+    busy = sum(tot.values())
+    span = spans[-1][1] - spans[0][0] if spans else 0.0
+    gaps = [max(0.0, b[0] - a[1]) for a, b in zip(spans, spans[1:])]
+    edges = [0, 2, 5, 10, 20, 50, 100, float("inf")]
+    lines = ["launches %d, kernel time %.2f ms, first-to-last span %.2f ms (idle %.2f ms)"
+             % (len(events), busy / 1e3, span / 1e3, (span - busy) / 1e3)]
+    lines.append("idle gaps between consecutive kernels (us): " + ", ".join(
+        "[%g,%g) %d = %.1f ms" % (lo, hi, sum(1 for g in gaps if lo <= g < hi),
+                                  sum(g for g in gaps if lo <= g < hi) / 1e3)
+        for lo, hi in zip(edges, edges[1:])))
+    lines.append("| kernel | launches | total ms | share | us/launch |")
+    lines.append("|---|---:|---:|---:|---:|")
+    for k, v in sorted(tot.items(), key=lambda kv: -kv[1])[:top]:
+        lines.append("| `%s` | %d | %.2f | %.1f%% | %.2f |" % (k[:70], cnt[k], v / 1e3,
+                                                               100 * v / busy, v / cnt[k]))
+    lines.append("\n| launch shape | launches | total ms | us/launch |")
+    lines.append("|---|---:|---:|---:|")
+    for k, v in sorted(shp.items(), key=lambda kv: -kv[1])[:top_shapes]:
+        lines.append("| `%s` | %d | %.2f | %.2f |" % (k[:100], shc[k], v / 1e3, v / shc[k]))
+    return "\n".join(lines)
 
 
 def dgemm_bench(args):
@@ -297,6 +373,7 @@ def main():
     am.add_argument("--tol", type=float, default=1e-8)
     am.add_argument("--reps", type=int, default=2)
     am.add_argument("--precision", default="fp64,mixed")
+    am.add_argument("--kernel-table", action="store_true")
     dg = sub.add_parser("dgemm")
     dg.add_argument("--size", type=int, default=8192)
     dg.add_argument("--reps", type=int, default=10)
