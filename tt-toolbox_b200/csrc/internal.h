@@ -135,6 +135,9 @@ struct Context {
   int64_t mv_count[2] = {0, 0};
   // Mixed local solves that finished in FP64 (see local_solve_mixed).
   int64_t mixed_fallbacks = 0;
+  // Krylov steps of the last restart of the previous low-precision inner
+  // solve: sizes the first chunk of queued steps of the next one.
+  int krylov_hint = 0;
   double mv_flops[2] = {0.0, 0.0};
   // Optional CUDA-event timing of every local matvec on the context stream.
   bool time_matvec = false;
@@ -143,10 +146,12 @@ struct Context {
   bool pdl = false;
   struct EvPair {
     cudaEvent_t a, b;
-    int kind;
+    int kind;       // -1: voided (a speculatively queued matvec that was skipped)
+    uint64_t seq;   // running number of the pair on this context
   };
   std::vector<EvPair> ev_pool;
   size_t ev_used = 0;
+  uint64_t ev_seq = 0;
   double mv_ms[2] = {0.0, 0.0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // While non-null, GEMM and matvec kernels launched on this context return
@@ -162,14 +167,21 @@ struct Context {
       ev_pool.push_back(p);
     }
     ev_pool[ev_used].kind = kind;
+    ev_pool[ev_used].seq = ev_seq++;
     cudaEventRecord(ev_pool[ev_used].a, stream);
     return int(ev_used++);
   }
   void ev_end(int i) { cudaEventRecord(ev_pool[i].b, stream); }
+  // Drop the pairs numbered [from, to) that are not collected yet.
+  void ev_void(uint64_t from, uint64_t to) {
+    for (size_t i = 0; i < ev_used; ++i)
+      if (ev_pool[i].seq >= from && ev_pool[i].seq < to) ev_pool[i].kind = -1;
+  }
   // Accumulate the elapsed time of all recorded pairs into mv_ms (syncs).
   void ev_collect() {
     cudaStreamSynchronize(stream);
     for (size_t i = 0; i < ev_used; ++i) {
+      if (ev_pool[i].kind < 0) continue;
       float ms = 0.f;
       cudaEventElapsedTime(&ms, ev_pool[i].a, ev_pool[i].b);
       mv_ms[ev_pool[i].kind] += ms;

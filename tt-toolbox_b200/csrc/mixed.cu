@@ -12,8 +12,10 @@
 // least-squares residual; partial sums are reduced in a fixed order.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "mixed.h"
 #include "mixed_ops.h"
@@ -38,11 +40,12 @@ struct ArArgs {
   double* sn;      // m
   double* g;       // m+1
   double* scal;    // [0] |g_{j+1}|  [1] norm of the new Arnoldi vector  [2] beta
+                   // [3] norm of the solve's right-hand side  [4] stop threshold
   double* part;    // 2 * (m+1) * gridDim.x
   unsigned* bar;   // [0] count [1] generation
   int* err;
-  int* stop;       // [0] converged flag, [1] step at which it converged
-  double thresh;   // absolute residual threshold of the current solve
+  int* stop;       // [0] converged flag, [1] step at which it converged (-1: at start)
+  double reltol;   // stop once |g_{j+1}| <= reltol * scal[3]
   // BF16 operand of the next local matvec, written with each new basis
   // vector: X[b + ldx * row] = bf16(V[b + rx2 * row]) (padding b >= rx2 stays
   // zero), so the matvec needs no conversion launch.
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
     a.g[j] = c0 * a.g[j];
     a.scal[0] = fabs(a.g[j + 1]);
     a.scal[1] = nrm;
-    if (a.scal[0] <= a.thresh) {
+    if (a.scal[0] <= a.scal[4]) {
       a.stop[1] = j;
       __threadfence();
       a.stop[0] = 1;
@@ -207,8 +210,12 @@ __global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
   }
 }
 
-// V(:,0) = r / ||r||, g = [||r||, 0, ...]; scal[2] = ||r||.
-__global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r) {
+// V(:,0) = r / ||r||, g = [||r||, 0, ...]; scal[2] = ||r||.  On the first
+// restart (first != 0) r is the right-hand side: scal[3] = ||r||.  The stop
+// threshold reltol * scal[3] goes to scal[4]; a residual already below it
+// (or zero) raises the stop flag with step -1, so the queued steps return at
+// once and the host learns it at its next read of the flags.
+__global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r, int first) {
   __shared__ float red[AR_WARPS];
   __shared__ double tot[1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -236,6 +243,14 @@ __global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r
     a.g[0] = beta;
     a.scal[2] = beta;
     a.scal[0] = beta;
+    if (first) a.scal[3] = beta;
+    const double thr = a.reltol * a.scal[3];
+    a.scal[4] = thr;
+    if (beta <= thr || beta == 0.0) {
+      a.stop[1] = -1;
+      __threadfence();
+      a.stop[0] = 1;
+    }
   }
 }
 
@@ -305,7 +320,7 @@ struct Gmres32 {
     a.err = c->d_err + 2;
     stop.reset(c, 4);
     a.stop = stop.p();
-    a.thresh = 0.0;
+    a.reltol = 0.0;
     a.X = nullptr;
   }
 
@@ -325,8 +340,8 @@ struct Gmres32 {
     a.X = op.X.p();
     a.rx2 = int(op.d.rx2);
     a.ldx = int(op.ldx);
+    a.reltol = reltol;
     TTG_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * sz, c->stream));
-    double bnorm = -1.0;
     for (int64_t it = 0; it < max_restarts; ++it) {
       const float* rr = b;
       if (it > 0) {
@@ -334,43 +349,67 @@ struct Gmres32 {
         launch(c, k_sub_f32, blocks, AR_THREADS, 0, sz, b, w.p(), r.p());
         rr = r.p();
       }
-      void* ai[] = {&a, &rr};
-      coop((const void*)k_ar_init, ai, 0);
       TTG_CUDA(cudaMemsetAsync(stop.p(), 0, 2 * sizeof(int), c->stream));
-      double sc[3];
-      read_scalars(c, a.scal, sc, 3);
-      if (bnorm < 0) bnorm = sc[2];
-      if (sc[2] <= reltol * bnorm || sc[2] == 0.0) break;
-      a.thresh = reltol * bnorm;
-      // Steps queued in growing chunks; k_arnoldi raises the stop flag and
-      // later queued kernels return at once (see gmres.cu).
-      int j = 0, chunk = 3;
-      bool conv = false;
+      int first = it == 0 ? 1 : 0;
+      void* ai[] = {&a, &rr, &first};
+      coop((const void*)k_ar_init, ai, 0);
+      // Steps queued in chunks; k_arnoldi (or k_ar_init, for a residual
+      // already below the threshold) raises the stop flag and later queued
+      // kernels return at once (see gmres.cu).  The first chunk is the step
+      // count of the context's previous inner solve, later ones half of it,
+      // so that most solves need one or two reads of the flags.  Matvecs
+      // queued past the converged step are taken out of the counters and
+      // timings afterwards.
+      int j = 0, queued = 0;
+      const int hint = std::max(3, c->krylov_hint);
+      int chunk = std::min(m, hint);
+      bool conv = false, at_start = false;
+      std::vector<uint64_t> seqs;
       SkipGuard guard(c, stop.p());
       while (j < m) {
         const int jend = std::min(m, j + chunk);
         for (int jj = j; jj < jend; ++jj) {
           int jv = jj;
+          seqs.push_back(c->ev_seq);
           op.apply_converted(c, w.p());  // X holds V(:, jv) (k_ar_init / k_arnoldi)
           void* aa[] = {&a, &jv};
           coop((const void*)k_arnoldi, aa, arnoldi_smem());
         }
+        queued = jend;
         TTG_CUDA(cudaMemcpyAsync(c->h_scal, stop.p(), 2 * sizeof(int), cudaMemcpyDeviceToHost,
                                  c->stream));
         sync(c);
         int flag[2];
         memcpy(flag, c->h_scal, sizeof(flag));
         if (flag[0]) {
-          conv = true;
-          j = flag[1];
+          if (flag[1] < 0) {
+            at_start = true;
+          } else {
+            conv = true;
+            j = flag[1];
+          }
           break;
         }
         j = jend;
-        chunk *= 2;
+        chunk = std::max(3, hint / 2);
       }
       guard.release();
-      steps += conv ? j + 1 : m;
+      {
+        const int done = at_start ? 0 : (conv ? j + 1 : m);
+        const int skipped = queued - done;
+        if (skipped > 0) {
+          const double fl = op.d.flops();
+          c->matvecs -= skipped;
+          c->matvec_flops -= int64_t(fl) * skipped;
+          c->mv_count[1] -= skipped;
+          c->mv_flops[1] -= fl * skipped;
+          if (c->time_matvec) c->ev_void(seqs[done], c->ev_seq);
+        }
+      }
+      if (at_start) break;  // nothing left to reduce: x stays as it is
       const int k = conv ? j + 1 : m;
+      steps += k;
+      c->krylov_hint = k;
       launch(c, k_ar_update, blocks, AR_THREADS, sizeof(double) * (m + 1), a, k, x);
       TTG_CHECK_LAUNCH();
       if (conv) break;
