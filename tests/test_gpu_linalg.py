@@ -25,6 +25,35 @@ def test_dense_svd_matches_lapack(ctx, m, n):
     assert np.all(np.diff(s) <= 0)
 
 
+@pytest.mark.parametrize("m,n", [(300, 6), (8, 8), (6, 3), (2048, 8)])
+def test_dense_svd_few_columns_rank_deficient(ctx, m, n):
+    """Tall matrices with at most 8 columns take the one-CTA Jacobi SVD of A
+    itself: zero and repeated columns must still give orthonormal U."""
+    rng = np.random.default_rng(m + n)
+    A = rng.standard_normal((m, n))
+    A[:, 1] = 0.0
+    A[:, n - 1] = A[:, 0]
+    U, s, VT = ttgpu.dense_svd(A, ctx=ctx)
+    s_ref = np.linalg.svd(A, compute_uv=False)
+    assert np.allclose(s, s_ref, rtol=0, atol=1e-13 * s_ref[0])
+    assert np.linalg.norm(U * s @ VT - A) / np.linalg.norm(A) < 1e-13
+    assert np.linalg.norm(U.T @ U - np.eye(n)) < 1e-12
+    assert np.linalg.norm(VT @ VT.T - np.eye(n)) < 1e-12
+    assert s[-1] == 0.0 or s[-1] < 1e-14 * s[0]
+
+
+def test_dense_svd_few_columns_graded(ctx):
+    rng = np.random.default_rng(11)
+    Q1, _ = np.linalg.qr(rng.standard_normal((512, 8)))
+    Q2, _ = np.linalg.qr(rng.standard_normal((8, 8)))
+    sv = 10.0 ** (-np.linspace(0, 14, 8))
+    A = (Q1 * sv) @ Q2.T
+    U, s, VT = ttgpu.dense_svd(A, ctx=ctx)
+    assert np.allclose(s, sv, rtol=0, atol=4e-16 * 8)
+    assert np.linalg.norm(U * s @ VT - A) / np.linalg.norm(A) < 1e-13
+    assert np.linalg.norm(U.T @ U - np.eye(8)) < 1e-12
+
+
 @pytest.mark.parametrize("n", [96, 180])
 def test_dense_svd_graded_spectrum(ctx, n):
     """Singular values spanning 14 decades (the truncation regime of AMEn);

@@ -130,9 +130,14 @@ int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, dou
 namespace {
 // Economy SVD of a tall m x n (m >= n) matrix: QR, then one-sided Jacobi SVD
 // of the n x n triangular factor R (small_dense.cu) run on the rows of R
-// (the columns of R^T), U = Q Ur.
+// (the columns of R^T), U = Q Ur; up to 8 columns, one-sided Jacobi on A
+// itself in one CTA.
 void svd_tall(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
               double* VT) {
+  if (svd_tall_small_fits(m, n)) {  // few columns: rotate A itself, one launch
+    svd_tall_small_f64(c, m, n, A, m, U, S, VT);
+    return;
+  }
   if (m == n) {
     jacobi_svd_f64(c, n, A, m, U, S, VT);
     return;

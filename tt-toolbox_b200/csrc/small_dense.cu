@@ -472,6 +472,163 @@ __global__ void __launch_bounds__(SD_THREADS) k_chol_inv(int n, const double* __
   if (tid == 0 && s_bad) atomicOr(err, 1);
 }
 
+
+// ---------------------------------------------------------------------------
+// One-sided Jacobi SVD of a tall m x n matrix with few columns (n <=
+// TS_MAX_N, m >= n), held in shared memory and rotated directly (no QR
+// first): one warp per column pair of a round-robin round, the rotation and
+// stopping rule of k_jacobi_svd.  U = A V diag(1/s) (m x n, ld m); columns of
+// exactly zero norm are completed to an orthonormal set (Gram-Schmidt of unit
+// vectors against the other columns), so U always has orthonormal columns.
+// S descending, VT (n x n, ld n).  One launch replaces QR + square SVD +
+// U = Q Ur for the small SVDs of the sweeps (Z updates, early truncations).
+// ---------------------------------------------------------------------------
+
+constexpr int TS_THREADS = 256;
+constexpr int TS_WARPS = TS_THREADS / 32;
+constexpr int TS_MAX_N = 8;
+
+__global__ void __launch_bounds__(TS_THREADS) k_svd_tall_small(int m, int n,
+                                                              const double* __restrict__ Ain,
+                                                              int lda, double* __restrict__ U,
+                                                              double* __restrict__ S,
+                                                              double* __restrict__ VT,
+                                                              int* err) {
+  pdl_begin();
+  extern __shared__ double A[];  // m x n
+  __shared__ double V[TS_MAX_N * TS_MAX_N];
+  __shared__ double sig[TS_MAX_N];
+  __shared__ int pos[TS_MAX_N];
+  __shared__ double s_off[TS_WARPS];
+  __shared__ int s_done;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < m * n; e += TS_THREADS) {
+    const int i = e % m, j = e / m;
+    A[e] = Ain[i + int64_t(j) * lda];
+  }
+  for (int e = tid; e < n * n; e += TS_THREADS) V[e] = (e % n == e / n) ? 1.0 : 0.0;
+  __syncthreads();
+  const int ne = (n + 1) & ~1;
+  const double tol = 4.0 * 2.220446049250313e-16, tol2 = tol * tol;
+  int sweep = 0;
+  for (sweep = 0; sweep < JAC_MAX_SWEEPS; ++sweep) {
+    double off = 0.0;
+    for (int r = 0; r < ne - 1; ++r) {
+      for (int pr = warp; pr < ne / 2; pr += TS_WARPS) {
+        int p = rr_player(pr, r, ne), q = rr_player(ne - 1 - pr, r, ne);
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        if (q >= n) continue;  // dummy player
+        double* ap = A + int64_t(p) * m;
+        double* aq = A + int64_t(q) * m;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int i = lane; i < m; i += 32) {
+          const double x = ap[i], y = aq[i];
+          al += x * x;
+          be += y * y;
+          ga += x * y;
+        }
+        al = wsum(al);
+        be = wsum(be);
+        ga = wsum(ga);
+        const double ab = al * be, g2 = ga * ga;
+        if (ab == 0.0 || g2 <= tol2 * ab) continue;
+        off = fmax(off, g2 / ab);
+        const double dd = be - al, gg = 2.0 * ga;
+        const double sg = ((dd >= 0.0) == (gg > 0.0) || dd == 0.0) ? 1.0 : -1.0;
+        const double t = sg * fabs(gg) / (fabs(dd) + sqrt(dd * dd + gg * gg));
+        const double c = rsqrt(1.0 + t * t), s = c * t;
+        for (int i = lane; i < m; i += 32) {
+          const double x = ap[i], y = aq[i];
+          ap[i] = c * x - s * y;
+          aq[i] = s * x + c * y;
+        }
+        if (lane < n) {
+          const double vx = V[lane + p * n], vy = V[lane + q * n];
+          V[lane + p * n] = c * vx - s * vy;
+          V[lane + q * n] = s * vx + c * vy;
+        }
+      }
+      __syncthreads();
+    }
+    if (lane == 0) s_off[warp] = off;
+    __syncthreads();
+    if (tid == 0) {
+      double mx = 0.0;
+      for (int w = 0; w < TS_WARPS; ++w) mx = fmax(mx, s_off[w]);
+      s_done = (mx <= tol2) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_done) break;
+  }
+  if (tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(err, 5);
+  // singular values = column norms, ranked descending (stable on index)
+  if (warp < n) {
+    const double* aj = A + int64_t(warp) * m;
+    double s = 0.0;
+    for (int i = lane; i < m; i += 32) s += aj[i] * aj[i];
+    s = wsum(s);
+    if (lane == 0) sig[warp] = sqrt(s);
+  }
+  __syncthreads();
+  if (tid < n) {
+    const double sj = sig[tid];
+    int p = 0;
+    for (int k = 0; k < n; ++k) p += (sig[k] > sj) || (sig[k] == sj && k < tid);
+    pos[tid] = p;
+  }
+  for (int e = tid; e < m * n; e += TS_THREADS) {
+    const double sj = sig[e / m];
+    if (sj > 0.0) A[e] /= sj;
+  }
+  __syncthreads();
+  // complete zero columns: e_k minus its projections on the columns kept so
+  // far (twice), accepted when at least 0.3 of it is left (the mean left
+  // over all k is at least 1 - (n - 1) / m >= 1 / n)
+  if (warp == 0) {
+    for (int j = 0; j < n; ++j) {
+      if (sig[j] > 0.0) continue;
+      double* aj = A + int64_t(j) * m;
+      for (int k = 0; k < m; ++k) {
+        for (int i = lane; i < m; i += 32) aj[i] = (i == k) ? 1.0 : 0.0;
+        __syncwarp();
+        for (int pass = 0; pass < 2; ++pass) {
+          for (int q = 0; q < n; ++q) {
+            if (q == j || (sig[q] == 0.0 && q > j)) continue;
+            const double* aq = A + int64_t(q) * m;
+            double d = 0.0;
+            for (int i = lane; i < m; i += 32) d += aq[i] * aj[i];
+            d = wsum(d);
+            for (int i = lane; i < m; i += 32) aj[i] -= d * aq[i];
+            __syncwarp();
+          }
+        }
+        double nr = 0.0;
+        for (int i = lane; i < m; i += 32) nr += aj[i] * aj[i];
+        nr = sqrt(wsum(nr));
+        if (nr > 0.3) {
+          for (int i = lane; i < m; i += 32) aj[i] /= nr;
+          __syncwarp();
+          break;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < m * n; e += TS_THREADS) {
+    const int i = e % m, j = e / m;
+    U[i + int64_t(pos[j]) * m] = A[e];
+  }
+  for (int e = tid; e < n * n; e += TS_THREADS) {
+    const int i = e % n, j = e / n;
+    VT[pos[j] + i * n] = V[e];
+  }
+  if (tid < n) S[pos[tid]] = sig[tid];
+}
+
 }  // namespace
 
 bool chol_inv_fits(int64_t n) { return 2 * n * n * int64_t(sizeof(double)) <= int64_t(SMEM_LIMIT); }
@@ -498,6 +655,22 @@ void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda
   TTG_CHECK_LAUNCH();
 }
 
+
+bool svd_tall_small_fits(int64_t m, int64_t n) {
+  return n >= 1 && n <= TS_MAX_N && m >= n && m * n * int64_t(sizeof(double)) <= int64_t(128 * 1024);
+}
+
+void svd_tall_small_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* U,
+                        double* S, double* VT) {
+  TTG_REQUIRE(svd_tall_small_fits(m, n), "svd_tall_small: %lld x %lld out of range",
+              (long long)m, (long long)n);
+  const size_t smem = sizeof(double) * size_t(m * n);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_svd_tall_small), c->device,
+                   int(128 * 1024 + 1024));
+  launch(c, k_svd_tall_small, 1, TS_THREADS, smem, int(m), int(n), A, int(lda), U, S, VT,
+         c->d_err + 3);
+  TTG_CHECK_LAUNCH();
+}
 
 void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
                     double* VT, bool via_transpose) {

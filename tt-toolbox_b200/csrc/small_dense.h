@@ -24,5 +24,11 @@ void chol_inv_f64(Context* c, int64_t n, const double* G, int64_t ldg, double sh
 // decay of 1e-8 to 1e-14 over 50-64 columns).
 void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
                     double* VT, bool via_transpose = false);
+// One-sided Jacobi SVD of a tall m x n matrix (m >= n, n <= 8, m n <= 16384)
+// rotated directly in one CTA: U (m x n, ld m, orthonormal columns), S (n,
+// descending), VT (n x n, ld n).
+bool svd_tall_small_fits(int64_t m, int64_t n);
+void svd_tall_small_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* U,
+                        double* S, double* VT);
 
 }  // namespace ttg
