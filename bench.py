@@ -164,19 +164,44 @@ def load_traffic():
         return None
 
 
-def cpu_baseline_run(W, reps=1):
-    """The FP64 oracle (reference algorithm restated) on the same workload."""
+def blas_threads():
+    """Threads of the BLAS library numpy uses (what the CPU leg actually ran on)."""
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i["num_threads"] for i in threadpool_info() if i.get("user_api") == "blas"]
+        return max(n) if n else os.cpu_count()
+    except Exception:
+        return os.cpu_count()
+
+
+def cpu_baseline_run(W, reps=1, threads=None):
+    """The FP64 oracle (reference algorithm restated) on the same workload;
+    ``threads`` caps the BLAS threads (1 matches the reference tests'
+    ``maxNumCompThreads(1)``), None leaves all of them."""
     sys.path.insert(0, ROOT)
+    from contextlib import nullcontext
     from oracle.amen import amen_solve2 as ref_solve
     from oracle.builders import aniso_config
     A, y, x0, z0 = aniso_config(d=W["d"], n=W["n"], seed=W["seed"])
+    limit = nullcontext()
+    if threads is not None:
+        from threadpoolctl import threadpool_limits
+        limit = threadpool_limits(threads)
     times = []
     info = None
-    for _ in range(reps):
-        t = time.perf_counter()
-        x, info = ref_solve(A, y, W["tol"], x0, z0, rmax=W["rmax"], nswp=50)
-        times.append(time.perf_counter() - t)
+    with limit:
+        for _ in range(reps):
+            t = time.perf_counter()
+            x, info = ref_solve(A, y, W["tol"], x0, z0, rmax=W["rmax"], nswp=50)
+            times.append(time.perf_counter() - t)
     return times, info
+
+
+def single_thread_baseline(W):
+    t1, info = cpu_baseline_run(W, reps=1, threads=1)
+    return {"value": t1[0], "unit": "s", "cores": 1,
+            "sample": "one full FP64 oracle solve, BLAS limited to one thread (%d sweeps)"
+                      % info["sweeps"]}
 
 
 def run_reference(args, dist):
@@ -187,7 +212,7 @@ def run_reference(args, dist):
     times, info = cpu_baseline_run(W, reps=max(1, n_total))
     timed = times[-args.steps:] if args.steps > 0 else times
     v = statistics.mean(timed)
-    cores = os.cpu_count()
+    cores = blas_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -196,7 +221,8 @@ def run_reference(args, dist):
         "config": {"workload": "amen_solve2 d=10 n=64 rank-3 anisotropic operator, rank-4 rhs, "
                                "rmax 128, tol 1e-8", "parallelism": "replicas", "sweeps": info["sweeps"]},
         "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
-                         "sample": "full FP64 oracle solve of the workload (numpy/OpenBLAS, all threads)"},
+                         "sample": "full FP64 oracle solve of the workload (numpy/OpenBLAS, all threads)",
+                         "single_thread": single_thread_baseline(W)},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
@@ -341,10 +367,11 @@ def run_ours(args, dist):
         line["compare"] = other
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         times, info = cpu_baseline_run(W, reps=1)
-        line["cpu_baseline"] = {"value": times[0], "unit": "s", "cores": os.cpu_count(),
+        line["cpu_baseline"] = {"value": times[0], "unit": "s", "cores": blas_threads(),
                                 "kind": "port",
                                 "sample": "one full FP64 oracle solve of the same workload "
-                                          "(numpy/OpenBLAS, all threads; %d sweeps)" % info["sweeps"]}
+                                          "(numpy/OpenBLAS, all threads; %d sweeps)" % info["sweeps"],
+                                "single_thread": single_thread_baseline(W)}
     for h in (dA, dy, dx0, dz0):
         h.free()
     ctx.close()
