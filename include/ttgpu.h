@@ -53,6 +53,27 @@ int ttg_context_create(int device, ttg_context* out);
 int ttg_context_destroy(ttg_context ctx);
 int ttg_context_sync(ttg_context ctx);
 
+/* Context options.  TTG_OPT_JACOBI_MAX_SWEEPS (default 40, 1..1000): sweep
+ * limit of the one-sided Jacobi SVDs.  An SVD that reaches it without
+ * converging makes ttg_dense_svd and ttg_amen_solve fail with
+ * TTG_ERR_NOCONV (MATLAB's svd errors there, which aborts amen_solve2), and
+ * makes ttg_round take the fallback SVD of the core, as round.m:64-74 falls
+ * back to svds. */
+enum { TTG_OPT_JACOBI_MAX_SWEEPS = 1 };
+int ttg_context_set_option(ttg_context ctx, int32_t key, int64_t value);
+
+/* Self-test of the bounded device waits.  No counterpart in the reference.
+ * Every kernel of this library that waits on the device (the grid barriers
+ * of the Householder GMRES (which = 0), of the cooperative Jacobi SVD (2)
+ * and of the mixed-precision Arnoldi kernels (3), the mbarrier waits of the
+ * tcgen05 pipeline (1)) gives up after a bounded number of polls, raises a
+ * device error flag and returns, so that a lost participant ends in an
+ * error status instead of a hang.  This entry runs the chosen wait helper
+ * on a condition that nothing satisfies, with a small poll limit, and
+ * returns TTG_ERR_TIMEOUT when the wait gave up as designed; the context
+ * stays usable. */
+int ttg_selftest_wait(ttg_context ctx, int32_t which);
+
 /* Device memory helpers for callers without an allocator of their own. */
 int ttg_malloc(ttg_context ctx, size_t bytes, void** out);
 int ttg_free(ttg_context ctx, void* p);
@@ -88,6 +109,8 @@ typedef struct {
   double ms_qr_sweep;  /* left-to-right QR sweep                       */
   double ms_svd_sweep; /* right-to-left SVD sweep                      */
   int64_t max_rank;    /* max rank of the result                       */
+  int64_t svd_fallbacks; /* cores whose Jacobi SVD reached the sweep limit
+                            and took the fallback SVD (round.m:64-74)    */
 } ttg_round_stats;
 
 int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax,
@@ -102,6 +125,23 @@ int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax,
  * x0 / z0 may be NULL: then a right-orthogonal random TT of rank 2 / kickrank
  * is drawn on the device (the reference's tt_rand(n,d,2,-1),
  * amen_solve2.m:222-224,250-252; the random stream differs from MATLAB's). */
+/* One local step of an AMEn sweep (core `core` of sweep `sweep`), recorded
+ * when ttg_amen_opts.trace is set.  It holds the discrete decisions of the
+ * step and the two local residuals that enter them, so that a caller can
+ * compare a solve decision by decision with another implementation of
+ * solve/amen_solve2.m. */
+typedef struct {
+  int64_t sweep;    /* 1-based sweep number                                   */
+  int64_t core;     /* 0-based core index                                     */
+  int64_t rank;     /* rank kept by the residual-based truncation, after the
+                       caps (amen_solve2.m:539-594), before the kick; -1 at
+                       the last core, which is not truncated                  */
+  int64_t iters;    /* Krylov steps of the local solve (over all restarts);
+                       -1: dense branch (:468-492) or zero right-hand side    */
+  double res_prev;  /* ||B x_prev - rhs|| / ||rhs||                   (:495)  */
+  double res_new;   /* ||B x_new - rhs|| / ||rhs||                    (:504)  */
+} ttg_amen_step;
+
 typedef struct {
   int64_t nswp;          /* 50   */
   int64_t rmax;          /* 1000 */
@@ -118,6 +158,8 @@ typedef struct {
   uint64_t seed;         /* seed for device-drawn x0/z0     */
   int32_t timing;        /* 1: time every local matvec with CUDA events */
   int32_t reserved;
+  ttg_amen_step* trace;  /* NULL, or room for trace_cap steps (host memory) */
+  int64_t trace_cap;     /* steps beyond the capacity are counted, not stored */
 } ttg_amen_opts;
 
 #define TTG_MAX_SWEEPS_RECORDED 64
@@ -139,6 +181,8 @@ typedef struct {
   double ms_lp;           /* their device time (opts.timing = 1)          */
   double gflop_fp64;      /* FP64 local-matvec FLOPs / 1e9                */
   double ms_fp64;         /* their device time (opts.timing = 1)          */
+  int64_t trace_len;      /* local steps run (entries written to opts.trace,
+                             up to its capacity)                          */
 } ttg_amen_stats;
 
 void ttg_amen_opts_default(ttg_amen_opts* opts);
@@ -194,10 +238,13 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2,
  * Sizes whose intermediates (rx1*n*ra2*rx2 + rx1*ra1*n*rx2 doubles) exceed
  * it are rejected with TTG_ERR_INVALID.  stream: a cudaStream_t (NULL = the
  * legacy default stream) of the current device; the call returns after the
- * stream has finished.  The first call on a device looks up the array's
- * device address, so make it before any stream capture.  All calls on a
- * device share the array: calls whose GPU work overlaps (other streams,
- * other host threads) race on it and must be serialised by the caller. */
+ * stream has finished (it synchronises the stream, so it cannot be recorded
+ * into a CUDA graph).  The first call on a device looks up the array's
+ * device address and caches it for the life of the process; after a
+ * cudaDeviceReset the cached address is stale, so do not call it again in
+ * that process.  All calls on a device share the array: calls whose GPU
+ * work overlaps (other streams, other host threads) race on it and must be
+ * serialised by the caller. */
 int ttg_local_matvec_noalloc(void* stream, int64_t rx1, int64_t n, int64_t rx2,
                              int64_t ra1, int64_t ra2, const double* Phi1,
                              const double* A, const double* Phi2, const double* x,

@@ -117,14 +117,19 @@ def _phi3_right(P):
 # Local GMRES (Householder Arnoldi + Givens), fmex/solve3d.c:339-518
 # ---------------------------------------------------------------------------
 
-def dgmresr_hh(mv, rhs, nrestart, tol, niters, stats=None):
+def dgmresr_hh(mv, rhs, nrestart, tol, niters, stats=None, force_iters=None):
     """Right-preconditioned GMRES with Householder orthogonalisation.
 
     Restates ``fmex/solve3d.c:339-518`` (no preconditioner).  Starts from
     ``sol = 0`` (``:366``); ``tol`` is relative to the initial residual norm
     of the first restart (``:383,473``).  ``mv`` applies the local operator.
-    Returns the solution.  ``stats`` (a dict) receives ``matvecs`` and
-    ``iters``.
+    Returns the solution.  ``stats`` (a dict) receives ``matvecs``,
+    ``gmres_calls``, and for this call ``iters`` (Krylov steps over all
+    restarts), ``hist`` (the residual estimate after every step) and
+    ``gm_tol``.  ``force_iters`` replaces the stopping test ``curres < tol``
+    (``:476,508``) by "stop after that many steps": a checker uses it to
+    follow another implementation's step count, after it has compared the
+    estimates in ``hist`` with ``tol``.
     """
     sz = rhs.size
     U = np.zeros((sz, nrestart + 1))
@@ -136,6 +141,13 @@ def dgmresr_hh(mv, rhs, nrestart, tol, niters, stats=None):
     curres = np.inf
     nmv = 0
     j = 0
+    hist = []
+
+    def stop():
+        if force_iters is None:
+            return curres < tol
+        return len(hist) >= force_iters
+
     for it in range(niters):
         w = mv(sol)                                     # :376
         nmv += 1
@@ -189,7 +201,8 @@ def dgmresr_hh(mv, rhs, nrestart, tol, niters, stats=None):
                 w[j + 1] = 0.0
             R[:, j] = w[:nrestart]                      # :469
             curres = abs(tau[j + 1]) / nrmrhs           # :473
-            if curres < tol:                            # :476
+            hist.append(curres)
+            if stop():                                  # :476
                 broke = True
                 break
         if not broke:                                   # :482-486
@@ -209,11 +222,14 @@ def dgmresr_hh(mv, rhs, nrestart, tol, niters, stats=None):
             w[i] += tau[i]
             w -= 2.0 * np.dot(U[:, i], w) * U[:, i]
         sol = sol + w
-        if curres < tol:                                # :508
+        if stop():                                      # :508
             break
     if stats is not None:
         stats["matvecs"] = stats.get("matvecs", 0) + nmv
         stats["gmres_calls"] = stats.get("gmres_calls", 0) + 1
+        stats["iters"] = len(hist)
+        stats["hist"] = hist
+        stats["gm_tol"] = tol
     return sol
 
 
@@ -270,7 +286,8 @@ def jac_apply(jacs, prec, x, rx1, n, rx2):
     return np.asfortranarray(Y).ravel(order="F")
 
 
-def solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, nrestart=40, niters=2, stats=None, prec=0):
+def solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, nrestart=40, niters=2, stats=None, prec=0,
+              force_iters=None):
     """MEX local solver, residual branch (``fmex/solve3d_2.c:121-300``).
 
     ``tol`` is relative to ``||rhs||``.  Computes ``dres = rhs - B sol_prev``,
@@ -293,7 +310,8 @@ def solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, nrestart=40, niters=2, stats=No
         mv = lambda v: bfun3(Phi1, A, Phi2, jac_apply(jacs, prec, v, rx1, n, rx2))
     else:
         mv = lambda v: bfun3(Phi1, A, Phi2, v)
-    dsol = dgmresr_hh(mv, dres, nrestart, tol / tol_prev, niters, stats)   # :267
+    dsol = dgmresr_hh(mv, dres, nrestart, tol / tol_prev, niters, stats,
+                      force_iters)                                          # :267
     if prec:
         dsol = jac_apply(jacs, prec, dsol, rx1, n, rx2)                    # :272-274
     return dsol + sol_prev                              # :277-278
@@ -325,7 +343,90 @@ DEFAULTS = dict(nswp=50, rmax=1000, max_full_size=50, local_restart=40, local_it
 LOCAL_PREC = {"": 0, "cjacobi": 1, "ljacobi": 2, "rjacobi": 3}
 
 
-def amen_solve2(A, y, tol, x0, z0=None, **opts):
+def _near(v, ref, near_tie):
+    """``v`` lies within relative ``near_tie`` of the threshold ``ref``."""
+    return ref > 0 and abs(v / ref - 1.0) < near_tie
+
+
+class _Follow:
+    """Decision checker: compares this solve's discrete decisions with those
+    another implementation recorded (``steps``: one dict per local step with
+    ``rank`` and ``iters``, as ``ttg_amen_step``; ``max_res``: its per-sweep
+    maxima).  Where the two differ and the compared quantity lies within
+    relative ``near_tie`` of its threshold (a near tie: rounding decides),
+    the other implementation's choice is adopted and the step is listed in
+    ``flips``; otherwise the difference is listed in ``mismatches`` (and the
+    choice adopted as well, so that the comparison can go on)."""
+
+    def __init__(self, steps, max_res, near_tie):
+        self.steps = {(s["sweep"], s["core"]): s for s in steps}
+        self.max_res = list(max_res)
+        self.near_tie = near_tie
+        self.flips = []
+        self.mismatches = []
+
+    def step(self, swp, i):
+        s = self.steps.get((swp, i))
+        if s is None:
+            self.mismatches.append(dict(kind="missing step", sweep=swp, core=i))
+        return s
+
+    def gmres(self, swp, i, hist, gm_tol, iters_o, iters_g, cap):
+        """Krylov step count: the other side stopped after ``iters_g`` steps,
+        i.e. its estimate stayed >= tol before and fell below at that step
+        (unless it hit the cap)."""
+        if iters_g == iters_o:
+            return
+        bad = []
+        for k, cr in enumerate(hist[:iters_g], start=1):
+            implied = (k == iters_g)
+            if k == iters_g and iters_g >= cap:
+                continue
+            if (cr < gm_tol) != implied and not _near(cr, gm_tol, self.near_tie):
+                bad.append(k)
+        rec = dict(kind="gmres steps", sweep=swp, core=i, own=iters_o, other=iters_g)
+        (self.mismatches if bad or len(hist) < iters_g else self.flips).append(rec)
+
+    def rank(self, swp, i, r_own, r_g, K, cap, thr, res_of):
+        """Truncation rank: the other side kept ``r_g`` (after the caps
+        ``min(., K, rmax)``), i.e. its candidate residuals stayed <= thr for
+        candidates >= r_g and exceeded thr at r_g - 1 (when r_g is not
+        capped and not the loop's fall-through value 2)."""
+        if r_g == r_own:
+            return
+        near = self.near_tie
+        bad = []
+        capped = r_g >= cap
+        for rr in range(K - 1, max(r_g - 1, 1) - 1, -1):
+            if rr >= r_g:
+                implied = False
+            elif capped or r_g == 2:
+                continue
+            else:
+                implied = True
+            v = res_of(rr)
+            if (v > thr) != implied and not _near(v, thr, near):
+                bad.append(rr)
+        if capped and r_g > r_own:
+            # the other side's exceeding candidate lies somewhere >= r_g - 1
+            if not any(_near(res_of(rr), thr, near) for rr in range(r_g - 1, K)):
+                bad.append(r_g - 1)
+        rec = dict(kind="rank", sweep=swp, core=i, own=r_own, other=r_g)
+        (self.mismatches if bad else self.flips).append(rec)
+
+    def stop(self, swp, max_res, tol_exit):
+        if swp - 1 >= len(self.max_res):
+            self.mismatches.append(dict(kind="missing sweep", sweep=swp))
+            return max_res < tol_exit
+        own = max_res < tol_exit
+        other = self.max_res[swp - 1] < tol_exit
+        if own != other:
+            rec = dict(kind="sweep stop", sweep=swp, own=own, other=other)
+            (self.flips if _near(max_res, tol_exit, self.near_tie) else self.mismatches).append(rec)
+        return other
+
+
+def amen_solve2(A, y, tol, x0, z0=None, trace=None, follow=None, near_tie=1e-6, **opts):
     """``[x, testdata, z] = amen_solve2(A, y, tol, ...)`` on the default path.
 
     ``x0`` is required (the reference draws ``tt_rand(n,d,2,-1)`` from
@@ -333,6 +434,18 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
     (``:250-252``; defaults to the rank-``kickrank`` right-orthogonal TT drawn
     from ``numpy`` with seed 0 when omitted).  Returns ``(x, info)``; ``info``
     holds per-sweep ``max_res``, ``max_dx``, ranks and operation counts.
+
+    ``trace`` (a list) receives one dict per local step: sweep, core, kept
+    rank, Krylov steps, local residuals, the truncation threshold and the
+    step's decision margins (``rank_margin``: the smallest
+    ``|res/thr - 1|`` over the candidates the rank loop examined;
+    ``gmres_margin``: the smallest ``|curres/tol - 1|`` over the Krylov
+    steps).  ``follow`` (dict with ``steps`` and ``max_res`` recorded by
+    another implementation) checks every discrete decision against the
+    other implementation's and adopts the other's choice at near ties
+    (relative distance to the threshold below ``near_tie``); ``info``
+    then holds ``flips`` (adopted near ties) and ``mismatches`` (differences
+    that were not near ties).
     """
     o = dict(DEFAULTS)
     for k, v in opts.items():
@@ -379,6 +492,7 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
 
     info = dict(max_res=[], max_dx=[], max_rank=[], matvecs=0, local_solves=0, sweeps=0,
                 res_prev=[])
+    fol = _Follow(follow["steps"], follow["max_res"], near_tie) if follow is not None else None
     st = {"matvecs": 0}
     last_sweep = False
 
@@ -438,6 +552,8 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
             Phi1 = phia[i]
             Phi2 = phia[i + 1]
             A1 = crA[i]
+            other = fol.step(swp, i) if fol is not None else None
+            step_iters, gm_margin = -1, None
             sol_prev = rs(crx[i], rx[i] * n[i] * rx[i + 1])            # :451
             y1 = cry[i] * nrmsc                                        # :453
             rhs = phiy[i] @ rs(y1, ry[i], n[i] * ry[i + 1])            # :456-458
@@ -455,8 +571,24 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
                 res_prev = np.linalg.norm(bfun3(Phi1, A1, Phi2, sol_prev) - rhs) / norm_rhs  # :495
                 mv_count()
                 if norm_rhs > 0:                                       # :497
+                    gst = {}
+                    force = None
+                    if other is not None and other["iters"] >= 0:
+                        # the step count this solve takes on its own (same
+                        # arithmetic, no side effects), then the check
+                        solve3d_2(Phi1, A1, Phi2, rhs, real_tol, sol_prev, local_restart,
+                                  local_iters, gst, prec)
+                        cap = min(local_restart, sol_prev.size) * local_iters
+                        fol.gmres(swp, i, gst["hist"], gst["gm_tol"], gst["iters"],
+                                  other["iters"], cap)
+                        force = other["iters"]
+                        gst = {}
                     sol = solve3d_2(Phi1, A1, Phi2, rhs, real_tol, sol_prev,
-                                    local_restart, local_iters, st, prec)  # :501
+                                    local_restart, local_iters, gst, prec, force)  # :501
+                    st["matvecs"] += gst.get("matvecs", 0)
+                    step_iters = gst["iters"]
+                    gm_margin = min((abs(v / gst["gm_tol"] - 1.0) for v in gst["hist"]),
+                                    default=None)
                     info["local_solves"] += 1
                     res_new = np.linalg.norm(bfun3(Phi1, A1, Phi2, sol) - rhs) / norm_rhs   # :504
                     mv_count()
@@ -470,26 +602,40 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
             res_list.append(res_prev)
 
             sol = rs(sol, rx[i] * n[i], rx[i + 1])                     # :530
+            thr, rank_margin = None, None
             if kickrank >= 0 and i < d - 1:                            # :532
                 u, s, vh = np.linalg.svd(sol, full_matrices=False)     # :533
                 v = vh.T
                 K = min(rx[i] * n[i], rx[i + 1])
                 thr = max(real_tol * resid_damp, res_new)
+                cand = {}
+
+                def res_of(rr):
+                    if rr not in cand:
+                        cursol = (u[:, :rr] * s[:rr]) @ v[:, :rr].T
+                        if full:
+                            cand[rr] = np.linalg.norm(B @ rs(cursol, cursol.size) - rhs) / norm_rhs
+                        else:
+                            cand[rr] = np.linalg.norm(bfun3(Phi1, A1, Phi2, rs(cursol, cursol.size))
+                                                      - rhs) / norm_rhs
+                            mv_count()
+                    return cand[rr]
+
                 r = None
                 for r in range(K - 1, 0, -1):                          # :539-550
-                    cursol = (u[:, :r] * s[:r]) @ v[:, :r].T
-                    if full:
-                        res = np.linalg.norm(B @ rs(cursol, cursol.size) - rhs) / norm_rhs
-                    else:
-                        res = np.linalg.norm(bfun3(Phi1, A1, Phi2, rs(cursol, cursol.size)) - rhs) / norm_rhs
-                        mv_count()
+                    res = res_of(r)
                     if res > thr:
                         break
+                rank_margin = min((abs(v_ / thr - 1.0) for v_ in cand.values()), default=None)
                 # MATLAB leaves r at the last loop value (1) when no break
                 # happens; an empty loop (K == 1) leaves r empty, treated as K-1.
                 r = (K - 1 if r is None else r) + 1                    # :551
                 r = min(r, s.size)                                     # :593
                 r = min(r, rmax)                                       # :594
+                if other is not None:
+                    r_own = r
+                    r = other["rank"]
+                    fol.rank(swp, i, r_own, r, K, min(s.size, rmax), thr, res_of)
             else:                                                      # :596-601
                 u, v = np.linalg.qr(sol)
                 v = v.T
@@ -497,6 +643,10 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
                 s = np.ones(r)
             u = u[:, :r]                                               # :603
             v = v[:, :r] * s[:r]                                       # :604
+            if trace is not None:
+                trace.append(dict(sweep=swp, core=i, rank=r if i < d - 1 else -1,
+                                  iters=step_iters, res_prev=res_prev, res_new=res_new,
+                                  thr=thr, rank_margin=rank_margin, gmres_margin=gm_margin))
 
             if use_z and not last_sweep:                               # :605-623
                 crzAt = bfun3(phiza[i], A1, phiza[i + 1], rs(u @ v.T, u.shape[0] * v.shape[0]))
@@ -545,8 +695,8 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
                 crx[i + 1] = v
                 if use_z and not last_sweep:                           # :770-774
                     rz[i + 1] = rznew
-                    phiza[i + 1], _ = compute_next_Phi(phiza[i], crznew_core(crz[i]), crA[i], crx[i], "lr", extnrm=nrmsa[i])
-                    phizy[i + 1], _ = compute_next_Phi(phizy[i], crznew_core(crz[i]), None, cry[i], "lr", extnrm=nrmsy[i])
+                    phiza[i + 1], _ = compute_next_Phi(phiza[i], crz[i], crA[i], crx[i], "lr", extnrm=nrmsa[i])
+                    phizy[i + 1], _ = compute_next_Phi(phizy[i], crz[i], None, cry[i], "lr", extnrm=nrmsy[i])
             else:
                 crx[i] = rs(sol, rx[i], n[i], rx[i + 1])               # :778-779
 
@@ -560,16 +710,17 @@ def amen_solve2(A, y, tol, x0, z0=None, **opts):
                   % (swp, max_dx, max_res, max(rx)))                   # :793-795
         if last_sweep:                                                 # :797-799
             break
-        if max_res < tol_exit:                                         # :806-808
+        stop = max_res < tol_exit                                      # :806-808
+        if fol is not None:
+            stop = fol.stop(swp, max_res, tol_exit)
+        if stop:
             last_sweep = True
 
     nx = np.exp(np.sum(np.log(nrmsx)) / d)                             # :816
     crx = [c * nx for c in crx]                                        # :818-820
     info["matvecs"] = st["matvecs"]
     info["ranks"] = list(rx)
+    if fol is not None:
+        info["flips"] = fol.flips
+        info["mismatches"] = fol.mismatches
     return TT(crx), info
-
-
-def crznew_core(c):
-    """Identity helper: the freshly orthogonalised Z core (``amen_solve2.m:621-622``)."""
-    return c

@@ -13,7 +13,7 @@ relative residual ``||A x - rhs|| / ||rhs||`` recomputed by the oracle.
 2x2 cores and a right-hand side): parsed header fields, shapes, cores and
 the SHA-256 of the original bytes, so the tests can rebuild the exact files.
 
-Usage: ``python tests/golden/make_golden.py [path-to-TT-Toolbox]``
+Usage: ``python tests/golden/make_golden.py <path-to-TT-Toolbox>`` (required).
 """
 import os
 import sys
@@ -76,4 +76,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <TT-Toolbox source tree>")
+    main(sys.argv[1])

@@ -130,6 +130,47 @@ def test_round_parity(ctx, cfg):
     assert tt_rel(got, x) <= max(cfg["eps"], 1e-13)
 
 
+def _round_strict(ctx, x, eps, rmax=None):
+    """Ranks identical at every core whose my_chop2 decision is not a near
+    tie; when none is, the rounded tensors agree to 1e-10."""
+    ref, info = tt_round(x, eps, rmax)
+    st = {}
+    got = back(ttgpu.round(host_tt(x), eps, rmax=rmax, ctx=ctx, stats=st))
+    ties = [i for i, m in enumerate(info["margins"]) if m is not None and m < NEAR_TIE]
+    for i in range(x.d + 1):
+        if i not in ties:
+            assert got.r[i] == ref.r[i], (i, got.r[i], ref.r[i])
+    if not ties:
+        assert tt_rel(got, ref) < SOLVE_TOL
+    return got, ref, info, st
+
+
+def test_round_parity_config2(ctx):
+    """Full size: d=20, n=16, the sum of four rank-64 Gaussian TTs (internal
+    ranks 256 by concatenation) rounded at eps 1e-8."""
+    x = round_config(d=20, n=16, r=64, terms=4, seed=2)
+    got, ref, info, st = _round_strict(ctx, x, 1e-8)
+    assert list(got.r) == [1, 16] + [256] * 17 + [16, 1]
+    # the round.m guarantee, measured on the GPU result
+    assert tt_rel(got, x) <= 1e-8
+
+
+@pytest.mark.parametrize("r,decay", [(40, 0.3), (128, 0.1)])
+def test_round_parity_truncating(ctx, r, decay):
+    """Ranks that are actually cut inside a decaying spectrum: every core's
+    right rank index is scaled by exp(-decay * j), so my_chop2 cuts each
+    unfolding part-way down its singular values at eps 1e-4."""
+    rng = np.random.default_rng(23)
+    x = tt_randn(16, 8, r, rng, scale=lambda r1, nn, r2: 1.0 / np.sqrt(r1 * nn))
+    cores = [c.copy() for c in x.cores]
+    for k in range(x.d - 1):
+        cores[k] = cores[k] * np.exp(-decay * np.arange(cores[k].shape[2]))[None, None, :]
+    xt = TT(cores)
+    got, ref, info, _ = _round_strict(ctx, xt, 1e-4)
+    assert 16 < max(ref.r[2:-2]) < r
+    assert tt_rel(got, xt) <= 1e-4
+
+
 def test_round_rmax_and_full_tensor(ctx):
     x = round_config(d=5, n=3, r=4, terms=2, seed=5)
     ref, _ = tt_round(x, 1e-14, 3)
@@ -169,34 +210,66 @@ def test_amen_parity_dense_branch(ctx):
     assert tt_rel(got, ref) < SOLVE_TOL
 
 
-def _trajectory_parity(A, y, ref, info, got, st, tol):
-    """Loose tolerance.  The reference's rank rule keeps the first rank whose
-    residual exceeds max(real_tol*resid_damp, res_new) (amen_solve2.m:547):
-    when the local GMRES stops above the threshold, candidate residuals sit
-    within rounding of res_new, so two FP64 implementations may pick
-    different ranks from the first sweep on.  The first sweep's max residual
-    (set by x0) must agree to 1e-6; both runs must stop on the reference's
-    criterion with comparable true residuals."""
-    np.testing.assert_allclose(st["max_res"][:1], info["max_res"][:1], rtol=1e-6)
-    assert abs(st["sweeps"] - info["sweeps"]) <= 2
-    assert st["max_res"][-1] < tol
-    rg, rr = true_residual(A, got, y), true_residual(A, ref, y)
-    assert rg < 10 * max(rr, tol)
-    assert tt_rel(got, ref) < 100 * tol
+# A decision is a near tie when the compared quantity (a candidate residual
+# against the truncation threshold, a Krylov residual estimate against the
+# GMRES tolerance, a sweep's max residual against tol) lies within this
+# relative distance of its threshold: two FP64 implementations that round
+# differently may then decide differently.  Everywhere else the decisions
+# must be identical.
+NEAR_TIE = 1e-6
+
+
+def _strict_parity(ctx, A, y, x0, z0, tol, **opts):
+    """The north-star bar for the FP64 form: the GPU solve records every
+    discrete decision (kept rank and Krylov step count of each local step,
+    the per-sweep stopping test); the oracle replays the solve, checks each
+    decision against its own, adopts the GPU's choice only at near ties and
+    lists every other difference.  Then: no non-near-tie difference, the
+    same sweep count and ranks, and the two solutions within 1e-10
+    (TT-relative, gauge-invariant)."""
+    trace, st = [], {}
+    got = back(ttgpu.amen_solve2(host_mat(A), host_tt(y), tol, x0=host_tt(x0), z0=host_tt(z0),
+                                 ctx=ctx, stats=st, trace=trace, **opts))
+    otrace = []
+    ref, info = oamen.amen_solve2(A, y, tol, x0, z0, trace=otrace,
+                                  follow=dict(steps=trace, max_res=st["max_res"]),
+                                  near_tie=NEAR_TIE, **opts)
+    assert info["mismatches"] == [], info["mismatches"][:5]
+    assert st["sweeps"] == info["sweeps"]
+    assert len(trace) == len(otrace)
+    for g, o in zip(trace, otrace):
+        assert (g["sweep"], g["core"], g["rank"], g["iters"]) == \
+            (o["sweep"], o["core"], o["rank"], o["iters"])
+        # the local residuals that enter the decisions, step by step
+        assert g["res_prev"] == pytest.approx(o["res_prev"], rel=1e-6, abs=1e-14)
+    assert list(got.r) == list(ref.r)
+    err = tt_rel(got, ref)
+    assert err < SOLVE_TOL, err
+    margins = [o["rank_margin"] for o in otrace if o["rank_margin"] is not None]
+    return dict(flips=info["flips"], err=err, sweeps=info["sweeps"],
+                min_rank_margin=min(margins) if margins else None)
 
 
 def test_amen_parity_config1(ctx):
-    """The reference's CPU-runnable workload: d=8, n=32 Laplacian, tol 1e-6, rmax 20."""
+    """The reference's CPU-runnable workload at full size: d=8, n=32
+    Laplacian, tol 1e-6, rmax 20."""
     A, y, x0, z0 = laplace_config(d=8, n=32)
-    ref, info, got, st = _amen_pair(ctx, A, y, x0, z0, 1e-6, rmax=20)
-    _trajectory_parity(A, y, ref, info, got, st, 1e-6)
-    assert true_residual(A, got, y) < 1e-5
+    r = _strict_parity(ctx, A, y, x0, z0, 1e-6, rmax=20)
+    assert r["sweeps"] >= 2
 
 
 def test_amen_parity_aniso_rank3(ctx):
     A, y, x0, z0 = aniso_config(d=5, n=16)
-    ref, info, got, st = _amen_pair(ctx, A, y, x0, z0, 1e-8, rmax=64, nswp=20)
-    _trajectory_parity(A, y, ref, info, got, st, 1e-8)
+    _strict_parity(ctx, A, y, x0, z0, 1e-8, rmax=64, nswp=20)
+
+
+def test_amen_parity_config3(ctx):
+    """The headline workload at full size, FP64 form: d=10, n=64
+    anisotropic diffusion + reaction (operator rank 3), rank-4 right-hand
+    side, rmax 128, tol 1e-8."""
+    A, y, x0, z0 = aniso_config(d=10, n=64, seed=3)
+    r = _strict_parity(ctx, A, y, x0, z0, 1e-8, rmax=128, nswp=50)
+    assert r["sweeps"] >= 2
 
 
 def test_amen_device_drawn_initial_guess(ctx):

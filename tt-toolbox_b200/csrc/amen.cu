@@ -235,6 +235,10 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   TTG_REQUIRE(o.nswp >= 1 && o.local_restart >= 1 && o.local_iters >= 1 && o.rmax >= 1 &&
                   o.kickrank >= 0,
               "invalid options");
+  require_finite(Ah, "A");
+  require_finite(yh, "y");
+  require_finite(x0h, "x0");
+  require_finite(z0h, "z0");
   const std::vector<int64_t> n = yh->n;
   const int64_t nswp = o.nswp, rmax = o.rmax, max_full_size = o.max_full_size;
   const int64_t kickrank = o.kickrank;
@@ -307,6 +311,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   bool last_sweep = false;
   int64_t local_solves = 0, gmres_iters = 0, mv_fp64 = 0;
   int64_t swp_done = 0;
+  int64_t trace_len = 0;
 
   for (int64_t swp = 1; swp <= nswp; ++swp) {                           // :296
     // ------------- right-to-left orthogonalisation (:299-438)
@@ -415,6 +420,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
       const bool full = N < max_full_size;                                // :468
       DBuf<double> sol(c, N), tmp(c, N), B, t1(c, md.t1_size()), t2(c, md.t2_size());
       bool have_bsol = false;  // tmp = B sol (FP64) after the local solve
+      int64_t step_iters = -1;  // Krylov steps of this local solve (trace)
       if (full) {
         B.reset(c, N * N);
         assemble_local_f64(c, rx[i], n[i], rx[i + 1], ra[i], ra[i + 1], Phi1, A1, Phi2, B.p());
@@ -444,6 +450,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
               tmp.p());                                                   // :501
           local_solves++;
           gmres_iters += lr.iters;
+          step_iters = lr.iters;
           mv_fp64 += lr.matvecs_fp64;
           if (lr.have_bsol) {  // the refinement's last FP64 matvec was B sol: reuse it
             diffnrm_f64(c, N, tmp.p(), rhs.p(), S.p(Scalars::T1), true);  // :504
@@ -551,6 +558,21 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
         u = std::move(Q);
         v.reset(c, r2 * K);
         transpose_f64(c, K, r2, R.p(), K, v.p(), r2);
+      }
+
+      if (o.trace) {  // decision record of this step (one extra read)
+        if (trace_len < o.trace_cap) {
+          double rr[2];
+          read_scalars(c, S.p(Scalars::RES_PREV), rr, 2);
+          ttg_amen_step& t = o.trace[trace_len];
+          t.sweep = swp;
+          t.core = i;
+          t.rank = i < d - 1 ? r : -1;
+          t.iters = step_iters;
+          t.res_prev = rr[0];
+          t.res_new = rr[1];
+        }
+        trace_len++;
       }
 
       prof.mark("lr_z");
@@ -747,6 +769,11 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
     ttg_tt_free(out);
     fail(TTG_ERR_SOLVER, "a device factorization reported a non-zero LAPACK info");
   }
+  if (herr[3]) {  // MATLAB's svd errors when it does not converge (amen_solve2.m:533)
+    ttg_tt_free(out);
+    fail(TTG_ERR_NOCONV, "a Jacobi SVD reached its sweep limit (%d sweeps)",
+         c->jacobi_max_sweeps);
+  }
   if (stats) {
     stats->sweeps = swp_done;
     stats->matvecs = c->matvecs - mv0;
@@ -766,6 +793,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
     stats->gflop_fp64 = (c->mv_flops[0] - flk0[0]) * 1e-9;
     stats->ms_fp64 = c->mv_ms[0] - msk0[0];
     stats->ms_matvec = o.precision == TTG_MIXED ? stats->ms_lp : stats->ms_fp64;
+    stats->trace_len = trace_len;
   }
   return out;
 }

@@ -81,6 +81,10 @@ int ttg_amen_mv(ttg_tt A, ttg_tt x, double tol, const ttg_amen_mv_opts* opts, tt
               "border ranks must be 1");
   Context* c = A->ctx;
   TTG_CUDA(cudaSetDevice(c->device));
+  require_finite(A, "A");
+  require_finite(x, "x");
+  require_finite(y0, "y0");
+  require_finite(z0, "z0");
   TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 8 * sizeof(int), c->stream));
   const std::vector<int64_t>& n = A->n;
   const std::vector<int64_t>& ra = A->r;

@@ -52,6 +52,45 @@ void ttg_amen_opts_default(ttg_amen_opts* o) {
   o->seed = 0x243F6A8885A308D3ull;
   o->timing = 0;
   o->reserved = 0;
+  o->trace = nullptr;
+  o->trace_cap = 0;
+}
+
+int ttg_context_set_option(ttg_context ctx, int32_t key, int64_t value) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx, "NULL argument");
+  switch (key) {
+    case TTG_OPT_JACOBI_MAX_SWEEPS:
+      TTG_REQUIRE(value >= 1 && value <= 1000, "Jacobi sweep limit %lld out of [1, 1000]",
+                  (long long)value);
+      ctx->c.jacobi_max_sweeps = int(value);
+      break;
+    default:
+      fail(TTG_ERR_INVALID, "unknown context option %d", int(key));
+  }
+  TTG_API_END
+}
+
+int ttg_selftest_wait(ttg_context ctx, int32_t which) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx, "NULL argument");
+  TTG_REQUIRE(which >= 0 && which <= 3, "unknown wait %d", int(which));
+  Context* c = &ctx->c;
+  TTG_CUDA(cudaSetDevice(c->device));
+  DBuf<int> flag(c, 1);
+  TTG_CUDA(cudaMemsetAsync(flag.p(), 0, sizeof(int), c->stream));
+  const long long limit = 1 << 14;
+  switch (which) {
+    case 0: selftest_wait_gmres(c, flag.p(), limit); break;
+    case 1: selftest_wait_mbarrier(c, flag.p(), limit); break;
+    case 2: selftest_wait_jacobi(c, flag.p(), limit); break;
+    default: selftest_wait_arnoldi(c, flag.p(), limit); break;
+  }
+  int h = 0;
+  TTG_CUDA(cudaMemcpyAsync(&h, flag.p(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  if (h) fail(TTG_ERR_TIMEOUT, "bounded device wait %d gave up (code %d)", int(which), h);
+  TTG_API_END
 }
 
 int ttg_round(ttg_tt in, double eps, const int64_t* rmax, int64_t nrmax, int32_t precision,
@@ -291,6 +330,7 @@ int ttg_amen_solve_batch(ttg_context ctx, int64_t count, const ttg_tt* A, const 
       // Cooperative Krylov grids are sized from num_sms: a share of the SMs
       // per worker lets the workers' grids be resident together.
       w[k]->num_sms = share;
+      w[k]->jacobi_max_sweeps = owner->jacobi_max_sweeps;
     }
   }
   ttg_amen_opts dflt;

@@ -66,7 +66,7 @@ __device__ double block_sum_all(double v) {
   return sh[32];
 }
 
-__device__ void grid_barrier(unsigned* bar, int* err) {
+__device__ void grid_barrier(unsigned* bar, int* err, long long limit = BAR_SPIN_LIMIT) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = bar + 1;
@@ -82,7 +82,7 @@ __device__ void grid_barrier(unsigned* bar, int* err) {
       long long spins = 0;
       while (*vgen == gen) {
         if (*verr) break;
-        if (++spins > BAR_SPIN_LIMIT) {
+        if (++spins > limit) {
           atomicExch(err, 1);
           break;
         }
@@ -398,6 +398,21 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
   }
   res.relres = curres;
   return res;
+}
+
+// Self-test of the bounded grid barrier: block 1 never arrives, so block 0
+// waits until its (small) poll limit runs out and raises *flag.
+__global__ void k_selftest_grid_barrier(unsigned* bar, int* flag, long long limit) {
+  if (blockIdx.x != 0) return;
+  grid_barrier(bar, flag, limit);
+}
+
+void selftest_wait_gmres(Context* c, int* flag, long long limit) {
+  DBuf<unsigned> bar(c, 2);
+  TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 2 * sizeof(unsigned), c->stream));
+  k_selftest_grid_barrier<<<2, 32, 0, c->stream>>>(bar.p(), flag, limit);
+  TTG_CHECK_LAUNCH();
+  sync(c);
 }
 
 }  // namespace ttg

@@ -124,6 +124,8 @@ struct Context {
   // Device int slots: 0-7 error flags of bounded waits and factorizations
   // (cleared per solve), 63 the arrival counter of the one-launch reductions.
   int* d_err = nullptr;
+  // Sweep limit of the one-sided Jacobi SVDs (ttg_context_set_option).
+  int jacobi_max_sweeps = 40;
   // Per-output-tile arrival counters of split-K GEMMs (GEMM_TILE_COUNTERS,
   // zero between launches: the last slice of a tile resets its counter).
   unsigned* d_tile_cnt = nullptr;

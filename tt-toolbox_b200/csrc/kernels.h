@@ -23,6 +23,22 @@ double nrm2_host(Context* c, int64_t n, const double* x);
 void diffnrm_f64(Context* c, int64_t n, const double* x, const double* y, double* out,
                  bool do_sqrt = true);
 
+// Number of NaN / Inf entries of x (synchronises): the input checks of the
+// API entries.
+int64_t count_nonfinite_f64(Context* c, int64_t n, const double* x);
+// Fails with TTG_ERR_INVALID when a core of t holds NaN or Inf (one device
+// pass and one read-back); name is the argument name in the message.
+void require_finite(const ttg_tt_s* t, const char* name);
+
+// Self-tests of the bounded device waits (ttg_selftest_wait): each runs the
+// wait helper of one kernel family with a small poll limit on a condition
+// that nothing satisfies, so that *flag (device int, zeroed by the caller)
+// ends up non-zero; synchronises.
+void selftest_wait_gmres(Context* c, int* flag, long long limit);
+void selftest_wait_mbarrier(Context* c, int* flag, long long limit);
+void selftest_wait_jacobi(Context* c, int* flag, long long limit);
+void selftest_wait_arnoldi(Context* c, int* flag, long long limit);
+
 // y = a*x + b*y ; with a, b host scalars.
 void axpby_f64(Context* c, int64_t n, double a, const double* x, double b, double* y);
 // y = x * s[0] / s[1] style scaling with device scalars: y = x * (num ? *num : 1) / (den ? *den : 1)

@@ -289,6 +289,17 @@ void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int 
 // Elementwise
 // ---------------------------------------------------------------------------
 
+__global__ void k_count_nonfinite(int64_t n, const double* __restrict__ x,
+                                  unsigned long long* __restrict__ out) {
+  pdl_begin();
+  unsigned long long cnt = 0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    cnt += isfinite(x[i]) ? 0ull : 1ull;
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
 __global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b,
                         double* __restrict__ y) {
   pdl_begin();
@@ -563,6 +574,24 @@ double nrm2_host(Context* c, int64_t n, const double* x) {
   double h = 0.0;
   read_scalars(c, s.p(), &h, 1);
   return h;
+}
+
+int64_t count_nonfinite_f64(Context* c, int64_t n, const double* x) {
+  if (n <= 0) return 0;
+  DBuf<unsigned long long> cnt(c, 1);
+  TTG_CUDA(cudaMemsetAsync(cnt.p(), 0, sizeof(unsigned long long), c->stream));
+  launch(c, k_count_nonfinite, grid_for(c, n), 256, 0, n, x, cnt.p());
+  TTG_CHECK_LAUNCH();
+  unsigned long long h = 0;
+  TTG_CUDA(cudaMemcpyAsync(&h, cnt.p(), sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  return int64_t(h);
+}
+
+void require_finite(const ttg_tt_s* t, const char* name) {
+  if (!t) return;
+  const int64_t bad = count_nonfinite_f64(t->ctx, t->numel, t->core);
+  TTG_REQUIRE(bad == 0, "%s holds %lld non-finite entries (NaN or Inf)", name, (long long)bad);
 }
 
 void axpby_f64(Context* c, int64_t n, double a, const double* x, double b, double* y) {

@@ -166,6 +166,40 @@ int64_t svd_f64(Context* c, int64_t m, int64_t n, const double* A, double* U, do
   return k;
 }
 
+namespace {
+// Economy SVD of a tall m x n (m >= n) matrix by cuSOLVER's bidiagonal QR
+// (gesvd): the fallback when the Jacobi SVD reaches its sweep limit.
+void svd_gesvd_tall(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
+                    double* VT) {
+  const int mi = as_int(m, "m"), ni = as_int(n, "n");
+  DBuf<double> W(c, m * n), rw(c, std::max<int64_t>(n, 1));
+  DBuf<int> info(c, 1);
+  copy_f64(c, m * n, A, W.p());
+  int lwork = 0;
+  TTG_SOLVER(cusolverDnDgesvd_bufferSize(c->solver, mi, ni, &lwork));
+  DBuf<double> ws(c, std::max(lwork, 1));
+  TTG_SOLVER(cusolverDnDgesvd(c->solver, 'S', 'S', mi, ni, W.p(), mi, S, U, mi, VT, ni, ws.p(),
+                              lwork, rw.p(), info.p()));
+  check_info(c, info.p(), "gesvd");
+}
+}  // namespace
+
+int64_t svd_f64_fallback(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
+                         double* VT) {
+  const int64_t k = std::min(m, n);
+  if (k <= 0) return 0;
+  if (m >= n) {
+    svd_gesvd_tall(c, m, n, A, U, S, VT);
+  } else {
+    DBuf<double> At(c, n * m), Up(c, n * m), VTp(c, m * m);
+    transpose_f64(c, m, n, A, m, At.p(), n);
+    svd_gesvd_tall(c, n, m, At.p(), Up.p(), S, VTp.p());
+    transpose_f64(c, m, m, VTp.p(), m, U, m);
+    transpose_f64(c, n, m, Up.p(), n, VT, m);
+  }
+  return k;
+}
+
 void lu_solve_f64(Context* c, int64_t N, const double* B, double* rhs, int64_t nrhs) {
   const int Ni = as_int(N, "N"), nr = as_int(nrhs, "nrhs");
   DBuf<double> W(c, N * N);

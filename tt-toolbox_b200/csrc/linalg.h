@@ -26,6 +26,12 @@ int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, dou
 int64_t svd_f64(Context* c, int64_t m, int64_t n, const double* A, double* U, double* S,
                 double* VT);
 
+// The same economy SVD by cuSOLVER's bidiagonal QR (gesvd): the fallback
+// of the rounding sweep when a Jacobi SVD reaches its sweep limit, as
+// round.m:64-74 falls back to svds when MATLAB's svd does not converge.
+int64_t svd_f64_fallback(Context* c, int64_t m, int64_t n, const double* A, double* U,
+                         double* S, double* VT);
+
 // Solve the square N x N system B X = RHS (nrhs columns) by LU with partial
 // pivoting; RHS is overwritten by X.  B is not modified.
 void lu_solve_f64(Context* c, int64_t N, const double* B, double* rhs, int64_t nrhs = 1);

@@ -70,7 +70,7 @@ __device__ __forceinline__ double warp_sumd(double v) {
   return v;
 }
 
-__device__ void ar_barrier(unsigned* bar, int* err) {
+__device__ void ar_barrier(unsigned* bar, int* err, long long limit = AR_SPIN_LIMIT) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = bar + 1;
@@ -86,7 +86,7 @@ __device__ void ar_barrier(unsigned* bar, int* err) {
       long long spins = 0;
       while (*vgen == gen) {
         if (*verr) break;
-        if (++spins > AR_SPIN_LIMIT) {
+        if (++spins > limit) {
           atomicExch(err, 4);
           break;
         }
@@ -495,6 +495,23 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
   // checked by the caller once its sequence is done.
   out.matvecs = out.iters;
   return out;
+}
+
+namespace {
+__global__ void k_selftest_ar_barrier(unsigned* bar, int* flag, long long limit) {
+  if (blockIdx.x != 0) return;
+  ar_barrier(bar, flag, limit);
+}
+}  // namespace
+
+// Self-test of the bounded barrier of the Arnoldi kernels: block 1 never
+// arrives; block 0 gives up after `limit` polls and raises *flag.
+void selftest_wait_arnoldi(Context* c, int* flag, long long limit) {
+  DBuf<unsigned> bar(c, 2);
+  TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 2 * sizeof(unsigned), c->stream));
+  k_selftest_ar_barrier<<<2, 32, 0, c->stream>>>(bar.p(), flag, limit);
+  TTG_CHECK_LAUNCH();
+  sync(c);
 }
 
 }  // namespace ttg

@@ -514,4 +514,25 @@ void rev_to_nat_add(Context* c, int64_t r1, int64_t n, int64_t r2, const float* 
   TTG_CHECK_LAUNCH();
 }
 
+namespace {
+// An mbarrier that expects one arrival which never comes: the bounded wait
+// of the tcgen05 pipeline gives up after `limit` polls and raises *flag.
+__global__ void k_selftest_mbar(int* flag, long long limit) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = umma::smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    umma::mbar_init(b, 1);
+    umma::fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) umma::mbar_wait(b, 0, flag, limit);
+}
+}  // namespace
+
+void selftest_wait_mbarrier(Context* c, int* flag, long long limit) {
+  k_selftest_mbar<<<1, 32, 0, c->stream>>>(flag, limit);
+  TTG_CHECK_LAUNCH();
+  sync(c);
+}
+
 }  // namespace ttg

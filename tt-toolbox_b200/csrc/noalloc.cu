@@ -51,7 +51,9 @@ extern "C" int ttg_local_matvec_noalloc(void* stream, int64_t rx1, int64_t n, in
   TTG_REQUIRE(Phi1 && A && Phi2 && x && y, "NULL argument");
   TTG_REQUIRE(rx1 >= 1 && n >= 1 && rx2 >= 1 && ra1 >= 1 && ra2 >= 1, "sizes must be >= 1");
   MvDims d{rx1, rx1, ra1, n, n, rx2, ra2, rx2};
-  const double need = double(d.t1_size()) + double(d.t2_size());
+  // In double from the start: int64 products of large sizes could wrap.
+  const double need = double(rx1) * double(n) * double(ra2) * double(rx2) +
+                      double(rx1) * double(ra1) * double(n) * double(rx2);
   TTG_REQUIRE(need <= double(kNoallocScratchDoubles),
               "ttg_local_matvec_noalloc: the intermediates need %.0f doubles, more than the "
               "built-in scratch of %zu doubles (64 MiB); use ttg_local_matvec",

@@ -56,6 +56,9 @@ ttg_tt_s* round_tt(ttg_tt_s* in, double eps, const std::vector<int64_t>& rmax_in
   TTG_REQUIRE(!in->is_matrix, "round: TT matrices are rounded through their tensor form");
   TTG_REQUIRE(precision == TTG_FP64 || precision == TTG_MIXED, "round: unknown precision %d",
               precision);
+  if (precision != TTG_FP64)
+    fail(TTG_ERR_UNSUPPORTED, "round: only precision TTG_FP64 is implemented");
+  require_finite(in, "the input tensor");
   const int64_t d = in->d;
   std::vector<int64_t> n = in->n, r = in->r;
   std::vector<int64_t> rmax(d + 1, INT64_MAX);
@@ -73,6 +76,7 @@ ttg_tt_s* round_tt(ttg_tt_s* in, double eps, const std::vector<int64_t>& rmax_in
   }
   std::vector<double> nrm(d, 0.0);
   double ms_qr = 0, ms_svd = 0;
+  int64_t fallbacks = 0;
   {
     Timer tq(c);
     // Left-to-right QR sweep (round.m:39-53).
@@ -102,8 +106,18 @@ ttg_tt_s* round_tt(ttg_tt_s* in, double eps, const std::vector<int64_t>& rmax_in
       const int64_t rows = r[i], cols = n[i] * r[i + 1];
       const int64_t K = std::min(rows, cols);
       DBuf<double> U(c, rows * K), S(c, K), VT(c, K * cols);
+      TTG_CUDA(cudaMemsetAsync(c->d_err + 3, 0, sizeof(int), c->stream));
       svd_f64(c, rows, cols, cr[i].p(), U.p(), S.p(), VT.p());          // round.m:65
       hs.resize(K);
+      int sweep_cap = 0;
+      TTG_CUDA(cudaMemcpyAsync(&sweep_cap, c->d_err + 3, sizeof(int), cudaMemcpyDeviceToHost,
+                               c->stream));
+      sync(c);
+      if (sweep_cap) {  // the Jacobi SVD did not converge: round.m:64-74's fallback
+        TTG_CUDA(cudaMemsetAsync(c->d_err + 3, 0, sizeof(int), c->stream));
+        svd_f64_fallback(c, rows, cols, cr[i].p(), U.p(), S.p(), VT.p());
+        fallbacks++;
+      }
       TTG_CUDA(cudaMemcpyAsync(hs.data(), S.p(), sizeof(double) * K, cudaMemcpyDeviceToHost,
                                c->stream));
       sync(c);
@@ -155,6 +169,7 @@ ttg_tt_s* round_tt(ttg_tt_s* in, double eps, const std::vector<int64_t>& rmax_in
     int64_t mr = 0;
     for (auto v : r) mr = std::max(mr, v);
     stats->max_rank = mr;
+    stats->svd_fallbacks = fallbacks;
   }
   return out;
 }

@@ -74,8 +74,12 @@ int ttg_tt_read_sdv(ttg_context ctx, const char* path, ttg_tt* out) {
   for (int64_t k = 0; k < d; ++k) {
     TTG_REQUIRE(n32[k] >= 1, "%s: mode size %d at %lld", path, n32[k], (long long)k);
     n[k] = n32[k];
+    // Each factor is below 2^31, so the product is formed in double first:
+    // an int64 product of three such values could overflow.
+    const double core_numel = double(r[k]) * double(n[k]) * double(r[k + 1]);
+    TTG_REQUIRE(core_numel + double(numel) < double(int64_t(1) << 40), "%s: core too large",
+                path);
     numel += r[k] * n[k] * r[k + 1];
-    TTG_REQUIRE(numel < (int64_t(1) << 40), "%s: core too large", path);
   }
   std::vector<double> core(numel);
   if (dtype == 0) {

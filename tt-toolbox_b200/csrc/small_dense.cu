@@ -21,7 +21,6 @@ namespace {
 
 constexpr int SD_THREADS = 1024;
 constexpr int SD_WARPS = SD_THREADS / 32;
-constexpr int JAC_MAX_SWEEPS = 40;
 constexpr size_t SMEM_LIMIT = 200 * 1024;
 
 __device__ __forceinline__ double wsum(double v) {
@@ -91,7 +90,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
                                                           double* __restrict__ VT,
                                                           double* __restrict__ Vg,
                                                           double* __restrict__ work, int in_smem,
-                                                          int trans, int* err) {
+                                                          int trans, int* err, int max_sweeps) {
   pdl_begin();
   extern __shared__ double sm[];
   __shared__ double s_off[SD_WARPS];
@@ -110,7 +109,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
   const int ne = (n + 1) & ~1;  // even number of players (dummy column n if odd)
   const double tol = 4.0 * 2.220446049250313e-16, tol2 = tol * tol;
   int sweep = 0;
-  for (sweep = 0; sweep < JAC_MAX_SWEEPS; ++sweep) {
+  for (sweep = 0; sweep < max_sweeps; ++sweep) {
     double off = 0.0;
     for (int r = 0; r < ne - 1; ++r) {
       for (int pr = warp; pr < ne / 2; pr += SD_WARPS) {
@@ -168,7 +167,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
     __syncthreads();
     if (s_done) break;
   }
-  if (tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(err, 5);
+  if (tid == 0 && sweep >= max_sweeps) atomicExch(err, 5);
   jacobi_finish(n, A, V, U, S, VT, work + int64_t(n) * n, trans);
 }
 
@@ -183,7 +182,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
 constexpr int JC_THREADS = 256;
 constexpr long long JC_SPIN_LIMIT = 1LL << 24;
 
-__device__ void jc_barrier(unsigned* bar, int* err) {
+__device__ void jc_barrier(unsigned* bar, int* err, long long limit = JC_SPIN_LIMIT) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = bar + 1;
@@ -199,7 +198,7 @@ __device__ void jc_barrier(unsigned* bar, int* err) {
       long long spins = 0;
       while (*vgen == gen) {
         if (*verr) break;
-        if (++spins > JC_SPIN_LIMIT) {
+        if (++spins > limit) {
           atomicExch(err, 6);
           break;
         }
@@ -218,7 +217,8 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
                                                            int lda, double* A, double* V,
                                                            unsigned* bar,
                                                            unsigned long long* offmax, int* err,
-                                                           int* sweep_err, int trans) {
+                                                           int* sweep_err, int trans,
+                                                           int max_sweeps) {
   __shared__ double red[3][JC_THREADS / 32];
   __shared__ double s_rot[2];
   __shared__ int s_skip;
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
   const int ne = (n + 1) & ~1;
   const double tol = 4.0 * 2.220446049250313e-16;
   int sweep = 0;
-  for (sweep = 0; sweep < JAC_MAX_SWEEPS; ++sweep) {
+  for (sweep = 0; sweep < max_sweeps; ++sweep) {
     const int slot = sweep % 3;
     if (blockIdx.x == 0 && tid == 0) offmax[(sweep + 1) % 3] = 0ull;
     double off = 0.0;
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
     if (m <= tol) break;
     if (*(volatile int*)err) break;
   }
-  if (blockIdx.x == 0 && tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(sweep_err, 5);
+  if (blockIdx.x == 0 && tid == 0 && sweep >= max_sweeps) atomicExch(sweep_err, 5);
 }
 
 __global__ void __launch_bounds__(SD_THREADS) k_jacobi_finish(int n, const double* A,
@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_svd_tall_small(int m, int n,
                                                               int lda, double* __restrict__ U,
                                                               double* __restrict__ S,
                                                               double* __restrict__ VT,
-                                                              int* err) {
+                                                              int* err, int max_sweeps) {
   pdl_begin();
   extern __shared__ double A[];  // m x n
   __shared__ double V[TS_MAX_N * TS_MAX_N];
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_svd_tall_small(int m, int n,
   const int ne = (n + 1) & ~1;
   const double tol = 4.0 * 2.220446049250313e-16, tol2 = tol * tol;
   int sweep = 0;
-  for (sweep = 0; sweep < JAC_MAX_SWEEPS; ++sweep) {
+  for (sweep = 0; sweep < max_sweeps; ++sweep) {
     double off = 0.0;
     for (int r = 0; r < ne - 1; ++r) {
       for (int pr = warp; pr < ne / 2; pr += TS_WARPS) {
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_svd_tall_small(int m, int n,
     __syncthreads();
     if (s_done) break;
   }
-  if (tid == 0 && sweep >= JAC_MAX_SWEEPS) atomicExch(err, 5);
+  if (tid == 0 && sweep >= max_sweeps) atomicExch(err, 5);
   // singular values = column norms, ranked descending (stable on index)
   if (warp < n) {
     const double* aj = A + int64_t(warp) * m;
@@ -668,7 +668,7 @@ void svd_tall_small_f64(Context* c, int64_t m, int64_t n, const double* A, int64
   ensure_smem_attr(reinterpret_cast<const void*>(k_svd_tall_small), c->device,
                    int(128 * 1024 + 1024));
   launch(c, k_svd_tall_small, 1, TS_THREADS, smem, int(m), int(n), A, int(lda), U, S, VT,
-         c->d_err + 3);
+         c->d_err + 3, c->jacobi_max_sweeps);
   TTG_CHECK_LAUNCH();
 }
 
@@ -696,7 +696,8 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
     unsigned long long* offp = offmax.p();
     int* errp = c->d_err + 0;
     int* swp = c->d_err + 3;
-    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp, &trans};
+    int msw = c->jacobi_max_sweeps;
+    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp, &trans, &msw};
     TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_jacobi_coop, dim3(blocks),
                                          dim3(JC_THREADS), args, 0, c->stream));
     launch(c, k_jacobi_finish, 1, SD_THREADS, 0, int(n), work.p(), V.p(), U, S, VT,
@@ -709,8 +710,25 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
                    int(SMEM_LIMIT + 1024));
   const size_t smem = size_t(mode) * mat;
   launch(c, k_jacobi_svd, 1, SD_THREADS, smem, int(n), A, int(lda), U, S, VT, V.p(), work.p(),
-         mode, trans, c->d_err + 3);
+         mode, trans, c->d_err + 3, c->jacobi_max_sweeps);
   TTG_CHECK_LAUNCH();
+}
+
+namespace {
+__global__ void k_selftest_jc_barrier(unsigned* bar, int* flag, long long limit) {
+  if (blockIdx.x != 0) return;
+  jc_barrier(bar, flag, limit);
+}
+}  // namespace
+
+// Self-test of the bounded barrier of the cooperative Jacobi SVD: block 1
+// never arrives; block 0 gives up after `limit` polls and raises *flag.
+void selftest_wait_jacobi(Context* c, int* flag, long long limit) {
+  DBuf<unsigned> bar(c, 2);
+  TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 2 * sizeof(unsigned), c->stream));
+  k_selftest_jc_barrier<<<2, 32, 0, c->stream>>>(bar.p(), flag, limit);
+  TTG_CHECK_LAUNCH();
+  sync(c);
 }
 
 }  // namespace ttg

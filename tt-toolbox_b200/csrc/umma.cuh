@@ -46,8 +46,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
 
 // Wait for the given phase parity; bounded.  Returns false (and sets *err)
 // when the limit is reached or another thread already reported an error.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int* err) {
-  for (long long it = 0; it < MBAR_SPIN_LIMIT; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int* err,
+                                          long long limit = MBAR_SPIN_LIMIT) {
+  for (long long it = 0; it < limit; ++it) {
     if (mbar_try_wait(bar, phase)) return true;
     if ((it & 1023) == 1023 && *(volatile int*)err) return false;
   }

@@ -37,13 +37,25 @@ class TTGError(RuntimeError):
         self.code = code
 
 
+class AmenStep(C.Structure):
+    """``ttg_amen_step``: the decisions of one local step of a sweep."""
+    _fields_ = [("sweep", _i64), ("core", _i64), ("rank", _i64), ("iters", _i64),
+                ("res_prev", C.c_double), ("res_new", C.c_double)]
+
+    def to_dict(self):
+        return dict(sweep=int(self.sweep), core=int(self.core), rank=int(self.rank),
+                    iters=int(self.iters), res_prev=float(self.res_prev),
+                    res_new=float(self.res_new))
+
+
 class AmenOpts(C.Structure):
     _fields_ = [("nswp", _i64), ("rmax", _i64), ("max_full_size", _i64),
                 ("local_restart", _i64), ("local_iters", _i64), ("kickrank", _i64),
                 ("resid_damp", C.c_double), ("tol_exit", C.c_double),
                 ("trunc_norm", C.c_int32), ("local_prec", C.c_int32),
                 ("precision", C.c_int32), ("verb", C.c_int32), ("seed", C.c_uint64),
-                ("timing", C.c_int32), ("reserved", C.c_int32)]
+                ("timing", C.c_int32), ("reserved", C.c_int32),
+                ("trace", C.POINTER(AmenStep)), ("trace_cap", _i64)]
 
 
 MAX_SWEEPS = 64
@@ -56,7 +68,7 @@ class AmenStats(C.Structure):
                 ("ms_total", C.c_double), ("ms_matvec", C.c_double),
                 ("matvec_gflop", C.c_double), ("launches", _i64), ("matvecs_lp", _i64),
                 ("gflop_lp", C.c_double), ("ms_lp", C.c_double), ("gflop_fp64", C.c_double),
-                ("ms_fp64", C.c_double)]
+                ("ms_fp64", C.c_double), ("trace_len", _i64)]
 
     def to_dict(self):
         s = int(self.sweeps)
@@ -68,7 +80,8 @@ class AmenStats(C.Structure):
                     matvec_gflop=float(self.matvec_gflop), launches=int(self.launches),
                     ms_matvec=float(self.ms_matvec), matvecs_lp=int(self.matvecs_lp),
                     gflop_lp=float(self.gflop_lp), ms_lp=float(self.ms_lp),
-                    gflop_fp64=float(self.gflop_fp64), ms_fp64=float(self.ms_fp64))
+                    gflop_fp64=float(self.gflop_fp64), ms_fp64=float(self.ms_fp64),
+                    trace_len=int(self.trace_len))
 
 
 class AmenMvOpts(C.Structure):
@@ -78,7 +91,7 @@ class AmenMvOpts(C.Structure):
 
 class RoundStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_qr_sweep", C.c_double),
-                ("ms_svd_sweep", C.c_double), ("max_rank", _i64)]
+                ("ms_svd_sweep", C.c_double), ("max_rank", _i64), ("svd_fallbacks", _i64)]
 
 
 _lib = None
@@ -139,6 +152,8 @@ def lib():
                                     C.POINTER(C.c_int32)]
     sigs["ttg_grad_xb"] = [_vp, _vp, _vp, _pd]
     sigs["ttg_grad_sampled"] = [_vp, _i64, _vp, _vp, _vp, _pd]
+    sigs["ttg_context_set_option"] = [_vp, C.c_int32, _i64]
+    sigs["ttg_selftest_wait"] = [_vp, C.c_int32]
     for name, args in sigs.items():
         f = getattr(L, name)
         f.argtypes = args
@@ -254,6 +269,19 @@ class Context:
 
     def sync(self):
         _check(lib().ttg_context_sync(self.h))
+
+    # ttg_context_set_option keys
+    OPT_JACOBI_MAX_SWEEPS = 1
+
+    def set_option(self, key, value):
+        """``ttg_context_set_option`` (e.g. the Jacobi SVD sweep limit)."""
+        _check(lib().ttg_context_set_option(self.h, int(key), int(value)))
+
+    def selftest_wait(self, which):
+        """``ttg_selftest_wait``: runs one bounded device wait on a condition
+        that nothing satisfies; raises ``TTGError`` (code 6, TTG_ERR_TIMEOUT)
+        when the wait gave up as designed."""
+        _check(lib().ttg_selftest_wait(self.h, int(which)))
 
     def launch_count(self):
         v = _i64(0)
@@ -393,7 +421,8 @@ def round(tt, eps, rmax=None, precision="fp64", ctx=None, stats=None):
     res = DeviceTT(ctx, out)
     if stats is not None:
         stats.update(ms_total=st.ms_total, ms_qr_sweep=st.ms_qr_sweep,
-                     ms_svd_sweep=st.ms_svd_sweep, max_rank=int(st.max_rank))
+                     ms_svd_sweep=st.ms_svd_sweep, max_rank=int(st.max_rank),
+                     svd_fallbacks=int(st.svd_fallbacks))
     if isinstance(tt, DeviceTT):
         return res
     host = res.download()
@@ -449,18 +478,27 @@ def _amen_opts(opts):
     return o
 
 
-def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
+def amen_solve2(A, y, tol, ctx=None, stats=None, trace=None, **opts):
     """``[x] = amen_solve2(A, y, tol, 'name', value, ...)`` (``solve/amen_solve2.m:1``).
 
     Options follow ``amen_solve2.m:161-203``; unknown names raise
     ``ValueError('Unrecognized option')`` as the reference errors (``:200-201``).
     ``A``: host ``TTMatrix`` or ``DeviceTT``; ``y``/``x0``/``z0``: host
     ``TensorTrain`` or ``DeviceTT``.  Returns a host ``TensorTrain`` when ``y``
-    is a host tensor, else a ``DeviceTT``.
+    is a host tensor, else a ``DeviceTT``.  ``trace``: optional list that
+    receives one dict per local step (``ttg_amen_step``: sweep, core, kept
+    rank, Krylov steps, local residuals before and after).
     """
     opts = _check_amen_opts(opts)
     ctx = ctx or (A.ctx if isinstance(A, DeviceTT) else default_context())
     o = _amen_opts(opts)
+    trace_buf = None
+    if trace is not None:
+        d = A.shape()[0].size if isinstance(A, DeviceTT) else len(A.n)
+        cap = int(o.nswp) * d
+        trace_buf = (AmenStep * max(cap, 1))()
+        o.trace = C.cast(trace_buf, C.POINTER(AmenStep))
+        o.trace_cap = cap
     owned = []
 
     def dev(t):
@@ -483,6 +521,8 @@ def amen_solve2(A, y, tol, ctx=None, stats=None, **opts):
         pass
     if stats is not None:
         stats.update(st.to_dict())
+    if trace is not None:
+        trace.extend(trace_buf[k].to_dict() for k in range(min(int(st.trace_len), o.trace_cap)))
     res = DeviceTT(ctx, out)
     if isinstance(y, DeviceTT):
         for h in owned:
