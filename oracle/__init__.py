@@ -19,6 +19,10 @@ Pinning status
   fixtures ``tests/tt-solve/*.mat`` (stored solutions and their residuals),
   converted into ``tests/golden/*.npz`` by ``tests/golden/make_golden.py``.
   Iterates are not pinned by the reference (MATLAB is not runnable here).
+* ``bfun3``, ``dgmresr_hh``, ``jac_gen``/``jac_apply`` (centre block
+  Jacobi): pinned against the reference's own C (``fmex/solve3d.c``) built
+  by ``oracle/build_ref.py`` into ``oracle/_ref/`` and called through ctypes
+  (``tests/test_oracle_ref.py``).
 * ``amen_sum``: the reference has no tests or golden vectors for it; pinned
   by the exact linear combination at tight tolerance (full tensors at small
   d), rank bounds and tolerance-following errors (``tests/test_oracle_amen_sum.py``).
