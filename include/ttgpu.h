@@ -280,6 +280,32 @@ int ttg_amen_mv_opts_default(ttg_amen_mv_opts* opts);
 int ttg_amen_mv(ttg_tt A, ttg_tt x, double tol, const ttg_amen_mv_opts* opts, ttg_tt y0,
                 ttg_tt z0, ttg_tt* y_out, ttg_tt* z_out, int64_t* sweeps_out);
 
+/* AMEn approximation of linear combinations of TT tensors
+ * ([y, z] = amen_sum(X, v, tol, 'name', value, ...), core/amen_sum.m:1-483,
+ * default path for TT inputs: renorm 'direct', fkick false, kickrank2 0,
+ * multrank false).  X: `count` TT tensors of one context with equal mode
+ * sizes and boundary ranks 1; coef: count x M host array (column-major):
+ * y(:, m) ~ sum_j X[j] coef(j, m), m = 1..M, returned as one TT whose last
+ * rank is M (one tensor for M = 1).  y0 / z0 (nullable) as the options
+ * 'y0' / 'z0'; when NULL, right-orthogonal random TTs of ranks 2 /
+ * kickrank are drawn from opts->seed (the reference draws its own,
+ * amen_sum.m:152-187, from MATLAB's generator).  z_out (nullable) receives
+ * the error TT, sweeps_out (nullable) the sweeps run. */
+typedef struct {
+  int64_t nswp;      /* 20 (amen_sum.m:56)             */
+  int64_t kickrank;  /* 4  (:57); 0 disables z          */
+  int32_t init_qr;   /* 1  (:63)                        */
+  int32_t verb;      /* 0                               */
+  uint64_t seed;     /* random y0 / z0 when NULL        */
+  int64_t rmax;      /* <= 0: no cap (:67, Inf)         */
+  int64_t reserved[3];
+} ttg_amen_sum_opts;
+
+int ttg_amen_sum_opts_default(ttg_amen_sum_opts* opts);
+int ttg_amen_sum(int64_t count, const ttg_tt* X, const double* coef, int64_t M, double tol,
+                 const ttg_amen_sum_opts* opts, ttg_tt y0, ttg_tt z0, ttg_tt* y_out,
+                 ttg_tt* z_out, int64_t* sweeps_out);
+
 /* TT algebra on device-resident handles (the caller side of the path: the
  * true residual ||A x - y|| / ||y||, round's inputs).  Results are new
  * handles of the operands' context; tensors need boundary ranks 1 for dot.

@@ -74,6 +74,7 @@ enum ScalOp : int {
   SC_MUL = 4,        // out *= p0
   SC_MAX_CONST = 5,  // out = max(p0, host constant)
   SC_DIV_NZ = 6,     // out = p1 > 0 ? p0 / p1 : 0
+  SC_ONE_IF_ZERO = 7,  // out = p0 == 0 ? 1 : p0
 };
 void scalar_op(Context* c, int op, double* out, const double* p0, const double* p1 = nullptr,
                const double* p2 = nullptr, double k = 0.0);

@@ -415,6 +415,7 @@ __global__ void k_scalar_op(int op, double* out, const double* p0, const double*
     case 4: *out = *out * *p0; break;
     case 5: *out = fmax(*p0, k); break;
     case 6: *out = (*p1 > 0.0) ? *p0 / *p1 : 0.0; break;
+    case 7: *out = (*p0 == 0.0) ? 1.0 : *p0; break;
     default: break;
   }
 }

@@ -89,6 +89,12 @@ class AmenMvOpts(C.Structure):
                 ("verb", C.c_int32), ("seed", C.c_uint64), ("reserved", _i64 * 4)]
 
 
+class AmenSumOpts(C.Structure):
+    _fields_ = [("nswp", _i64), ("kickrank", _i64), ("init_qr", C.c_int32),
+                ("verb", C.c_int32), ("seed", C.c_uint64), ("rmax", _i64),
+                ("reserved", _i64 * 3)]
+
+
 class RoundStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_qr_sweep", C.c_double),
                 ("ms_svd_sweep", C.c_double), ("max_rank", _i64), ("svd_fallbacks", _i64)]
@@ -153,11 +159,16 @@ def lib():
     sigs["ttg_grad_xb"] = [_vp, _vp, _vp, _pd]
     sigs["ttg_grad_sampled"] = [_vp, _i64, _vp, _vp, _vp, _pd]
     sigs["ttg_context_set_option"] = [_vp, C.c_int32, _i64]
+    sigs["ttg_amen_sum"] = [_i64, C.POINTER(_vp), _pd, _i64, C.c_double,
+                            C.POINTER(AmenSumOpts), _vp, _vp, C.POINTER(_vp), C.POINTER(_vp),
+                            _p64]
     sigs["ttg_selftest_wait"] = [_vp, C.c_int32]
     for name, args in sigs.items():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = C.c_int
+    L.ttg_amen_sum_opts_default.argtypes = [C.POINTER(AmenSumOpts)]
+    L.ttg_amen_sum_opts_default.restype = C.c_int
     L.ttg_amen_mv_opts_default.argtypes = [C.POINTER(AmenMvOpts)]
     L.ttg_amen_mv_opts_default.restype = C.c_int
     L.ttg_amen_opts_default.argtypes = [C.POINTER(AmenOpts)]
@@ -996,3 +1007,46 @@ def amen_mv(A, x, tol, y0=None, z0=None, ctx=None, nswp=20, kickrank=4, init_qr=
         for t in owned:
             t.free()
 
+
+def amen_sum(X, c, tol, y0=None, z0=None, ctx=None, nswp=20, kickrank=4, init_qr=True, rmax=None,
+             verb=0, seed=None):
+    """``[y, z] = amen_sum(X, c, tol, 'y0', y0, 'z0', z0, ...)``
+    (``core/amen_sum.m``): ``y(:, m) ~ sum_j X[j] c[j, m]``.  ``X``: list of
+    TT tensors (host or ``DeviceTT``); ``c``: ``len(X)`` coefficients or a
+    ``len(X) x M`` array.  Returns ``(y, z, sweeps)``: host TTs unless
+    ``X[0]`` is a ``DeviceTT``; ``y`` has last rank ``M``; ``z`` is None
+    when ``kickrank`` is 0."""
+    coef = np.asarray(c, dtype=np.float64)
+    if coef.ndim == 1:
+        coef = coef[:, None]
+    N, M = coef.shape
+    if len(X) != N:
+        raise ValueError("c must have len(X) rows")
+    ctx = _ctx_of(ctx, *X)
+    o = AmenSumOpts()
+    lib().ttg_amen_sum_opts_default(C.byref(o))
+    o.nswp, o.kickrank, o.init_qr, o.verb = int(nswp), int(kickrank), int(bool(init_qr)), int(verb)
+    if rmax is not None and np.isfinite(rmax):
+        o.rmax = int(rmax)
+    if seed is not None:
+        o.seed = int(seed)
+    owned, hs = _dev_args(ctx, *(list(X) + [t for t in (y0, z0) if t is not None]))
+    dX = hs[:N]
+    rest = iter(hs[N:])
+    dy0 = next(rest) if y0 is not None else None
+    dz0 = next(rest) if z0 is not None else None
+    HX = (_vp * N)(*[h.h for h in dX])
+    cf = np.asfortranarray(coef).ravel(order="F").copy()
+    yh, zh, sw = _vp(), _vp(), _i64(0)
+    try:
+        _check(lib().ttg_amen_sum(N, HX, _ptrd(cf), M, float(tol), C.byref(o),
+                                  dy0.h if dy0 is not None else None,
+                                  dz0.h if dz0 is not None else None,
+                                  C.byref(yh), C.byref(zh), C.byref(sw)))
+        dev = isinstance(X[0], DeviceTT)
+        y = _result(ctx, yh, dev)
+        z = _result(ctx, zh, dev) if zh.value else None
+        return y, z, sw.value
+    finally:
+        for t in owned:
+            t.free()
