@@ -152,7 +152,8 @@ typedef struct {
   double resid_damp;     /* 2    */
   double tol_exit;       /* <= 0: tol                       */
   int32_t trunc_norm;    /* 1 = 'residual' (only value supported) */
-  int32_t local_prec;    /* 0 = '', 1 = 'cjacobi' (FP64 only); amen_solve2.m:205-207 */
+  int32_t local_prec;    /* 0 '', 1 'cjacobi', 2 'ljacobi', 3 'rjacobi' (FP64 only);
+                            amen_solve2.m:205-207                           */
   int32_t precision;     /* TTG_FP64 or TTG_MIXED           */
   int32_t verb;          /* 0 silent, 1 per-sweep line on stderr */
   uint64_t seed;         /* seed for device-drawn x0/z0     */
@@ -215,9 +216,10 @@ int ttg_next_phi(ttg_context ctx, int32_t dir, int64_t rx1, int64_t n,
 /* Local solve with the signature of the MEX gateway
  * sol = solve3d_2(Phi1, A, Phi2, rhs, tol, trunc_norm, sol_prev, prec,
  *                 nrestart, niters, verb)       (fmex/solve3d_2.c:121-122)
- * Residual branch (trunc_norm = 1) only; prec 0 (none) or 1 ('cjacobi', the
- * centre block-Jacobi preconditioner of solve/solve3d_2ml.m:50-67, FP64 only;
- * 2 and 3 fail with TTG_ERR_INVALID).  tol is relative to
+ * Residual branch (trunc_norm = 1) only; prec 0 (none), 1 ('cjacobi'),
+ * 2 ('ljacobi') or 3 ('rjacobi'): the block-Jacobi right preconditioners
+ * of solve/solve3d_2ml.m:21-70, FP64 only (the ljacobi / rjacobi inverse
+ * blocks are limited to 2^28 doubles in total).  tol is relative to
  * ||rhs|| as in the MEX (fmex/solve3d_2.c:263-267).  nrestart is clamped to
  * rx1*n*rx2 (:184).  *iters_out (nullable) receives the Krylov iterations. */
 int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2,

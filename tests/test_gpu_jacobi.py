@@ -1,6 +1,7 @@
-"""Centre block-Jacobi local preconditioner ('cjacobi', MEX prec = 1,
-solve/solve3d_2ml.m:50-67,138-146): the preconditioned device local solve
-and AMEn with local_prec='cjacobi' against the FP64 oracle (1e-10)."""
+"""Block-Jacobi local preconditioners (solve/solve3d_2ml.m:21-70,120-146):
+'cjacobi' (MEX prec 1), 'ljacobi' (2) and 'rjacobi' (3).  The preconditioned
+device local solves and AMEn with each local_prec against the FP64 oracle
+(1e-10)."""
 import numpy as np
 import pytest
 
@@ -75,12 +76,46 @@ def test_cjacobi_reduces_iterations_on_aniso(ctx):
     assert s1["gmres_iters"] < s0["gmres_iters"]
 
 
+@pytest.mark.parametrize("prec", [2, 3])
+@pytest.mark.parametrize("rx1,n,rx2,tol", [(3, 5, 4, 1e-11), (6, 16, 5, 1e-9), (9, 20, 7, 1e-10)])
+def test_lr_jacobi_local_solve_parity(ctx, prec, rx1, n, rx2, tol):
+    """Left / right block-Jacobi: blocks of rx1 n (ljacobi) or n rx2
+    (rjacobi) rows; the last case has blocks above 128 rows (LU path)."""
+    rng = np.random.default_rng(rx1 * n + prec)
+    Phi1, A, Phi2 = _system(rng, rx1, n, rx2)
+    sz = rx1 * n * rx2
+    rhs = rng.standard_normal(sz)
+    sol_prev = 0.01 * rng.standard_normal(sz)
+    ref = oamen.solve3d_2(Phi1, A, Phi2, rhs, tol, sol_prev, 40, 2, prec=prec)
+    info = {}
+    got = ttgpu.solve3d_2(Phi1, A, Phi2, rhs, tol, 1, sol_prev, prec, 40, 2, ctx=ctx, info=info)
+    assert rel(got, ref) < 1e-10
+    res = np.linalg.norm(oamen.bfun3(Phi1, A, Phi2, got) - rhs) / np.linalg.norm(rhs)
+    assert res <= 10 * tol
+
+
+@pytest.mark.parametrize("name", ["ljacobi", "rjacobi"])
+def test_lr_jacobi_amen_parity(ctx, name):
+    A, y, x0, z0 = laplace_config(d=4, n=8)
+    ref, info = oamen.amen_solve2(A, y, 1e-12, x0, z0, rmax=64, nswp=10, local_prec=name)
+    st = {}
+    got = ttgpu.amen_solve2(ttgpu.TTMatrix(A.n, A.m, A.r, A.flat()),
+                            ttgpu.TensorTrain(y.n, y.r, y.flat()), 1e-12,
+                            x0=ttgpu.TensorTrain(x0.n, x0.r, x0.flat()),
+                            z0=ttgpu.TensorTrain(z0.n, z0.r, z0.flat()), ctx=ctx, stats=st,
+                            rmax=64, nswp=10, local_prec=name)
+    got = TT.from_flat(got.n, got.r, got.core)
+    assert st["sweeps"] == info["sweeps"]
+    assert list(got.r) == list(ref.r)
+    assert tt_norm(got - ref) < 1e-10 * tt_norm(ref)
+
+
 def test_preconditioner_errors(ctx):
     rng = np.random.default_rng(1)
     Phi1, A, Phi2 = _system(rng, 3, 4, 3)
     rhs = rng.standard_normal(36)
-    with pytest.raises(ttgpu.TTGError, match="not implemented"):
-        ttgpu.solve3d_2(Phi1, A, Phi2, rhs, 1e-8, 1, np.zeros(36), 2, ctx=ctx)
+    with pytest.raises(ttgpu.TTGError, match="unknown"):
+        ttgpu.solve3d_2(Phi1, A, Phi2, rhs, 1e-8, 1, np.zeros(36), 4, ctx=ctx)
     with pytest.raises(ttgpu.TTGError, match="mixed"):
         ttgpu.solve3d_2(Phi1, A, Phi2, rhs, 1e-8, 1, np.zeros(36), 1, ctx=ctx, precision="mixed")
     A0 = A.copy()

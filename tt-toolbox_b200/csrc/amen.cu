@@ -32,8 +32,9 @@ LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const do
                                            int64_t nrestart, int64_t niters, double* sol,
                                            int precision, int prec = 0,
                                            double* bsol_out = nullptr) {
-  TTG_REQUIRE(prec == 0 || prec == 1,
-              "local preconditioner %d is not implemented (only 0 and 1 = 'cjacobi')", prec);
+  TTG_REQUIRE(prec >= 0 && prec <= 3,
+              "local preconditioner %d is unknown (0 none, 1 'cjacobi', 2 'ljacobi', "
+              "3 'rjacobi')", prec);
   if (precision == TTG_MIXED) {
     TTG_REQUIRE(prec == 0, "the mixed-precision local solve has no local preconditioner");
     return local_solve_mixed(c, d, Phi1, A, Phi2, rhs, dres, nres, nrhs, tol, sol_prev, nrestart,
@@ -42,15 +43,16 @@ LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const do
   LocalSolveResult out;
   const int64_t sz = d.in_size();
   if (nrestart > sz) nrestart = sz;                                   // solve3d_2.c:184
-  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size()), J, pw;
-  if (prec == 1) {                                                    // solve3d_2.c:212-231
-    J.reset(c, d.rx1 * d.n * d.n * d.rx2);
+  DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size()), J, pw, js;
+  if (prec != 0) {                                                    // solve3d_2.c:212-231
+    J.reset(c, jac_size(prec, d.rx1, d.n, d.rx2));
     pw.reset(c, sz);
-    jac_gen_c_f64(c, d.rx1, d.n, d.rx2, d.ra1, d.ra2, Phi1, A, Phi2, J.p());
+    if (prec == 3) js.reset(c, 2 * sz);
+    jac_gen_f64(c, prec, d.rx1, d.n, d.rx2, d.ra1, d.ra2, Phi1, A, Phi2, J.p());
   }
   auto mv = [&](const double* x, double* y) {
-    if (prec == 1) {  // right preconditioning: B P x
-      jac_apply_c_f64(c, d.rx1, d.n, d.rx2, J.p(), x, pw.p());
+    if (prec != 0) {  // right preconditioning: B P x
+      jac_apply_f64(c, prec, d.rx1, d.n, d.rx2, J.p(), x, pw.p(), js.p());
       local_matvec_f64(c, d, Phi1, A, Phi2, pw.p(), y, t1.p(), t2.p());
     } else {
       local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
@@ -59,8 +61,8 @@ LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const do
   double tol_prev = nres / nrhs;                                      // :263
   if (tol_prev < tol) tol_prev = tol;                                 // :264
   GmresResult g = gmres_hh_f64(c, mv, dres, sz, nrestart, tol / tol_prev, niters, sol);  // :267
-  if (prec == 1) {                                                    // :272-274
-    jac_apply_c_f64(c, d.rx1, d.n, d.rx2, J.p(), sol, pw.p());
+  if (prec != 0) {                                                    // :272-274
+    jac_apply_f64(c, prec, d.rx1, d.n, d.rx2, J.p(), sol, pw.p(), js.p());
     copy_f64(c, sz, pw.p(), sol);
   }
   axpby_f64(c, sz, 1.0, sol_prev, 1.0, sol);                          // :277-278
@@ -226,10 +228,11 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   TTG_REQUIRE(Ah->r[0] == 1 && Ah->r[d] == 1 && yh->r[0] == 1 && yh->r[d] == 1,
               "border ranks must be 1");
   TTG_REQUIRE(o.trunc_norm == 1, "only trunc_norm 'residual' is implemented");
-  TTG_REQUIRE(o.local_prec == 0 || o.local_prec == 1,
-              "local_prec %d is not implemented (0 = none, 1 = 'cjacobi')", o.local_prec);
+  TTG_REQUIRE(o.local_prec >= 0 && o.local_prec <= 3,
+              "local_prec %d is unknown (0 = none, 1 'cjacobi', 2 'ljacobi', 3 'rjacobi')",
+              o.local_prec);
   TTG_REQUIRE(o.local_prec == 0 || o.precision == TTG_FP64,
-              "local_prec 'cjacobi' runs with precision TTG_FP64 only");
+              "the local preconditioners run with precision TTG_FP64 only");
   TTG_REQUIRE(o.precision == TTG_FP64 || o.precision == TTG_MIXED, "unknown precision %d",
               o.precision);
   TTG_REQUIRE(o.nswp >= 1 && o.local_restart >= 1 && o.local_iters >= 1 && o.rmax >= 1 &&

@@ -227,8 +227,8 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_
   TTG_REQUIRE(ctx && Phi1 && A && Phi2 && rhs && sol_prev && sol_out, "NULL argument");
   TTG_REQUIRE(rx1 >= 1 && n >= 1 && rx2 >= 1 && ra1 >= 1 && ra2 >= 1, "sizes must be >= 1");
   TTG_REQUIRE(trunc_norm == 1, "only the residual branch (trunc_norm = 1) is implemented");
-  TTG_REQUIRE(prec == 0 || prec == 1,
-              "prec %d is not implemented (0 = none, 1 = 'cjacobi')", int(prec));
+  TTG_REQUIRE(prec >= 0 && prec <= 3,
+              "prec %d is unknown (0 none, 1 'cjacobi', 2 'ljacobi', 3 'rjacobi')", int(prec));
   TTG_REQUIRE(nrestart >= 1 && niters >= 1, "nrestart and niters must be >= 1");
   TTG_REQUIRE(std::isfinite(tol) && tol > 0, "tol must be > 0");
   Context* c = &ctx->c;

@@ -14,6 +14,7 @@
 // the row interchanges are undone as column interchanges at the end.
 // Application is HBM-bound: every inverse entry is read once per apply.
 #include "jacobi.h"
+#include "linalg.h"
 
 #include <cmath>
 
@@ -152,6 +153,52 @@ __global__ void k_jac_apply_c(int64_t rx1, int64_t n, int64_t rx2, const double*
   }
 }
 
+// Left block-Jacobi ('ljacobi'): J[(i + rx1 j) + B (a + rx1 m) + B^2 k] =
+// sum_al Phi1[i, a, al] AK[al, j, m, k], B = rx1 n, with
+// AK[al, j, m, k] = sum_be A[al, j, m, be] Phi2[k, be, k].
+__global__ void k_jac_build_l(int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
+                              const double* __restrict__ Phi1, const double* __restrict__ AK,
+                              double* __restrict__ J) {
+  pdl_begin();
+  const int64_t B = rx1 * n, total = B * B * rx2;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t row = e % B, col = (e / B) % B, k = e / (B * B);
+    const int64_t i = row % rx1, j = row / rx1, a = col % rx1, m = col / rx1;
+    double s = 0.0;
+    for (int64_t al = 0; al < ra1; ++al)
+      s += Phi1[i + rx1 * a + rx1 * rx1 * al] * AK[al + ra1 * (j + n * m) + ra1 * n * n * k];
+    J[e] = s;
+  }
+}
+
+// Right block-Jacobi ('rjacobi'): J[(j + n k) + B (m + n q) + B^2 i] =
+// sum_be G[i, j, m, be] Phi2[q, be, k], B = n rx2, with
+// G[i, j, m, be] = sum_al Phi1[i, i, al] A[al, j, m, be].
+__global__ void k_jac_build_r(int64_t rx1, int64_t n, int64_t rx2, int64_t ra2,
+                              const double* __restrict__ G, const double* __restrict__ Phi2,
+                              double* __restrict__ J) {
+  pdl_begin();
+  const int64_t B = n * rx2, total = B * B * rx1;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t row = e % B, col = (e / B) % B, i = e / (B * B);
+    const int64_t j = row % n, k = row / n, m = col % n, q = col / n;
+    double s = 0.0;
+    for (int64_t be = 0; be < ra2; ++be)
+      s += G[i + rx1 * (j + n * m + n * n * be)] * Phi2[q + rx2 * be + rx2 * ra2 * k];
+    J[e] = s;
+  }
+}
+
+// blk = I (B x B, column-major)
+__global__ void k_set_identity(int64_t B, double* __restrict__ blk) {
+  pdl_begin();
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < B * B;
+       e += int64_t(gridDim.x) * blockDim.x)
+    blk[e] = (e % B == e / B) ? 1.0 : 0.0;
+}
+
 int blocks_for(Context* c, int64_t n) {
   int64_t b = (n + 255) / 256;
   const int64_t cap = int64_t(c->num_sms) * 8;
@@ -186,6 +233,87 @@ void jac_apply_c_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, const doub
                      const double* x, double* y) {
   launch(c, k_jac_apply_c, blocks_for(c, rx1 * n * rx2), 256, 0, rx1, n, rx2, J, x, y);
   TTG_CHECK_LAUNCH();
+}
+
+void inv_blocks_f64(Context* c, int64_t B, int64_t nblocks, double* J) {
+  if (B <= JAC_MAX_N) {  // one CTA per block, Gauss-Jordan in shared memory
+    TTG_REQUIRE(nblocks <= int64_t(0x7fffffff), "too many blocks");
+    const size_t smem = sizeof(double) * size_t(B) * size_t(B);
+    ensure_smem_attr(reinterpret_cast<const void*>(k_block_inv), c->device, int(smem));
+    launch(c, k_block_inv, unsigned(nblocks), GJ_THREADS, smem, int64_t(1), int(B), J,
+           c->d_err + 4);
+    TTG_CHECK_LAUNCH();
+    return;
+  }
+  // Larger blocks: LU with partial pivoting and B X = I per block.
+  DBuf<double> W(c, B * B);
+  for (int64_t k = 0; k < nblocks; ++k) {
+    double* blk = J + B * B * k;
+    copy_f64(c, B * B, blk, W.p());
+    launch(c, k_set_identity, blocks_for(c, B * B), 256, 0, B, blk);
+    TTG_CHECK_LAUNCH();
+    lu_solve_f64(c, B, W.p(), blk, B);
+  }
+}
+
+int64_t jac_size(int prec, int64_t rx1, int64_t n, int64_t rx2) {
+  if (prec == 1) return rx1 * n * n * rx2;
+  if (prec == 2) return (rx1 * n) * (rx1 * n) * rx2;
+  return (n * rx2) * (n * rx2) * rx1;
+}
+
+void jac_gen_f64(Context* c, int prec, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
+                 int64_t ra2, const double* Phi1, const double* A, const double* Phi2,
+                 double* J) {
+  if (prec == 1) {
+    jac_gen_c_f64(c, rx1, n, rx2, ra1, ra2, Phi1, A, Phi2, J);
+    return;
+  }
+  TTG_REQUIRE(prec == 2 || prec == 3, "unknown local preconditioner %d", prec);
+  TTG_REQUIRE(jac_size(prec, rx1, n, rx2) <= JAC_MAX_ELEMS,
+              "%s: the inverse blocks need %lld doubles, above the limit of %lld",
+              prec == 2 ? "ljacobi" : "rjacobi", (long long)jac_size(prec, rx1, n, rx2),
+              (long long)JAC_MAX_ELEMS);
+  if (prec == 2) {  // solve/solve3d_2ml.m:33-48
+    DBuf<double> d2(c, ra2 * rx2), AK(c, ra1 * n * n * rx2);
+    launch(c, k_diag_phi2, blocks_for(c, ra2 * rx2), 256, 0, rx2, ra2, Phi2, d2.p());
+    TTG_CHECK_LAUNCH();
+    gemm_f64(c, false, false, ra1 * n * n, rx2, ra2, 1.0, A, ra1 * n * n, 0, d2.p(), ra2, 0, 0.0,
+             AK.p(), ra1 * n * n, 0, 1);
+    const int64_t B = rx1 * n;
+    launch(c, k_jac_build_l, blocks_for(c, B * B * rx2), 256, 0, rx1, n, rx2, ra1, Phi1, AK.p(),
+           J);
+    TTG_CHECK_LAUNCH();
+    inv_blocks_f64(c, B, rx2, J);
+  } else {          // solve/solve3d_2ml.m:21-32
+    DBuf<double> d1(c, rx1 * ra1), G(c, rx1 * n * n * ra2);
+    launch(c, k_diag_phi1, blocks_for(c, rx1 * ra1), 256, 0, rx1, ra1, Phi1, d1.p());
+    TTG_CHECK_LAUNCH();
+    gemm_f64(c, false, false, rx1, n * n * ra2, ra1, 1.0, d1.p(), rx1, 0, A, ra1, 0, 0.0, G.p(),
+             rx1, 0, 1);
+    const int64_t B = n * rx2;
+    launch(c, k_jac_build_r, blocks_for(c, B * B * rx1), 256, 0, rx1, n, rx2, ra2, G.p(), Phi2,
+           J);
+    TTG_CHECK_LAUNCH();
+    inv_blocks_f64(c, B, rx1, J);
+  }
+}
+
+void jac_apply_f64(Context* c, int prec, int64_t rx1, int64_t n, int64_t rx2, const double* J,
+                   const double* x, double* y, double* scratch) {
+  if (prec == 1) {
+    jac_apply_c_f64(c, rx1, n, rx2, J, x, y);
+  } else if (prec == 2) {  // y(:, k) = J_k x(:, k), x as (rx1 n) x rx2 (solve3d_2ml.m:130-137)
+    const int64_t B = rx1 * n;
+    gemm_f64(c, false, false, B, 1, B, 1.0, J, B, B * B, x, B, B, 0.0, y, B, B, rx2);
+  } else {                 // per i over (j, k)  (solve3d_2ml.m:120-129)
+    const int64_t B = n * rx2;
+    double* xt = scratch;
+    double* yt = scratch + B * rx1;
+    transpose_f64(c, rx1, B, x, rx1, xt, B);
+    gemm_f64(c, false, false, B, 1, B, 1.0, J, B, B * B, xt, B, B, 0.0, yt, B, B, rx1);
+    transpose_f64(c, B, rx1, yt, B, y, rx1);
+  }
 }
 
 }  // namespace ttg

@@ -442,9 +442,8 @@ def round(tt, eps, rmax=None, precision="fp64", ctx=None, stats=None):
     return host
 
 
-# local_prec names -> MEX prec codes (solve/amen_solve2.m:205-207); 'ljacobi'
-# and 'rjacobi' are not implemented on the device.
-_LOCAL_PREC = {"": 0, None: 0, 0: 0, "cjacobi": 1, 1: 1}
+# local_prec names -> MEX prec codes (solve/amen_solve2.m:205-207).
+_LOCAL_PREC = {"": 0, None: 0, 0: 0, "cjacobi": 1, 1: 1, "ljacobi": 2, 2: 2, "rjacobi": 3, 3: 3}
 
 _AMEN_KEYS = {"nswp", "rmax", "x0", "z0", "verb", "local_prec", "local_restart", "local_iters",
               "kickrank", "kicktype", "ismex", "max_full_size", "resid_damp", "trunc_norm",
@@ -462,7 +461,8 @@ def _check_amen_opts(opts):
         raise TTGError(7, "trunc_norm %r is not implemented (only 'residual')" % opts["trunc_norm"])
     lp = opts.get("local_prec", "")
     if lp not in _LOCAL_PREC:
-        raise TTGError(7, "local_prec %r is not implemented ('' or 'cjacobi')" % (lp,))
+        raise TTGError(7, "local_prec %r is unknown ('', 'cjacobi', 'ljacobi', 'rjacobi')"
+                       % (lp,))
     return opts
 
 
