@@ -51,7 +51,7 @@ def test_amen_option_checks():
     with pytest.raises(ttgpu.TTGError, match="trunc_norm"):
         ttgpu.amen_solve2(None, None, 1e-6, trunc_norm="fro")
     with pytest.raises(ttgpu.TTGError, match="local_prec"):
-        ttgpu.amen_solve2(None, None, 1e-6, local_prec="ljacobi")
+        ttgpu.amen_solve2(None, None, 1e-6, local_prec="ilu")
     # option names are case-insensitive, as in the reference's parser
     assert ttgpu._check_amen_opts({"NSWP": 3, "Local_Prec": "cjacobi"})["nswp"] == 3
 
