@@ -175,6 +175,252 @@ __global__ void __launch_bounds__(128, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Fused local matvec: the three GEMM stages in ONE persistent launch.
+//
+// One CTA per SM (cooperative launch, so all CTAs are resident) walks the
+// output tiles of stage 1, then -- after a grid-wide barrier that makes the
+// stage's T1 writes visible -- those of stage 2, then of stage 3.  T1 and T2
+// (a few MB) are written by one stage and read by the next inside the same
+// launch, so they stay in L2: DRAM sees the operands and y only.  Roles:
+// warp 0 issues TMA loads into a FU_STAGES-deep shared-memory ring (across
+// tile and stage boundaries), one thread of warp 1 issues tcgen05.mma into
+// one of two TMEM accumulators, warps 2-5 drain the other accumulator
+// (tcgen05.ld) and store it in the next stage's K-major layout.  Every wait
+// is bounded: a timeout raises the error flag and every role winds down.
+// ---------------------------------------------------------------------------
+
+constexpr int FU_STAGES = 4;
+constexpr int FU_BN_MAX = 128;
+constexpr int FU_THREADS = 192;
+constexpr int FU_B_BYTES = FU_BN_MAX * UM_BK * 2;
+constexpr uint32_t FU_TMEM_COLS = 2 * FU_BN_MAX;
+constexpr long long FU_BAR_SPIN_LIMIT = 1LL << 24;
+
+constexpr size_t fused_smem_bytes() {
+  return 1024 + size_t(FU_STAGES) * (UM_A_BYTES + FU_B_BYTES) + (2 * FU_STAGES + 4) * 8 + 64;
+}
+
+struct FusedStage {
+  OutMap om;
+  int K, a_rows_pb, b_rows_pb;
+  int mt, nt, batch;  // tiles: M tiles of 128 rows, N tiles of bn columns, batches
+  int bn;             // 64 or 128
+  int out_bf16;
+};
+
+struct FusedArgs {
+  FusedStage st[3];
+  unsigned* bar;      // grid barrier: arrival counter, generation
+  int* err;
+  const int* skip;
+};
+
+// Generation barrier over the grid (all CTAs resident: cooperative launch);
+// bounded, the waiting thread gives up and raises *err.
+__device__ void fu_grid_barrier(unsigned* bar, int* err) {
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = bar + 1;
+    volatile int* verr = err;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == gen) {
+        if (*verr) break;
+        if (++spins > FU_BAR_SPIN_LIMIT) {
+          atomicExch(err, 7);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+}
+
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(FU_THREADS, 1)
+    k_mv_fused(const __grid_constant__ CUtensorMap tA1, const __grid_constant__ CUtensorMap tB1,
+               const __grid_constant__ CUtensorMap tA2, const __grid_constant__ CUtensorMap tB2,
+               const __grid_constant__ CUtensorMap tA3, const __grid_constant__ CUtensorMap tB3,
+               const __grid_constant__ FusedArgs fa) {
+  using namespace umma;
+  if (fa.skip && *fa.skip) return;  // queued Krylov step after convergence (uniform)
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + FU_STAGES * UM_A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + FU_STAGES * FU_B_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * FU_STAGES + 4);
+  uint32_t* consumed_slot = tmem_slot + 1;
+  const uint32_t bar_full = smem_u32(bars);
+  const uint32_t bar_empty = smem_u32(bars + FU_STAGES);
+  const uint32_t bar_accf = smem_u32(bars + 2 * FU_STAGES);      // 2: accumulator ready
+  const uint32_t bar_acce = smem_u32(bars + 2 * FU_STAGES + 2);  // 2: accumulator drained
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* err = fa.err;
+
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), FU_TMEM_COLS);
+    tmem_relinquish();
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < FU_STAGES; ++s) {
+      mbar_init(bar_full + 8 * s, 1);
+      mbar_init(bar_empty + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(bar_accf + 8 * b, 1);
+      mbar_init(bar_acce + 8 * b, 4);  // one arrival per epilogue warp
+    }
+    fence_barrier_init();
+    fence_proxy_async();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  // Counters advance identically in the roles that share a barrier ring.
+  uint32_t kb_cnt = 0;    // K-blocks issued (producer) / consumed (MMA)
+  uint32_t tile_cnt = 0;  // tiles accumulated (MMA) / drained (epilogue)
+  for (int s = 0; s < 3; ++s) {
+    const FusedStage& S = fa.st[s];
+    const CUtensorMap* tA = s == 0 ? &tA1 : (s == 1 ? &tA2 : &tA3);
+    const CUtensorMap* tB = s == 0 ? &tB1 : (s == 1 ? &tB2 : &tB3);
+    const int ntiles = S.mt * S.nt * S.batch;
+    const int nk = (S.K + UM_BK - 1) / UM_BK;
+    const uint32_t b_bytes = uint32_t(S.bn) * UM_BK * 2;
+    if (warp == 0) {
+      if (lane == 0) {  // TMA producer
+        if (s > 0) fence_proxy_async_global();  // the previous stage's stores, seen by TMA
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+          const int mi = t % S.mt, rest = t / S.mt, ni = rest % S.nt, bz = rest / S.nt;
+          const int arow = bz * S.a_rows_pb + mi * UM_BM, brow = bz * S.b_rows_pb + ni * S.bn;
+          for (int kb = 0; kb < nk; ++kb, ++kb_cnt) {
+            const uint32_t slot = kb_cnt % FU_STAGES;
+            if (kb_cnt >= FU_STAGES &&
+                !mbar_wait(bar_empty + 8 * slot, ((kb_cnt / FU_STAGES) - 1) & 1, err)) {
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(bar_full + 8 * slot, UM_A_BYTES + b_bytes);
+            tma_load_2d(smem_u32(sA + slot * UM_A_BYTES), tA, kb * UM_BK, arow,
+                        bar_full + 8 * slot);
+            tma_load_2d(smem_u32(sB + slot * FU_B_BYTES), tB, kb * UM_BK, brow,
+                        bar_full + 8 * slot);
+          }
+        }
+      }
+      __syncwarp();
+    } else if (warp == 1) {
+      if (lane == 0) {  // MMA issuer
+        const uint32_t idesc = idesc_bf16_f32(UM_BM, S.bn);
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tile_cnt) {
+          const uint32_t buf = tile_cnt & 1;
+          if (tile_cnt >= 2 && !mbar_wait(bar_acce + 8 * buf, ((tile_cnt >> 1) - 1) & 1, err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t tacc = tmem + buf * FU_BN_MAX;
+          for (int kb = 0; kb < nk; ++kb, ++kb_cnt) {
+            const uint32_t slot = kb_cnt % FU_STAGES;
+            if (!mbar_wait(bar_full + 8 * slot, (kb_cnt / FU_STAGES) & 1, err)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sA + slot * UM_A_BYTES);
+            const uint32_t b0 = smem_u32(sB + slot * FU_B_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < UM_BK / 16; ++kk)
+              mma_bf16(tacc, desc_k_sw128(a0 + kk * 32), desc_k_sw128(b0 + kk * 32), idesc,
+                       (kb > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(bar_empty + 8 * slot);
+          }
+          if (ok) mma_commit(bar_accf + 8 * buf);
+        }
+        *consumed_slot = kb_cnt;
+      }
+      __syncwarp();
+    } else {  // epilogue: warps 2..5 own TMEM lanes 32 (warp % 4) ..
+      const int ew = warp & 3;
+      const int row = ew * 32 + lane;
+      const OutMap& om = S.om;
+      for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tile_cnt) {
+        const uint32_t buf = tile_cnt & 1;
+        const bool ok = mbar_wait(bar_accf + 8 * buf, (tile_cnt >> 1) & 1, err);
+        tc_fence_after();
+        if (!ok) break;
+        const int mi = t % S.mt, rest = t / S.mt, ni = rest % S.nt, bz = rest / S.nt;
+        const int m0 = mi * UM_BM, n0 = ni * S.bn;
+        const int64_t m = int64_t(m0) + row;
+        const bool row_ok = m < om.M;
+        const int64_t roff = row_ok ? map2(m, om.r_s1, om.r_t1, om.r_t2) : 0;
+        const int64_t boff = int64_t(bz) * om.batch_stride;
+        int64_t cq = int64_t(n0) / om.c_s1, cr = int64_t(n0) % om.c_s1;
+        const uint32_t tbase = tmem + (uint32_t(ew * 32) << 16) + buf * FU_BN_MAX;
+#pragma unroll 1
+        for (int c0 = 0; c0 < S.bn; c0 += 16) {
+          if (n0 + c0 >= om.N) break;  // uniform across the CTA
+          float v[16];
+          tmem_ld16(tbase + uint32_t(c0), v);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int64_t n = int64_t(n0) + c0 + j;
+            if (row_ok && n < om.N) {
+              const int64_t off = boff + roff + cr * om.c_t1 + cq * om.c_t2;
+              if (S.out_bf16)
+                static_cast<__nv_bfloat16*>(om.base)[off] = __float2bfloat16_rn(v[j]);
+              else
+                static_cast<float*>(om.base)[off] = v[j];
+            }
+            if (++cr == om.c_s1) {
+              cr = 0;
+              ++cq;
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar_acce + 8 * buf);
+      }
+      if (s < 2) fence_proxy_async_global();  // this stage's stores, for the next TMA loads
+    }
+    if (s < 2) {
+      __syncthreads();
+      fu_grid_barrier(fa.bar, err);
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  // Wind-down after an error: loads issued but never consumed must land
+  // before the CTA (and its shared memory) goes away.  Bounded.
+  if (threadIdx.x == 0 && *(volatile int*)err) {
+    for (uint32_t k = *consumed_slot; k < kb_cnt; ++k)
+      mbar_wait(bar_full + 8 * (k % FU_STAGES), (k / FU_STAGES) & 1, err, 1 << 16);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, FU_TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Operand conversion kernels (FP64/FP32 -> BF16, K-major layouts)
 // ---------------------------------------------------------------------------
 
@@ -336,6 +582,16 @@ int pick_bn(Context* c, int64_t M, int64_t N, int64_t batch) {
 
 int64_t up8(int64_t v) { return (v + 7) / 8 * 8; }
 
+// TTG_FUSED_MV=0 keeps the three-launch local matvec (for comparisons).
+bool fused_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("TTG_FUSED_MV");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+
 }  // namespace
 
 void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const double* A,
@@ -365,6 +621,10 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
   make_map(&mapX, X.p(), d.rx2, d.m * d.rx1, ldx, UM_BM);
   make_map(&mapT1, T1.p(), d.n * d.ra2, d.rx1 * d.ry2, ld1, UM_BM);
   make_map(&mapT2, T2.p(), d.rx1 * d.ra1, d.ry2 * d.n, ld2, UM_BM);
+  if (fused_enabled()) {
+    prepare_fused(c);
+    return;
+  }
   bn1 = tuned_bn(c, 1);
   bn2 = tuned_bn(c, 2);
   bn3 = tuned_bn(c, 3);
@@ -492,10 +752,74 @@ void MixedOp::apply_converted(Context* c, float* y) {
   stages(c, y);
 }
 
+void MixedOp::prepare_fused(Context* c) {
+  // Tile width per stage: 128 columns when that still gives every SM a
+  // tile, else 64 (more, shorter tiles).
+  const int64_t M[3] = {d.m * d.rx1, d.rx1, d.ry2 * d.n};
+  const int64_t N[3] = {d.ra2 * d.ry2, d.ra1 * d.n, d.ry1};
+  const int64_t B[3] = {1, d.ry2, 1};
+  int64_t most = 1;
+  for (int s = 0; s < 3; ++s) {
+    const int64_t mt = (M[s] + UM_BM - 1) / UM_BM;
+    const int64_t t128 = mt * ((N[s] + 127) / 128) * B[s];
+    fbn[s] = (N[s] > 64 && t128 >= c->num_sms) ? 128 : 64;
+    most = std::max(most, mt * ((N[s] + fbn[s] - 1) / fbn[s]) * B[s]);
+  }
+  make_map(&fmapB[0], phi2b.p(), d.rx2, N[0], ldx, fbn[0]);
+  make_map(&fmapB[1], AT.p(), d.n * d.ra2, N[1], ld1, fbn[1]);
+  make_map(&fmapB[2], phi1T.p(), d.rx1 * d.ra1, N[2], ld2, fbn[2]);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_mv_fused), c->device,
+                   int(fused_smem_bytes()));
+  int occ = 0;
+  TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mv_fused, FU_THREADS,
+                                                         fused_smem_bytes()));
+  TTG_REQUIRE(occ >= 1, "fused matvec: no resident CTA fits");
+  fblocks = int(std::min<int64_t>(most, int64_t(c->num_sms) * occ));
+  fbar.reset(c, 2);
+  TTG_CUDA(cudaMemsetAsync(fbar.p(), 0, 2 * sizeof(unsigned), c->stream));
+  TTG_REQUIRE(d.n * d.rx1 < (1ll << 31) && d.ry2 * d.n < (1ll << 31) && most < (1ll << 31),
+              "fused matvec too large");
+}
+
+void MixedOp::stages_fused(Context* c, float* y) {
+  const int64_t rows = d.m * d.rx1;
+  FusedArgs fa{};
+  const int64_t M[3] = {rows, d.rx1, d.ry2 * d.n};
+  const int64_t N[3] = {d.ra2 * d.ry2, d.ra1 * d.n, d.ry1};
+  const int64_t K[3] = {d.rx2, d.n * d.ra2, d.rx1 * d.ra1};
+  const int64_t B[3] = {1, d.ry2, 1};
+  fa.st[0].om = OutMap{T1.p(), rows, d.ra2 * d.ry2, d.m, 1, ld1, d.ra2, d.m, ld1 * d.rx1, 0};
+  fa.st[1].om = OutMap{T2.p(), d.rx1, d.ra1 * d.n, d.rx1, 1, 0, d.ra1, d.rx1, ld2 * d.ry2, ld2};
+  fa.st[2].om = OutMap{y, M[2], d.ry1, M[2], 1, 0, d.ry1, M[2], 0, 0};
+  for (int s = 0; s < 3; ++s) {
+    FusedStage& S = fa.st[s];
+    S.K = int(K[s]);
+    S.a_rows_pb = s == 1 ? int(d.rx1) : 0;
+    S.b_rows_pb = 0;
+    S.mt = int((M[s] + UM_BM - 1) / UM_BM);
+    S.nt = int((N[s] + fbn[s] - 1) / fbn[s]);
+    S.batch = int(B[s]);
+    S.bn = fbn[s];
+    S.out_bf16 = s < 2 ? 1 : 0;
+  }
+  fa.bar = fbar.p();
+  fa.err = c->d_err + 1;
+  fa.skip = c->skip;
+  void* args[] = {(void*)&mapX, (void*)&fmapB[0], (void*)&mapT1, (void*)&fmapB[1],
+                  (void*)&mapT2, (void*)&fmapB[2], (void*)&fa};
+  TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_mv_fused, dim3(fblocks), dim3(FU_THREADS),
+                                       args, fused_smem_bytes(), c->stream));
+  c->launches += 1;
+}
+
 void MixedOp::stages(Context* c, float* y) {
-  run_stage(c, 1, bn1, mapP2, y);  // T1[(m,a),(be,k)]
-  run_stage(c, 2, bn2, mapAT, y);  // per k, T2_k[a,(al,j)]
-  run_stage(c, 3, bn3, mapP1, y);  // y[(k,j), i] in the reversed vector layout
+  if (fblocks > 0) {
+    stages_fused(c, y);  // T1, T2 and y in one launch
+  } else {
+    run_stage(c, 1, bn1, mapP2, y);  // T1[(m,a),(be,k)]
+    run_stage(c, 2, bn2, mapAT, y);  // per k, T2_k[a,(al,j)]
+    run_stage(c, 3, bn3, mapP1, y);  // y[(k,j), i] in the reversed vector layout
+  }
   c->matvecs += 1;
   c->matvec_flops += int64_t(d.flops());
   c->mv_count[1] += 1;

@@ -27,8 +27,16 @@ struct MixedOp {
   void run_stage(Context* c, int stage, int bn, const CUtensorMap& mapB, float* y);
   // Tile width of a stage: autotuned once per shape and device (mixed_ops.cu).
   int tuned_bn(Context* c, int stage);
-  // The three GEMM stages from X to y, with the matvec counters.
+  // The three GEMM stages from X to y, with the matvec counters: one fused
+  // persistent launch (default) or three GEMM launches (TTG_FUSED_MV=0).
   void stages(Context* c, float* y);
+  // Fused single-launch form: tile widths and B-operand maps per stage.
+  int fbn[3] = {64, 64, 64};
+  CUtensorMap fmapB[3];
+  int fblocks = 0;
+  DBuf<unsigned> fbar;
+  void prepare_fused(Context* c);
+  void stages_fused(Context* c, float* y);
 };
 
 // Natural [i, j, k] FP64 <-> reversed [k, j, i] FP32 vector layouts.
