@@ -40,6 +40,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the rounding and gradient configurations")
     p.add_argument("--workload", default="amen", choices=["amen", "batch"],
                    help="amen: the headline single solve; batch: 512 independent systems "
                         "(one timed batch; --steps/--warmup do not apply)")
@@ -369,6 +371,12 @@ def run_ours(args, dist):
     }
     if other is not None:
         line["compare"] = other
+    if dist.rank == 0 and not args.no_configs:
+        # The other configurations of the hot path, measured in the same run
+        # (not part of the headline value).
+        line["configs"] = {"round": run_round_config(ctx, cpu=dist.world == 1
+                                                     and not args.no_cpu_baseline),
+                           "grad": run_grad_config(ctx)}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         times, info = cpu_baseline_run(W, reps=1)
         line["cpu_baseline"] = {"value": times[0], "unit": "s", "cores": blas_threads(),
@@ -380,6 +388,104 @@ def run_ours(args, dist):
         h.free()
     ctx.close()
     return line
+
+
+def round_flops(n, r):
+    """Algorithmic FLOPs of rounding a TT with mode sizes n and ranks r: per
+    core the left-to-right QR (4 m p^2 - 4/3 p^3, m = r_k n_k, p = r_{k+1}) and
+    R * core product, the right-to-left SVD of the r_k x (n_k r_{k+1})
+    unfolding (6 (n r) r^2 + 20 r^3, QR-based) and the core * (U S) product."""
+    d = len(n)
+    fl = 0.0
+    for k in range(d - 1):
+        m, p = r[k] * n[k], r[k + 1]
+        fl += 4.0 * m * p * p - 4.0 / 3.0 * p ** 3 + 2.0 * p * p * n[k + 1] * r[k + 2]
+    for k in range(d - 1, 0, -1):
+        rk, cols = r[k], n[k] * r[k + 1]
+        fl += 6.0 * cols * rk * rk + 20.0 * rk ** 3 + 2.0 * r[k - 1] * n[k - 1] * rk * rk
+    return fl
+
+
+def run_round_config(ctx, reps=3, cpu=True):
+    """Rounding of the sum of four rank-64 Gaussian TTs (d=20, n=16, internal
+    ranks 256) to eps 1e-8, FP64 on the device; the mixed form (TF32/BF16
+    contractions) is not implemented and is refused by the library."""
+    import ttgpu
+    from ttgpu import workloads
+    W = dict(d=20, n=16, r=64, terms=4, seed=2, eps=1e-8)
+    X = workloads.round_input(d=W["d"], n=W["n"], r=W["r"], terms=W["terms"], seed=W["seed"])
+    dX = ttgpu.DeviceTT.upload(ctx, X)
+    ms, st = [], {}
+    Y = None
+    for it in range(reps + 1):
+        if Y is not None:
+            Y.free()
+        ctx.flush_l2()
+        st = {}
+        Y = ttgpu.round(dX, W["eps"], ctx=ctx, stats=st)
+        if it:
+            ms.append(st["ms_total"])
+    ranks = [int(v) for v in Y.shape()[2]]
+    D = ttgpu.tt_axpby(1.0, Y, -1.0, dX, ctx=ctx)
+    err = ttgpu.tt_norm(D, ctx=ctx) / ttgpu.tt_norm(dX, ctx=ctx)
+    D.free()
+    Y.free()
+    t0 = time.perf_counter()
+    Yh = ttgpu.round(X, W["eps"], ctx=ctx)
+    e2e = time.perf_counter() - t0
+    dX.free()
+    fl = round_flops([int(v) for v in X.n], [int(v) for v in X.r])
+    v = statistics.median(ms) * 1e-3
+    out = {"workload": "round: d=20 n=16, sum of 4 rank-64 Gaussian TTs (ranks 256), eps 1e-8",
+           "precision": "fp64", "value": v, "unit": "s", "gflop": fl * 1e-9,
+           "gflops": fl / v * 1e-9, "ms_qr_sweep": st["ms_qr_sweep"],
+           "ms_svd_sweep": st["ms_svd_sweep"], "ranks_max": max(ranks),
+           "rel_err": err, "e2e_s": e2e, "e2e_ranks_max": int(max(Yh.r)),
+           "mixed": "unavailable: the TF32/BF16-contraction rounding is not implemented "
+                    "(ttg_round refuses TTG_MIXED)"}
+    if cpu:
+        sys.path.insert(0, ROOT)
+        from oracle.builders import round_config
+        from oracle.round import tt_round
+        Xo = round_config(d=W["d"], n=W["n"], r=W["r"], terms=W["terms"], seed=W["seed"])
+        t0 = time.perf_counter()
+        tt_round(Xo, W["eps"])
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": cpu_s, "unit": "s", "cores": blas_threads(),
+                               "kind": "port", "sample": "one full FP64 oracle rounding"}
+    return out
+
+
+def run_grad_config(ctx, reps=5):
+    """Gradients of <x,Ax>, <x,b> and the 1e6-sample loss with respect to every
+    core (d=12, n=32, rank-64 x, rank-3 operator), FP64 on the device."""
+    import ttgpu
+    from ttgpu import workloads
+    x, A, b, idx, y = workloads.grad_inputs()
+    dx, dA, db = (ttgpu.DeviceTT.upload(ctx, t) for t in (x, A, b))
+    ss = ttgpu.SampleSet(ctx, idx, y)
+    g = ttgpu.DeviceArray(ctx, None, x.core.size)
+    out = {"workload": "grad: d=12 n=32 rank-64 x, rank-3 operator, rank-4 b, 1e6 samples"}
+    runs = [("xAx", lambda: ttgpu.grad_xAx(dx, dA, ctx=ctx, out=g)),
+            ("xb", lambda: ttgpu.grad_xb(dx, db, ctx=ctx, out=g)),
+            ("sampled", lambda: ttgpu.grad_sampled(dx, ss, ctx=ctx, out=g))]
+    for name, fn in runs:
+        fn()
+        ctx.sync()
+        ts = []
+        for _ in range(reps):
+            ctx.flush_l2()
+            ctx.sync()
+            t0 = time.perf_counter()
+            fn()
+            ctx.sync()
+            ts.append(time.perf_counter() - t0)
+        out[name + "_ms"] = statistics.median(ts) * 1e3
+    g.free()
+    ss.free()
+    for h in (dx, dA, db):
+        h.free()
+    return out
 
 
 BATCH_METRIC = "batched AMEn: independent Laplacian systems to tol 1e-8, total time"

@@ -54,6 +54,69 @@ void extract_triu_f64(Context* c, int64_t k, int64_t n, const double* A, int64_t
 
 namespace {
 
+// Columns per diagonal block of the blocked Cholesky (one-CTA factor +
+// inverse of each block, chol_inv_f64).
+constexpr int64_t CHB = 96;
+
+// diag(G) += factor * trace(G), one CTA (the shift of the first pass).
+__global__ void k_add_trace_shift(int64_t n, double* __restrict__ G, int64_t ldg, double factor) {
+  pdl_begin();
+  __shared__ double red[32];
+  double t = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) t += G[i + i * ldg];
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) red[0] = v;
+  }
+  __syncthreads();
+  const double s = factor * red[0];
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) G[i + i * ldg] += s;
+}
+
+// Blocked right-looking Cholesky R' R = G of an n x n SPD matrix (G is
+// overwritten by its Schur complements).  Each diagonal block of at most
+// CHB columns is factored in one CTA together with its inverse; the panel
+// below it is L_ik = G_ik R_kk^{-1} and the trailing matrix loses L_ik L_jk'.
+// R: n x n upper (ld n); Rinv_d: the inverses of the diagonal blocks, block
+// k (bk x bk, ld bk) at offset k0 * CHB.
+void chol_blocked_f64(Context* c, int64_t n, double* G, double* R, double* Rinv_d, int* flag) {
+  fill_f64(c, n * n, 0.0, R);
+  DBuf<double> Rkk(c, CHB * CHB), P(c, n * CHB);
+  for (int64_t k0 = 0; k0 < n; k0 += CHB) {
+    const int64_t bk = std::min(CHB, n - k0), rest = n - k0 - bk;
+    double* Rinv_k = Rinv_d + k0 * CHB;
+    chol_inv_f64(c, bk, G + k0 + k0 * n, n, 0.0, Rkk.p(), Rinv_k, flag);
+    copy2d_f64(c, bk, bk, Rkk.p(), bk, R + k0 + k0 * n, n);
+    if (rest == 0) break;
+    const int64_t r0 = k0 + bk;
+    gemm_f64(c, false, false, rest, bk, bk, 1.0, G + r0 + k0 * n, n, 0, Rinv_k, bk, 0, 0.0,
+             P.p(), rest, 0, 1);                                       // L_ik
+    transpose_f64(c, rest, bk, P.p(), rest, R + k0 + r0 * n, n);       // R_ki = L_ik'
+    gemm_f64(c, false, true, rest, rest, bk, -1.0, P.p(), rest, 0, P.p(), rest, 0, 1.0,
+             G + r0 + r0 * n, n, 0, 1);                                // Schur complement
+  }
+}
+
+// dst = src R^{-1} by block forward substitution over the column blocks:
+// dst_k = (src_k - dst_{<k} R_{<k,k}) R_kk^{-1}.  src, dst: m x n (ld m).
+void solve_blocked_f64(Context* c, int64_t m, int64_t n, const double* src, const double* R,
+                       const double* Rinv_d, double* dst) {
+  DBuf<double> W(c, m * CHB);
+  for (int64_t k0 = 0; k0 < n; k0 += CHB) {
+    const int64_t bk = std::min(CHB, n - k0);
+    copy_f64(c, m * bk, src + k0 * m, W.p());
+    if (k0 > 0)
+      gemm_f64(c, false, false, m, bk, k0, -1.0, dst, m, 0, R + k0 * n, n, 0, 1.0, W.p(), m, 0,
+               1);
+    gemm_f64(c, false, false, m, bk, bk, 1.0, W.p(), m, 0, Rinv_d + k0 * CHB, bk, 0, 0.0,
+             dst + k0 * m, m, 0, 1);
+  }
+}
+
 // Shifted Cholesky QR, three passes (sCholeskyQR3: Fukaya, Kannan,
 // Nakatsukasa, Yamamoto, Yanagisawa, SIAM J. Sci. Comput. 42 (2020)
 // A477-A503).  Pass 1 factors the Gram matrix shifted by
@@ -67,6 +130,7 @@ namespace {
 bool scholqr3_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, double* R) {
   DBuf<double> G(c, n * n), Ri(c, n * n), Rinv(c, n * n), Racc(c, n * n), T(c, n * n),
       W(c, m * n);
+  const bool blocked = n > CHB;  // beyond one CTA: blocked Cholesky and solve
   DBuf<int> flag(c, 1);
   TTG_CUDA(cudaMemsetAsync(flag.p(), 0, sizeof(int), c->stream));
   const double u = 1.1102230246251565e-16;
@@ -75,8 +139,17 @@ bool scholqr3_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, 
   for (int pass = 0; pass < 3; ++pass) {
     double* dst = (pass == 1) ? W.p() : Q;  // Q1 -> Q, Q2 -> W, Q3 -> Q
     gemm_f64(c, true, false, n, n, m, 1.0, src, m, 0, src, m, 0, 0.0, G.p(), n, 0, 1);
-    chol_inv_f64(c, n, G.p(), n, pass == 0 ? shift : 0.0, Ri.p(), Rinv.p(), flag.p());
-    gemm_f64(c, false, false, m, n, n, 1.0, src, m, 0, Rinv.p(), n, 0, 0.0, dst, m, 0, 1);
+    if (blocked) {
+      if (pass == 0) {
+        launch(c, k_add_trace_shift, 1, 256, 0, n, G.p(), n, shift);
+        TTG_CHECK_LAUNCH();
+      }
+      chol_blocked_f64(c, n, G.p(), Ri.p(), Rinv.p(), flag.p());
+      solve_blocked_f64(c, m, n, src, Ri.p(), Rinv.p(), dst);
+    } else {
+      chol_inv_f64(c, n, G.p(), n, pass == 0 ? shift : 0.0, Ri.p(), Rinv.p(), flag.p());
+      gemm_f64(c, false, false, m, n, n, 1.0, src, m, 0, Rinv.p(), n, 0, 0.0, dst, m, 0, 1);
+    }
     if (pass == 0) {
       copy_f64(c, n * n, Ri.p(), Racc.p());
     } else {  // Racc = Ri * Racc
@@ -98,7 +171,7 @@ bool scholqr3_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, 
 }
 
 bool scholqr_ok(int64_t m, int64_t n) {
-  return n >= 8 && n <= 96 && m >= 4 * n && chol_inv_fits(n);
+  return n >= 8 && n <= 1024 && m >= 4 * n && chol_inv_fits(std::min(n, CHB));
 }
 
 }  // namespace
