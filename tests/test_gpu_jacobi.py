@@ -116,8 +116,8 @@ def test_preconditioner_errors(ctx):
     rhs = rng.standard_normal(36)
     with pytest.raises(ttgpu.TTGError, match="unknown"):
         ttgpu.solve3d_2(Phi1, A, Phi2, rhs, 1e-8, 1, np.zeros(36), 4, ctx=ctx)
-    with pytest.raises(ttgpu.TTGError, match="mixed"):
-        ttgpu.solve3d_2(Phi1, A, Phi2, rhs, 1e-8, 1, np.zeros(36), 1, ctx=ctx, precision="mixed")
+    with pytest.raises(ttgpu.TTGError, match="cjacobi"):
+        ttgpu.solve3d_2(Phi1, A, Phi2, rhs, 1e-8, 1, np.zeros(36), 2, ctx=ctx, precision="mixed")
     A0 = A.copy()
     A0[:] = 0.0  # every Jacobi block singular: the factorization error surfaces
     with pytest.raises(ttgpu.TTGError):
@@ -126,3 +126,40 @@ def test_preconditioner_errors(ctx):
     M = rng.standard_normal((8, 8))
     U, s, VT = ttgpu.dense_svd(M, ctx=ctx)
     assert np.allclose(U * s @ VT, M)
+
+
+@pytest.mark.parametrize("rx1,n,rx2", [(6, 32, 5), (12, 64, 10)])
+def test_cjacobi_mixed_local_solve(ctx, rx1, n, rx2):
+    """'cjacobi' in the mixed-precision local solve (BF16 matvecs of B P in
+    the FP32 Krylov solves, FP64 refinement): the FP64 residual target is
+    met, with fewer Krylov steps than without the preconditioner."""
+    rng = np.random.default_rng(rx1 * n + 11)
+    Phi1, A, Phi2 = _system(rng, rx1, n, rx2)
+    sz = rx1 * n * rx2
+    rhs = rng.standard_normal(sz)
+    sol_prev = np.zeros(sz)
+    tol = 1e-9
+    i1, i0 = {}, {}
+    got = ttgpu.solve3d_2(Phi1, A, Phi2, rhs, tol, 1, sol_prev, 1, 40, 2, ctx=ctx,
+                          precision="mixed", info=i1)
+    ttgpu.solve3d_2(Phi1, A, Phi2, rhs, tol, 1, sol_prev, 0, 40, 2, ctx=ctx, precision="mixed",
+                    info=i0)
+    res = np.linalg.norm(oamen.bfun3(Phi1, A, Phi2, got) - rhs) / np.linalg.norm(rhs)
+    assert res <= tol * 1.0001
+    assert i1["iters"] < i0["iters"]
+
+
+def test_cjacobi_mixed_amen(ctx):
+    """AMEn in mixed precision with local_prec 'cjacobi' meets its stopping
+    test with a true residual within the tolerance, like the FP64 solve."""
+    from oracle.tt import true_residual
+    A, y, x0, z0 = aniso_config(d=5, n=32)
+    kw = dict(x0=ttgpu.TensorTrain(x0.n, x0.r, x0.flat()),
+              z0=ttgpu.TensorTrain(z0.n, z0.r, z0.flat()), ctx=ctx, rmax=48, nswp=20)
+    st = {}
+    got = ttgpu.amen_solve2(ttgpu.TTMatrix(A.n, A.m, A.r, A.flat()),
+                            ttgpu.TensorTrain(y.n, y.r, y.flat()), 1e-8, stats=st,
+                            local_prec="cjacobi", precision="mixed", **kw)
+    assert st["max_res"][st["sweeps"] - 1] < 1e-8
+    assert true_residual(A, TT.from_flat(got.n, got.r, got.core), y) <= 1e-8
+

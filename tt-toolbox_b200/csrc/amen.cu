@@ -36,9 +36,10 @@ LocalSolveResult local_solve_from_residual(Context* c, const MvDims& d, const do
               "local preconditioner %d is unknown (0 none, 1 'cjacobi', 2 'ljacobi', "
               "3 'rjacobi')", prec);
   if (precision == TTG_MIXED) {
-    TTG_REQUIRE(prec == 0, "the mixed-precision local solve has no local preconditioner");
+    TTG_REQUIRE(prec == 0 || prec == 1,
+                "the mixed-precision local solve has the 'cjacobi' preconditioner only");
     return local_solve_mixed(c, d, Phi1, A, Phi2, rhs, dres, nres, nrhs, tol, sol_prev, nrestart,
-                             niters, sol, bsol_out);
+                             niters, sol, bsol_out, prec);
   }
   LocalSolveResult out;
   const int64_t sz = d.in_size();
@@ -231,8 +232,8 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   TTG_REQUIRE(o.local_prec >= 0 && o.local_prec <= 3,
               "local_prec %d is unknown (0 = none, 1 'cjacobi', 2 'ljacobi', 3 'rjacobi')",
               o.local_prec);
-  TTG_REQUIRE(o.local_prec == 0 || o.precision == TTG_FP64,
-              "the local preconditioners run with precision TTG_FP64 only");
+  TTG_REQUIRE(o.local_prec <= 1 || o.precision == TTG_FP64,
+              "'ljacobi' and 'rjacobi' run with precision TTG_FP64 only");
   TTG_REQUIRE(o.precision == TTG_FP64 || o.precision == TTG_MIXED, "unknown precision %d",
               o.precision);
   TTG_REQUIRE(o.nswp >= 1 && o.local_restart >= 1 && o.local_iters >= 1 && o.rmax >= 1 &&

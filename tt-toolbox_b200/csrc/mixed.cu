@@ -17,6 +17,7 @@
 #include <cstring>
 #include <vector>
 
+#include "jacobi.h"
 #include "mixed.h"
 #include "mixed_ops.h"
 
@@ -55,6 +56,7 @@ struct ArArgs {
 };
 
 __device__ __forceinline__ void put_x(const ArArgs& a, int64_t i, float v) {
+  if (!a.X) return;  // preconditioned solve: the operand is P v, written apart
   const int64_t row = i / a.rx2, b = i - row * a.rx2;
   a.X[b + int64_t(a.ldx) * row] = __float2bfloat16_rn(v);
 }
@@ -274,6 +276,29 @@ __global__ void k_ar_update(ArArgs a, int k, float* x) {
   }
 }
 
+// Centre block-Jacobi on vectors in the reversed layout v[k + rx2 (j + n i)]:
+// out[k, j, i] = sum_m J[i, j, m, k] v[k, m, i] with the FP64 blocks J of
+// jac_gen_c_f64 (natural layout J[i + rx1 (j + n (m + n k))]).  To BF16 in
+// the matvec's K-major operand layout (xb, ld ldx) or to FP32 (xf).
+__global__ void k_prec_rev(int64_t rx1, int64_t n, int64_t rx2, const double* __restrict__ J,
+                           const float* __restrict__ v, __nv_bfloat16* __restrict__ xb,
+                           int64_t ldx, float* __restrict__ xf, const int* skip) {
+  pdl_begin();
+  if (skip && *skip) return;
+  const int64_t total = rx1 * n * rx2;
+  AR_LOOP(e, total) {
+    const int64_t k = e % rx2, j = (e / rx2) % n, i = e / (rx2 * n);
+    const double* Jr = J + i + rx1 * j + rx1 * n * n * k;
+    const float* vr = v + k + rx2 * n * i;
+    double s = 0.0;
+    for (int64_t m = 0; m < n; ++m) s += Jr[rx1 * n * m] * double(vr[rx2 * m]);
+    if (xb)
+      xb[k + ldx * (j + n * i)] = __float2bfloat16_rn(float(s));
+    else
+      xf[e] = float(s);
+  }
+}
+
 // r = b - y (FP32)
 __global__ void k_sub_f32(int64_t n, const float* b, const float* y, float* r) {
   pdl_begin();
@@ -334,10 +359,20 @@ struct Gmres32 {
     c->launches += 1;
   }
 
-  // Solve B x = b approximately; x (FP32, zeroed here); returns Krylov steps.
-  int64_t solve(MixedOp& op, const float* b, float* x, double reltol, int64_t max_restarts) {
+  // Right-preconditioned operand: X = bf16(P v) for the centre block-Jacobi
+  // blocks J (FP64, natural layout), v in the reversed layout.
+  void prec_x(MixedOp& op, const double* J, const float* v) {
+    launch(c, k_prec_rev, blocks, AR_THREADS, 0, op.d.rx1, op.d.n, op.d.rx2, J, v, op.X.p(),
+           op.ldx, static_cast<float*>(nullptr), c->skip);
+    TTG_CHECK_LAUNCH();
+  }
+
+  // Solve B x = b approximately (B P y = b, x = y, when J is given: the
+  // caller applies P to x); x (FP32, zeroed here); returns Krylov steps.
+  int64_t solve(MixedOp& op, const float* b, float* x, double reltol, int64_t max_restarts,
+                const double* J = nullptr) {
     int64_t steps = 0;
-    a.X = op.X.p();
+    a.X = J ? nullptr : op.X.p();
     a.rx2 = int(op.d.rx2);
     a.ldx = int(op.ldx);
     a.reltol = reltol;
@@ -345,7 +380,12 @@ struct Gmres32 {
     for (int64_t it = 0; it < max_restarts; ++it) {
       const float* rr = b;
       if (it > 0) {
-        op.apply(c, x, w.p());
+        if (J) {
+          prec_x(op, J, x);
+          op.apply_converted(c, w.p());
+        } else {
+          op.apply(c, x, w.p());
+        }
         launch(c, k_sub_f32, blocks, AR_THREADS, 0, sz, b, w.p(), r.p());
         rr = r.p();
       }
@@ -371,6 +411,7 @@ struct Gmres32 {
         for (int jj = j; jj < jend; ++jj) {
           int jv = jj;
           seqs.push_back(c->ev_seq);
+          if (J) prec_x(op, J, V.p() + int64_t(jj) * sz);  // X = bf16(P V(:, jv))
           op.apply_converted(c, w.p());  // X holds V(:, jv) (k_ar_init / k_arnoldi)
           void* aa[] = {&a, &jv};
           coop((const void*)k_arnoldi, aa, arnoldi_smem());
@@ -424,16 +465,27 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
                                    const double* A, const double* Phi2, const double* rhs,
                                    const double* dres, double nres, double nrhs, double tol,
                                    const double* sol_prev, int64_t nrestart, int64_t niters,
-                                   double* sol, double* bsol_out) {
+                                   double* sol, double* bsol_out, int prec) {
   LocalSolveResult out;
   const int64_t sz = d.in_size();
+  TTG_REQUIRE(prec == 0 || prec == 1,
+              "the mixed-precision local solve has the 'cjacobi' preconditioner only");
+  // Centre block-Jacobi blocks (FP64) for the right preconditioning of the
+  // low-precision Krylov solves and of the FP64 fallback.
+  DBuf<double> J, pw;
+  if (prec == 1) {
+    J.reset(c, jac_size(1, d.rx1, d.n, d.rx2));
+    pw.reset(c, sz);
+    jac_gen_c_f64(c, d.rx1, d.n, d.rx2, d.ra1, d.ra2, Phi1, A, Phi2, J.p());
+  }
   if (nrestart > sz) nrestart = sz;
   TTG_REQUIRE(nrestart <= 1024, "mixed solve: restart length %lld too large", (long long)nrestart);
   MixedOp op;
   op.prepare(c, d, Phi1, A, Phi2);
   Gmres32 gm(c, sz, int(nrestart));
   DBuf<double> t1(c, d.t1_size()), t2(c, d.t2_size()), r64(c, sz), prev(c, sz), s(c, 2);
-  DBuf<float> rrev(c, sz), dx(c, sz);
+  DBuf<float> rrev(c, sz), dx(c, sz), dxp;
+  if (prec == 1) dxp.reset(c, sz);
   copy_f64(c, sz, sol_prev, sol);
   auto residual = [&]() -> double {
     if (bsol_out) {
@@ -457,9 +509,17 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
     if (!(nr > target)) break;
     nat_to_rev(c, d.rx1, d.n, d.rx2, r64.p(), rrev.p(), 1.0 / nr);
     const double reltol = std::max(target / nr, INNER_TOL);
-    out.iters += gm.solve(op, rrev.p(), dx.p(), reltol, niters);
+    out.iters += gm.solve(op, rrev.p(), dx.p(), reltol, niters, prec ? J.p() : nullptr);
     copy_f64(c, sz, sol, prev.p());
-    rev_to_nat_add(c, d.rx1, d.n, d.rx2, dx.p(), sol, nr);
+    if (prec) {  // the correction is P y
+      launch(c, k_prec_rev, gm.blocks, AR_THREADS, 0, d.rx1, d.n, d.rx2, J.p(), dx.p(),
+             static_cast<__nv_bfloat16*>(nullptr), int64_t(0), dxp.p(),
+             static_cast<const int*>(nullptr));
+      TTG_CHECK_LAUNCH();
+      rev_to_nat_add(c, d.rx1, d.n, d.rx2, dxp.p(), sol, nr);
+    } else {
+      rev_to_nat_add(c, d.rx1, d.n, d.rx2, dx.p(), sol, nr);
+    }
     const double nr_new = residual();
     out.have_bsol = bsol_out != nullptr;
     if (!(nr_new < nr)) {  // no progress: keep the better iterate and stop
@@ -481,9 +541,18 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
     if (nr > target) {
       DBuf<double> dsol(c, sz);
       auto mv = [&](const double* x, double* y) {
-        local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
+        if (prec == 1) {  // B P x
+          jac_apply_c_f64(c, d.rx1, d.n, d.rx2, J.p(), x, pw.p());
+          local_matvec_f64(c, d, Phi1, A, Phi2, pw.p(), y, t1.p(), t2.p());
+        } else {
+          local_matvec_f64(c, d, Phi1, A, Phi2, x, y, t1.p(), t2.p());
+        }
       };
       GmresResult g = gmres_hh_f64(c, mv, r64.p(), sz, nrestart, target / nr, niters, dsol.p());
+      if (prec == 1) {
+        jac_apply_c_f64(c, d.rx1, d.n, d.rx2, J.p(), dsol.p(), pw.p());
+        copy_f64(c, sz, pw.p(), dsol.p());
+      }
       axpby_f64(c, sz, 1.0, dsol.p(), 1.0, sol);
       out.iters += g.iters;
       out.matvecs_fp64 += g.matvecs;
