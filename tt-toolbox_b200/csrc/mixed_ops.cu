@@ -826,6 +826,53 @@ void MixedOp::stages(Context* c, float* y) {
   c->mv_flops[1] += d.flops();
 }
 
+namespace {
+// out[kk + ldk * row] = bf16(src(row, kk)), zero for kk >= K, with
+// src(row, kk) = src[row + ld * kk] (trans = 0) or src[kk + ld * row] (1).
+__global__ void k_cvt_kmajor(int64_t rows, int64_t K, int64_t ldk, const double* __restrict__ src,
+                             int64_t ld, int trans, __nv_bfloat16* __restrict__ out) {
+  pdl_begin();
+  const int64_t total = rows * ldk;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t kk = e % ldk, row = e / ldk;
+    float v = 0.f;
+    if (kk < K) v = float(trans ? src[kk + ld * row] : src[row + ld * kk]);
+    out[e] = __float2bfloat16_rn(v);
+  }
+}
+
+// C[m + ldc n] = Cf[m + M n] (FP32 -> FP64)
+__global__ void k_f32_to_f64(int64_t M, int64_t N, const float* __restrict__ Cf,
+                             double* __restrict__ C, int64_t ldc) {
+  pdl_begin();
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < M * N;
+       e += int64_t(gridDim.x) * blockDim.x)
+    C[(e % M) + ldc * (e / M)] = double(Cf[e]);
+}
+}  // namespace
+
+void gemm_bf16(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, const double* A,
+               int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc) {
+  TTG_REQUIRE(M >= 1 && N >= 1 && K >= 1 && M < (1ll << 31) && N < (1ll << 31),
+              "bf16 gemm: sizes out of range");
+  const int64_t ldk = up8(K);
+  DBuf<__nv_bfloat16> Ab(c, ldk * M), Bb(c, ldk * N);
+  DBuf<float> Cf(c, M * N);
+  // A operand rows m: op(A)(m, kk); B operand rows n: op(B)(kk, n).
+  launch(c, k_cvt_kmajor, blocks_for(c, ldk * M), 256, 0, M, K, ldk, A, lda, tA ? 1 : 0, Ab.p());
+  launch(c, k_cvt_kmajor, blocks_for(c, ldk * N), 256, 0, N, K, ldk, B, ldb, tB ? 0 : 1, Bb.p());
+  TTG_CHECK_LAUNCH();
+  const int bn = pick_bn(c, M, N, 1);
+  CUtensorMap mA, mB;
+  make_map(&mA, Ab.p(), K, M, ldk, UM_BM);
+  make_map(&mB, Bb.p(), K, N, ldk, bn);
+  OutMap om{Cf.p(), M, N, M, 1, 0, N, M, 0, 0};
+  umma_gemm(c, mA, mB, K, 0, 0, M, N, 1, om, false, bn);
+  launch(c, k_f32_to_f64, blocks_for(c, M * N), 256, 0, M, N, Cf.p(), C, ldc);
+  TTG_CHECK_LAUNCH();
+}
+
 void nat_to_rev(Context* c, int64_t r1, int64_t n, int64_t r2, const double* x, float* y,
                 double scale) {
   launch(c, k_nat_to_rev, blocks_for(c, r1 * n * r2), 256, 0, r1, n, r2, x, y, scale);

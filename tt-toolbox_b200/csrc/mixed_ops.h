@@ -39,6 +39,13 @@ struct MixedOp {
   void stages_fused(Context* c, float* y);
 };
 
+// C (M x N, ld ldc, FP64) = op(A) op(B) on the BF16 tensor cores with FP32
+// accumulation: FP64 operands converted to BF16 (K-major), one tcgen05
+// GEMM, the FP32 result widened.  op(A) is M x K, op(B) K x N, column-major
+// as gemm_f64.  The contractions of the mixed-precision rounding.
+void gemm_bf16(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, const double* A,
+               int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc);
+
 // Natural [i, j, k] FP64 <-> reversed [k, j, i] FP32 vector layouts.
 void nat_to_rev(Context* c, int64_t r1, int64_t n, int64_t r2, const double* x, float* y,
                 double scale);

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "linalg.h"
+#include "mixed_ops.h"
 #include "round.h"
 
 namespace ttg {
@@ -56,8 +57,6 @@ ttg_tt_s* round_tt(ttg_tt_s* in, double eps, const std::vector<int64_t>& rmax_in
   TTG_REQUIRE(!in->is_matrix, "round: TT matrices are rounded through their tensor form");
   TTG_REQUIRE(precision == TTG_FP64 || precision == TTG_MIXED, "round: unknown precision %d",
               precision);
-  if (precision != TTG_FP64)
-    fail(TTG_ERR_UNSUPPORTED, "round: only precision TTG_FP64 is implemented");
   require_finite(in, "the input tensor");
   const int64_t d = in->d;
   std::vector<int64_t> n = in->n, r = in->r;
@@ -89,8 +88,11 @@ ttg_tt_s* round_tt(ttg_tt_s* in, double eps, const std::vector<int64_t>& rmax_in
       if (nrm[i + 1] != 0.0) axpby_f64(c, k * cols, 1.0 / nrm[i + 1], R.p(), 0.0, R.p());
       const int64_t nc = n[i + 1] * r[i + 2];
       DBuf<double> c1(c, k * nc);
-      gemm_f64(c, false, false, k, nc, cols, 1.0, R.p(), k, 0, cr[i + 1].p(), cols, 0, 0.0,
-               c1.p(), k, 0, 1);                                        // round.m:47
+      if (precision == TTG_MIXED)                                       // round.m:47
+        gemm_bf16(c, false, false, k, nc, cols, R.p(), k, cr[i + 1].p(), cols, c1.p(), k);
+      else
+        gemm_f64(c, false, false, k, nc, cols, 1.0, R.p(), k, 0, cr[i + 1].p(), cols, 0, 0.0,
+                 c1.p(), k, 0, 1);
       r[i + 1] = k;                                                     // round.m:48
       cr[i] = std::move(Q);
       cr[i + 1] = std::move(c1);
@@ -131,8 +133,11 @@ ttg_tt_s* round_tt(ttg_tt_s* in, double eps, const std::vector<int64_t>& rmax_in
       copy2d_f64(c, rows, r1, U.p(), rows, US.p(), rows, S.p());
       const int64_t m1 = r[i - 1] * n[i - 1];
       DBuf<double> c1(c, m1 * r1);
-      gemm_f64(c, false, false, m1, r1, rows, 1.0, cr[i - 1].p(), m1, 0, US.p(), rows, 0, 0.0,
-               c1.p(), m1, 0, 1);
+      if (precision == TTG_MIXED)                                       // round.m:83
+        gemm_bf16(c, false, false, m1, r1, rows, cr[i - 1].p(), m1, US.p(), rows, c1.p(), m1);
+      else
+        gemm_f64(c, false, false, m1, r1, rows, 1.0, cr[i - 1].p(), m1, 0, US.p(), rows, 0, 0.0,
+                 c1.p(), m1, 0, 1);
       // core_i = VT(1:r1, :)  (round.m:84)
       DBuf<double> c0(c, r1 * cols);
       copy2d_f64(c, r1, cols, VT.p(), K, c0.p(), r1);
