@@ -408,41 +408,41 @@ def round_flops(n, r):
 
 def run_round_config(ctx, reps=3, cpu=True):
     """Rounding of the sum of four rank-64 Gaussian TTs (d=20, n=16, internal
-    ranks 256) to eps 1e-8, FP64 on the device; the mixed form (TF32/BF16
-    contractions) is not implemented and is refused by the library."""
+    ranks 256) to eps 1e-8 on the device: the FP64 form and the mixed form
+    (R * core and core * (U S) on BF16 tensor cores, FP64 QR/SVD)."""
     import ttgpu
     from ttgpu import workloads
     W = dict(d=20, n=16, r=64, terms=4, seed=2, eps=1e-8)
     X = workloads.round_input(d=W["d"], n=W["n"], r=W["r"], terms=W["terms"], seed=W["seed"])
     dX = ttgpu.DeviceTT.upload(ctx, X)
-    ms, st = [], {}
-    Y = None
-    for it in range(reps + 1):
-        if Y is not None:
-            Y.free()
-        ctx.flush_l2()
-        st = {}
-        Y = ttgpu.round(dX, W["eps"], ctx=ctx, stats=st)
-        if it:
-            ms.append(st["ms_total"])
-    ranks = [int(v) for v in Y.shape()[2]]
-    D = ttgpu.tt_axpby(1.0, Y, -1.0, dX, ctx=ctx)
-    err = ttgpu.tt_norm(D, ctx=ctx) / ttgpu.tt_norm(dX, ctx=ctx)
-    D.free()
-    Y.free()
-    t0 = time.perf_counter()
-    Yh = ttgpu.round(X, W["eps"], ctx=ctx)
-    e2e = time.perf_counter() - t0
-    dX.free()
     fl = round_flops([int(v) for v in X.n], [int(v) for v in X.r])
-    v = statistics.median(ms) * 1e-3
     out = {"workload": "round: d=20 n=16, sum of 4 rank-64 Gaussian TTs (ranks 256), eps 1e-8",
-           "precision": "fp64", "value": v, "unit": "s", "gflop": fl * 1e-9,
-           "gflops": fl / v * 1e-9, "ms_qr_sweep": st["ms_qr_sweep"],
-           "ms_svd_sweep": st["ms_svd_sweep"], "ranks_max": max(ranks),
-           "rel_err": err, "e2e_s": e2e, "e2e_ranks_max": int(max(Yh.r)),
-           "mixed": "unavailable: the TF32/BF16-contraction rounding is not implemented "
-                    "(ttg_round refuses TTG_MIXED)"}
+           "gflop": fl * 1e-9}
+    xnorm = ttgpu.tt_norm(dX, ctx=ctx)
+    for prec in ("fp64", "mixed"):
+        ms, st = [], {}
+        Y = None
+        for it in range(reps + 1):
+            if Y is not None:
+                Y.free()
+            ctx.flush_l2()
+            st = {}
+            Y = ttgpu.round(dX, W["eps"], precision=prec, ctx=ctx, stats=st)
+            if it:
+                ms.append(st["ms_total"])
+        ranks = [int(v) for v in Y.shape()[2]]
+        D = ttgpu.tt_axpby(1.0, Y, -1.0, dX, ctx=ctx)
+        err = ttgpu.tt_norm(D, ctx=ctx) / xnorm
+        D.free()
+        Y.free()
+        v = statistics.median(ms) * 1e-3
+        out[prec] = {"value": v, "unit": "s", "gflops": fl / v * 1e-9,
+                     "ms_qr_sweep": st["ms_qr_sweep"], "ms_svd_sweep": st["ms_svd_sweep"],
+                     "ranks_max": max(ranks), "rel_err": err}
+    t0 = time.perf_counter()
+    ttgpu.round(X, W["eps"], ctx=ctx)
+    out["fp64"]["e2e_s"] = time.perf_counter() - t0
+    dX.free()
     if cpu:
         sys.path.insert(0, ROOT)
         from oracle.builders import round_config
