@@ -341,19 +341,22 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
           DBuf<double> U(c, rz[i] * K), Sv(c, K), VT(c, K * ncols);
           svd_f64(c, rz[i], ncols, crzy.p(), U.p(), Sv.p(), VT.p());     // :311
           kz = std::min(kickrank, K);                                     // :312
-          zt.reset(c, ncols * kz);
-          transpose_f64(c, kz, ncols, VT.p(), K, zt.p(), ncols);
+          // The rows of V' are orthonormal, so the QR of :320 returns them
+          // up to column signs (a gauge of z): they are the new core.
+          rznew = kz;
+          crz[i].buf.reset(c, kz * ncols);
+          copy2d_f64(c, kz, ncols, VT.p(), K, crz[i].p(), kz);            // :322-323
         } else {
           kz = rz[i];
           zt.reset(c, ncols * kz);
           transpose_f64(c, rz[i], ncols, crz[i].p(), rz[i], zt.p(), ncols);  // :317
+          const int64_t kq = std::min(ncols, kz);
+          DBuf<double> Q(c, ncols * kq), R(c, kq * kz);
+          qr_f64(c, ncols, kz, zt.p(), Q.p(), R.p());                    // :320
+          rznew = kq;
+          crz[i].buf.reset(c, kq * ncols);
+          transpose_f64(c, ncols, kq, Q.p(), ncols, crz[i].p(), kq);     // :322-323
         }
-        const int64_t kq = std::min(ncols, kz);
-        DBuf<double> Q(c, ncols * kq), R(c, kq * kz);
-        qr_f64(c, ncols, kz, zt.p(), Q.p(), R.p());                      // :320
-        rznew = kq;
-        crz[i].buf.reset(c, kq * ncols);
-        transpose_f64(c, ncols, kq, Q.p(), ncols, crz[i].p(), kq);       // :322-323
       }
       if (swp > 1)                                                      // :325-328
         scalar_op(c, SC_NRMSC_DIV, NC, S.y(i - 1), S.a(i - 1), S.x(i - 1));
@@ -601,11 +604,11 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
         DBuf<double> U(c, mz * K), Sv(c, K), VT(c, K * rz[i + 1]);
         svd_f64(c, mz, rz[i + 1], crzy.p(), U.p(), Sv.p(), VT.p());       // :613
         const int64_t kz = std::min(kickrank, K);                          // :614
-        const int64_t kq = std::min(mz, kz);
-        DBuf<double> Q(c, mz * kq), R(c, kq * kz);
-        qr_f64(c, mz, kz, U.p(), Q.p(), R.p());                            // :619
-        rznew = kq;
-        crz[i].buf = std::move(Q);                                         // :621-622
+        // U has orthonormal columns: the QR of :619 returns its first kz
+        // columns up to signs (a gauge of z).
+        rznew = kz;
+        crz[i].buf.reset(c, mz * kz);
+        copy_f64(c, mz * kz, U.p(), crz[i].p());                           // :621-622
       }
 
       if (i < d - 1) {                                                     // :625
@@ -615,10 +618,9 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
           DBuf<double> leftresid(c, ld.out_size());
           local_matvec_f64(c, ld, Phi1, A1, phiza[i + 1].p(), uv.p(), leftresid.p());  // :702
           mv_fp64++;
-          DBuf<double> ty(c, rx[i] * n[i] * ry[i + 1]), uk(c, M * rz[i + 1]);
-          gemm_f64(c, false, false, rx[i], n[i] * ry[i + 1], ry[i], 1.0, phiy[i].p(), rx[i], 0,
-                   y1.p(), ry[i], 0, 0.0, ty.p(), rx[i], 0, 1);            // :704
-          gemm_f64(c, false, false, M, rz[i + 1], ry[i + 1], 1.0, ty.p(), M, 0, phizy[i + 1].p(),
+          // lefty = phiy{i} * y1 (:704) is t, already formed for the rhs (:456)
+          DBuf<double> uk(c, M * rz[i + 1]);
+          gemm_f64(c, false, false, M, rz[i + 1], ry[i + 1], 1.0, t.p(), M, 0, phizy[i + 1].p(),
                    ry[i + 1], 0, 0.0, uk.p(), M, 0, 1);                     // :706
           axpby_f64(c, M * rz[i + 1], -1.0, leftresid.p(), 1.0, uk.p());   // :707
           // [u, rv] = qr([u, uk]) ; v = [v, 0] * rv.'  (:713-716)
