@@ -41,7 +41,9 @@ def parse():
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision")
     p.add_argument("--no-configs", action="store_true",
-                   help="skip the rounding and gradient configurations")
+                   help="skip the rounding, gradient and batched configurations")
+    p.add_argument("--no-batch", action="store_true",
+                   help="skip the batched configuration in the configs block")
     p.add_argument("--workload", default="amen", choices=["amen", "batch"],
                    help="amen: the headline single solve; batch: 512 independent systems "
                         "(one timed batch; --steps/--warmup do not apply)")
@@ -377,6 +379,12 @@ def run_ours(args, dist):
         line["configs"] = {"round": run_round_config(ctx, cpu=dist.world == 1
                                                      and not args.no_cpu_baseline),
                            "grad": run_grad_config(ctx)}
+        if not args.no_batch:
+            bargs = argparse.Namespace(batch_count=args.batch_count,
+                                       batch_workers=args.batch_workers,
+                                       batch_sample=min(args.batch_sample, 16),
+                                       no_cpu_baseline=args.no_cpu_baseline or dist.world > 1)
+            line["configs"]["batch"] = run_batch(bargs, dist)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         times, info = cpu_baseline_run(W, reps=1)
         line["cpu_baseline"] = {"value": times[0], "unit": "s", "cores": blas_threads(),
