@@ -90,3 +90,16 @@ def test_dense_qr_rank_deficient(ctx):
     Q, R = ttgpu.dense_qr(A, ctx=ctx)
     assert np.linalg.norm(Q @ R - A) / np.linalg.norm(A) < 1e-13
     assert np.linalg.norm(Q.T @ Q - np.eye(5)) < 1e-12
+
+
+@pytest.mark.parametrize("m,n", [(8192, 4), (40000, 1), (9000, 8), (30000, 5)])
+def test_skinny_qr_matches_lapack(ctx, m, n):
+    """Skinny matrices too tall for one CTA's shared memory: the one-CTA
+    Householder QR from global memory gives LAPACK's factors, signs included."""
+    rng = np.random.default_rng(m + 3 * n)
+    A = rng.standard_normal((m, n))
+    Q, R = ttgpu.dense_qr(A, ctx=ctx)
+    Qr, Rr = np.linalg.qr(A)
+    assert np.linalg.norm(R - Rr) <= 1e-12 * np.linalg.norm(Rr)
+    assert np.linalg.norm(Q.T @ Q - np.eye(n)) < 1e-12
+    assert np.linalg.norm(Q @ R - A) <= 1e-13 * np.linalg.norm(A)

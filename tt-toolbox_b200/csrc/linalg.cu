@@ -183,6 +183,10 @@ int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, dou
     small_qr_f64(c, m, n, A, m, Q, R);
     return k;
   }
+  if (skinny_qr_fits(m, n)) {  // a few columns, too tall for shared memory
+    skinny_qr_f64(c, m, n, A, m, Q, R);
+    return k;
+  }
   if (!lapack_signs && scholqr_ok(m, n) && scholqr3_f64(c, m, n, A, Q, R)) return k;
   const int mi = as_int(m, "m"), ni = as_int(n, "n"), ki = as_int(k, "k");
   DBuf<double> work(c, m * n), tau(c, k > 0 ? k : 1);

@@ -410,6 +410,120 @@ __global__ void __launch_bounds__(SD_THREADS) k_house_qr(int m, int n, const dou
 
 
 // ---------------------------------------------------------------------------
+// Householder QR of a skinny m x n matrix (n <= SK_MAX_N) too tall for shared
+// memory: the work copy W lives in global memory (L2), every thread owns the
+// rows i = tid (mod SD_THREADS), and each reflector needs two block-wide
+// reductions -- the column norm, then the n - j - 1 inner products of all
+// trailing columns at once -- instead of one warp per column.  Same
+// reflectors and signs as k_house_qr (LAPACK's dlarfg convention).
+// ---------------------------------------------------------------------------
+
+constexpr int SK_MAX_N = 8;
+
+// Block-wide sums of cnt <= SK_MAX_N values per thread; every thread gets
+// the totals in out[0..cnt).  scratch: SD_WARPS * SK_MAX_N doubles (shared).
+__device__ void block_sums(const double* v, int cnt, double* scratch, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = 0; q < cnt; ++q) {
+    const double s = wsum(v[q]);
+    if (lane == 0) scratch[warp * SK_MAX_N + q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < cnt) {
+    double t = 0.0;
+    for (int w = 0; w < SD_WARPS; ++w) t += scratch[w * SK_MAX_N + threadIdx.x];
+    scratch[SD_WARPS * SK_MAX_N + threadIdx.x] = t;
+  }
+  __syncthreads();
+  for (int q = 0; q < cnt; ++q) out[q] = scratch[SD_WARPS * SK_MAX_N + q];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(SD_THREADS) k_house_qr_skinny(int64_t m, int n,
+                                                               const double* __restrict__ Ain,
+                                                               int64_t lda, double* __restrict__ W,
+                                                               double* __restrict__ Q,
+                                                               double* __restrict__ R) {
+  pdl_begin();
+  __shared__ double scratch[(SD_WARPS + 1) * SK_MAX_N];
+  __shared__ double tau[SK_MAX_N];
+  const int tid = threadIdx.x;
+  const int k = int(m < n ? m : n);
+  for (int64_t e = tid; e < m * n; e += SD_THREADS) W[e] = Ain[(e % m) + (e / m) * lda];
+  __syncthreads();
+  double part[SK_MAX_N], tot[SK_MAX_N];
+  for (int j = 0; j < k; ++j) {
+    double* wj = W + int64_t(j) * m;
+    double s = 0.0;
+    for (int64_t i = j + 1 + tid; i < m; i += SD_THREADS) s += wj[i] * wj[i];
+    part[0] = s;
+    block_sums(part, 1, scratch, tot);
+    const double alpha = wj[j];
+    __syncthreads();  // every thread has read alpha before wj[j] changes
+    double beta, tj, scal;
+    if (tot[0] == 0.0) {
+      beta = alpha;
+      tj = 0.0;
+      scal = 0.0;
+    } else {
+      beta = -copysign(sqrt(alpha * alpha + tot[0]), alpha);
+      tj = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    for (int64_t i = j + 1 + tid; i < m; i += SD_THREADS) wj[i] *= scal;  // v, v(j) = 1
+    if (tid == 0) {
+      tau[j] = tj;
+      wj[j] = beta;
+    }
+    __syncthreads();
+    const int nc = n - j - 1;
+    if (tj != 0.0 && nc > 0) {
+      for (int q = 0; q < nc; ++q) part[q] = 0.0;
+      for (int64_t i = j + 1 + tid; i < m; i += SD_THREADS) {
+        const double vi = wj[i];
+        for (int q = 0; q < nc; ++q) part[q] += vi * W[i + int64_t(j + 1 + q) * m];
+      }
+      block_sums(part, nc, scratch, tot);
+      for (int q = 0; q < nc; ++q) tot[q] = tj * (tot[q] + W[j + int64_t(j + 1 + q) * m]);
+      __syncthreads();  // row j read by all before it changes
+      for (int q = 0; q < nc; ++q) {
+        double* wc = W + int64_t(j + 1 + q) * m;
+        for (int64_t i = j + 1 + tid; i < m; i += SD_THREADS) wc[i] -= tot[q] * wj[i];
+        if (tid == 0) wc[j] -= tot[q];
+      }
+      __syncthreads();
+    }
+  }
+  for (int e = tid; e < k * n; e += SD_THREADS) {
+    const int i = e % k, c = e / k;
+    R[i + int64_t(c) * k] = (i <= c) ? W[i + int64_t(c) * m] : 0.0;
+  }
+  // Q = H_0 ... H_{k-1} I(:, 0:k), right to left.
+  for (int64_t e = tid; e < m * k; e += SD_THREADS) Q[e] = ((e % m) == (e / m)) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int j = k - 1; j >= 0; --j) {
+    const double tj = tau[j];
+    if (tj == 0.0) continue;  // uniform
+    const double* v = W + int64_t(j) * m;
+    const int nc = k - j;
+    for (int q = 0; q < nc; ++q) part[q] = 0.0;
+    for (int64_t i = j + 1 + tid; i < m; i += SD_THREADS) {
+      const double vi = v[i];
+      for (int q = 0; q < nc; ++q) part[q] += vi * Q[i + int64_t(j + q) * m];
+    }
+    block_sums(part, nc, scratch, tot);
+    for (int q = 0; q < nc; ++q) tot[q] = tj * (tot[q] + Q[j + int64_t(j + q) * m]);
+    __syncthreads();  // row j read by all before it changes
+    for (int q = 0; q < nc; ++q) {
+      double* qc = Q + int64_t(j + q) * m;
+      for (int64_t i = j + 1 + tid; i < m; i += SD_THREADS) qc[i] -= tot[q] * v[i];
+      if (tid == 0) qc[j] -= tot[q];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Cholesky factor and its inverse for shifted Cholesky QR
 // ---------------------------------------------------------------------------
 
@@ -640,6 +754,17 @@ void chol_inv_f64(Context* c, int64_t n, const double* G, int64_t ldg, double sh
   ensure_smem_attr(reinterpret_cast<const void*>(k_chol_inv), c->device, int(SMEM_LIMIT + 1024));
   launch(c, k_chol_inv, 1, SD_THREADS, smem, int(n), G, int(ldg), shift_factor, R, Rinv,
          flag ? flag : c->d_err + 4);
+  TTG_CHECK_LAUNCH();
+}
+
+bool skinny_qr_fits(int64_t m, int64_t n) { return n >= 1 && n <= SK_MAX_N && m >= n; }
+
+void skinny_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
+                   double* R) {
+  TTG_REQUIRE(skinny_qr_fits(m, n), "skinny QR: %lld x %lld out of range", (long long)m,
+              (long long)n);
+  DBuf<double> W(c, m * n);
+  launch(c, k_house_qr_skinny, 1, SD_THREADS, 0, m, int(n), A, lda, W.p(), Q, R);
   TTG_CHECK_LAUNCH();
 }
 

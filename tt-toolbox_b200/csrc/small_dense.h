@@ -9,6 +9,12 @@ bool small_qr_fits(int64_t m, int64_t n);
 // Thin Householder QR in one CTA: Q (m x k, ld m), R (k x n, ld k).
 void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
                   double* R);
+// Thin Householder QR of a skinny m x n matrix (n <= 8, any m >= n) in one
+// CTA working from global memory: Q (m x n, ld m), R (n x n, ld n); the
+// signs of k_house_qr / LAPACK.
+bool skinny_qr_fits(int64_t m, int64_t n);
+void skinny_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
+                   double* R);
 // Cholesky factor of a shifted Gram matrix and its inverse, one CTA:
 // R' R = G + shift_factor * trace(G) * I, Rinv = R^{-1} (n x n, ld n, upper).
 // A non-positive pivot sets *flag (nullptr: the context's factorization
