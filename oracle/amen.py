@@ -384,7 +384,9 @@ class _Follow:
                 continue
             if (cr < gm_tol) != implied and not _near(cr, gm_tol, self.near_tie):
                 bad.append(k)
-        rec = dict(kind="gmres steps", sweep=swp, core=i, own=iters_o, other=iters_g)
+        lo, hi = min(iters_o, iters_g), max(iters_o, iters_g)
+        rec = dict(kind="gmres steps", sweep=swp, core=i, own=iters_o, other=iters_g,
+                   ratio_to_tol=[float(v / gm_tol) for v in hist[max(lo - 2, 0):hi + 1]])
         (self.mismatches if bad or len(hist) < iters_g else self.flips).append(rec)
 
     def rank(self, swp, i, r_own, r_g, K, cap, thr, res_of):
@@ -411,7 +413,10 @@ class _Follow:
             # the other side's exceeding candidate lies somewhere >= r_g - 1
             if not any(_near(res_of(rr), thr, near) for rr in range(r_g - 1, K)):
                 bad.append(r_g - 1)
-        rec = dict(kind="rank", sweep=swp, core=i, own=r_own, other=r_g)
+        lo = max(min(r_own, r_g) - 1, 1)
+        rec = dict(kind="rank", sweep=swp, core=i, own=r_own, other=r_g,
+                   ratio_to_thr={rr: float(res_of(rr) / thr)
+                                 for rr in range(lo, min(max(r_own, r_g) + 1, K))})
         (self.mismatches if bad else self.flips).append(rec)
 
     def stop(self, swp, max_res, tol_exit):
