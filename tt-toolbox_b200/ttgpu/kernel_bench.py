@@ -207,7 +207,7 @@ def amen_bench(args):
 
             def solve():
                 x = amen_solve2(dA, dy, args.tol, x0=dx0, z0=dz0, ctx=ctx, stats=st,
-                                rmax=args.rmax, nswp=50, precision=prec)
+                                rmax=args.rmax, nswp=50, precision=prec, timing=args.timing)
                 ctx.sync()
                 x.free()
 
@@ -217,6 +217,11 @@ def amen_bench(args):
                 solve()
         out[prec] = {k: st[k] for k in ("ms_total", "sweeps", "matvecs", "matvecs_fp64",
                                         "gmres_iters", "launches", "max_rank")}
+        if args.timing:  # per-matvec CUDA events: average in-solve matvec
+            n_lp = max(1, st["matvecs_lp"])
+            out[prec]["lp_matvec_us"] = st["ms_lp"] / n_lp * 1e3
+            out[prec]["lp_matvec_gflop"] = st["gflop_lp"] / n_lp
+            out[prec]["fp64_matvec_us"] = st["ms_fp64"] / max(1, st["matvecs_fp64"]) * 1e3
     print(json.dumps(out))
     for prec, tab in tables.items():
         print("\n# kernels of one warm solve, precision %s\n%s" % (prec, tab))
@@ -374,6 +379,8 @@ def main():
     am.add_argument("--reps", type=int, default=2)
     am.add_argument("--precision", default="fp64,mixed")
     am.add_argument("--kernel-table", action="store_true")
+    am.add_argument("--timing", action="store_true",
+                    help="time every local matvec with CUDA events (slows the solve)")
     dg = sub.add_parser("dgemm")
     dg.add_argument("--size", type=int, default=8192)
     dg.add_argument("--reps", type=int, default=10)
