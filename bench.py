@@ -254,7 +254,7 @@ def run_ours(args, dist):
     def timed_steps(prec, K, timing=False):
         ms, launches, sweeps, gflop = [], 0, [], 0.0
         last = None
-        acc = {"gflop_lp": 0.0, "ms_lp": 0.0, "gflop_fp64": 0.0, "ms_fp64": 0.0,
+        acc = {"gflop_lp": 0.0, "ms_lp": 0.0, "gflop_fp64": 0.0, "ms_fp64": 0.0, "gbyte_lp": 0.0,
                "matvecs_lp": 0, "matvecs": 0}
         for _ in range(K):
             ctx.flush_l2()
@@ -329,21 +329,32 @@ def run_ours(args, dist):
     peaks, peaks_kind = load_peaks()
     a = agg[args.precision]
     if args.precision == "mixed" and a["ms_lp"] > 0:
-        # BF16 tcgen05 local matvec (3 tensor-core GEMMs) per launch.
-        per_launch_tflop = a["gflop_lp"] / max(1, a["matvecs_lp"]) * 1e-3
-        per_launch_ms = a["ms_lp"] / max(1, a["matvecs_lp"])
+        # BF16 tcgen05 local matvec: average over the solve's matvecs of
+        # algorithmic FLOPs (and bytes) per launch / CUDA-event duration.
+        nlp = max(1, a["matvecs_lp"])
+        per_launch_tflop = a["gflop_lp"] / nlp * 1e-3
+        per_launch_ms = a["ms_lp"] / nlp
+        alg_bytes = a["gbyte_lp"] / nlp * 1e9
         achieved = per_launch_tflop / (per_launch_ms * 1e-3)
         peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1590.0))
         tr = load_traffic()
-        # The solve's matvecs span many local sizes; ncu traffic is committed
-        # for one fixed size, so it is reported beside (not as) the in-solve
-        # per-launch traffic.
-        roof = {"kernel": "local matvec, BF16 tcgen05 (3 GEMM launches; the BF16 operand is "
-                          "written by the Arnoldi kernel)", "bound": "tensor",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": None,
-                "traffic_fixed_shape": ({"bytes": tr.get("bytes_per_launch"),
-                                         "shape": tr.get("shape")} if tr else None),
+        fused = os.environ.get("TTG_FUSED_MV", "1") != "0"
+        # ncu measures one fixed shape; its DRAM bytes over the algorithmic
+        # bytes of that shape, times the in-solve algorithmic bytes per
+        # launch, gives the in-solve traffic (DRAM traffic of this kernel
+        # scales with the operand and result sizes).
+        traffic = None
+        if tr and tr.get("ratio"):
+            traffic = tr["ratio"] * alg_bytes
+        roof = {"kernel": ("local matvec, BF16 tcgen05, one persistent launch (k_mv_fused)"
+                           if fused else "local matvec, BF16 tcgen05, three GEMM launches"),
+                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "traffic_basis": (("ncu DRAM bytes / algorithmic bytes = %.3f at %s, times the "
+                                   "in-solve algorithmic bytes per launch"
+                                   % (tr["ratio"], tr.get("shape"))) if traffic else None),
+                "alg_bytes_per_launch": alg_bytes,
+                "hbm_gbs_per_launch": alg_bytes / (per_launch_ms * 1e-3) * 1e-9,
                 "peak_kind": "bf16 sustained, %s" % peaks_kind,
                 "launch_ms": per_launch_ms, "gflop_per_launch": per_launch_tflop * 1e3}
     else:

@@ -184,6 +184,8 @@ typedef struct {
   double ms_fp64;         /* their device time (opts.timing = 1)          */
   int64_t trace_len;      /* local steps run (entries written to opts.trace,
                              up to its capacity)                          */
+  double gbyte_lp;        /* algorithmic DRAM bytes of the BF16 matvecs / 1e9
+                             (operand, operators and result once each)    */
 } ttg_amen_stats;
 
 void ttg_amen_opts_default(ttg_amen_opts* opts);

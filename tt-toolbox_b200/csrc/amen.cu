@@ -257,6 +257,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   TTG_CUDA(cudaEventRecord(e0, c->stream));
   const int64_t mv0 = c->matvecs, fl0 = c->matvec_flops, la0 = c->launches;
   const double flk0[2] = {c->mv_flops[0], c->mv_flops[1]};
+  const double byl0 = c->mv_bytes_lp;
   const int64_t mvk0[2] = {c->mv_count[0], c->mv_count[1]};
   c->ev_collect();
   const double msk0[2] = {c->mv_ms[0], c->mv_ms[1]};
@@ -795,6 +796,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
     c->ev_collect();
     stats->matvecs_lp = c->mv_count[1] - mvk0[1];
     stats->gflop_lp = (c->mv_flops[1] - flk0[1]) * 1e-9;
+    stats->gbyte_lp = (c->mv_bytes_lp - byl0) * 1e-9;
     stats->ms_lp = c->mv_ms[1] - msk0[1];
     stats->gflop_fp64 = (c->mv_flops[0] - flk0[0]) * 1e-9;
     stats->ms_fp64 = c->mv_ms[0] - msk0[0];

@@ -141,6 +141,9 @@ struct Context {
   // solve: sizes the first chunk of queued steps of the next one.
   int krylov_hint = 0;
   double mv_flops[2] = {0.0, 0.0};
+  // Algorithmic DRAM bytes of the BF16 local matvecs: the BF16 operand X,
+  // the three BF16 operators and the FP32 result, once each.
+  double mv_bytes_lp = 0.0;
   // Optional CUDA-event timing of every local matvec on the context stream.
   bool time_matvec = false;
   // Launch the library's stream-ordered kernels as programmatic dependent

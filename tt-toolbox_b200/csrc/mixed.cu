@@ -444,6 +444,7 @@ struct Gmres32 {
           c->matvec_flops -= int64_t(fl) * skipped;
           c->mv_count[1] -= skipped;
           c->mv_flops[1] -= fl * skipped;
+          c->mv_bytes_lp -= op.bytes_per_matvec() * skipped;
           if (c->time_matvec) c->ev_void(seqs[done], c->ev_seq);
         }
       }

@@ -824,6 +824,7 @@ void MixedOp::stages(Context* c, float* y) {
   c->matvec_flops += int64_t(d.flops());
   c->mv_count[1] += 1;
   c->mv_flops[1] += d.flops();
+  c->mv_bytes_lp += bytes_per_matvec();
 }
 
 namespace {

@@ -27,6 +27,14 @@ struct MixedOp {
   void run_stage(Context* c, int stage, int bn, const CUtensorMap& mapB, float* y);
   // Tile width of a stage: autotuned once per shape and device (mixed_ops.cu).
   int tuned_bn(Context* c, int stage);
+  // Algorithmic DRAM bytes of one matvec: X (BF16), Phi2, A, Phi1 (BF16)
+  // read once, y (FP32) written once.
+  double bytes_per_matvec() const {
+    return 2.0 * double(d.rx1) * d.m * d.rx2 +
+           2.0 * (double(d.rx2) * d.ra2 * d.ry2 + double(d.ra1) * d.n * d.m * d.ra2 +
+                  double(d.ry1) * d.rx1 * d.ra1) +
+           4.0 * double(d.ry1) * d.n * d.ry2;
+  }
   // The three GEMM stages from X to y, with the matvec counters: one fused
   // persistent launch (default) or three GEMM launches (TTG_FUSED_MV=0).
   void stages(Context* c, float* y);

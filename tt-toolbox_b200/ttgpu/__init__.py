@@ -68,7 +68,7 @@ class AmenStats(C.Structure):
                 ("ms_total", C.c_double), ("ms_matvec", C.c_double),
                 ("matvec_gflop", C.c_double), ("launches", _i64), ("matvecs_lp", _i64),
                 ("gflop_lp", C.c_double), ("ms_lp", C.c_double), ("gflop_fp64", C.c_double),
-                ("ms_fp64", C.c_double), ("trace_len", _i64)]
+                ("ms_fp64", C.c_double), ("trace_len", _i64), ("gbyte_lp", C.c_double)]
 
     def to_dict(self):
         s = int(self.sweeps)
@@ -81,7 +81,7 @@ class AmenStats(C.Structure):
                     ms_matvec=float(self.ms_matvec), matvecs_lp=int(self.matvecs_lp),
                     gflop_lp=float(self.gflop_lp), ms_lp=float(self.ms_lp),
                     gflop_fp64=float(self.gflop_fp64), ms_fp64=float(self.ms_fp64),
-                    trace_len=int(self.trace_len))
+                    trace_len=int(self.trace_len), gbyte_lp=float(self.gbyte_lp))
 
 
 class AmenMvOpts(C.Structure):
