@@ -351,12 +351,16 @@ def _near(v, ref, near_tie):
 class _Follow:
     """Decision checker: compares this solve's discrete decisions with those
     another implementation recorded (``steps``: one dict per local step with
-    ``rank`` and ``iters``, as ``ttg_amen_step``; ``max_res``: its per-sweep
-    maxima).  Where the two differ and the compared quantity lies within
-    relative ``near_tie`` of its threshold (a near tie: rounding decides),
+    ``rank``, ``iters``, ``res_prev`` and ``res_new``, as ``ttg_amen_step``;
+    ``max_res``: its per-sweep maxima).  Where the two differ and the
+    compared quantity lies near its threshold (a near tie: rounding decides),
     the other implementation's choice is adopted and the step is listed in
     ``flips``; otherwise the difference is listed in ``mismatches`` (and the
-    choice adopted as well, so that the comparison can go on)."""
+    choice adopted as well, so that the comparison can go on).  "Near" is
+    relative ``near_tie``, or four times the relative difference of the two
+    implementations' own local residuals of that step when that is larger:
+    the residuals that set the thresholds carry that much rounding noise
+    (it grows where a local solve ends close to the FP64 floor)."""
 
     def __init__(self, steps, max_res, near_tie):
         self.steps = {(s["sweep"], s["core"]): s for s in steps}
@@ -371,32 +375,43 @@ class _Follow:
             self.mismatches.append(dict(kind="missing step", sweep=swp, core=i))
         return s
 
-    def gmres(self, swp, i, hist, gm_tol, iters_o, iters_g, cap):
+    def noise(self, step, res_prev, res_new=None):
+        """Tie bound of a step: near_tie, or 4x the relative difference of
+        the two sides' local residuals of the step."""
+        d = 0.0
+        for mine, key in ((res_prev, "res_prev"), (res_new, "res_new")):
+            other = step.get(key) if step is not None else None
+            if mine is not None and other is not None and mine > 0:
+                d = max(d, abs(other / mine - 1.0))
+        return max(self.near_tie, 4.0 * d)
+
+    def gmres(self, swp, i, hist, gm_tol, iters_o, iters_g, cap, tie=None):
         """Krylov step count: the other side stopped after ``iters_g`` steps,
         i.e. its estimate stayed >= tol before and fell below at that step
         (unless it hit the cap)."""
         if iters_g == iters_o:
             return
+        near = self.near_tie if tie is None else tie
         bad = []
         for k, cr in enumerate(hist[:iters_g], start=1):
             implied = (k == iters_g)
             if k == iters_g and iters_g >= cap:
                 continue
-            if (cr < gm_tol) != implied and not _near(cr, gm_tol, self.near_tie):
+            if (cr < gm_tol) != implied and not _near(cr, gm_tol, near):
                 bad.append(k)
         lo, hi = min(iters_o, iters_g), max(iters_o, iters_g)
         rec = dict(kind="gmres steps", sweep=swp, core=i, own=iters_o, other=iters_g,
                    ratio_to_tol=[float(v / gm_tol) for v in hist[max(lo - 2, 0):hi + 1]])
         (self.mismatches if bad or len(hist) < iters_g else self.flips).append(rec)
 
-    def rank(self, swp, i, r_own, r_g, K, cap, thr, res_of):
+    def rank(self, swp, i, r_own, r_g, K, cap, thr, res_of, tie=None):
         """Truncation rank: the other side kept ``r_g`` (after the caps
         ``min(., K, rmax)``), i.e. its candidate residuals stayed <= thr for
         candidates >= r_g and exceeded thr at r_g - 1 (when r_g is not
         capped and not the loop's fall-through value 2)."""
         if r_g == r_own:
             return
-        near = self.near_tie
+        near = self.near_tie if tie is None else tie
         bad = []
         capped = r_g >= cap
         for rr in range(K - 1, max(r_g - 1, 1) - 1, -1):
@@ -426,8 +441,9 @@ class _Follow:
         own = max_res < tol_exit
         other = self.max_res[swp - 1] < tol_exit
         if own != other:
+            tie = max(self.near_tie, 4.0 * abs(self.max_res[swp - 1] / max_res - 1.0))
             rec = dict(kind="sweep stop", sweep=swp, own=own, other=other)
-            (self.flips if _near(max_res, tol_exit, self.near_tie) else self.mismatches).append(rec)
+            (self.flips if _near(max_res, tol_exit, tie) else self.mismatches).append(rec)
         return other
 
 
@@ -585,7 +601,7 @@ def amen_solve2(A, y, tol, x0, z0=None, trace=None, follow=None, near_tie=1e-6, 
                                   local_iters, gst, prec)
                         cap = min(local_restart, sol_prev.size) * local_iters
                         fol.gmres(swp, i, gst["hist"], gst["gm_tol"], gst["iters"],
-                                  other["iters"], cap)
+                                  other["iters"], cap, fol.noise(other, res_prev))
                         force = other["iters"]
                         gst = {}
                     sol = solve3d_2(Phi1, A1, Phi2, rhs, real_tol, sol_prev,
@@ -640,7 +656,8 @@ def amen_solve2(A, y, tol, x0, z0=None, trace=None, follow=None, near_tie=1e-6, 
                 if other is not None:
                     r_own = r
                     r = other["rank"]
-                    fol.rank(swp, i, r_own, r, K, min(s.size, rmax), thr, res_of)
+                    fol.rank(swp, i, r_own, r, K, min(s.size, rmax), thr, res_of,
+                             fol.noise(other, res_prev, res_new))
             else:                                                      # :596-601
                 u, v = np.linalg.qr(sol)
                 v = v.T
