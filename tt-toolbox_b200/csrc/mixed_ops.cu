@@ -184,14 +184,18 @@ __global__ void __launch_bounds__(128, 1)
 // launch, so they stay in L2: DRAM sees the operands and y only.  Roles:
 // warp 0 issues TMA loads into a FU_STAGES-deep shared-memory ring (across
 // tile and stage boundaries), one thread of warp 1 issues tcgen05.mma into
-// one of two TMEM accumulators, warps 2-5 drain the other accumulator
-// (tcgen05.ld) and store it in the next stage's K-major layout.  Every wait
+// one of two TMEM accumulators, warps 2-9 drain the other accumulator
+// (tcgen05.ld) and store it in the next stage's K-major layout.  Two CTAs
+// fit on an SM (shared memory and TMEM).  Every wait
 // is bounded: a timeout raises the error flag and every role winds down.
 // ---------------------------------------------------------------------------
 
-constexpr int FU_STAGES = 4;
+constexpr int FU_STAGES = 3;
 constexpr int FU_BN_MAX = 128;
-constexpr int FU_THREADS = 192;
+// warp 0 TMA, warp 1 MMA, warps 2-9 drain the accumulator: two warps per
+// TMEM lane quarter, each taking every other 16-column chunk.
+constexpr int FU_THREADS = 320;
+constexpr int FU_EPI_WARPS = 8;
 constexpr int FU_B_BYTES = FU_BN_MAX * UM_BK * 2;
 constexpr uint32_t FU_TMEM_COLS = 2 * FU_BN_MAX;
 constexpr long long FU_BAR_SPIN_LIMIT = 1LL << 24;
@@ -247,7 +251,7 @@ __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(FU_THREADS, 1)
+__global__ void __launch_bounds__(FU_THREADS, 2)
     k_mv_fused(const __grid_constant__ CUtensorMap tA1, const __grid_constant__ CUtensorMap tB1,
                const __grid_constant__ CUtensorMap tA2, const __grid_constant__ CUtensorMap tB2,
                const __grid_constant__ CUtensorMap tA3, const __grid_constant__ CUtensorMap tB3,
@@ -280,7 +284,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(bar_accf + 8 * b, 1);
-      mbar_init(bar_acce + 8 * b, 4);  // one arrival per epilogue warp
+      mbar_init(bar_acce + 8 * b, FU_EPI_WARPS);  // one arrival per epilogue warp
     }
     fence_barrier_init();
     fence_proxy_async();
@@ -355,8 +359,9 @@ __global__ void __launch_bounds__(FU_THREADS, 1)
         *consumed_slot = kb_cnt;
       }
       __syncwarp();
-    } else {  // epilogue: warps 2..5 own TMEM lanes 32 (warp % 4) ..
+    } else {  // epilogue: warp w owns TMEM lanes 32 (w % 4) .., column half (w - 2) / 4
       const int ew = warp & 3;
+      const int half = (warp - 2) >> 2;
       const int row = ew * 32 + lane;
       const OutMap& om = S.om;
       for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tile_cnt) {
@@ -370,13 +375,13 @@ __global__ void __launch_bounds__(FU_THREADS, 1)
         const bool row_ok = m < om.M;
         const int64_t roff = row_ok ? map2(m, om.r_s1, om.r_t1, om.r_t2) : 0;
         const int64_t boff = int64_t(bz) * om.batch_stride;
-        int64_t cq = int64_t(n0) / om.c_s1, cr = int64_t(n0) % om.c_s1;
         const uint32_t tbase = tmem + (uint32_t(ew * 32) << 16) + buf * FU_BN_MAX;
 #pragma unroll 1
-        for (int c0 = 0; c0 < S.bn; c0 += 16) {
-          if (n0 + c0 >= om.N) break;  // uniform across the CTA
+        for (int c0 = 16 * half; c0 < S.bn; c0 += 32) {
+          if (n0 + c0 >= om.N) break;  // uniform across the warp
           float v[16];
           tmem_ld16(tbase + uint32_t(c0), v);
+          int64_t cq = int64_t(n0 + c0) / om.c_s1, cr = int64_t(n0 + c0) % om.c_s1;
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int64_t n = int64_t(n0) + c0 + j;
