@@ -12,6 +12,7 @@
 //                  of an m x n matrix that fits in shared memory; forms the
 //                  thin Q and R.
 #include <cmath>
+#include <cstdlib>
 
 #include "small_dense.h"
 
@@ -305,6 +306,137 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
       jc_barrier(bar, err);
     }
     if (tid == 0) atomicMax(offmax + slot, (unsigned long long)__double_as_longlong(off));
+    jc_barrier(bar, err);
+    const double m = __longlong_as_double((long long)(*(volatile unsigned long long*)(offmax + slot)));
+    if (m <= tol) break;
+    if (*(volatile int*)err) break;
+  }
+  if (blockIdx.x == 0 && tid == 0 && sweep >= max_sweeps) atomicExch(sweep_err, 5);
+}
+
+// ---------------------------------------------------------------------------
+// Block-cyclic form of the grid-wide Jacobi SVD: the n columns fall into
+// blocks of JB_W; each round of a round-robin tournament on the blocks
+// gives every CTA one block pair, whose 2 JB_W columns of A and of V it
+// loads into shared memory and rotates through one full inner sweep of
+// one-sided Jacobi (every pair of its columns) before writing them back.
+// One grid barrier per block round instead of one per column round (31
+// instead of 255 barriers per sweep at n = 256); the rotations and the
+// stopping rule are those of k_jacobi_coop.
+// ---------------------------------------------------------------------------
+
+constexpr int JB_W = 8;
+constexpr int JB_THREADS = 256;
+constexpr int JB_WARPS = JB_THREADS / 32;
+
+__global__ void __launch_bounds__(JB_THREADS) k_jacobi_block(int n, const double* __restrict__ Ain,
+                                                            int lda, double* A, double* V,
+                                                            unsigned* bar,
+                                                            unsigned long long* offmax, int* err,
+                                                            int* sweep_err, int trans,
+                                                            int max_sweeps) {
+  extern __shared__ double sjb[];  // [2 JB_W][n] columns of A, then of V
+  __shared__ int s_col[2 * JB_W];
+  __shared__ double s_off[JB_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t nn = int64_t(n) * n;
+  for (int64_t e = blockIdx.x * int64_t(JB_THREADS) + tid; e < nn;
+       e += int64_t(gridDim.x) * JB_THREADS) {
+    const int64_t i = e % n, j = e / n;
+    A[e] = trans ? Ain[j + i * lda] : Ain[i + j * lda];
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+  if (blockIdx.x == 0 && tid < 3) offmax[tid] = 0ull;
+  jc_barrier(bar, err);
+  double* sA = sjb;
+  double* sV = sjb + int64_t(2 * JB_W) * n;
+  const int nb = (n + JB_W - 1) / JB_W;
+  const int nbe = (nb + 1) & ~1;  // even number of block players (dummy block if odd)
+  const double tol = 4.0 * 2.220446049250313e-16;
+  int sweep = 0;
+  for (sweep = 0; sweep < max_sweeps; ++sweep) {
+    const int slot = sweep % 3;
+    if (blockIdx.x == 0 && tid == 0) offmax[(sweep + 1) % 3] = 0ull;
+    double off = 0.0;  // per warp
+    for (int r = 0; r < nbe - 1; ++r) {
+      for (int pr = blockIdx.x; pr < nbe / 2; pr += gridDim.x) {
+        const int P = rr_player(pr, r, nbe), Q = rr_player(nbe - 1 - pr, r, nbe);
+        // the block pair's columns (a dummy block contributes none)
+        int nc = 0;
+        if (tid == 0) {
+          for (int b : {P, Q})
+            for (int c = b * JB_W; c < (b + 1) * JB_W && c < n && b < nb; ++c) s_col[nc++] = c;
+          for (int k = nc; k < 2 * JB_W; ++k) s_col[k] = -1;
+        }
+        __syncthreads();
+        nc = 0;
+        for (int k = 0; k < 2 * JB_W; ++k) nc += s_col[k] >= 0;
+        for (int64_t e = tid; e < int64_t(nc) * n; e += JB_THREADS) {
+          const int k = int(e / n);
+          const int64_t i = e % n;
+          sA[e] = A[i + int64_t(s_col[k]) * n];
+          sV[e] = V[i + int64_t(s_col[k]) * n];
+        }
+        __syncthreads();
+        // one inner sweep over all column pairs of the block pair
+        const int ne = (nc + 1) & ~1;
+        for (int ir = 0; ir < ne - 1; ++ir) {
+          for (int ip = warp; ip < ne / 2; ip += JB_WARPS) {
+            int p = rr_player(ip, ir, ne), q = rr_player(ne - 1 - ip, ir, ne);
+            if (p > q) {
+              const int t = p;
+              p = q;
+              q = t;
+            }
+            if (q >= nc) continue;  // dummy
+            double* ap = sA + int64_t(p) * n;
+            double* aq = sA + int64_t(q) * n;
+            double al = 0.0, be = 0.0, ga = 0.0;
+            for (int i = lane; i < n; i += 32) {
+              const double x = ap[i], y = aq[i];
+              al += x * x;
+              be += y * y;
+              ga += x * y;
+            }
+            al = wsum(al);
+            be = wsum(be);
+            ga = wsum(ga);
+            const double nrm = sqrt(al * be);
+            if (nrm == 0.0 || fabs(ga) <= tol * nrm) continue;  // uniform in the warp
+            off = fmax(off, fabs(ga) / nrm);
+            const double zeta = (be - al) / (2.0 * ga);
+            const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            const double cc = 1.0 / sqrt(1.0 + t * t), sn = cc * t;
+            double* vp = sV + int64_t(p) * n;
+            double* vq = sV + int64_t(q) * n;
+            for (int i = lane; i < n; i += 32) {
+              const double x = ap[i], y = aq[i];
+              ap[i] = cc * x - sn * y;
+              aq[i] = sn * x + cc * y;
+              const double vx = vp[i], vy = vq[i];
+              vp[i] = cc * vx - sn * vy;
+              vq[i] = sn * vx + cc * vy;
+            }
+          }
+          __syncthreads();
+        }
+        for (int64_t e = tid; e < int64_t(nc) * n; e += JB_THREADS) {
+          const int k = int(e / n);
+          const int64_t i = e % n;
+          A[i + int64_t(s_col[k]) * n] = sA[e];
+          V[i + int64_t(s_col[k]) * n] = sV[e];
+        }
+        __syncthreads();
+      }
+      jc_barrier(bar, err);
+    }
+    if (lane == 0) s_off[warp] = off;
+    __syncthreads();
+    if (tid == 0) {
+      double m = 0.0;
+      for (int w = 0; w < JB_WARPS; ++w) m = fmax(m, s_off[w]);
+      atomicMax(offmax + slot, (unsigned long long)__double_as_longlong(m));
+    }
     jc_barrier(bar, err);
     const double m = __longlong_as_double((long long)(*(volatile unsigned long long*)(offmax + slot)));
     if (m <= tol) break;
@@ -797,6 +929,18 @@ void svd_tall_small_f64(Context* c, int64_t m, int64_t n, const double* A, int64
   TTG_CHECK_LAUNCH();
 }
 
+// TTG_JACOBI_BLOCK=0 keeps the one-pair-per-CTA grid-wide Jacobi SVD.
+static bool getenv_flag_on(const char* name) {
+  const char* e = getenv(name);
+  return !(e && e[0] == '0');
+}
+
+// The block-pair columns of A and V (4 JB_W n doubles) fit in shared memory.
+static bool jacobi_block_fits(int64_t n) {
+  return n >= 4 * JB_W && sizeof(double) * 4 * JB_W * size_t(n) <= SMEM_LIMIT &&
+         getenv_flag_on("TTG_JACOBI_BLOCK");
+}
+
 void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
                     double* VT, bool via_transpose) {
   int trans = via_transpose ? 1 : 0;
@@ -804,6 +948,36 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
   const size_t mat = size_t(n * n) * sizeof(double);
   const int mode = 2 * mat <= SMEM_LIMIT ? 2 : (mat <= SMEM_LIMIT ? 1 : 0);
   DBuf<double> V(c, n * n), work(c, n * n + 2 * n);
+  if (mode == 0 && jacobi_block_fits(n)) {
+    // Block-cyclic grid-wide rounds: one CTA per block pair.
+    const size_t bsm = sizeof(double) * 4 * JB_W * size_t(n);
+    ensure_smem_attr(reinterpret_cast<const void*>(k_jacobi_block), c->device, int(bsm));
+    int occ = 0;
+    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_block, JB_THREADS,
+                                                           bsm));
+    const int64_t bpairs = ((n + JB_W - 1) / JB_W + 1) / 2;
+    const int blocks = int(std::max<int64_t>(
+        1, std::min<int64_t>(bpairs, int64_t(c->num_sms) * std::max(occ, 1))));
+    DBuf<unsigned> bar(c, 2);
+    DBuf<unsigned long long> offmax(c, 3);
+    TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 2 * sizeof(unsigned), c->stream));
+    int ni = int(n), ldi = int(lda);
+    double* Aw = work.p();
+    double* Vp = V.p();
+    unsigned* barp = bar.p();
+    unsigned long long* offp = offmax.p();
+    int* errp = c->d_err + 0;
+    int* swp = c->d_err + 3;
+    int msw = c->jacobi_max_sweeps;
+    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp, &trans, &msw};
+    TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_jacobi_block, dim3(blocks),
+                                         dim3(JB_THREADS), args, bsm, c->stream));
+    launch(c, k_jacobi_finish, 1, SD_THREADS, 0, int(n), work.p(), V.p(), U, S, VT,
+           work.p() + int64_t(n) * n, trans);
+    c->launches += 1;  // the cooperative sweep kernel
+    TTG_CHECK_LAUNCH();
+    return;
+  }
   if (mode != 2) {
     // Grid-wide rounds: one CTA per column pair (up to what fits at once).
     int occ = 0;
