@@ -338,7 +338,7 @@ def run_ours(args, dist):
         achieved = per_launch_tflop / (per_launch_ms * 1e-3)
         peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1590.0))
         tr = load_traffic()
-        fused = os.environ.get("TTG_FUSED_MV", "1") != "0"
+        fused = os.environ.get("TTG_FUSED_MV", "0") == "1"
         # ncu measures one fixed shape; its DRAM bytes over the algorithmic
         # bytes of that shape, times the in-solve algorithmic bytes per
         # launch, gives the in-solve traffic (DRAM traffic of this kernel

@@ -35,8 +35,8 @@ struct MixedOp {
                   double(d.ry1) * d.rx1 * d.ra1) +
            4.0 * double(d.ry1) * d.n * d.ry2;
   }
-  // The three GEMM stages from X to y, with the matvec counters: one fused
-  // persistent launch (default) or three GEMM launches (TTG_FUSED_MV=0).
+  // The three GEMM stages from X to y, with the matvec counters: three GEMM
+  // launches (default) or one fused persistent launch (TTG_FUSED_MV=1).
   void stages(Context* c, float* y);
   // Fused single-launch form: tile widths and B-operand maps per stage.
   int fbn[3] = {64, 64, 64};
