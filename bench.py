@@ -344,15 +344,17 @@ def run_ours(args, dist):
         # launch, gives the in-solve traffic (DRAM traffic of this kernel
         # scales with the operand and result sizes).
         traffic = None
-        if tr and tr.get("ratio"):
-            traffic = tr["ratio"] * alg_bytes
+        form = "fused" if fused else "split"
+        ratio = (tr.get("ratio") or {}).get(form) if tr else None
+        if ratio:
+            traffic = ratio * alg_bytes
         roof = {"kernel": ("local matvec, BF16 tcgen05, one persistent launch (k_mv_fused)"
                            if fused else "local matvec, BF16 tcgen05, three GEMM launches"),
                 "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "traffic_basis": (("ncu DRAM bytes / algorithmic bytes = %.3f at %s, times the "
                                    "in-solve algorithmic bytes per launch"
-                                   % (tr["ratio"], tr.get("shape"))) if traffic else None),
+                                   % (ratio, tr.get("shape"))) if traffic else None),
                 "alg_bytes_per_launch": alg_bytes,
                 "hbm_gbs_per_launch": alg_bytes / (per_launch_ms * 1e-3) * 1e-9,
                 "peak_kind": "bf16 sustained, %s" % peaks_kind,
