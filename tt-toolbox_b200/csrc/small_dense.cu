@@ -683,37 +683,40 @@ __global__ void __launch_bounds__(SD_THREADS) k_chol_inv(int n, const double* __
   }
   __syncthreads();
   for (int i = tid; i < n; i += SD_THREADS) L[i + n * i] += s_shift;
-  for (int e = tid; e < n * n; e += SD_THREADS) X[e] = (e % n == e / n) ? 1.0 : 0.0;
+  for (int e = tid; e < n * n; e += SD_THREADS) {
+    const int r = e % n, c = e / n;
+    X[e] = (r == c) ? 1.0 : 0.0;
+    if (r > c) {  // strictly lower parts of the triangular outputs
+      R[e] = 0.0;
+      Rinv[e] = 0.0;
+    }
+  }
   __syncthreads();
-  // Right-looking Cholesky G = L L', with the row operations of the forward
-  // elimination L X = I applied to X = I in the same steps (X = L^{-1} at
-  // the end): step j scales column j of L and row j of X by the pivot, then
-  // removes column j from the trailing lower triangle and row j from the rows
-  // of X below it.  Two barriers per column.
+  // Right-looking Cholesky G = L L', with the forward elimination L X = I
+  // applied to X = I in the same steps (X = L^{-1} at the end).  Step j
+  // reads column j of L and row j of X unscaled (nothing writes them in
+  // that step), removes column j from the trailing lower triangle and row j
+  // from the rows of X below it (with the pivot's reciprocal squared), and
+  // writes row j of R = L' and column j of Rinv = X' scaled: one barrier
+  // per column.
   for (int j = 0; j < n; ++j) {
     const double d = L[j + n * j];
     const double dj = d > 0.0 ? sqrt(d) : 1.0;
     if (tid == 0 && !(d > 0.0)) s_bad = 1;
-    for (int i = j + 1 + tid; i < n; i += SD_THREADS) L[i + n * j] /= dj;
-    for (int cc = tid; cc <= j; cc += SD_THREADS) X[j + n * cc] /= dj;
-    __syncthreads();
+    const double inv = 1.0 / dj, inv2 = inv * inv;
     const int m = n - j - 1;
     for (int e = tid; e < m * m; e += SD_THREADS) {
       const int i = j + 1 + e % m, k = j + 1 + e / m;
-      if (k <= i) L[i + n * k] -= L[i + n * j] * L[k + n * j];
+      if (k <= i) L[i + n * k] -= L[i + n * j] * L[k + n * j] * inv2;
     }
     for (int e = tid; e < m * (j + 1); e += SD_THREADS) {
       const int i = j + 1 + e % m, cc = e / m;
-      X[i + n * cc] -= L[i + n * j] * X[j + n * cc];
+      X[i + n * cc] -= L[i + n * j] * X[j + n * cc] * inv2;
     }
-    if (tid == 0) L[j + n * j] = dj;
+    for (int i = j + tid; i < n; i += SD_THREADS)
+      R[j + int64_t(n) * i] = (i == j) ? dj : L[i + n * j] * inv;
+    for (int cc = tid; cc <= j; cc += SD_THREADS) Rinv[cc + int64_t(n) * j] = X[j + n * cc] * inv;
     __syncthreads();
-  }
-  // R = L', Rinv = X' (both upper triangular)
-  for (int e = tid; e < n * n; e += SD_THREADS) {
-    const int r = e % n, c = e / n;
-    R[e] = r <= c ? L[c + n * r] : 0.0;
-    Rinv[e] = r <= c ? X[c + n * r] : 0.0;
   }
   if (tid == 0 && s_bad) atomicOr(err, 1);
 }
