@@ -18,10 +18,13 @@ def test_dense_svd_matches_lapack(ctx, m, n):
     U, s, VT = ttgpu.dense_svd(A, ctx=ctx)
     s_ref = np.linalg.svd(A, compute_uv=False)
     k = min(m, n)
-    assert np.allclose(s, s_ref, rtol=0, atol=1e-13 * s_ref[0])
-    assert np.linalg.norm(U * s @ VT - A) / np.linalg.norm(A) < 1e-13
-    assert np.linalg.norm(U.T @ U - np.eye(k)) < 1e-12
-    assert np.linalg.norm(VT @ VT.T - np.eye(k)) < 1e-12
+    # backward error of a one-sided Jacobi SVD grows like k * eps: 1e-13 up
+    # to k = 256, 2.4e-13 at k = 600
+    tol = max(1e-13, 4e-16 * k)
+    assert np.allclose(s, s_ref, rtol=0, atol=tol * s_ref[0])
+    assert np.linalg.norm(U * s @ VT - A) / np.linalg.norm(A) < tol
+    assert np.linalg.norm(U.T @ U - np.eye(k)) < 10 * tol
+    assert np.linalg.norm(VT @ VT.T - np.eye(k)) < 10 * tol
     assert np.all(np.diff(s) <= 0)
 
 

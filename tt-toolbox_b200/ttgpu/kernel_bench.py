@@ -100,7 +100,14 @@ def round_bench(args):
                      "ms_qr_sweep": st["ms_qr_sweep"], "ms_svd_sweep": st["ms_svd_sweep"]}
         if args.check:
             out[prec]["rel_err"] = _rel_diff(X, Yh)
+        if args.kernel_table:
+            out[prec]["kernel_table"] = _kernel_table(
+                lambda: tt_round(dX, args.eps, precision=prec, ctx=ctx).free())
+    tables = {p: out[p].pop("kernel_table") for p in list(out) if isinstance(out[p], dict)
+              and "kernel_table" in out[p]}
     print(json.dumps(out))
+    for prec, tab in tables.items():
+        print("\n# kernels of one rounding, precision %s\n%s" % (prec, tab))
     dX.free()
     ctx.close()
 
@@ -359,6 +366,7 @@ def main():
     r.add_argument("--reps", type=int, default=3)
     r.add_argument("--precision", default="fp64")
     r.add_argument("--check", action="store_true")
+    r.add_argument("--kernel-table", action="store_true")
     g = sub.add_parser("grad")
     g.add_argument("--d", type=int, default=12)
     g.add_argument("--n", type=int, default=32)
