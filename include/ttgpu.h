@@ -58,8 +58,12 @@ int ttg_context_sync(ttg_context ctx);
  * converging makes ttg_dense_svd and ttg_amen_solve fail with
  * TTG_ERR_NOCONV (MATLAB's svd errors there, which aborts amen_solve2), and
  * makes ttg_round take the fallback SVD of the core, as round.m:64-74 falls
- * back to svds. */
-enum { TTG_OPT_JACOBI_MAX_SWEEPS = 1 };
+ * back to svds.  TTG_OPT_GROUP_SMS (default 0): the SM count each solve of a
+ * grouped batch sizes its own grids with (cooperative Krylov grids, split-K
+ * slices, grid-stride loops); 0 = twice the device's SMs divided among the
+ * solves in flight, re-evaluated at every flush; the device's SM count gives
+ * every solve the launch configurations of a solve run alone. */
+enum { TTG_OPT_JACOBI_MAX_SWEEPS = 1, TTG_OPT_GROUP_SMS = 2 };
 int ttg_context_set_option(ttg_context ctx, int32_t key, int64_t value);
 
 /* Self-test of the bounded device waits.  No counterpart in the reference.
@@ -348,6 +352,34 @@ int ttg_amen_solve_batch(ttg_context ctx, int64_t count, const ttg_tt* A, const 
                          const double* tol, const ttg_amen_opts* opts, const ttg_tt* x0,
                          const ttg_tt* z0, int32_t workers, ttg_tt* x_out,
                          ttg_amen_stats* stats, int32_t* status);
+
+/* Counters of a grouped batch (ttg_amen_solve_grouped). */
+typedef struct {
+  int64_t flushes;          /* times every solve in flight waited for the device */
+  int64_t launches;         /* launches and stream operations issued */
+  int64_t records;          /* launches and stream operations the solves recorded */
+  int64_t grouped_records;  /* recorded launches issued inside grouped launches */
+  double ms_plan;           /* host time merging records and writing argument packs */
+  double ms_issue_wait;     /* host time issuing and waiting for the device */
+  double ms_total;          /* wall time of the call */
+} ttg_group_stats;
+
+/* Grouped batch: the same solves as ttg_amen_solve_batch (same arguments,
+ * results and per-system status), advanced together on the context's
+ * stream.  Every system in flight runs on a host thread of its own whose
+ * stream work is recorded; whenever all of them wait for the device, the
+ * recorded launches of all systems are merged kernel by kernel into grouped
+ * launches (one launch runs a kernel's CTAs for many systems, each system
+ * with its own grid and arguments) and issued with one copy of their
+ * arguments.  Each system's kernels run in its own order with its own
+ * arguments, so every system gets the result of its own sequential solve.
+ * `width` systems are in flight at once (<= 0: all of them, at most 1024);
+ * group_stats (nullable) receives the counters above. */
+int ttg_amen_solve_grouped(ttg_context ctx, int64_t count, const ttg_tt* A, const ttg_tt* y,
+                           const double* tol, const ttg_amen_opts* opts, const ttg_tt* x0,
+                           const ttg_tt* z0, int32_t width, ttg_tt* x_out,
+                           ttg_amen_stats* stats, int32_t* status,
+                           ttg_group_stats* group_stats);
 
 /* ---- Gradients with respect to every core (FP64) ----------------------
  * No counterpart in the reference: TT-Toolbox has no derivative code.  The

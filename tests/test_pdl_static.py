@@ -5,7 +5,9 @@ predecessor on the stream is still running; it is only correct if its first
 statement is ``pdl_begin()`` (``griddepcontrol.wait`` before any memory
 access, and before any early return).  This test reads the CUDA sources and
 checks that rule for every kernel launched that way, and that no such kernel
-is also launched with the plain ``<<<...>>>`` syntax elsewhere.
+is also launched with the plain ``<<<...>>>`` syntax elsewhere.  Kernels
+written as a ``TTG_BODY`` (csrc/group.cuh) count with their body; cooperative
+ones (``TTG_COOP_KERNEL``) are launched without the attribute and are exempt.
 """
 import pathlib
 import re
@@ -24,9 +26,13 @@ def test_every_pdl_launched_kernel_waits_first():
         names.update(re.findall(r"\blaunch\(c,\s*([A-Za-z_][A-Za-z_0-9]*)", text))
     assert names, "no launch() call sites found"
     allsrc = "\n".join(src.values())
+    # cooperative kernels are launched without the PDL attribute
+    coop = set(re.findall(r"TTG_COOP_KERNEL\((\w+)", allsrc))
     bad = []
-    for name in sorted(names):
+    for name in sorted(names - coop):
         m = re.search(r"__global__ void[^;{]*?\b%s\s*\([^{]*\{\n(.*)\n" % re.escape(name), allsrc)
+        if m is None:  # a TTG_BODY kernel (group.cuh)
+            m = re.search(r"TTG_BODY\(%s\)\s*\([^{]*\{\n(.*)\n" % re.escape(name), allsrc)
         if m is None or m.group(1).strip() != "pdl_begin();":
             bad.append((name, None if m is None else m.group(1).strip()))
     assert not bad, "kernels launched with launch() that do not start with pdl_begin(): %r" % bad

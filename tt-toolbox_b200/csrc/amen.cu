@@ -169,6 +169,16 @@ void dense_residual_dev(Context* c, int64_t N, const double* B, const double* x,
   diffnrm_f64(c, N, tmp, rhs, out, true);
 }
 
+// Free a TT handle whose core the context's recorded work may still use.
+void release_tt(Context* c, ttg_tt_s* t) {
+  if (c->rec) {
+    rec_free(c->rec, t->core);
+    delete t;
+  } else {
+    ttg_tt_free(t);
+  }
+}
+
 // Normalise in place by the Frobenius norm, the norm (1 if zero) into *slot
 // (compute_next_Phi with nargout > 1, amen_solve2.m:907-914).
 void normalize_dev(Context* c, int64_t n, double* x, double* slot) {
@@ -239,10 +249,7 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   TTG_REQUIRE(o.nswp >= 1 && o.local_restart >= 1 && o.local_iters >= 1 && o.rmax >= 1 &&
                   o.kickrank >= 0,
               "invalid options");
-  require_finite(Ah, "A");
-  require_finite(yh, "y");
-  require_finite(x0h, "x0");
-  require_finite(z0h, "z0");
+  require_finite(c, {{Ah, "A"}, {yh, "y"}, {x0h, "x0"}, {z0h, "z0"}});
   const std::vector<int64_t> n = yh->n;
   const int64_t nswp = o.nswp, rmax = o.rmax, max_full_size = o.max_full_size;
   const int64_t kickrank = o.kickrank;
@@ -251,22 +258,27 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   const bool use_z = kickrank > 0;                                      // :246
   const double real_tol = (tol / std::sqrt(double(d))) / resid_damp;   // :466
 
-  cudaEvent_t e0, e1;
-  TTG_CUDA(cudaEventCreate(&e0));
-  TTG_CUDA(cudaEventCreate(&e1));
-  TTG_CUDA(cudaEventRecord(e0, c->stream));
+  // Device time of the solve from an event pair; a solve of a grouped batch
+  // (recorded stream work) takes the host clock instead.
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const auto host_t0 = std::chrono::steady_clock::now();
+  if (!c->rec) {
+    TTG_CUDA(cudaEventCreate(&e0));
+    TTG_CUDA(cudaEventCreate(&e1));
+    TTG_CUDA(cudaEventRecord(e0, c->stream));
+  }
   const int64_t mv0 = c->matvecs, fl0 = c->matvec_flops, la0 = c->launches;
   const double flk0[2] = {c->mv_flops[0], c->mv_flops[1]};
   const double byl0 = c->mv_bytes_lp;
   const int64_t mvk0[2] = {c->mv_count[0], c->mv_count[1]};
   c->ev_collect();
   const double msk0[2] = {c->mv_ms[0], c->mv_ms[1]};
-  c->time_matvec = o.timing != 0;
+  c->time_matvec = o.timing != 0 && !c->rec;
   struct TimingOff {
     Context* c;
     ~TimingOff() { c->time_matvec = false; }
   } timing_off{c};
-  TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 8 * sizeof(int), c->stream));
+  memset_async(c, c->d_err, 0, 8 * sizeof(int));
 
   PhaseProf prof;
   prof.start(c);
@@ -298,8 +310,8 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
       copy_f64(c, sz, z0h->core + z0h->ps[k], crz[k].p());
     }
   }
-  if (x0own) ttg_tt_free(x0own);
-  if (z0own) ttg_tt_free(z0own);
+  if (x0own) release_tt(c, x0own);
+  if (z0own) release_tt(c, z0own);
   auto cry = [&](int64_t k) { return yh->core + yh->ps[k]; };
   auto crA = [&](int64_t k) { return Ah->core + Ah->ps[k]; };
 
@@ -759,25 +771,31 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   out->core = static_cast<double*>(out_ctx->alloc->get(sizeof(double) * out->numel));
   for (int64_t k = 0; k < d; ++k)
     axpby_f64(c, out->ps[k + 1] - out->ps[k], nx, crx[k].p(), 0.0, out->core + out->ps[k]);
-  TTG_CUDA(cudaEventRecord(e1, c->stream));
-  TTG_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (!c->rec) {
+    TTG_CUDA(cudaEventRecord(e1, c->stream));
+    TTG_CUDA(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
   int herr[8];
-  TTG_CUDA(cudaMemcpy(herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
+  read_device(c, herr, c->d_err, sizeof(herr));
+  if (c->rec)
+    ms = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                         host_t0)
+                   .count());
   if (herr[0] || herr[1] || herr[2]) {
-    ttg_tt_free(out);
+    release_tt(c, out);
     fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out (codes %d %d %d)", herr[0],
          herr[1], herr[2]);
   }
   if (herr[4]) {
-    ttg_tt_free(out);
+    release_tt(c, out);
     fail(TTG_ERR_SOLVER, "a device factorization reported a non-zero LAPACK info");
   }
   if (herr[3]) {  // MATLAB's svd errors when it does not converge (amen_solve2.m:533)
-    ttg_tt_free(out);
+    release_tt(c, out);
     fail(TTG_ERR_NOCONV, "a Jacobi SVD reached its sweep limit (%d sweeps)",
          c->jacobi_max_sweeps);
   }

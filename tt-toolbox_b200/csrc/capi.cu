@@ -4,6 +4,7 @@
 #include <thread>
 
 #include "amen.h"
+#include "group.cuh"
 #include "grad.h"
 #include "linalg.h"
 #include "round.h"
@@ -29,6 +30,25 @@ void clear_error_slots(ttg::Context* c) {
 
 void grad_value_out(ttg::Context* c, const double* dval, double* value) {
   if (value) ttg::read_scalars(c, dval, value, 1);
+}
+
+// Checks shared by the batched entries; clears the outputs.
+void check_batch(Context* owner, int64_t count, const ttg_tt* A, const ttg_tt* y,
+                 const double* tol, const ttg_tt* x0, const ttg_tt* z0, ttg_tt* x_out,
+                 ttg_amen_stats* stats, int32_t* status) {
+  TTG_REQUIRE(A && y && tol, "NULL argument");
+  for (int64_t i = 0; i < count; ++i) {
+    x_out[i] = nullptr;
+    if (status) status[i] = TTG_OK;
+    if (stats) stats[i] = ttg_amen_stats{};
+    TTG_REQUIRE(A[i] && y[i], "system %lld: NULL handle", (long long)i);
+    TTG_REQUIRE(A[i]->ctx == owner && y[i]->ctx == owner,
+                "system %lld: handles belong to another context", (long long)i);
+    if (x0 && x0[i]) TTG_REQUIRE(x0[i]->ctx == owner, "system %lld: x0 context", (long long)i);
+    if (z0 && z0[i]) TTG_REQUIRE(z0[i]->ctx == owner, "system %lld: z0 context", (long long)i);
+    TTG_REQUIRE(std::isfinite(tol[i]) && tol[i] > 0, "system %lld: tol must be > 0",
+                (long long)i);
+  }
 }
 
 }  // namespace
@@ -64,6 +84,11 @@ int ttg_context_set_option(ttg_context ctx, int32_t key, int64_t value) {
       TTG_REQUIRE(value >= 1 && value <= 1000, "Jacobi sweep limit %lld out of [1, 1000]",
                   (long long)value);
       ctx->c.jacobi_max_sweeps = int(value);
+      break;
+    case TTG_OPT_GROUP_SMS:
+      TTG_REQUIRE(value >= 0 && value <= 4096, "SM count %lld out of [0, 4096]",
+                  (long long)value);
+      ctx->c.group_sms = int(value);
       break;
     default:
       fail(TTG_ERR_INVALID, "unknown context option %d", int(key));
@@ -283,6 +308,55 @@ int ttg_grad_sampled(ttg_tt x, int64_t nsamples, const int32_t* idx, const doubl
   TTG_API_END
 }
 
+
+int ttg_amen_solve_grouped(ttg_context ctx, int64_t count, const ttg_tt* A, const ttg_tt* y,
+                           const double* tol, const ttg_amen_opts* opts, const ttg_tt* x0,
+                           const ttg_tt* z0, int32_t width, ttg_tt* x_out,
+                           ttg_amen_stats* stats, int32_t* status,
+                           ttg_group_stats* group_stats) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(ctx && x_out, "NULL argument");
+  TTG_REQUIRE(count >= 0, "count must be >= 0");
+  if (group_stats) *group_stats = ttg_group_stats{};
+  if (count == 0) return TTG_OK;
+  Context* owner = &ctx->c;
+  TTG_CUDA(cudaSetDevice(owner->device));
+  check_batch(owner, count, A, y, tol, x0, z0, x_out, stats, status);
+  int64_t w = width > 0 ? width : count;
+  w = std::max<int64_t>(1, std::min<int64_t>({w, count, 1024}));
+  ttg_amen_opts dflt;
+  ttg_amen_opts_default(&dflt);
+  std::mutex emu;
+  int64_t first_bad = -1;
+  int first_code = TTG_OK;
+  std::string first_msg;
+  auto record = [&](int64_t i, int code, const char* msg) {
+    if (status) status[i] = code;
+    std::lock_guard<std::mutex> lock(emu);
+    if (first_bad < 0 || i < first_bad) {
+      first_bad = i;
+      first_code = code;
+      first_msg = msg;
+    }
+  };
+  auto body = [&](int64_t i, Context* c) {
+    try {
+      ttg_amen_opts o = opts ? opts[i] : dflt;
+      o.timing = 0;  // no event timing inside a grouped batch
+      x_out[i] = amen_solve(c, A[i], y[i], tol[i], o, x0 ? x0[i] : nullptr,
+                            z0 ? z0[i] : nullptr, stats ? &stats[i] : nullptr, owner);
+    } catch (const Error& e) {
+      record(i, e.code, e.msg.c_str());
+    } catch (const std::exception& e) {
+      record(i, TTG_ERR_INVALID, e.what());
+    }
+  };
+  run_grouped(owner, int(w), count, body, group_stats);
+  if (first_bad >= 0)
+    fail(first_code, "system %lld: %s", (long long)first_bad, first_msg.c_str());
+  TTG_API_END
+}
+
 int ttg_amen_solve_batch(ttg_context ctx, int64_t count, const ttg_tt* A, const ttg_tt* y,
                          const double* tol, const ttg_amen_opts* opts, const ttg_tt* x0,
                          const ttg_tt* z0, int32_t workers, ttg_tt* x_out,
@@ -291,21 +365,9 @@ int ttg_amen_solve_batch(ttg_context ctx, int64_t count, const ttg_tt* A, const 
   TTG_REQUIRE(ctx && x_out, "NULL argument");
   TTG_REQUIRE(count >= 0, "count must be >= 0");
   if (count == 0) return TTG_OK;
-  TTG_REQUIRE(A && y && tol, "NULL argument");
   Context* owner = &ctx->c;
   TTG_CUDA(cudaSetDevice(owner->device));
-  for (int64_t i = 0; i < count; ++i) {
-    x_out[i] = nullptr;
-    if (status) status[i] = TTG_OK;
-    if (stats) stats[i] = ttg_amen_stats{};
-    TTG_REQUIRE(A[i] && y[i], "system %lld: NULL handle", (long long)i);
-    TTG_REQUIRE(A[i]->ctx == owner && y[i]->ctx == owner,
-                "system %lld: handles belong to another context", (long long)i);
-    if (x0 && x0[i]) TTG_REQUIRE(x0[i]->ctx == owner, "system %lld: x0 context", (long long)i);
-    if (z0 && z0[i]) TTG_REQUIRE(z0[i]->ctx == owner, "system %lld: z0 context", (long long)i);
-    TTG_REQUIRE(std::isfinite(tol[i]) && tol[i] > 0, "system %lld: tol must be > 0",
-                (long long)i);
-  }
+  check_batch(owner, count, A, y, tol, x0, z0, x_out, stats, status);
   int64_t nw = workers > 0 ? workers : 8;
   nw = std::max<int64_t>(1, std::min<int64_t>({nw, count, 64}));
   // Inputs uploaded on the owner's stream are complete before other streams

@@ -85,7 +85,13 @@ void Allocator::put(void* p) {
 
 void set_last_error(const char* msg) { g_last_error = msg; }
 
-void sync(Context* c) { TTG_CUDA(cudaStreamSynchronize(c->stream)); }
+void sync(Context* c) {
+  if (c->rec) {
+    rec_wait(c->rec);
+    return;
+  }
+  TTG_CUDA(cudaStreamSynchronize(c->stream));
+}
 
 void context_init(Context& c, int device) {
   c.device = device;
@@ -139,11 +145,47 @@ void ensure_smem_attr(const void* func, int device, int bytes) {
   done[{func, device}] = bytes;
 }
 
+void read_device(Context* c, void* h, const void* d, size_t bytes) {
+  TTG_REQUIRE(bytes <= 4096 * sizeof(double), "read_device: %zu bytes", bytes);
+  double* stage = c->h_scal;
+  if (c->rec) {
+    rec_read(c, 0, d, bytes);
+    rec_wait(c->rec);
+  } else {
+    TTG_CUDA(cudaMemcpyAsync(stage, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+    TTG_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  memcpy(h, stage, bytes);
+}
+
 void read_scalars(Context* c, const double* d, double* h, int count) {
-  TTG_CUDA(cudaMemcpyAsync(c->h_scal, d, sizeof(double) * count, cudaMemcpyDeviceToHost,
-                           c->stream));
-  TTG_CUDA(cudaStreamSynchronize(c->stream));
-  memcpy(h, c->h_scal, sizeof(double) * count);
+  read_device(c, h, d, sizeof(double) * count);
+}
+
+void memset_async(Context* c, void* p, int value, size_t bytes) {
+  if (c->rec) {
+    rec_memset(c, p, value, bytes);
+    return;
+  }
+  TTG_CUDA(cudaMemsetAsync(p, value, bytes, c->stream));
+}
+
+void copy_async(Context* c, void* dst, const void* src, size_t bytes) {
+  if (c->rec) {
+    rec_op(c->rec, [dst, src, bytes](cudaStream_t s, cusolverDnHandle_t) {
+      TTG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    });
+    return;
+  }
+  TTG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+}
+
+void solver_call(Context* c, const StreamOp& op) {
+  if (c->rec) {
+    rec_op(c->rec, op);
+    return;
+  }
+  op(c->stream, c->solver);
 }
 
 }  // namespace ttg

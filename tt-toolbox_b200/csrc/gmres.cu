@@ -16,6 +16,7 @@
 #include <cstring>
 
 #include "gmres.h"
+#include "group.cuh"
 
 namespace ttg {
 
@@ -66,7 +67,8 @@ __device__ double block_sum_all(double v) {
   return sh[32];
 }
 
-__device__ void grid_barrier(unsigned* bar, int* err, long long limit = BAR_SPIN_LIMIT) {
+__device__ void grid_barrier(TTG_BLOCK, unsigned* bar, int* err,
+                             long long limit = BAR_SPIN_LIMIT) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = bar + 1;
@@ -96,11 +98,11 @@ __device__ void grid_barrier(unsigned* bar, int* err, long long limit = BAR_SPIN
 
 // Grid-wide deterministic sum; every thread of every block gets the result.
 // Partial buffers alternate so one barrier per reduction suffices.
-__device__ double grid_sum(double v, const HhArgs& a, unsigned& parity) {
+__device__ double grid_sum(TTG_BLOCK, double v, const HhArgs& a, unsigned& parity) {
   v = block_sum_all(v);
   double* part = a.part + (parity & 1u) * gridDim.x;
   if (threadIdx.x == 0) part[blockIdx.x] = v;
-  grid_barrier(a.bar, a.err);
+  grid_barrier(blockIdx, gridDim, a.bar, a.err);
   double s = 0.0;
   for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(part + i);
   s = block_sum_all(s);
@@ -113,7 +115,7 @@ __device__ double grid_sum(double v, const HhArgs& a, unsigned& parity) {
        idx += int64_t(gridDim.x) * blockDim.x)
 
 // w = rhs - w2 ; U_0 = Householder vector of w ; tau_0 = -beta  (:376-392)
-__global__ void __launch_bounds__(HH_THREADS) k_hh_init(HhArgs a, int it) {
+TTG_BODY(k_hh_init)(TTG_BLOCK, HhArgs a, int it) {
   unsigned parity = 0;
   const int64_t sz = a.sz;
   double s = 0.0;
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_init(HhArgs a, int it) {
     a.w[i] = v;
     s += v * v;
   }
-  const double nrmr = sqrt(grid_sum(s, a, parity));
+  const double nrmr = sqrt(grid_sum(blockIdx, gridDim, s, a, parity));
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (it == 0) a.scal[0] = nrmr;
     a.scal[2] = nrmr;
@@ -142,9 +144,10 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_init(HhArgs a, int it) {
     if (threadIdx.x == 0) a.tau[0] = -beta;
   }
 }
+TTG_COOP_KERNEL(k_hh_init, HH_THREADS);
 
 // v_j = P_0 ... P_{j-1} (P_j e_j), normalised, into w  (:396-406)
-__global__ void __launch_bounds__(HH_THREADS) k_hh_build(HhArgs a, int64_t j) {
+TTG_BODY(k_hh_build)(TTG_BLOCK, HhArgs a, int64_t j) {
   if (*(volatile int*)a.stop) return;  // queued after convergence
   unsigned parity = 0;
   const int64_t sz = a.sz;
@@ -155,17 +158,18 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_build(HhArgs a, int64_t j) {
     const double* Ur = a.U + r * sz;
     double s = 0.0;
     GRID_LOOP(i, sz) s += Ur[i] * a.w[i];
-    const double dot = grid_sum(s, a, parity);
+    const double dot = grid_sum(blockIdx, gridDim, s, a, parity);
     GRID_LOOP(i, sz) a.w[i] -= 2.0 * dot * Ur[i];
   }
   double s = 0.0;
   GRID_LOOP(i, sz) s += a.w[i] * a.w[i];
-  const double inv = 1.0 / sqrt(grid_sum(s, a, parity));
+  const double inv = 1.0 / sqrt(grid_sum(blockIdx, gridDim, s, a, parity));
   GRID_LOOP(i, sz) a.w[i] *= inv;
 }
+TTG_COOP_KERNEL(k_hh_build, HH_THREADS);
 
 // w2 = P_j ... P_0 w2 ; new reflector U_{j+1} ; Givens ; R(:,j) ; residual (:421-473)
-__global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
+TTG_BODY(k_hh_tail)(TTG_BLOCK, HhArgs a, int64_t j) {
   if (*(volatile int*)a.stop) return;  // queued after convergence
   unsigned parity = 0;
   const int64_t sz = a.sz;
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
     const double* Ur = a.U + r * sz;
     double s = 0.0;
     GRID_LOOP(i, sz) s += Ur[i] * w[i];
-    const double dot = grid_sum(s, a, parity);
+    const double dot = grid_sum(blockIdx, gridDim, s, a, parity);
     GRID_LOOP(i, sz) w[i] -= 2.0 * dot * Ur[i];
   }
   if (j < sz - 1) {
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
       if (i > j) s += w[i] * w[i];
       if (i == j + 1) a.scal[4] = w[i];
     }
-    double alpha = sqrt(grid_sum(s, a, parity));
+    double alpha = sqrt(grid_sum(blockIdx, gridDim, s, a, parity));
     const double wj1 = __ldcg(a.scal + 4);
     double* Un = a.U + (j + 1) * sz;
     if (alpha != 0.0) {
@@ -209,7 +213,7 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
       GRID_LOOP(i, sz) Un[i] = (i <= j) ? 0.0 : w[i];
     }
   }
-  grid_barrier(a.bar, a.err);
+  grid_barrier(blockIdx, gridDim, a.bar, a.err);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     // Givens rotations to the top of w (:445-449)
     for (int64_t i = 0; i < j; ++i) {
@@ -239,9 +243,10 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_tail(HhArgs a, int64_t j) {
     }
   }
 }
+TTG_COOP_KERNEL(k_hh_tail, HH_THREADS);
 
 // Triangular solve + correction sol += P_0..P_j (sum y_i e_i)  (:487-507)
-__global__ void __launch_bounds__(HH_THREADS) k_hh_correct(HhArgs a, int64_t j, int64_t ni) {
+TTG_BODY(k_hh_correct)(TTG_BLOCK, HhArgs a, int64_t j, int64_t ni) {
   extern __shared__ double y[];
   unsigned parity = 0;
   const int64_t sz = a.sz;
@@ -264,11 +269,12 @@ __global__ void __launch_bounds__(HH_THREADS) k_hh_correct(HhArgs a, int64_t j, 
       if (i == r) a.w[i] += y[r];
       s += Ur[i] * a.w[i];
     }
-    const double dot = grid_sum(s, a, parity);
+    const double dot = grid_sum(blockIdx, gridDim, s, a, parity);
     GRID_LOOP(i, sz) a.w[i] -= 2.0 * dot * Ur[i];
   }
   GRID_LOOP(i, sz) a.sol[i] += a.w[i];
 }
+TTG_COOP_KERNEL(k_hh_correct, HH_THREADS);
 
 int coop_blocks(Context* c, const void* kernel, size_t smem, int64_t sz) {
   int occ = 0;
@@ -281,11 +287,6 @@ int coop_blocks(Context* c, const void* kernel, size_t smem, int64_t sz) {
   return int(want);
 }
 
-void launch_coop(Context* c, const void* kernel, int blocks, size_t smem, void** args) {
-  TTG_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(HH_THREADS), args, smem,
-                                       c->stream));
-  c->launches += 1;
-}
 
 }  // namespace
 
@@ -297,14 +298,14 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
   DBuf<double> U(c, size_t(sz) * (nrestart + 1)), w(c, sz), w2(c, sz);
   DBuf<double> small(c, (nrestart + 1) + 2 * nrestart + nrestart * nrestart + 8);
   const int blocks = std::min(
-      std::min(coop_blocks(c, (const void*)k_hh_init, 0, sz), coop_blocks(c, (const void*)k_hh_build, 0, sz)),
-      std::min(coop_blocks(c, (const void*)k_hh_tail, 0, sz),
-               coop_blocks(c, (const void*)k_hh_correct, sizeof(double) * nrestart, sz)));
+      std::min(coop_blocks(c, k_hh_init.fn(), 0, sz), coop_blocks(c, k_hh_build.fn(), 0, sz)),
+      std::min(coop_blocks(c, k_hh_tail.fn(), 0, sz),
+               coop_blocks(c, k_hh_correct.fn(), sizeof(double) * nrestart, sz)));
   DBuf<double> part(c, 2 * blocks);
   DBuf<unsigned> bar(c, 4);
   DBuf<int> stop(c, 4);
-  TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 4 * sizeof(unsigned), c->stream));
-  TTG_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+  memset_async(c, bar.p(), 0, 4 * sizeof(unsigned));
+  memset_async(c, c->d_err, 0, sizeof(int));
 
   HhArgs a;
   a.sz = sz;
@@ -335,22 +336,28 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
     double curres;
   };
   auto probe = [&](Probe& p) {
-    TTG_CUDA(cudaMemcpyAsync(c->h_scal, stop.p(), 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                             c->stream));
-    TTG_CUDA(cudaMemcpyAsync(c->h_scal + 1, a.scal + 1, sizeof(double), cudaMemcpyDeviceToHost,
-                             c->stream));
-    sync(c);
-    memcpy(p.flag, c->h_scal, 2 * sizeof(int));
-    p.curres = c->h_scal[1];
+    double* stage = c->h_scal;
+    const int* sp = stop.p();
+    const double* cp = a.scal + 1;
+    if (c->rec) {
+      rec_read(c, 0, sp, 2 * sizeof(int));
+      rec_read(c, sizeof(double), cp, sizeof(double));
+      rec_wait(c->rec);
+    } else {
+      TTG_CUDA(cudaMemcpyAsync(stage, sp, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      TTG_CUDA(
+          cudaMemcpyAsync(stage + 1, cp, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      sync(c);
+    }
+    memcpy(p.flag, stage, 2 * sizeof(int));
+    p.curres = stage[1];
   };
   double curres = INFINITY;
   for (int64_t it = 0; it < niters; ++it) {
     apply(sol, w2.p());
     res.matvecs++;
-    int itv = int(it);
-    void* args_init[] = {&a, &itv};
-    launch_coop(c, (const void*)k_hh_init, blocks, 0, args_init);
-    TTG_CUDA(cudaMemsetAsync(stop.p(), 0, 2 * sizeof(int), c->stream));
+    launch(c, k_hh_init, blocks, HH_THREADS, 0, a, int(it));
+    memset_async(c, stop.p(), 0, 2 * sizeof(int));
     double hs[4];
     read_scalars(c, a.scal, hs, 4);
     if (hs[3] != 0.0) {  // exact solution: nothing to correct
@@ -363,12 +370,9 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
     while (j < nrestart) {
       const int64_t jend = std::min(nrestart, j + chunk);
       for (int64_t jj = j; jj < jend; ++jj) {
-        int64_t jv = jj;
-        void* args_b[] = {&a, &jv};
-        launch_coop(c, (const void*)k_hh_build, blocks, 0, args_b);
+        launch(c, k_hh_build, blocks, HH_THREADS, 0, a, jj);
         apply(w.p(), w2.p());
-        void* args_t[] = {&a, &jv};
-        launch_coop(c, (const void*)k_hh_tail, blocks, 0, args_t);
+        launch(c, k_hh_tail, blocks, HH_THREADS, 0, a, jj);
       }
       Probe p;
       probe(p);
@@ -392,8 +396,7 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
     } else {
       ni = j + 1;
     }
-    void* args_c[] = {&a, &j, &ni};
-    launch_coop(c, (const void*)k_hh_correct, blocks, sizeof(double) * nrestart, args_c);
+    launch(c, k_hh_correct, blocks, HH_THREADS, sizeof(double) * nrestart, a, j, ni);
     if (curres < tol) break;
   }
   res.relres = curres;
@@ -404,7 +407,7 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
 // waits until its (small) poll limit runs out and raises *flag.
 __global__ void k_selftest_grid_barrier(unsigned* bar, int* flag, long long limit) {
   if (blockIdx.x != 0) return;
-  grid_barrier(bar, flag, limit);
+  grid_barrier(blockIdx, gridDim, bar, flag, limit);
 }
 
 void selftest_wait_gmres(Context* c, int* flag, long long limit) {

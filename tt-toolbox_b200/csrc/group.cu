@@ -1,0 +1,561 @@
+// Executor of grouped batches: many independent solves advance together on
+// one stream, and launches of the same kernel are merged into one launch.
+//
+// Each solve runs the ordinary host code on a host thread of its own with a
+// recording context (Context::rec): launches, memsets, copies and library
+// calls are appended to the solve's record instead of being issued, and
+// device blocks it frees go back to the allocator only after the records
+// that may use them are issued.  A solve that needs a device result (a host
+// read or a synchronisation) blocks.  Once every running solve is blocked,
+// the executor "flushes": it merges the records of all solves, issues them
+// on the stream and waits for the device, then wakes the solves, which go on
+// recording from where they stopped.
+//
+// Merging keeps each solve's own order.  The executor repeatedly looks at
+// the first unissued record of every solve: stream operations are issued
+// one by one; among the launches of TTG_KERNEL kernels it picks the kernel
+// (and block shape) at the head of the most solves and issues one grouped
+// launch over all of them (group.cuh).  Records of different solves touch
+// disjoint memory, so any interleaving that keeps every solve's order gives
+// each solve the results of its own sequential run.  The argument packs,
+// launch headers and CTA maps of a flush are written to one pinned staging
+// buffer and copied to the device with a single copy before the launches.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "group.cuh"
+
+namespace ttg {
+
+namespace {
+
+struct RecOp {
+  const GroupInfo* info;  // null: a stream operation (Recorder::closures[closure])
+  dim3 grid, block;
+  uint32_t smem;
+  uint32_t pack_off;      // argument pack in Recorder::arena
+  uint32_t closure;
+};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// TTG_GROUP=0 issues every recorded launch on its own (plain kernels, in the
+// merged order): the grouped launches can then be compared with it.
+// TTG_GROUP_COOP=0 does so for the cooperative kernels only.
+bool env_on(const char* name) {
+  const char* e = getenv(name);
+  return !(e && e[0] == '0');
+}
+
+}  // namespace
+
+// Stream operations of a recording context, as grouped kernels: a memset,
+// and a read of device bytes into the context's mapped pinned buffer (the
+// host sees the bytes once the flush has synchronised the stream).
+TTG_BODY(k_fill_bytes)(TTG_BLOCK, unsigned char* p, int value, int64_t bytes) {
+  pdl_begin();
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+    const unsigned char b = static_cast<unsigned char>(value);
+    const unsigned w = b * 0x01010101u;
+    const uint4 v = make_uint4(w, w, w, w);
+    const int64_t n16 = bytes / 16;
+    for (int64_t i = t0; i < n16; i += stride) reinterpret_cast<uint4*>(p)[i] = v;
+    for (int64_t i = n16 * 16 + t0; i < bytes; i += stride) p[i] = b;
+  } else {
+    for (int64_t i = t0; i < bytes; i += stride) p[i] = static_cast<unsigned char>(value);
+  }
+}
+TTG_KERNEL(k_fill_bytes, 0);
+
+TTG_BODY(k_read_host)(TTG_BLOCK, const unsigned char* src, unsigned char* dst, int64_t bytes) {
+  pdl_begin();
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < bytes;
+       i += int64_t(gridDim.x) * blockDim.x)
+    dst[i] = src[i];
+  __threadfence_system();
+}
+TTG_KERNEL(k_read_host, 0);
+
+class Executor;
+
+struct Recorder {
+  Executor* ex = nullptr;
+  std::vector<RecOp> ops;
+  std::vector<StreamOp> closures;
+  std::vector<char> arena;
+  std::vector<void*> frees;
+};
+
+class Executor {
+ public:
+  Executor(Context* owner, int width);
+  ~Executor();
+  void run(int64_t count, const std::function<void(int64_t, Context*)>& body);
+  void wait(Recorder* r);
+  ttg_group_stats st{};
+
+ private:
+  void flush();
+  int coop_capacity(const GroupInfo* info, dim3 block, size_t smem);
+  void ensure_stage(size_t bytes);
+
+  Context* owner_;
+  int width_;
+  std::vector<std::unique_ptr<Recorder>> recs_;
+  std::vector<std::unique_ptr<Context>> ctxs_;
+  double* h_slab_ = nullptr;
+  int* d_err_slab_ = nullptr;
+  unsigned* d_tile_slab_ = nullptr;
+  char* h_stage_ = nullptr;
+  char* d_stage_ = nullptr;
+  size_t stage_cap_ = 0;
+  std::map<std::tuple<const void*, unsigned, size_t>, int> occ_;
+  const bool group_on_ = env_on("TTG_GROUP");
+  const bool group_coop_ = env_on("TTG_GROUP_COOP");
+  std::string group_skip_ = getenv("TTG_GROUP_SKIP") ? getenv("TTG_GROUP_SKIP") : "";
+  std::map<const GroupInfo*, bool> groupable_;
+  bool groupable(const GroupInfo* info) {
+    if (!group_on_ || (info->coop && !group_coop_)) return false;
+    if (group_skip_.empty()) return true;
+    auto it = groupable_.find(info);
+    if (it != groupable_.end()) return it->second;
+    const char* name = "";
+    cudaFuncGetName(&name, info->plain);
+    bool ok = true;
+    size_t b = 0;
+    while (b <= group_skip_.size()) {
+      size_t e = group_skip_.find(',', b);
+      if (e == std::string::npos) e = group_skip_.size();
+      const std::string tok = group_skip_.substr(b, e - b);
+      if (!tok.empty() && name && strstr(name, tok.c_str())) ok = false;
+      b = e + 1;
+    }
+    groupable_[info] = ok;
+    return ok;
+  }
+
+  std::mutex mu_;
+  std::condition_variable cv_main_, cv_sys_;
+  int live_ = 0, blocked_ = 0;
+  uint64_t epoch_ = 0;
+  bool failed_ = false;
+  int fail_code_ = TTG_OK;
+  std::string fail_msg_;
+};
+
+Executor::Executor(Context* owner, int width) : owner_(owner), width_(width) {
+  TTG_CUDA(cudaHostAlloc(&h_slab_, sizeof(double) * 4096 * size_t(width), cudaHostAllocMapped));
+  double* h_slab_dev = nullptr;
+  TTG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&h_slab_dev), h_slab_, 0));
+  TTG_CUDA(cudaMalloc(&d_err_slab_, sizeof(int) * 64 * size_t(width)));
+  TTG_CUDA(cudaMemset(d_err_slab_, 0, sizeof(int) * 64 * size_t(width)));
+  TTG_CUDA(cudaMalloc(&d_tile_slab_, sizeof(unsigned) * GEMM_TILE_COUNTERS * size_t(width)));
+  TTG_CUDA(cudaMemset(d_tile_slab_, 0, sizeof(unsigned) * GEMM_TILE_COUNTERS * size_t(width)));
+  TTG_CUDA(cudaDeviceSynchronize());
+  for (int k = 0; k < width; ++k) {
+    recs_.emplace_back(new Recorder());
+    recs_.back()->ex = this;
+    std::unique_ptr<Context> c(new Context());
+    c->device = owner->device;
+    c->num_sms = owner->num_sms;
+    c->stream = owner->stream;
+    c->solver = nullptr;
+    c->alloc = owner->alloc;
+    c->h_scal = h_slab_ + size_t(k) * 4096;
+    c->h_scal_dev = h_slab_dev + size_t(k) * 4096;
+    c->d_err = d_err_slab_ + size_t(k) * 64;
+    c->d_tile_cnt = d_tile_slab_ + size_t(k) * GEMM_TILE_COUNTERS;
+    c->pdl = owner->pdl;
+    c->jacobi_max_sweeps = owner->jacobi_max_sweeps;
+    c->rec = recs_.back().get();
+    ctxs_.push_back(std::move(c));
+  }
+}
+
+Executor::~Executor() {
+  cudaStreamSynchronize(owner_->stream);
+  if (h_slab_) cudaFreeHost(h_slab_);
+  if (d_err_slab_) cudaFree(d_err_slab_);
+  if (d_tile_slab_) cudaFree(d_tile_slab_);
+  if (h_stage_) cudaFreeHost(h_stage_);
+  if (d_stage_) cudaFree(d_stage_);
+}
+
+void Executor::ensure_stage(size_t bytes) {
+  if (bytes <= stage_cap_) return;
+  size_t cap = std::max<size_t>(bytes + bytes / 2, size_t(8) << 20);
+  // Called at the start of a flush: the stream is idle.
+  if (h_stage_) cudaFreeHost(h_stage_);
+  if (d_stage_) cudaFree(d_stage_);
+  h_stage_ = nullptr;
+  d_stage_ = nullptr;
+  stage_cap_ = 0;
+  TTG_CUDA(cudaMallocHost(&h_stage_, cap));
+  TTG_CUDA(cudaMalloc(&d_stage_, cap));
+  stage_cap_ = cap;
+}
+
+int Executor::coop_capacity(const GroupInfo* info, dim3 block, size_t smem) {
+  const auto key = std::make_tuple(info->group, block.x * block.y * block.z, smem);
+  auto it = occ_.find(key);
+  if (it != occ_.end()) return it->second;
+  int occ = 0;
+  TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ, info->group, int(block.x * block.y * block.z), smem));
+  const int cap = std::max(0, occ) * owner_->num_sms;
+  occ_[key] = cap;
+  return cap;
+}
+
+void Executor::wait(Recorder* r) {
+  (void)r;
+  std::unique_lock<std::mutex> lk(mu_);
+  const uint64_t e = epoch_;
+  ++blocked_;
+  if (blocked_ == live_) cv_main_.notify_one();
+  cv_sys_.wait(lk, [&] { return epoch_ != e; });
+  if (failed_) throw Error{fail_code_, fail_msg_};
+}
+
+void Executor::run(int64_t count, const std::function<void(int64_t, Context*)>& body) {
+  const int nthreads = int(std::min<int64_t>(width_, count));
+  std::atomic<int64_t> next{0};
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    live_ = nthreads;
+    blocked_ = 0;
+  }
+  {
+    const int share = owner_->group_sms > 0
+                          ? std::min(owner_->group_sms, owner_->num_sms)
+                          : std::max(1, 2 * owner_->num_sms / std::max(1, nthreads));
+    for (auto& c : ctxs_) c->num_sms = share;
+  }
+  auto worker = [&](int k) {
+    cudaSetDevice(owner_->device);
+    Context* c = ctxs_[k].get();
+    for (;;) {
+      const int64_t i = next.fetch_add(1);
+      if (i >= count) break;
+      body(i, c);
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    --live_;
+    if (blocked_ == live_) cv_main_.notify_one();
+  };
+  std::vector<std::thread> th;
+  th.reserve(nthreads);
+  for (int k = 0; k < nthreads; ++k) th.emplace_back(worker, k);
+  {
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_main_.wait(lk, [&] { return blocked_ == live_; });
+      const bool last = live_ == 0;
+      // Per-solve share of the SMs for the grids the solves size themselves
+      // (cooperative Krylov grids, split-K slices, grid-stride loops): the
+      // grouped launches fill the device across solves.
+      const int share =
+          owner_->group_sms > 0
+              ? std::min(owner_->group_sms, owner_->num_sms)
+              : std::max(1, std::min(owner_->num_sms, 2 * owner_->num_sms / std::max(1, live_)));
+      for (auto& c : ctxs_) c->num_sms = share;
+      lk.unlock();
+      try {
+        flush();
+      } catch (const Error& e) {
+        lk.lock();
+        if (!failed_) {
+          failed_ = true;
+          fail_code_ = e.code;
+          fail_msg_ = e.msg;
+        }
+        lk.unlock();
+      }
+      lk.lock();
+      blocked_ = 0;
+      ++epoch_;
+      cv_sys_.notify_all();
+      if (last) break;
+    }
+  }
+  for (auto& t : th) t.join();
+  if (failed_) fail(fail_code_, "grouped batch: %s", fail_msg_.c_str());
+}
+
+void Executor::flush() {
+  const auto t0 = std::chrono::steady_clock::now();
+  st.flushes += 1;
+  cudaStream_t s = owner_->stream;
+  std::vector<Recorder*> R;
+  size_t remaining = 0;
+  for (auto& r : recs_)
+    if (!r->ops.empty()) {
+      R.push_back(r.get());
+      remaining += r->ops.size();
+    }
+  st.records += int64_t(remaining);
+
+  // ---- plan: steps in issue order
+  struct Member {
+    Recorder* r;
+    uint32_t op;
+  };
+  struct Step {
+    bool group;
+    Recorder* r;        // stream operation
+    uint32_t op;
+    size_t first, n;    // group members
+  };
+  std::vector<Step> steps;
+  std::vector<Member> members;
+  std::vector<size_t> head(R.size(), 0);
+  struct Key {
+    const GroupInfo* info;
+    dim3 block;
+    int count;
+  };
+  std::vector<Key> keys;
+  while (remaining) {
+    for (size_t q = 0; q < R.size(); ++q) {
+      auto& ops = R[q]->ops;
+      while (head[q] < ops.size() && !ops[head[q]].info) {
+        steps.push_back(Step{false, R[q], uint32_t(head[q]), 0, 0});
+        ++head[q];
+        --remaining;
+      }
+    }
+    if (!remaining) break;
+    keys.clear();
+    for (size_t q = 0; q < R.size(); ++q) {
+      if (head[q] >= R[q]->ops.size()) continue;
+      const RecOp& o = R[q]->ops[head[q]];
+      bool found = false;
+      for (auto& k : keys)
+        if (k.info == o.info && k.block.x == o.block.x && k.block.y == o.block.y &&
+            k.block.z == o.block.z) {
+          ++k.count;
+          found = true;
+          break;
+        }
+      if (!found) keys.push_back(Key{o.info, o.block, 1});
+    }
+    const Key* best = &keys[0];
+    for (auto& k : keys)
+      if (k.count > best->count) best = &k;
+    const Key kb = *best;
+    Step g{true, nullptr, 0, members.size(), 0};
+    for (size_t q = 0; q < R.size(); ++q) {
+      if (head[q] >= R[q]->ops.size()) continue;
+      const RecOp& o = R[q]->ops[head[q]];
+      if (o.info == kb.info && o.block.x == kb.block.x && o.block.y == kb.block.y &&
+          o.block.z == kb.block.z) {
+        members.push_back(Member{R[q], uint32_t(head[q])});
+        ++head[q];
+        --remaining;
+      }
+    }
+    g.n = members.size() - g.first;
+    steps.push_back(g);
+  }
+
+  // ---- launches: split cooperative groups by residency, lay out staging
+  struct Launch {
+    size_t step;        // index in steps
+    size_t first, n;    // members
+    uint32_t ctas;
+    uint32_t smem;
+    size_t map_off, hdr_off, pack_off;
+    uint32_t stride;
+  };
+  std::vector<Launch> launches;
+  std::vector<size_t> launch_of_step(steps.size(), SIZE_MAX);
+  size_t bytes = 0;
+  auto ctas_of = [](const RecOp& o) -> uint64_t {
+    return uint64_t(o.grid.x) * o.grid.y * o.grid.z;
+  };
+  for (size_t si = 0; si < steps.size(); ++si) {
+    const Step& sp = steps[si];
+    if (!sp.group) continue;
+    const GroupInfo* info = members[sp.first].r->ops[members[sp.first].op].info;
+    const dim3 block = members[sp.first].r->ops[members[sp.first].op].block;
+    if (sp.n == 1 || !groupable(info)) continue;  // plain launches
+    uint32_t smem = 0;
+    for (size_t m = sp.first; m < sp.first + sp.n; ++m)
+      smem = std::max(smem, members[m].r->ops[members[m].op].smem);
+    uint64_t cap = UINT32_MAX / 2;
+    if (info->coop) cap = uint64_t(std::max(1, coop_capacity(info, block, smem)));
+    const uint32_t stride = uint32_t(align_up(info->pack_size, std::max<uint32_t>(16, info->pack_align)));
+    size_t m = sp.first;
+    launch_of_step[si] = launches.size();
+    while (m < sp.first + sp.n) {
+      Launch L{si, m, 0, 0, smem, 0, 0, 0, stride};
+      uint64_t ctas = 0;
+      while (m < sp.first + sp.n) {
+        const uint64_t k = ctas_of(members[m].r->ops[members[m].op]);
+        if (L.n > 0 && ctas + k > cap) break;
+        ctas += k;
+        ++L.n;
+        ++m;
+      }
+      L.ctas = uint32_t(ctas);
+      bytes = align_up(bytes, 256);
+      L.map_off = bytes;
+      bytes += sizeof(uint32_t) * ctas;
+      bytes = align_up(bytes, 256);
+      L.hdr_off = bytes;
+      bytes += sizeof(uint4) * L.n;
+      bytes = align_up(bytes, 256);
+      L.pack_off = bytes;
+      bytes += size_t(stride) * L.n;
+      launches.push_back(L);
+    }
+  }
+  ensure_stage(bytes + 256);
+  for (auto& L : launches) {
+    uint32_t* map = reinterpret_cast<uint32_t*>(h_stage_ + L.map_off);
+    uint4* hdr = reinterpret_cast<uint4*>(h_stage_ + L.hdr_off);
+    char* packs = h_stage_ + L.pack_off;
+    uint32_t cta = 0;
+    for (size_t j = 0; j < L.n; ++j) {
+      const Member& mb = members[L.first + j];
+      const RecOp& o = mb.r->ops[mb.op];
+      const uint32_t k = uint32_t(ctas_of(o));
+      hdr[j] = make_uint4(cta, o.grid.x, o.grid.y, o.grid.z);
+      for (uint32_t b = 0; b < k; ++b) map[cta + b] = uint32_t(j);
+      cta += k;
+      memcpy(packs + size_t(L.stride) * j, mb.r->arena.data() + o.pack_off, o.info->pack_size);
+    }
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  st.ms_plan += std::chrono::duration<double, std::milli>(t1 - t0).count();
+
+  // ---- issue
+  if (bytes) TTG_CUDA(cudaMemcpyAsync(d_stage_, h_stage_, bytes, cudaMemcpyHostToDevice, s));
+  for (size_t si = 0; si < steps.size(); ++si) {
+    const Step& sp = steps[si];
+    if (!sp.group) {
+      sp.r->closures[sp.r->ops[sp.op].closure](s, owner_->solver);
+      st.launches += 1;
+      continue;
+    }
+    const GroupInfo* info = members[sp.first].r->ops[members[sp.first].op].info;
+    const dim3 block = members[sp.first].r->ops[members[sp.first].op].block;
+    auto plain_one = [&](const Member& mb) {
+      const RecOp& o = mb.r->ops[mb.op];
+      info->issue(mb.r->arena.data() + o.pack_off, o.grid, o.block, o.smem, s, owner_->pdl);
+      st.launches += 1;
+    };
+    if (sp.n == 1 || !groupable(info)) {
+      for (size_t m = sp.first; m < sp.first + sp.n; ++m) plain_one(members[m]);
+      continue;
+    }
+    st.grouped_records += int64_t(sp.n);
+    for (size_t li = launch_of_step[si]; li < launches.size() && launches[li].step == si; ++li) {
+      const Launch& L = launches[li];
+      if (L.n == 1) {  // one launch alone (a cooperative grid at its residency limit)
+        plain_one(members[L.first]);
+        continue;
+      }
+      if (L.smem > 48 * 1024) ensure_smem_attr(info->group, owner_->device, int(L.smem));
+      GroupArgs ga{reinterpret_cast<const uint32_t*>(d_stage_ + L.map_off),
+                   reinterpret_cast<const uint4*>(d_stage_ + L.hdr_off), d_stage_ + L.pack_off,
+                   L.stride};
+      void* kargs[] = {&ga};
+      if (info->coop) {
+        TTG_CUDA(cudaLaunchCooperativeKernel(info->group, dim3(L.ctas), block, kargs, L.smem, s));
+      } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(L.ctas);
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = L.smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = owner_->pdl ? 1 : 0;
+        TTG_CUDA(cudaLaunchKernelExC(&cfg, info->group, kargs));
+      }
+      st.launches += 1;
+    }
+  }
+  const cudaError_t e = cudaStreamSynchronize(s);
+  const auto t2 = std::chrono::steady_clock::now();
+  st.ms_issue_wait += std::chrono::duration<double, std::milli>(t2 - t1).count();
+  for (Recorder* r : R) {
+    r->ops.clear();
+    r->closures.clear();
+    r->arena.clear();
+  }
+  for (auto& r : recs_) {
+    for (void* p : r->frees) owner_->alloc->put(p);
+    r->frees.clear();
+  }
+  if (e != cudaSuccess) fail(TTG_ERR_CUDA, "grouped launch: %s", cudaGetErrorString(e));
+}
+
+void rec_op(Recorder* r, StreamOp op) {
+  RecOp o{};
+  o.info = nullptr;
+  o.closure = uint32_t(r->closures.size());
+  r->closures.push_back(std::move(op));
+  r->ops.push_back(o);
+}
+
+void rec_group(Recorder* r, const GroupInfo* info, dim3 grid, dim3 block, size_t smem,
+               const void* pack) {
+  const size_t off = align_up(r->arena.size(), 16);
+  r->arena.resize(off + info->pack_size);
+  memcpy(r->arena.data() + off, pack, info->pack_size);
+  RecOp o{};
+  o.info = info;
+  o.grid = grid;
+  o.block = block;
+  o.smem = uint32_t(smem);
+  o.pack_off = uint32_t(off);
+  r->ops.push_back(o);
+}
+
+void rec_wait(Recorder* r) { r->ex->wait(r); }
+
+void rec_memset(Context* c, void* p, int value, size_t bytes) {
+  if (bytes == 0) return;
+  const int64_t blocks = std::max<int64_t>(
+      1, std::min<int64_t>((int64_t(bytes) / 16 + 255) / 256, int64_t(c->num_sms) * 4));
+  launch(c, k_fill_bytes, unsigned(blocks), 256, 0, static_cast<unsigned char*>(p), value,
+         int64_t(bytes));
+}
+
+void rec_read(Context* c, size_t off, const void* src, size_t bytes) {
+  TTG_REQUIRE(off + bytes <= 4096 * sizeof(double), "rec_read: %zu bytes at %zu", bytes, off);
+  launch(c, k_read_host, 1, 256, 0, static_cast<const unsigned char*>(src),
+         reinterpret_cast<unsigned char*>(c->h_scal_dev) + off, int64_t(bytes));
+}
+
+void rec_free(Recorder* r, void* p) { r->frees.push_back(p); }
+
+void run_grouped(Context* owner, int width, int64_t count,
+                 const std::function<void(int64_t, Context*)>& body, ttg_group_stats* gs) {
+  const auto t0 = std::chrono::steady_clock::now();
+  sync(owner);
+  Executor ex(owner, width);
+  ex.run(count, body);
+  if (gs) {
+    *gs = ex.st;
+    gs->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+}
+
+}  // namespace ttg

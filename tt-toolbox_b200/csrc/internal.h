@@ -11,10 +11,12 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -82,6 +84,26 @@ class Allocator {
 
 struct Context;
 
+// Grouped batch (group.cu).  A context whose `rec` is set belongs to one
+// solve of a grouped batch: its stream work is recorded in order instead of
+// issued, and the batch executor issues the records of all solves together,
+// merging launches of the same kernel into grouped launches, whenever every
+// solve waits for the device (a host read or a synchronisation).
+struct Recorder;
+using StreamOp = std::function<void(cudaStream_t, cusolverDnHandle_t)>;
+// Record a stream operation (issued by the executor in the solve's order).
+void rec_op(Recorder* r, StreamOp op);
+// Block until the executor has issued and completed everything recorded.
+void rec_wait(Recorder* r);
+// Return a device block to the allocator once the recorded work that may
+// use it has been issued.
+void rec_free(Recorder* r, void* p);
+struct Context;
+// Recorded memset and device-to-host read (into the context's pinned,
+// device-mapped scalar buffer at byte offset `off`) as grouped kernels.
+void rec_memset(Context* c, void* p, int value, size_t bytes);
+void rec_read(Context* c, size_t off, const void* src, size_t bytes);
+
 // RAII device buffer drawn from a context's allocator.
 template <typename T>
 class DBuf {
@@ -119,13 +141,17 @@ struct Context {
   cudaStream_t stream = nullptr;
   cusolverDnHandle_t solver = nullptr;
   Allocator* alloc = nullptr;
-  // Small pinned host buffer for scalar read-back.
+  // Small pinned host buffer for scalar read-back (a grouped batch's
+  // contexts: mapped, h_scal_dev its device address).
   double* h_scal = nullptr;
+  double* h_scal_dev = nullptr;
   // Device int slots: 0-7 error flags of bounded waits and factorizations
   // (cleared per solve), 63 the arrival counter of the one-launch reductions.
   int* d_err = nullptr;
   // Sweep limit of the one-sided Jacobi SVDs (ttg_context_set_option).
   int jacobi_max_sweeps = 40;
+  // SM count the solves of a grouped batch size their grids with (0: share).
+  int group_sms = 0;
   // Per-output-tile arrival counters of split-K GEMMs (GEMM_TILE_COUNTERS,
   // zero between launches: the last slice of a tile resets its counter).
   unsigned* d_tile_cnt = nullptr;
@@ -163,6 +189,8 @@ struct Context {
   // immediately when *skip != 0 (speculatively queued Krylov steps after
   // convergence).
   const int* skip = nullptr;
+  // Non-null: the context records its stream work for a grouped batch.
+  Recorder* rec = nullptr;
 
   int ev_begin(int kind) {
     if (ev_used == ev_pool.size()) {
@@ -184,6 +212,10 @@ struct Context {
   }
   // Accumulate the elapsed time of all recorded pairs into mv_ms (syncs).
   void ev_collect() {
+    if (rec) {  // no event timing in a grouped batch
+      ev_used = 0;
+      return;
+    }
     cudaStreamSynchronize(stream);
     for (size_t i = 0; i < ev_used; ++i) {
       if (ev_pool[i].kind < 0) continue;
@@ -232,7 +264,12 @@ void DBuf<T>::reset(Context* c, size_t n) {
 }
 template <typename T>
 void DBuf<T>::release() {
-  if (p_ && c_) c_->alloc->put(p_);
+  if (p_ && c_) {
+    if (c_->rec)
+      rec_free(c_->rec, p_);
+    else
+      c_->alloc->put(p_);
+  }
   p_ = nullptr;
   n_ = 0;
 }
@@ -259,6 +296,29 @@ __device__ __forceinline__ void pdl_begin() {
 template <typename... KArgs, typename... Args>
 void launch(Context* c, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
             Args&&... args) {
+  if (c->rec) {  // grouped batch: one recorded launch of its own
+    std::tuple<std::decay_t<KArgs>...> t(std::forward<Args>(args)...);
+    const bool pdl = c->pdl;
+    rec_op(c->rec, [kernel, grid, block, smem, t, pdl](cudaStream_t s, cusolverDnHandle_t) {
+      std::apply(
+          [&](const auto&... a) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = grid;
+            cfg.blockDim = block;
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = pdl ? 1 : 0;
+            TTG_CUDA(cudaLaunchKernelEx(&cfg, kernel, a...));
+          },
+          t);
+    });
+    c->launches += 1;
+    return;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
@@ -289,7 +349,14 @@ void launch(Context* c, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t 
 
 // Copy a device scalar (or a few) to the host; synchronises the stream.
 void read_scalars(Context* c, const double* d, double* h, int count);
+// Copy `bytes` (at most 32 KiB) of device memory to the host; synchronises.
+void read_device(Context* c, void* h, const void* d, size_t bytes);
 void sync(Context* c);
+// Stream-ordered memset / device-to-device copy on the context's stream.
+void memset_async(Context* c, void* p, int value, size_t bytes);
+void copy_async(Context* c, void* dst, const void* src, size_t bytes);
+// A cuSOLVER call on the context's stream and handle.
+void solver_call(Context* c, const StreamOp& op);
 // Stream, solver handle, allocator, pinned scalars and error slots of a
 // context on `device` (the current device must be `device`).
 void context_init(Context& c, int device);

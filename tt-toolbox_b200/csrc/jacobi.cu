@@ -13,6 +13,7 @@
 // the pivot is the first entry of largest magnitude, LAPACK's choice, and
 // the row interchanges are undone as column interchanges at the end.
 // Application is HBM-bound: every inverse entry is read once per apply.
+#include "group.cuh"
 #include "jacobi.h"
 #include "linalg.h"
 
@@ -24,7 +25,7 @@ namespace {
 
 constexpr int GJ_THREADS = 256;
 
-__global__ void k_diag_phi1(int64_t rx1, int64_t ra1, const double* __restrict__ Phi1,
+TTG_BODY(k_diag_phi1)(TTG_BLOCK, int64_t rx1, int64_t ra1, const double* __restrict__ Phi1,
                             double* __restrict__ d1) {
   pdl_begin();
   const int64_t total = rx1 * ra1;
@@ -34,8 +35,9 @@ __global__ void k_diag_phi1(int64_t rx1, int64_t ra1, const double* __restrict__
     d1[e] = Phi1[i + rx1 * i + rx1 * rx1 * a];  // d1[i, a] = Phi1[i, i, a]
   }
 }
+TTG_KERNEL(k_diag_phi1, 0);
 
-__global__ void k_diag_phi2(int64_t rx2, int64_t ra2, const double* __restrict__ Phi2,
+TTG_BODY(k_diag_phi2)(TTG_BLOCK, int64_t rx2, int64_t ra2, const double* __restrict__ Phi2,
                             double* __restrict__ d2) {
   pdl_begin();
   const int64_t total = ra2 * rx2;
@@ -45,10 +47,11 @@ __global__ void k_diag_phi2(int64_t rx2, int64_t ra2, const double* __restrict__
     d2[e] = Phi2[k + rx2 * b + rx2 * ra2 * k];  // d2[b, k] = Phi2[k, b, k]
   }
 }
+TTG_KERNEL(k_diag_phi2, 0);
 
 // One CTA per block (i, k), blockIdx.x = i + rx1 k; the block's entry (j, m)
 // lives at J[i + rx1 (j + n m) + rx1 n n k].  In place.
-__global__ void __launch_bounds__(GJ_THREADS) k_block_inv(int64_t rx1, int n,
+TTG_BODY(k_block_inv)(TTG_BLOCK, int64_t rx1, int n,
                                                           double* __restrict__ J,
                                                           int* __restrict__ err) {
   pdl_begin();
@@ -136,9 +139,10 @@ __global__ void __launch_bounds__(GJ_THREADS) k_block_inv(int64_t rx1, int n,
   }
   for (int e = tid; e < n * n; e += GJ_THREADS) blk[rx1 * int64_t(e)] = a[e];
 }
+TTG_KERNEL(k_block_inv, GJ_THREADS);
 
 // y[i, j, k] = sum_m J[i, j, m, k] x[i, m, k]; threads over (i, j, k), i fastest.
-__global__ void k_jac_apply_c(int64_t rx1, int64_t n, int64_t rx2, const double* __restrict__ J,
+TTG_BODY(k_jac_apply_c)(TTG_BLOCK, int64_t rx1, int64_t n, int64_t rx2, const double* __restrict__ J,
                               const double* __restrict__ x, double* __restrict__ y) {
   pdl_begin();
   const int64_t total = rx1 * n * rx2;
@@ -152,11 +156,12 @@ __global__ void k_jac_apply_c(int64_t rx1, int64_t n, int64_t rx2, const double*
     y[e] = s;
   }
 }
+TTG_KERNEL(k_jac_apply_c, 0);
 
 // Left block-Jacobi ('ljacobi'): J[(i + rx1 j) + B (a + rx1 m) + B^2 k] =
 // sum_al Phi1[i, a, al] AK[al, j, m, k], B = rx1 n, with
 // AK[al, j, m, k] = sum_be A[al, j, m, be] Phi2[k, be, k].
-__global__ void k_jac_build_l(int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
+TTG_BODY(k_jac_build_l)(TTG_BLOCK, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
                               const double* __restrict__ Phi1, const double* __restrict__ AK,
                               double* __restrict__ J) {
   pdl_begin();
@@ -171,11 +176,12 @@ __global__ void k_jac_build_l(int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
     J[e] = s;
   }
 }
+TTG_KERNEL(k_jac_build_l, 0);
 
 // Right block-Jacobi ('rjacobi'): J[(j + n k) + B (m + n q) + B^2 i] =
 // sum_be G[i, j, m, be] Phi2[q, be, k], B = n rx2, with
 // G[i, j, m, be] = sum_al Phi1[i, i, al] A[al, j, m, be].
-__global__ void k_jac_build_r(int64_t rx1, int64_t n, int64_t rx2, int64_t ra2,
+TTG_BODY(k_jac_build_r)(TTG_BLOCK, int64_t rx1, int64_t n, int64_t rx2, int64_t ra2,
                               const double* __restrict__ G, const double* __restrict__ Phi2,
                               double* __restrict__ J) {
   pdl_begin();
@@ -190,14 +196,16 @@ __global__ void k_jac_build_r(int64_t rx1, int64_t n, int64_t rx2, int64_t ra2,
     J[e] = s;
   }
 }
+TTG_KERNEL(k_jac_build_r, 0);
 
 // blk = I (B x B, column-major)
-__global__ void k_set_identity(int64_t B, double* __restrict__ blk) {
+TTG_BODY(k_set_identity)(TTG_BLOCK, int64_t B, double* __restrict__ blk) {
   pdl_begin();
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < B * B;
        e += int64_t(gridDim.x) * blockDim.x)
     blk[e] = (e % B == e / B) ? 1.0 : 0.0;
 }
+TTG_KERNEL(k_set_identity, 0);
 
 int blocks_for(Context* c, int64_t n) {
   int64_t b = (n + 255) / 256;
@@ -224,7 +232,7 @@ void jac_gen_c_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
   gemm_f64(c, false, false, rx1 * n * n, rx2, ra2, 1.0, G.p(), rx1 * n * n, 0, d2.p(), ra2, 0,
            0.0, J, rx1 * n * n, 0, 1);
   const size_t smem = sizeof(double) * size_t(n) * size_t(n);
-  ensure_smem_attr(reinterpret_cast<const void*>(k_block_inv), c->device, int(smem));
+  ensure_smem_attr(k_block_inv.fn(), c->device, int(smem));
   launch(c, k_block_inv, unsigned(rx1 * rx2), GJ_THREADS, smem, rx1, int(n), J, c->d_err + 4);
   TTG_CHECK_LAUNCH();
 }
@@ -239,7 +247,7 @@ void inv_blocks_f64(Context* c, int64_t B, int64_t nblocks, double* J) {
   if (B <= JAC_MAX_N) {  // one CTA per block, Gauss-Jordan in shared memory
     TTG_REQUIRE(nblocks <= int64_t(0x7fffffff), "too many blocks");
     const size_t smem = sizeof(double) * size_t(B) * size_t(B);
-    ensure_smem_attr(reinterpret_cast<const void*>(k_block_inv), c->device, int(smem));
+    ensure_smem_attr(k_block_inv.fn(), c->device, int(smem));
     launch(c, k_block_inv, unsigned(nblocks), GJ_THREADS, smem, int64_t(1), int(B), J,
            c->d_err + 4);
     TTG_CHECK_LAUNCH();

@@ -1,5 +1,8 @@
 // Launchers of the device kernels used by the host drivers.
 #pragma once
+
+#include <initializer_list>
+#include <utility>
 #include "internal.h"
 
 namespace ttg {
@@ -29,6 +32,8 @@ int64_t count_nonfinite_f64(Context* c, int64_t n, const double* x);
 // Fails with TTG_ERR_INVALID when a core of t holds NaN or Inf (one device
 // pass and one read-back); name is the argument name in the message.
 void require_finite(const ttg_tt_s* t, const char* name);
+// The same for several tensors on context c, with one host read.
+void require_finite(Context* c, std::initializer_list<std::pair<const ttg_tt_s*, const char*>> ts);
 
 // Self-tests of the bounded device waits (ttg_selftest_wait): each runs the
 // wait helper of one kernel family with a small poll limit on a condition

@@ -8,6 +8,7 @@
 // 32x32, each warp issuing mma.sync.m8n8k4 f64 (the FP64 tensor path; tcgen05
 // has no FP64 kind).  Global->shared staging with cp.async (8-byte granules so
 // any leading dimension works), double buffered.
+#include "group.cuh"
 #include "kernels.h"
 #include "dmma.cuh"
 
@@ -41,7 +42,7 @@ struct GemmP {
 };
 
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
+TTG_BODY(k_gemm_f64)(TTG_BLOCK, GemmP p) {
   pdl_begin();
   __shared__ double As[2][BK][BM + PADS];
   __shared__ double Bs[2][BK][BN + PADS];
@@ -204,6 +205,8 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmP p) {
     *dst = v;
   }
 }
+template <bool TA, bool TB>
+TTG_KERNEL_T(k_gemm_f64, 128, TA, TB);
 
 // ---------------------------------------------------------------------------
 // Reductions
@@ -237,7 +240,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 // Per-block partial sums; the last block to finish adds the partials in
 // block order (deterministic) and writes the result: one launch.  `counter` is a
 // device int that is zero between reductions (reset by the last block).
-__global__ void k_reduce_fused(int64_t n, const double* __restrict__ x,
+TTG_BODY(k_reduce_fused)(TTG_BLOCK, int64_t n, const double* __restrict__ x,
                                const double* __restrict__ y, int mode, double* __restrict__ part,
                                unsigned* counter, double* out, int do_sqrt) {
   pdl_begin();
@@ -274,6 +277,7 @@ __global__ void k_reduce_fused(int64_t n, const double* __restrict__ x,
     *counter = 0u;
   }
 }
+TTG_KERNEL(k_reduce_fused, 0);
 
 void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int mode,
                    double* out, bool do_sqrt) {
@@ -289,7 +293,7 @@ void reduce_launch(Context* c, int64_t n, const double* x, const double* y, int 
 // Elementwise
 // ---------------------------------------------------------------------------
 
-__global__ void k_count_nonfinite(int64_t n, const double* __restrict__ x,
+TTG_BODY(k_count_nonfinite)(TTG_BLOCK, int64_t n, const double* __restrict__ x,
                                   unsigned long long* __restrict__ out) {
   pdl_begin();
   unsigned long long cnt = 0;
@@ -299,16 +303,18 @@ __global__ void k_count_nonfinite(int64_t n, const double* __restrict__ x,
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
 }
+TTG_KERNEL(k_count_nonfinite, 0);
 
-__global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b,
+TTG_BODY(k_axpby)(TTG_BLOCK, int64_t n, double a, const double* __restrict__ x, double b,
                         double* __restrict__ y) {
   pdl_begin();
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = (b == 0.0 ? 0.0 : b * y[i]) + a * x[i];
 }
+TTG_KERNEL(k_axpby, 0);
 
-__global__ void k_scale_dev(int64_t n, const double* __restrict__ x, double* __restrict__ y,
+TTG_BODY(k_scale_dev)(TTG_BLOCK, int64_t n, const double* __restrict__ x, double* __restrict__ y,
                             const double* num, const double* den) {
   pdl_begin();
   const double s = (num ? *num : 1.0) / (den ? *den : 1.0);
@@ -316,22 +322,25 @@ __global__ void k_scale_dev(int64_t n, const double* __restrict__ x, double* __r
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = x[i] * s;
 }
+TTG_KERNEL(k_scale_dev, 0);
 
-__global__ void k_copy(int64_t n, const double* __restrict__ x, double* __restrict__ y) {
+TTG_BODY(k_copy)(TTG_BLOCK, int64_t n, const double* __restrict__ x, double* __restrict__ y) {
   pdl_begin();
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = x[i];
 }
+TTG_KERNEL(k_copy, 0);
 
-__global__ void k_fill(int64_t n, double v, double* y) {
+TTG_BODY(k_fill)(TTG_BLOCK, int64_t n, double v, double* y) {
   pdl_begin();
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = v;
 }
+TTG_KERNEL(k_fill, 0);
 
-__global__ void k_transpose(int64_t rows, int64_t cols, const double* __restrict__ in,
+TTG_BODY(k_transpose)(TTG_BLOCK, int64_t rows, int64_t cols, const double* __restrict__ in,
                             int64_t ldi, int64_t si, double* __restrict__ out, int64_t ldo,
                             int64_t so) {
   pdl_begin();
@@ -350,8 +359,9 @@ __global__ void k_transpose(int64_t rows, int64_t cols, const double* __restrict
     if (r < rows && cc < cols) out[cc + r * ldo] = tile[threadIdx.x][j];
   }
 }
+TTG_KERNEL(k_transpose, 0);
 
-__global__ void k_copy2d(int64_t rows, int64_t cols, const double* __restrict__ in, int64_t ldi,
+TTG_BODY(k_copy2d)(TTG_BLOCK, int64_t rows, int64_t cols, const double* __restrict__ in, int64_t ldi,
                          double* __restrict__ out, int64_t ldo, const double* scale_col) {
   pdl_begin();
   const int64_t total = rows * cols;
@@ -363,6 +373,7 @@ __global__ void k_copy2d(int64_t rows, int64_t cols, const double* __restrict__ 
     out[r + cidx * ldo] = v;
   }
 }
+TTG_KERNEL(k_copy2d, 0);
 
 // splitmix64-based counter hash -> two uniforms -> Box-Muller normal.
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
@@ -372,7 +383,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
-__global__ void k_randn(int64_t n, uint64_t seed, uint64_t offset, double* y) {
+TTG_BODY(k_randn)(TTG_BLOCK, int64_t n, uint64_t seed, uint64_t offset, double* y) {
   pdl_begin();
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
@@ -383,8 +394,9 @@ __global__ void k_randn(int64_t n, uint64_t seed, uint64_t offset, double* y) {
     y[i] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
   }
 }
+TTG_KERNEL(k_randn, 0);
 
-__global__ void k_normalize_by(int64_t n, double* __restrict__ x, double* nrm) {
+TTG_BODY(k_normalize_by)(TTG_BLOCK, int64_t n, double* __restrict__ x, double* nrm) {
   pdl_begin();
   const double v = *nrm;
   const double s = v > 0.0 ? 1.0 / v : 1.0;
@@ -394,8 +406,9 @@ __global__ void k_normalize_by(int64_t n, double* __restrict__ x, double* nrm) {
   // Every block has read *nrm above; a zero norm is reported as 1.
   if (blockIdx.x == 0 && threadIdx.x == 0 && !(v > 0.0)) *nrm = 1.0;
 }
+TTG_KERNEL(k_normalize_by, 0);
 
-__global__ void k_axpby_dev(int64_t n, double a, const double* __restrict__ x,
+TTG_BODY(k_axpby_dev)(TTG_BLOCK, int64_t n, double a, const double* __restrict__ x,
                             const double* __restrict__ b, double* __restrict__ y) {
   pdl_begin();
   const double bv = *b;
@@ -403,8 +416,9 @@ __global__ void k_axpby_dev(int64_t n, double a, const double* __restrict__ x,
        i += int64_t(gridDim.x) * blockDim.x)
     y[i] = bv * y[i] + a * x[i];
 }
+TTG_KERNEL(k_axpby_dev, 0);
 
-__global__ void k_scalar_op(int op, double* out, const double* p0, const double* p1,
+TTG_BODY(k_scalar_op)(TTG_BLOCK, int op, double* out, const double* p0, const double* p1,
                             const double* p2, double k) {
   pdl_begin();
   switch (op) {
@@ -419,8 +433,9 @@ __global__ void k_scalar_op(int op, double* out, const double* p0, const double*
     default: break;
   }
 }
+TTG_KERNEL(k_scalar_op, 0);
 
-__global__ void k_first_exceeding(int64_t nb, const double* cand, const double* den,
+TTG_BODY(k_first_exceeding)(TTG_BLOCK, int64_t nb, const double* cand, const double* den,
                                   const double* thr, double* out) {
   pdl_begin();
   double r = -1.0;
@@ -432,10 +447,11 @@ __global__ void k_first_exceeding(int64_t nb, const double* cand, const double* 
   }
   *out = r;
 }
+TTG_KERNEL(k_first_exceeding, 0);
 
 // C_b = alpha * sum_z part[b][z] + beta * C_b over the split-K slices, in
 // slice order (deterministic).  part: batch x s blocks of M x N (ld M).
-__global__ void k_splitk_reduce(int64_t M, int64_t N, int64_t s, int64_t batch,
+TTG_BODY(k_splitk_reduce)(TTG_BLOCK, int64_t M, int64_t N, int64_t s, int64_t batch,
                                 const double* __restrict__ part, double alpha, double beta,
                                 double* __restrict__ C, int64_t ldc, int64_t sC,
                                 const int* skip) {
@@ -455,9 +471,10 @@ __global__ void k_splitk_reduce(int64_t M, int64_t N, int64_t s, int64_t batch,
     *dst = v;
   }
 }
+TTG_KERNEL(k_splitk_reduce, 0);
 
 // *keep = 1 when every column j kept G1[j,j] > tau^2 G0[j,j] (one thread).
-__global__ void k_collapse_flag(int64_t k, const double* G0, int64_t ld0, const double* G1,
+TTG_BODY(k_collapse_flag)(TTG_BLOCK, int64_t k, const double* G0, int64_t ld0, const double* G1,
                                 int64_t ld1, double tau, int* keep) {
   pdl_begin();
   int ok = 1;
@@ -465,9 +482,10 @@ __global__ void k_collapse_flag(int64_t k, const double* G0, int64_t ld0, const 
     if (!(G1[j + j * ld1] > tau * tau * G0[j + j * ld0])) ok = 0;
   *keep = ok;
 }
+TTG_KERNEL(k_collapse_flag, 0);
 
 // *flag |= 1 when max |G - I| > tol (G: n x n Gram matrix of a basis).
-__global__ void k_orth_check(int64_t n, const double* G, double tol, int* flag) {
+TTG_BODY(k_orth_check)(TTG_BLOCK, int64_t n, const double* G, double tol, int* flag) {
   pdl_begin();
   int bad = 0;
   for (int64_t e = threadIdx.x; e < n * n; e += blockDim.x) {
@@ -476,11 +494,13 @@ __global__ void k_orth_check(int64_t n, const double* G, double tol, int* flag) 
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
+TTG_KERNEL(k_orth_check, 0);
 
-__global__ void k_accumulate_info(const int* info, int* err_slot) {
+TTG_BODY(k_accumulate_info)(TTG_BLOCK, const int* info, int* err_slot) {
   pdl_begin();
   if (*info != 0) atomicOr(err_slot, 1);
 }
+TTG_KERNEL(k_accumulate_info, 0);
 
 int grid_for(Context* c, int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
@@ -580,19 +600,40 @@ double nrm2_host(Context* c, int64_t n, const double* x) {
 int64_t count_nonfinite_f64(Context* c, int64_t n, const double* x) {
   if (n <= 0) return 0;
   DBuf<unsigned long long> cnt(c, 1);
-  TTG_CUDA(cudaMemsetAsync(cnt.p(), 0, sizeof(unsigned long long), c->stream));
+  memset_async(c, cnt.p(), 0, sizeof(unsigned long long));
   launch(c, k_count_nonfinite, grid_for(c, n), 256, 0, n, x, cnt.p());
   TTG_CHECK_LAUNCH();
   unsigned long long h = 0;
-  TTG_CUDA(cudaMemcpyAsync(&h, cnt.p(), sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-  sync(c);
+  read_device(c, &h, cnt.p(), sizeof(h));
   return int64_t(h);
 }
 
 void require_finite(const ttg_tt_s* t, const char* name) {
   if (!t) return;
-  const int64_t bad = count_nonfinite_f64(t->ctx, t->numel, t->core);
-  TTG_REQUIRE(bad == 0, "%s holds %lld non-finite entries (NaN or Inf)", name, (long long)bad);
+  require_finite(t->ctx, {{t, name}});
+}
+
+void require_finite(Context* c, std::initializer_list<std::pair<const ttg_tt_s*, const char*>> ts) {
+  const int64_t k = int64_t(ts.size());
+  DBuf<unsigned long long> cnt(c, k);
+  memset_async(c, cnt.p(), 0, sizeof(unsigned long long) * k);
+  int64_t j = 0;
+  for (const auto& t : ts) {
+    if (t.first && t.first->numel > 0)
+      launch(c, k_count_nonfinite, grid_for(c, t.first->numel), 256, 0, t.first->numel,
+             t.first->core, cnt.p() + j);
+    ++j;
+  }
+  TTG_CHECK_LAUNCH();
+  unsigned long long h[16] = {};
+  TTG_REQUIRE(k <= 16, "require_finite: too many tensors");
+  read_device(c, h, cnt.p(), sizeof(unsigned long long) * k);  // one read for all
+  j = 0;
+  for (const auto& t : ts) {
+    TTG_REQUIRE(h[j] == 0, "%s holds %lld non-finite entries (NaN or Inf)", t.second,
+                (long long)h[j]);
+    ++j;
+  }
 }
 
 void axpby_f64(Context* c, int64_t n, double a, const double* x, double b, double* y) {

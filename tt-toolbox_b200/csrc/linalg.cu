@@ -1,5 +1,9 @@
-// FP64 QR / SVD / LU on the device through cuSOLVER (library factorizations;
-// the contractions around them are this library's own kernels).
+// FP64 QR / SVD / LU on the device: the library's own one-CTA and blocked
+// factorizations, with cuSOLVER only for the shapes they do not cover.
+#include <map>
+#include <mutex>
+
+#include "group.cuh"
 #include "linalg.h"
 #include "small_dense.h"
 
@@ -7,7 +11,7 @@ namespace ttg {
 
 namespace {
 
-__global__ void k_triu(int64_t k, int64_t n, const double* __restrict__ A, int64_t lda,
+TTG_BODY(k_triu)(TTG_BLOCK, int64_t k, int64_t n, const double* __restrict__ A, int64_t lda,
                        double* __restrict__ R) {
   pdl_begin();
   const int64_t total = k * n;
@@ -17,6 +21,7 @@ __global__ void k_triu(int64_t k, int64_t n, const double* __restrict__ A, int64
     R[e] = (i <= j) ? A[i + j * lda] : 0.0;
   }
 }
+TTG_KERNEL(k_triu, 0);
 
 // A non-zero info is folded into the context error slot 4 on the device (no
 // host round trip); callers check the slot once their sequence is done.
@@ -32,12 +37,28 @@ int as_int(int64_t v, const char* what) {
 
 }  // namespace
 
+// cuSOLVER workspace queries need a handle; a context of a grouped batch
+// has none (its library calls are recorded and issued with the executor's),
+// so queries then go through one shared handle per device.
+template <class F>
+void with_query_handle(Context* c, F f) {
+  if (c->solver) {
+    f(c->solver);
+    return;
+  }
+  static std::mutex mu;
+  static std::map<int, cusolverDnHandle_t> handles;
+  std::lock_guard<std::mutex> lock(mu);
+  cusolverDnHandle_t& h = handles[c->device];
+  if (!h) TTG_SOLVER(cusolverDnCreate(&h));
+  f(h);
+}
+
 void check_factorizations(Context* c) {
   int h[5] = {0, 0, 0, 0, 0};
-  TTG_CUDA(cudaMemcpyAsync(h, c->d_err, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-  sync(c);
+  read_device(c, h, c->d_err, sizeof(h));
   if (h[0] || h[1] || h[2] || h[4]) {
-    TTG_CUDA(cudaMemsetAsync(c->d_err, 0, 5 * sizeof(int), c->stream));
+    memset_async(c, c->d_err, 0, 5 * sizeof(int));
     if (h[0] || h[1] || h[2])
       fail(TTG_ERR_TIMEOUT, "a bounded device-side wait timed out in a factorization");
     fail(TTG_ERR_SOLVER, "a device factorization reported a non-zero LAPACK info");
@@ -59,7 +80,7 @@ namespace {
 constexpr int64_t CHB = 96;
 
 // diag(G) += factor * trace(G), one CTA (the shift of the first pass).
-__global__ void k_add_trace_shift(int64_t n, double* __restrict__ G, int64_t ldg, double factor) {
+TTG_BODY(k_add_trace_shift)(TTG_BLOCK, int64_t n, double* __restrict__ G, int64_t ldg, double factor) {
   pdl_begin();
   __shared__ double red[32];
   double t = 0.0;
@@ -76,6 +97,7 @@ __global__ void k_add_trace_shift(int64_t n, double* __restrict__ G, int64_t ldg
   const double s = factor * red[0];
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) G[i + i * ldg] += s;
 }
+TTG_KERNEL(k_add_trace_shift, 0);
 
 // Blocked right-looking Cholesky R' R = G of an n x n SPD matrix (G is
 // overwritten by its Schur complements).  Each diagonal block of at most
@@ -132,7 +154,7 @@ bool scholqr3_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, 
       W(c, m * n);
   const bool blocked = n > CHB;  // beyond one CTA: blocked Cholesky and solve
   DBuf<int> flag(c, 1);
-  TTG_CUDA(cudaMemsetAsync(flag.p(), 0, sizeof(int), c->stream));
+  memset_async(c, flag.p(), 0, sizeof(int));
   const double u = 1.1102230246251565e-16;
   const double shift = 11.0 * (double(m) * n + double(n) * (n + 1)) * u;
   const double* src = A;
@@ -165,8 +187,7 @@ bool scholqr3_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, 
   gemm_f64(c, true, false, n, n, m, 1.0, Q, m, 0, Q, m, 0, 0.0, G.p(), n, 0, 1);
   orth_check(c, n, G.p(), 1e-12, flag.p());
   int h = 0;
-  TTG_CUDA(cudaMemcpyAsync(&h, flag.p(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  sync(c);
+  read_device(c, &h, flag.p(), sizeof(int));
   return h == 0;
 }
 
@@ -193,12 +214,22 @@ int64_t qr_f64(Context* c, int64_t m, int64_t n, const double* A, double* Q, dou
   DBuf<int> info(c, 1);
   copy_f64(c, m * n, A, work.p());
   int lw1 = 0, lw2 = 0;
-  TTG_SOLVER(cusolverDnDgeqrf_bufferSize(c->solver, mi, ni, work.p(), mi, &lw1));
-  TTG_SOLVER(cusolverDnDorgqr_bufferSize(c->solver, mi, ki, ki, work.p(), mi, tau.p(), &lw2));
+  double* wp = work.p();
+  double* tp = tau.p();
+  int* ip = info.p();
+  with_query_handle(c, [&](cusolverDnHandle_t h) {
+    TTG_SOLVER(cusolverDnDgeqrf_bufferSize(h, mi, ni, wp, mi, &lw1));
+    TTG_SOLVER(cusolverDnDorgqr_bufferSize(h, mi, ki, ki, wp, mi, tp, &lw2));
+  });
   DBuf<double> ws(c, std::max(std::max(lw1, lw2), 1));
-  TTG_SOLVER(cusolverDnDgeqrf(c->solver, mi, ni, work.p(), mi, tau.p(), ws.p(), lw1, info.p()));
+  double* sp = ws.p();
+  solver_call(c, [=](cudaStream_t, cusolverDnHandle_t h) {
+    TTG_SOLVER(cusolverDnDgeqrf(h, mi, ni, wp, mi, tp, sp, lw1, ip));
+  });
   extract_triu_f64(c, k, n, work.p(), m, R);
-  TTG_SOLVER(cusolverDnDorgqr(c->solver, mi, ki, ki, work.p(), mi, tau.p(), ws.p(), lw2, info.p()));
+  solver_call(c, [=](cudaStream_t, cusolverDnHandle_t h) {
+    TTG_SOLVER(cusolverDnDorgqr(h, mi, ki, ki, wp, mi, tp, sp, lw2, ip));
+  });
   copy_f64(c, m * k, work.p(), Q);
   check_info(c, info.p(), "geqrf/orgqr");
   return k;
@@ -253,10 +284,18 @@ void svd_gesvd_tall(Context* c, int64_t m, int64_t n, const double* A, double* U
   DBuf<int> info(c, 1);
   copy_f64(c, m * n, A, W.p());
   int lwork = 0;
-  TTG_SOLVER(cusolverDnDgesvd_bufferSize(c->solver, mi, ni, &lwork));
+  with_query_handle(c, [&](cusolverDnHandle_t h) {
+    TTG_SOLVER(cusolverDnDgesvd_bufferSize(h, mi, ni, &lwork));
+  });
   DBuf<double> ws(c, std::max(lwork, 1));
-  TTG_SOLVER(cusolverDnDgesvd(c->solver, 'S', 'S', mi, ni, W.p(), mi, S, U, mi, VT, ni, ws.p(),
-                              lwork, rw.p(), info.p()));
+  double* wp = W.p();
+  double* sp = ws.p();
+  double* rp = rw.p();
+  int* ip = info.p();
+  solver_call(c, [=](cudaStream_t, cusolverDnHandle_t h) {
+    TTG_SOLVER(cusolverDnDgesvd(h, 'S', 'S', mi, ni, wp, mi, S, U, mi, VT, ni, sp, lwork, rp,
+                                ip));
+  });
   check_info(c, info.p(), "gesvd");
 }
 }  // namespace
@@ -278,15 +317,27 @@ int64_t svd_f64_fallback(Context* c, int64_t m, int64_t n, const double* A, doub
 }
 
 void lu_solve_f64(Context* c, int64_t N, const double* B, double* rhs, int64_t nrhs) {
+  if (lu_small_fits(N, nrhs)) {  // the dense local systems (N < max_full_size)
+    lu_small_f64(c, N, B, rhs, nrhs);
+    return;
+  }
   const int Ni = as_int(N, "N"), nr = as_int(nrhs, "nrhs");
   DBuf<double> W(c, N * N);
   DBuf<int> piv(c, std::max<int64_t>(N, 1)), info(c, 1);
   copy_f64(c, N * N, B, W.p());
   int lwork = 0;
-  TTG_SOLVER(cusolverDnDgetrf_bufferSize(c->solver, Ni, Ni, W.p(), Ni, &lwork));
+  double* wp = W.p();
+  with_query_handle(c, [&](cusolverDnHandle_t h) {
+    TTG_SOLVER(cusolverDnDgetrf_bufferSize(h, Ni, Ni, wp, Ni, &lwork));
+  });
   DBuf<double> ws(c, std::max(lwork, 1));
-  TTG_SOLVER(cusolverDnDgetrf(c->solver, Ni, Ni, W.p(), Ni, ws.p(), piv.p(), info.p()));
-  TTG_SOLVER(cusolverDnDgetrs(c->solver, CUBLAS_OP_N, Ni, nr, W.p(), Ni, piv.p(), rhs, Ni, info.p()));
+  double* sp = ws.p();
+  int* pp = piv.p();
+  int* ip = info.p();
+  solver_call(c, [=](cudaStream_t, cusolverDnHandle_t h) {
+    TTG_SOLVER(cusolverDnDgetrf(h, Ni, Ni, wp, Ni, sp, pp, ip));
+    TTG_SOLVER(cusolverDnDgetrs(h, CUBLAS_OP_N, Ni, nr, wp, Ni, pp, rhs, Ni, ip));
+  });
   check_info(c, info.p(), "getrf/getrs");
 }
 

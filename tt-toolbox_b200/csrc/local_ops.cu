@@ -6,6 +6,7 @@
 // GEMMs with two explicit transposes (amen_solve2.m:937-950, :857-905).
 #include <algorithm>
 
+#include "group.cuh"
 #include "local_ops.h"
 
 namespace ttg {
@@ -83,7 +84,7 @@ int64_t next_phi_f64(Context* c, int dir, int64_t rx1, int64_t n, int64_t rx2, i
 }
 
 namespace {
-__global__ void k_assemble(int64_t rx1, int64_t n, int64_t rx2, int64_t ra1, int64_t ra2,
+TTG_BODY(k_assemble)(TTG_BLOCK, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1, int64_t ra2,
                            const double* __restrict__ Phi1, const double* __restrict__ A,
                            const double* __restrict__ Phi2, double* __restrict__ B) {
   pdl_begin();
@@ -105,6 +106,7 @@ __global__ void k_assemble(int64_t rx1, int64_t n, int64_t rx2, int64_t ra1, int
     B[e] = s;
   }
 }
+TTG_KERNEL(k_assemble, 0);
 }  // namespace
 
 void assemble_local_f64(Context* c, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
@@ -157,7 +159,7 @@ namespace {
 constexpr int CN_THREADS = 256;
 
 // part[blk * MAXC + b] = sum over this block's i of (R[i] + sum_{t >= cnt-1-b} W[i + N t])^2
-__global__ void __launch_bounds__(CN_THREADS) k_cumnorm(int64_t N, int cnt,
+TTG_BODY(k_cumnorm)(TTG_BLOCK, int64_t N, int cnt,
                                                          double* __restrict__ R,
                                                          const double* __restrict__ W,
                                                          double* __restrict__ part) {
@@ -192,10 +194,11 @@ __global__ void __launch_bounds__(CN_THREADS) k_cumnorm(int64_t N, int cnt,
     part[int64_t(blockIdx.x) * CUMNORM_MAXC + threadIdx.x] = x;
   }
 }
+TTG_KERNEL(k_cumnorm, CN_THREADS);
 
 // One warp per candidate: lanes stride over the block partials, then a fixed
 // shuffle tree (deterministic).
-__global__ void k_cumnorm_final(int nblk, int cnt, const double* __restrict__ part,
+TTG_BODY(k_cumnorm_final)(TTG_BLOCK, int nblk, int cnt, const double* __restrict__ part,
                                 double* __restrict__ out) {
   pdl_begin();
   const int b = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -205,6 +208,7 @@ __global__ void k_cumnorm_final(int nblk, int cnt, const double* __restrict__ pa
   for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   if (lane == 0) out[b] = sqrt(x);
 }
+TTG_KERNEL(k_cumnorm_final, 0);
 
 }  // namespace
 

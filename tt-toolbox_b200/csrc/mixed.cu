@@ -17,6 +17,7 @@
 #include <cstring>
 #include <vector>
 
+#include "group.cuh"
 #include "jacobi.h"
 #include "mixed.h"
 #include "mixed_ops.h"
@@ -72,7 +73,7 @@ __device__ __forceinline__ double warp_sumd(double v) {
   return v;
 }
 
-__device__ void ar_barrier(unsigned* bar, int* err, long long limit = AR_SPIN_LIMIT) {
+__device__ void ar_barrier(TTG_BLOCK, unsigned* bar, int* err, long long limit = AR_SPIN_LIMIT) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = bar + 1;
@@ -105,7 +106,7 @@ __device__ void ar_barrier(unsigned* bar, int* err, long long limit = AR_SPIN_LI
        idx += int64_t(gridDim.x) * blockDim.x)
 
 // part[c*nb + block] = block partial of V(:,c)'w, c < ncol.  red: AR_WARPS*(m+1) floats.
-__device__ void partial_dots(const ArArgs& a, int ncol, double* part, float* red) {
+__device__ void partial_dots(TTG_BLOCK, const ArArgs& a, int ncol, double* part, float* red) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int c = 0; c < ncol; ++c) {
     const float* Vc = a.V + int64_t(c) * a.sz;
@@ -123,7 +124,7 @@ __device__ void partial_dots(const ArArgs& a, int ncol, double* part, float* red
 }
 
 // Sum the block partials of ncol columns (same fixed order in every block).
-__device__ void reduce_parts(const double* part, int ncol, double* out) {
+__device__ void reduce_parts(TTG_BLOCK, const double* part, int ncol, double* out) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int c = warp; c < ncol; c += AR_WARPS) {
     double s = 0.0;
@@ -136,7 +137,7 @@ __device__ void reduce_parts(const double* part, int ncol, double* out) {
 
 // One Arnoldi step for column j: w -= V h twice (CGS2), normalise into
 // V(:, j+1), Givens update of H(:, j) and g; scal[0] = |g_{j+1}|.
-__global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
+TTG_BODY(k_arnoldi)(TTG_BLOCK, ArArgs a, int j) {
   if (*(volatile int*)a.stop) return;  // queued after convergence
   extern __shared__ double shd[];
   double* hp = shd;                 // m+1 : this pass's coefficients
@@ -148,9 +149,9 @@ __global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
   for (int c = threadIdx.x; c <= ncol; c += blockDim.x) ht[c] = 0.0;
   for (int pass = 0; pass < 2; ++pass) {
     double* part = pass ? part1 : part0;
-    partial_dots(a, ncol, part, red);
-    ar_barrier(a.bar, a.err);
-    reduce_parts(part, ncol, hp);
+    partial_dots(blockIdx, gridDim, a, ncol, part, red);
+    ar_barrier(blockIdx, gridDim, a.bar, a.err);
+    reduce_parts(blockIdx, gridDim, part, ncol, hp);
     AR_LOOP(i, a.sz) {
       float s = 0.f;
       for (int c = 0; c < ncol; ++c) s += a.V[int64_t(c) * a.sz + i] * float(hp[c]);
@@ -173,8 +174,8 @@ __global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
       for (int q = 0; q < AR_WARPS; ++q) t += double(red[q]);
       part0[blockIdx.x] = t;
     }
-    ar_barrier(a.bar, a.err);
-    reduce_parts(part0, 1, hp);
+    ar_barrier(blockIdx, gridDim, a.bar, a.err);
+    reduce_parts(blockIdx, gridDim, part0, 1, hp);
   }
   const double nrm = sqrt(hp[0]);
   float* Vn = a.V + int64_t(j + 1) * a.sz;
@@ -211,13 +212,14 @@ __global__ void __launch_bounds__(AR_THREADS) k_arnoldi(ArArgs a, int j) {
     }
   }
 }
+TTG_COOP_KERNEL(k_arnoldi, AR_THREADS);
 
 // V(:,0) = r / ||r||, g = [||r||, 0, ...]; scal[2] = ||r||.  On the first
 // restart (first != 0) r is the right-hand side: scal[3] = ||r||.  The stop
 // threshold reltol * scal[3] goes to scal[4]; a residual already below it
 // (or zero) raises the stop flag with step -1, so the queued steps return at
 // once and the host learns it at its next read of the flags.
-__global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r, int first) {
+TTG_BODY(k_ar_init)(TTG_BLOCK, ArArgs a, const float* r, int first) {
   __shared__ float red[AR_WARPS];
   __shared__ double tot[1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -231,8 +233,8 @@ __global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r
     for (int q = 0; q < AR_WARPS; ++q) t += double(red[q]);
     a.part[blockIdx.x] = t;
   }
-  ar_barrier(a.bar, a.err);
-  reduce_parts(a.part, 1, tot);
+  ar_barrier(blockIdx, gridDim, a.bar, a.err);
+  reduce_parts(blockIdx, gridDim, a.part, 1, tot);
   const double beta = sqrt(tot[0]);
   const float inv = beta > 0.0 ? float(1.0 / beta) : 0.f;
   AR_LOOP(i, a.sz) {
@@ -255,9 +257,10 @@ __global__ void __launch_bounds__(AR_THREADS) k_ar_init(ArArgs a, const float* r
     }
   }
 }
+TTG_COOP_KERNEL(k_ar_init, AR_THREADS);
 
 // x += V(:, 0:k) y with H(0:k,0:k) y = g(0:k) (upper triangular after Givens).
-__global__ void k_ar_update(ArArgs a, int k, float* x) {
+TTG_BODY(k_ar_update)(TTG_BLOCK, ArArgs a, int k, float* x) {
   pdl_begin();
   extern __shared__ double y[];
   if (threadIdx.x == 0) {
@@ -275,12 +278,13 @@ __global__ void k_ar_update(ArArgs a, int k, float* x) {
     x[i] += s;
   }
 }
+TTG_KERNEL(k_ar_update, 0);
 
 // Centre block-Jacobi on vectors in the reversed layout v[k + rx2 (j + n i)]:
 // out[k, j, i] = sum_m J[i, j, m, k] v[k, m, i] with the FP64 blocks J of
 // jac_gen_c_f64 (natural layout J[i + rx1 (j + n (m + n k))]).  To BF16 in
 // the matvec's K-major operand layout (xb, ld ldx) or to FP32 (xf).
-__global__ void k_prec_rev(int64_t rx1, int64_t n, int64_t rx2, const double* __restrict__ J,
+TTG_BODY(k_prec_rev)(TTG_BLOCK, int64_t rx1, int64_t n, int64_t rx2, const double* __restrict__ J,
                            const float* __restrict__ v, __nv_bfloat16* __restrict__ xb,
                            int64_t ldx, float* __restrict__ xf, const int* skip) {
   pdl_begin();
@@ -298,12 +302,14 @@ __global__ void k_prec_rev(int64_t rx1, int64_t n, int64_t rx2, const double* __
       xf[e] = float(s);
   }
 }
+TTG_KERNEL(k_prec_rev, 0);
 
 // r = b - y (FP32)
-__global__ void k_sub_f32(int64_t n, const float* b, const float* y, float* r) {
+TTG_BODY(k_sub_f32)(TTG_BLOCK, int64_t n, const float* b, const float* y, float* r) {
   pdl_begin();
   AR_LOOP(i, n) r[i] = b[i] - y[i];
 }
+TTG_KERNEL(k_sub_f32, 0);
 
 struct Gmres32 {
   Context* c;
@@ -322,7 +328,7 @@ struct Gmres32 {
     r.reset(c, sz);
     small.reset(c, size_t(m + 1) * m + 2 * m + (m + 1) + 8);
     int occ = 0;
-    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_arnoldi, AR_THREADS,
+    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_arnoldi.plain(), AR_THREADS,
                                                            arnoldi_smem()));
     if (occ < 1) occ = 1;
     int64_t want = (sz + AR_THREADS * 4 - 1) / (AR_THREADS * 4);
@@ -330,7 +336,7 @@ struct Gmres32 {
     blocks = int(std::max<int64_t>(1, std::min(want, cap)));
     part.reset(c, size_t(2) * (m + 1) * blocks);
     bar.reset(c, 4);
-    TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 4 * sizeof(unsigned), c->stream));
+    memset_async(c, bar.p(), 0, 4 * sizeof(unsigned));
     a.sz = sz;
     a.m = m;
     a.V = V.p();
@@ -353,11 +359,6 @@ struct Gmres32 {
     return sizeof(double) * (2 * (m + 2)) + sizeof(float) * AR_WARPS * (m + 1) + 16;
   }
 
-  void coop(const void* k, void** args, size_t smem) {
-    TTG_CUDA(cudaLaunchCooperativeKernel(k, dim3(blocks), dim3(AR_THREADS), args, smem,
-                                         c->stream));
-    c->launches += 1;
-  }
 
   // Right-preconditioned operand: X = bf16(P v) for the centre block-Jacobi
   // blocks J (FP64, natural layout), v in the reversed layout.
@@ -376,7 +377,7 @@ struct Gmres32 {
     a.rx2 = int(op.d.rx2);
     a.ldx = int(op.ldx);
     a.reltol = reltol;
-    TTG_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * sz, c->stream));
+    memset_async(c, x, 0, sizeof(float) * sz);
     for (int64_t it = 0; it < max_restarts; ++it) {
       const float* rr = b;
       if (it > 0) {
@@ -389,10 +390,9 @@ struct Gmres32 {
         launch(c, k_sub_f32, blocks, AR_THREADS, 0, sz, b, w.p(), r.p());
         rr = r.p();
       }
-      TTG_CUDA(cudaMemsetAsync(stop.p(), 0, 2 * sizeof(int), c->stream));
-      int first = it == 0 ? 1 : 0;
-      void* ai[] = {&a, &rr, &first};
-      coop((const void*)k_ar_init, ai, 0);
+      memset_async(c, stop.p(), 0, 2 * sizeof(int));
+      const int first = it == 0 ? 1 : 0;
+      launch(c, k_ar_init, blocks, AR_THREADS, 0, a, rr, first);
       // Steps queued in chunks; k_arnoldi (or k_ar_init, for a residual
       // already below the threshold) raises the stop flag and later queued
       // kernels return at once (see gmres.cu).  The first chunk is the step
@@ -409,19 +409,15 @@ struct Gmres32 {
       while (j < m) {
         const int jend = std::min(m, j + chunk);
         for (int jj = j; jj < jend; ++jj) {
-          int jv = jj;
+          const int jv = jj;
           seqs.push_back(c->ev_seq);
           if (J) prec_x(op, J, V.p() + int64_t(jj) * sz);  // X = bf16(P V(:, jv))
           op.apply_converted(c, w.p());  // X holds V(:, jv) (k_ar_init / k_arnoldi)
-          void* aa[] = {&a, &jv};
-          coop((const void*)k_arnoldi, aa, arnoldi_smem());
+          launch(c, k_arnoldi, blocks, AR_THREADS, arnoldi_smem(), a, jv);
         }
         queued = jend;
-        TTG_CUDA(cudaMemcpyAsync(c->h_scal, stop.p(), 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                                 c->stream));
-        sync(c);
         int flag[2];
-        memcpy(flag, c->h_scal, sizeof(flag));
+        read_device(c, flag, stop.p(), sizeof(flag));
         if (flag[0]) {
           if (flag[1] < 0) {
             at_start = true;
@@ -570,7 +566,7 @@ LocalSolveResult local_solve_mixed(Context* c, const MvDims& d, const double* Ph
 namespace {
 __global__ void k_selftest_ar_barrier(unsigned* bar, int* flag, long long limit) {
   if (blockIdx.x != 0) return;
-  ar_barrier(bar, flag, limit);
+  ar_barrier(blockIdx, gridDim, bar, flag, limit);
 }
 }  // namespace
 

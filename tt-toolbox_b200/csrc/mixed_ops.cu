@@ -28,6 +28,7 @@
 #include <map>
 #include <mutex>
 
+#include "group.cuh"
 #include "mixed_ops.h"
 #include "umma.cuh"
 
@@ -57,10 +58,14 @@ constexpr size_t umma_smem_bytes() {
   return 1024 + size_t(UM_STAGES) * (UM_A_BYTES + BN * UM_BK * 2) + (2 * UM_STAGES + 1) * 8 + 16;
 }
 
+// Body of the BF16 GEMM tile kernel; the tensor maps are passed by address
+// (kernel parameters of the plain launch, argument packs in global memory
+// in a grouped launch).
 template <int BN, bool OUT_BF16>
-__global__ void __launch_bounds__(128, 1)
-    k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                int K, int a_rows_pb, int b_rows_pb, OutMap om, int* err, const int* skip) {
+__device__ __forceinline__ void umma_body(TTG_BLOCK, const CUtensorMap* tmA,
+                                          const CUtensorMap* tmB, int K, int a_rows_pb,
+                                          int b_rows_pb, const OutMap& om, int* err,
+                                          const int* skip) {
   pdl_begin();
   using namespace umma;
   if (skip && *skip) return;  // queued Krylov step after convergence
@@ -108,8 +113,8 @@ __global__ void __launch_bounds__(128, 1)
         if (!mbar_wait(bar_empty + 8 * s, ((kb / UM_STAGES) - 1) & 1, err)) break;
       }
       mbar_expect_tx(bar_full + 8 * s, UM_A_BYTES + B_BYTES);
-      tma_load_2d(smem_u32(sA + s * UM_A_BYTES), &tmA, kb * UM_BK, arow, bar_full + 8 * s);
-      tma_load_2d(smem_u32(sB + s * B_BYTES), &tmB, kb * UM_BK, brow, bar_full + 8 * s);
+      tma_load_2d(smem_u32(sA + s * UM_A_BYTES), tmA, kb * UM_BK, arow, bar_full + 8 * s);
+      tma_load_2d(smem_u32(sB + s * B_BYTES), tmB, kb * UM_BK, brow, bar_full + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer.
@@ -172,6 +177,50 @@ __global__ void __launch_bounds__(128, 1)
     tc_fence_after();
     tmem_dealloc(tmem, TMEM_COLS);
   }
+}
+
+template <int BN, bool OUT_BF16>
+__global__ void __launch_bounds__(128, 1)
+    k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                int K, int a_rows_pb, int b_rows_pb, OutMap om, int* err, const int* skip) {
+  umma_body<BN, OUT_BF16>(blockIdx, gridDim, &tmA, &tmB, K, a_rows_pb, b_rows_pb, om, err,
+                          skip);
+}
+
+// Grouped form: the argument packs (tensor maps first, 64-byte aligned) sit
+// in global memory, written by the host-to-device copy before the launch.
+using UmmaPack = Pack<CUtensorMap, CUtensorMap, int, int, int, OutMap, int*, const int*>;
+
+template <int BN, bool OUT_BF16>
+__global__ void __launch_bounds__(128, 1) k_umma_group(GroupArgs g) {
+  uint3 b;
+  dim3 gd;
+  const uint32_t r = group_locate(g, b, gd);
+  UmmaPack& p = *reinterpret_cast<UmmaPack*>(const_cast<char*>(g.packs) + size_t(r) * g.stride);
+  // The staging buffer is reused flush after flush: take the maps as they
+  // are now, not as the tensor-map proxy may have cached them earlier.
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&pk<0>(p))
+               : "memory");
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&pk<1>(p))
+               : "memory");
+  umma_body<BN, OUT_BF16>(b, gd, &pk<0>(p), &pk<1>(p), pk<2>(p), pk<3>(p), pk<4>(p), pk<5>(p),
+                          pk<6>(p), pk<7>(p));
+}
+
+template <int BN, bool OUT_BF16>
+void umma_issue(const void* pack, dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl) {
+  issue_plain<false, CUtensorMap, CUtensorMap, int, int, int, OutMap, int*, const int*>(
+      reinterpret_cast<const void*>(&k_umma_gemm<BN, OUT_BF16>), pack, grid, block, smem, s,
+      pdl);
+}
+
+template <int BN, bool OUT_BF16>
+const GroupInfo* umma_info() {
+  static const GroupInfo gi{reinterpret_cast<const void*>(&k_umma_gemm<BN, OUT_BF16>),
+                            reinterpret_cast<const void*>(&k_umma_group<BN, OUT_BF16>), false,
+                            uint32_t(sizeof(UmmaPack)), uint32_t(alignof(UmmaPack)),
+                            &umma_issue<BN, OUT_BF16>};
+  return &gi;
 }
 
 // ---------------------------------------------------------------------------
@@ -430,7 +479,7 @@ __global__ void __launch_bounds__(FU_THREADS, 2)
 // ---------------------------------------------------------------------------
 
 // Phi2b[b + ldp*col] = Phi2[b, col], col = (be, k)  (zero padding b >= rx2)
-__global__ void k_cvt_phi2(int64_t rx2, int64_t ncols, int64_t ldp, const double* __restrict__ P,
+TTG_BODY(k_cvt_phi2)(TTG_BLOCK, int64_t rx2, int64_t ncols, int64_t ldp, const double* __restrict__ P,
                            __nv_bfloat16* __restrict__ out) {
   pdl_begin();
   const int64_t total = ldp * ncols;
@@ -440,9 +489,10 @@ __global__ void k_cvt_phi2(int64_t rx2, int64_t ncols, int64_t ldp, const double
     out[e] = __float2bfloat16_rn(b < rx2 ? float(P[b + rx2 * col]) : 0.f);
   }
 }
+TTG_KERNEL(k_cvt_phi2, 0);
 
 // AT[(m + n*be) + ld1*(al + ra1*j)] = A[al, j, m, be]
-__global__ void k_cvt_AT(int64_t ra1, int64_t n, int64_t ra2, int64_t ld1,
+TTG_BODY(k_cvt_AT)(TTG_BLOCK, int64_t ra1, int64_t n, int64_t ra2, int64_t ld1,
                          const double* __restrict__ A, __nv_bfloat16* __restrict__ out) {
   pdl_begin();
   const int64_t total = ld1 * ra1 * n;
@@ -457,9 +507,10 @@ __global__ void k_cvt_AT(int64_t ra1, int64_t n, int64_t ra2, int64_t ld1,
     out[e] = __float2bfloat16_rn(v);
   }
 }
+TTG_KERNEL(k_cvt_AT, 0);
 
 // Phi1T[(a + rx1*al) + ld2*i] = Phi1[i, a, al]
-__global__ void k_cvt_phi1(int64_t ry1, int64_t rx1, int64_t ra1, int64_t ld2,
+TTG_BODY(k_cvt_phi1)(TTG_BLOCK, int64_t ry1, int64_t rx1, int64_t ra1, int64_t ld2,
                            const double* __restrict__ P, __nv_bfloat16* __restrict__ out) {
   pdl_begin();
   const int64_t total = ld2 * ry1;
@@ -474,9 +525,10 @@ __global__ void k_cvt_phi1(int64_t ry1, int64_t rx1, int64_t ra1, int64_t ld2,
     out[e] = __float2bfloat16_rn(v);
   }
 }
+TTG_KERNEL(k_cvt_phi1, 0);
 
 // X[b + ldx*row] = v[b + rx2*row]  (row = m + n*a; zero padding)
-__global__ void k_cvt_x(int64_t rx2, int64_t rows, int64_t ldx, const float* __restrict__ v,
+TTG_BODY(k_cvt_x)(TTG_BLOCK, int64_t rx2, int64_t rows, int64_t ldx, const float* __restrict__ v,
                         __nv_bfloat16* __restrict__ out, const int* skip) {
   pdl_begin();
   if (skip && *skip) return;
@@ -487,9 +539,10 @@ __global__ void k_cvt_x(int64_t rx2, int64_t rows, int64_t ldx, const float* __r
     out[e] = __float2bfloat16_rn(b < rx2 ? v[b + rx2 * row] : 0.f);
   }
 }
+TTG_KERNEL(k_cvt_x, 0);
 
 // Natural [i, j, k] (FP64) <-> reversed [k, j, i] (FP32) vector layouts.
-__global__ void k_nat_to_rev(int64_t r1, int64_t n, int64_t r2, const double* __restrict__ x,
+TTG_BODY(k_nat_to_rev)(TTG_BLOCK, int64_t r1, int64_t n, int64_t r2, const double* __restrict__ x,
                              float* __restrict__ y, double scale) {
   pdl_begin();
   const int64_t total = r1 * n * r2;
@@ -499,8 +552,9 @@ __global__ void k_nat_to_rev(int64_t r1, int64_t n, int64_t r2, const double* __
     y[e] = float(x[i + r1 * (j + n * k)] * scale);
   }
 }
+TTG_KERNEL(k_nat_to_rev, 0);
 
-__global__ void k_rev_to_nat_add(int64_t r1, int64_t n, int64_t r2, const float* __restrict__ y,
+TTG_BODY(k_rev_to_nat_add)(TTG_BLOCK, int64_t r1, int64_t n, int64_t r2, const float* __restrict__ y,
                                  double* __restrict__ x, double scale) {
   pdl_begin();
   const int64_t total = r1 * n * r2;
@@ -510,6 +564,7 @@ __global__ void k_rev_to_nat_add(int64_t r1, int64_t n, int64_t r2, const float*
     x[e] += scale * double(y[k + r2 * (j + n * i)]);
   }
 }
+TTG_KERNEL(k_rev_to_nat_add, 0);
 
 int blocks_for(Context* c, int64_t n) {
   int64_t b = (n + 255) / 256;
@@ -552,6 +607,15 @@ void launch_bn(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t
   const size_t smem = umma_smem_bytes<BN>();
   ensure_smem_attr(reinterpret_cast<const void*>(k_umma_gemm<BN, OB>), c->device, int(smem));
   dim3 grid{unsigned((M + UM_BM - 1) / UM_BM), unsigned((N + BN - 1) / BN), unsigned(batch)};
+  if (c->rec) {  // grouped batch: one record of the grouped GEMM
+    UmmaPack p{};
+    fill_pack(p, std::index_sequence_for<CUtensorMap, CUtensorMap, int, int, int, OutMap, int*,
+                                         const int*>{},
+              ta, tb, int(K), int(a_rows_pb), int(b_rows_pb), om, c->d_err + 1, c->skip);
+    rec_group(c->rec, umma_info<BN, OB>(), grid, 128, smem, &p);
+    c->launches += 1;
+    return;
+  }
   launch(c, k_umma_gemm<BN, OB>, grid, 128, smem, ta, tb, int(K), int(a_rows_pb),
          int(b_rows_pb), om, c->d_err + 1, c->skip);
   TTG_CHECK_LAUNCH();
@@ -618,8 +682,7 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
   X.reset(c, ldx * d.m * d.rx1);
   // Padding columns (b >= rx2) must read as zero: the Krylov kernels write
   // only the valid part of X.
-  if (ldx != d.rx2)
-    TTG_CUDA(cudaMemsetAsync(X.p(), 0, sizeof(__nv_bfloat16) * X.size(), c->stream));
+  if (ldx != d.rx2) memset_async(c, X.p(), 0, sizeof(__nv_bfloat16) * X.size());
   T1.reset(c, ld1 * d.rx1 * d.ry2);
   T2.reset(c, ld2 * d.ry2 * d.n);
   launch(c, k_cvt_phi2, blocks_for(c, phi2b.size()), 256, 0, d.rx2, d.ra2 * d.ry2, ldx, Phi2,
@@ -631,7 +694,7 @@ void MixedOp::prepare(Context* c, const MvDims& dd, const double* Phi1, const do
   make_map(&mapX, X.p(), d.rx2, d.m * d.rx1, ldx, UM_BM);
   make_map(&mapT1, T1.p(), d.n * d.ra2, d.rx1 * d.ry2, ld1, UM_BM);
   make_map(&mapT2, T2.p(), d.rx1 * d.ra1, d.ry2 * d.n, ld2, UM_BM);
-  if (fused_enabled()) {
+  if (fused_enabled() && !c->rec) {  // a grouped batch takes the three-launch form
     prepare_fused(c);
     return;
   }
@@ -717,6 +780,7 @@ int MixedOp::tuned_bn(Context* c, int stage) {
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) return it->second;
   }
+  if (c->rec) return fallback;  // recorded stream work cannot be timed
   DBuf<float> ysc;
   if (stage == 3) ysc.reset(c, d.ry2 * d.n * d.ry1);
   float best_ms = 1e30f;
@@ -840,7 +904,7 @@ void MixedOp::stages(Context* c, float* y) {
 namespace {
 // out[kk + ldk * row] = bf16(src(row, kk)), zero for kk >= K, with
 // src(row, kk) = src[row + ld * kk] (trans = 0) or src[kk + ld * row] (1).
-__global__ void k_cvt_kmajor(int64_t rows, int64_t K, int64_t ldk, const double* __restrict__ src,
+TTG_BODY(k_cvt_kmajor)(TTG_BLOCK, int64_t rows, int64_t K, int64_t ldk, const double* __restrict__ src,
                              int64_t ld, int trans, __nv_bfloat16* __restrict__ out) {
   pdl_begin();
   const int64_t total = rows * ldk;
@@ -852,15 +916,17 @@ __global__ void k_cvt_kmajor(int64_t rows, int64_t K, int64_t ldk, const double*
     out[e] = __float2bfloat16_rn(v);
   }
 }
+TTG_KERNEL(k_cvt_kmajor, 0);
 
 // C[m + ldc n] = Cf[m + M n] (FP32 -> FP64)
-__global__ void k_f32_to_f64(int64_t M, int64_t N, const float* __restrict__ Cf,
+TTG_BODY(k_f32_to_f64)(TTG_BLOCK, int64_t M, int64_t N, const float* __restrict__ Cf,
                              double* __restrict__ C, int64_t ldc) {
   pdl_begin();
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < M * N;
        e += int64_t(gridDim.x) * blockDim.x)
     C[(e % M) + ldc * (e / M)] = double(Cf[e]);
 }
+TTG_KERNEL(k_f32_to_f64, 0);
 }  // namespace
 
 void gemm_bf16(Context* c, bool tA, bool tB, int64_t M, int64_t N, int64_t K, const double* A,

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdlib>
 
+#include "group.cuh"
 #include "small_dense.h"
 
 namespace ttg {
@@ -85,7 +86,7 @@ __device__ void jacobi_finish(int n, const double* A, const double* V, double* _
 // A: n x n (column-major, lda) input; U (n x n, ld n), S (n), VT (n x n, ld n)
 // outputs.  work: n*n doubles of global scratch used when A does not fit in
 // shared memory.  Status: *err = 5 if the sweep limit is reached.
-__global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* __restrict__ Ain,
+TTG_BODY(k_jacobi_svd)(TTG_BLOCK, int n, const double* __restrict__ Ain,
                                                           int lda, double* __restrict__ U,
                                                           double* __restrict__ S,
                                                           double* __restrict__ VT,
@@ -171,6 +172,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
   if (tid == 0 && sweep >= max_sweeps) atomicExch(err, 5);
   jacobi_finish(n, A, V, U, S, VT, work + int64_t(n) * n, trans);
 }
+TTG_KERNEL(k_jacobi_svd, SD_THREADS);
 
 
 // ---------------------------------------------------------------------------
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_jacobi_svd(int n, const double* 
 constexpr int JC_THREADS = 256;
 constexpr long long JC_SPIN_LIMIT = 1LL << 24;
 
-__device__ void jc_barrier(unsigned* bar, int* err, long long limit = JC_SPIN_LIMIT) {
+__device__ void jc_barrier(TTG_BLOCK, unsigned* bar, int* err, long long limit = JC_SPIN_LIMIT) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = bar + 1;
@@ -214,7 +216,7 @@ __device__ void jc_barrier(unsigned* bar, int* err, long long limit = JC_SPIN_LI
 // A (n x n work copy, ld n) and V (n x n) in global memory; offmax: three
 // u64 slots holding the per-sweep maximum off-diagonal measure (bit pattern
 // of a non-negative double).  *sweeps_out = sweeps run.
-__global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double* __restrict__ Ain,
+TTG_BODY(k_jacobi_coop)(TTG_BLOCK, int n, const double* __restrict__ Ain,
                                                            int lda, double* A, double* V,
                                                            unsigned* bar,
                                                            unsigned long long* offmax, int* err,
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
     V[e] = (i == j) ? 1.0 : 0.0;
   }
   if (blockIdx.x == 0 && tid < 3) offmax[tid] = 0ull;
-  jc_barrier(bar, err);
+  jc_barrier(blockIdx, gridDim, bar, err);
   const int ne = (n + 1) & ~1;
   const double tol = 4.0 * 2.220446049250313e-16;
   int sweep = 0;
@@ -303,16 +305,17 @@ __global__ void __launch_bounds__(JC_THREADS) k_jacobi_coop(int n, const double*
         }
         __syncthreads();
       }
-      jc_barrier(bar, err);
+      jc_barrier(blockIdx, gridDim, bar, err);
     }
     if (tid == 0) atomicMax(offmax + slot, (unsigned long long)__double_as_longlong(off));
-    jc_barrier(bar, err);
+    jc_barrier(blockIdx, gridDim, bar, err);
     const double m = __longlong_as_double((long long)(*(volatile unsigned long long*)(offmax + slot)));
     if (m <= tol) break;
     if (*(volatile int*)err) break;
   }
   if (blockIdx.x == 0 && tid == 0 && sweep >= max_sweeps) atomicExch(sweep_err, 5);
 }
+TTG_COOP_KERNEL(k_jacobi_coop, JC_THREADS);
 
 // ---------------------------------------------------------------------------
 // Block-cyclic form of the grid-wide Jacobi SVD: the n columns fall into
@@ -329,7 +332,7 @@ constexpr int JB_W = 8;
 constexpr int JB_THREADS = 256;
 constexpr int JB_WARPS = JB_THREADS / 32;
 
-__global__ void __launch_bounds__(JB_THREADS) k_jacobi_block(int n, const double* __restrict__ Ain,
+TTG_BODY(k_jacobi_block)(TTG_BLOCK, int n, const double* __restrict__ Ain,
                                                             int lda, double* A, double* V,
                                                             unsigned* bar,
                                                             unsigned long long* offmax, int* err,
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(JB_THREADS) k_jacobi_block(int n, const double
     V[e] = (i == j) ? 1.0 : 0.0;
   }
   if (blockIdx.x == 0 && tid < 3) offmax[tid] = 0ull;
-  jc_barrier(bar, err);
+  jc_barrier(blockIdx, gridDim, bar, err);
   double* sA = sjb;
   double* sV = sjb + int64_t(2 * JB_W) * n;
   const int nb = (n + JB_W - 1) / JB_W;
@@ -428,7 +431,7 @@ __global__ void __launch_bounds__(JB_THREADS) k_jacobi_block(int n, const double
         }
         __syncthreads();
       }
-      jc_barrier(bar, err);
+      jc_barrier(blockIdx, gridDim, bar, err);
     }
     if (lane == 0) s_off[warp] = off;
     __syncthreads();
@@ -437,25 +440,27 @@ __global__ void __launch_bounds__(JB_THREADS) k_jacobi_block(int n, const double
       for (int w = 0; w < JB_WARPS; ++w) m = fmax(m, s_off[w]);
       atomicMax(offmax + slot, (unsigned long long)__double_as_longlong(m));
     }
-    jc_barrier(bar, err);
+    jc_barrier(blockIdx, gridDim, bar, err);
     const double m = __longlong_as_double((long long)(*(volatile unsigned long long*)(offmax + slot)));
     if (m <= tol) break;
     if (*(volatile int*)err) break;
   }
   if (blockIdx.x == 0 && tid == 0 && sweep >= max_sweeps) atomicExch(sweep_err, 5);
 }
+TTG_COOP_KERNEL(k_jacobi_block, JB_THREADS);
 
-__global__ void __launch_bounds__(SD_THREADS) k_jacobi_finish(int n, const double* A,
+TTG_BODY(k_jacobi_finish)(TTG_BLOCK, int n, const double* A,
                                                              const double* V, double* U,
                                                              double* S, double* VT, double* sig,
                                                              int trans) {
   pdl_begin();
   jacobi_finish(n, A, V, U, S, VT, sig, trans);
 }
+TTG_KERNEL(k_jacobi_finish, SD_THREADS);
 
 // Householder QR of the m x n matrix A (column-major, lda) held in shared
 // memory: Q (m x k, ld m), R (k x n, ld k), k = min(m, n).
-__global__ void __launch_bounds__(SD_THREADS) k_house_qr(int m, int n, const double* __restrict__ Ain,
+TTG_BODY(k_house_qr)(TTG_BLOCK, int m, int n, const double* __restrict__ Ain,
                                                         int lda, double* __restrict__ Q,
                                                         double* __restrict__ R,
                                                         const int* skip) {
@@ -539,6 +544,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_house_qr(int m, int n, const dou
     __syncthreads();
   }
 }
+TTG_KERNEL(k_house_qr, SD_THREADS);
 
 
 // ---------------------------------------------------------------------------
@@ -571,7 +577,7 @@ __device__ void block_sums(const double* v, int cnt, double* scratch, double* ou
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(SD_THREADS) k_house_qr_skinny(int64_t m, int n,
+TTG_BODY(k_house_qr_skinny)(TTG_BLOCK, int64_t m, int n,
                                                                const double* __restrict__ Ain,
                                                                int64_t lda, double* __restrict__ W,
                                                                double* __restrict__ Q,
@@ -654,6 +660,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_house_qr_skinny(int64_t m, int n
     __syncthreads();
   }
 }
+TTG_KERNEL(k_house_qr_skinny, SD_THREADS);
 
 // ---------------------------------------------------------------------------
 // Cholesky factor and its inverse for shifted Cholesky QR
@@ -662,7 +669,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_house_qr_skinny(int64_t m, int n
 // G (n x n SPD Gram matrix, ldg) -> R = chol(G + shift I) upper (R' R = G +
 // shift I) and Rinv = R^{-1}, both n x n with leading dimension n.  shift =
 // shift_factor * trace(G).  err_slot |= 1 if a pivot is not positive.
-__global__ void __launch_bounds__(SD_THREADS) k_chol_inv(int n, const double* __restrict__ G,
+TTG_BODY(k_chol_inv)(TTG_BLOCK, int n, const double* __restrict__ G,
                                                         int ldg, double shift_factor,
                                                         double* __restrict__ R,
                                                         double* __restrict__ Rinv, int* err) {
@@ -720,6 +727,7 @@ __global__ void __launch_bounds__(SD_THREADS) k_chol_inv(int n, const double* __
   }
   if (tid == 0 && s_bad) atomicOr(err, 1);
 }
+TTG_KERNEL(k_chol_inv, SD_THREADS);
 
 
 // ---------------------------------------------------------------------------
@@ -737,7 +745,7 @@ constexpr int TS_THREADS = 256;
 constexpr int TS_WARPS = TS_THREADS / 32;
 constexpr int TS_MAX_N = 8;
 
-__global__ void __launch_bounds__(TS_THREADS) k_svd_tall_small(int m, int n,
+TTG_BODY(k_svd_tall_small)(TTG_BLOCK, int m, int n,
                                                               const double* __restrict__ Ain,
                                                               int lda, double* __restrict__ U,
                                                               double* __restrict__ S,
@@ -877,8 +885,121 @@ __global__ void __launch_bounds__(TS_THREADS) k_svd_tall_small(int m, int n,
   }
   if (tid < n) S[pos[tid]] = sig[tid];
 }
+TTG_KERNEL(k_svd_tall_small, TS_THREADS);
+
+// ---------------------------------------------------------------------------
+// LU with partial pivoting and the two triangular solves (LAPACK getf2 +
+// getrs, unblocked) of an n x n matrix held in shared memory, for the dense
+// local systems of AMEn (n < max_full_size): X <- B^{-1} X for nrhs
+// right-hand sides.  The pivot is the first entry of largest magnitude in
+// its column (idamax); the multipliers are formed with the pivot's
+// reciprocal; the row swaps and the unit-lower elimination are applied to X
+// as the factorization proceeds, then X is solved with the upper factor
+// column by column.  *err |= 1 on an exactly zero pivot (getrf's info > 0).
+// ---------------------------------------------------------------------------
+
+TTG_BODY(k_lu_small)(TTG_BLOCK, int n, const double* __restrict__ B, int nrhs,
+                     double* __restrict__ X, int* err) {
+  pdl_begin();
+  extern __shared__ double slu[];
+  double* a = slu;             // n x n, column-major
+  double* x = slu + n * n;     // n x nrhs
+  __shared__ int s_piv, s_bad;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < n * n; e += blockDim.x) a[e] = B[e];
+  for (int e = tid; e < n * nrhs; e += blockDim.x) x[e] = X[e];
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (tid < 32) {  // idamax over rows k..n-1 of column k
+      double best = -1.0;
+      int bi = k;
+      for (int i = k + tid; i < n; i += 32) {
+        const double v = fabs(a[i + n * k]);
+        if (v > best) {
+          best = v;
+          bi = i;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (tid == 0) {
+        s_piv = bi;
+        if (!(best > 0.0)) s_bad = 1;
+      }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != k) {
+      for (int j = tid; j < n; j += blockDim.x) {
+        const double t = a[k + n * j];
+        a[k + n * j] = a[p + n * j];
+        a[p + n * j] = t;
+      }
+      for (int r = tid; r < nrhs; r += blockDim.x) {
+        const double t = x[k + n * r];
+        x[k + n * r] = x[p + n * r];
+        x[p + n * r] = t;
+      }
+    }
+    __syncthreads();
+    const double piv = a[k + n * k];
+    if (piv != 0.0) {
+      const double rinv = 1.0 / piv;
+      for (int i = k + 1 + tid; i < n; i += blockDim.x) a[i + n * k] *= rinv;
+    }
+    __syncthreads();
+    const int rows = n - k - 1;
+    if (rows > 0) {
+      const int tot = rows * (n - k - 1 + nrhs);
+      for (int e = tid; e < tot; e += blockDim.x) {
+        const int i = k + 1 + e % rows, c = e / rows;
+        const double l = a[i + n * k];
+        if (c < n - k - 1) {
+          const int j = k + 1 + c;
+          a[i + n * j] -= l * a[k + n * j];
+        } else {
+          const int r = c - (n - k - 1);
+          x[i + n * r] -= l * x[k + n * r];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    for (int r = tid; r < nrhs; r += blockDim.x) x[k + n * r] /= a[k + n * k];
+    __syncthreads();
+    for (int e = tid; e < k * nrhs; e += blockDim.x) {
+      const int i = e % k, r = e / k;
+      x[i + n * r] -= x[k + n * r] * a[i + n * k];
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < n * nrhs; e += blockDim.x) X[e] = x[e];
+  if (tid == 0 && s_bad) atomicOr(err, 1);
+}
+TTG_KERNEL(k_lu_small, SD_THREADS);
 
 }  // namespace
+
+bool lu_small_fits(int64_t n, int64_t nrhs) {
+  return n >= 1 && nrhs >= 1 && sizeof(double) * size_t(n) * size_t(n + nrhs) <= SMEM_LIMIT;
+}
+
+void lu_small_f64(Context* c, int64_t n, const double* B, double* X, int64_t nrhs) {
+  TTG_REQUIRE(lu_small_fits(n, nrhs), "lu_small: n = %lld, nrhs = %lld out of range",
+              (long long)n, (long long)nrhs);
+  const size_t smem = sizeof(double) * size_t(n) * size_t(n + nrhs);
+  ensure_smem_attr(k_lu_small.fn(), c->device, int(SMEM_LIMIT + 1024));
+  launch(c, k_lu_small, 1, SD_THREADS, smem, int(n), B, int(nrhs), X, c->d_err + 4);
+  TTG_CHECK_LAUNCH();
+}
 
 bool chol_inv_fits(int64_t n) { return 2 * n * n * int64_t(sizeof(double)) <= int64_t(SMEM_LIMIT); }
 
@@ -886,7 +1007,7 @@ void chol_inv_f64(Context* c, int64_t n, const double* G, int64_t ldg, double sh
                   double* R, double* Rinv, int* flag) {
   TTG_REQUIRE(chol_inv_fits(n), "chol_inv: n = %lld too large", (long long)n);
   const size_t smem = 2 * sizeof(double) * size_t(n * n);
-  ensure_smem_attr(reinterpret_cast<const void*>(k_chol_inv), c->device, int(SMEM_LIMIT + 1024));
+  ensure_smem_attr(k_chol_inv.fn(), c->device, int(SMEM_LIMIT + 1024));
   launch(c, k_chol_inv, 1, SD_THREADS, smem, int(n), G, int(ldg), shift_factor, R, Rinv,
          flag ? flag : c->d_err + 4);
   TTG_CHECK_LAUNCH();
@@ -910,7 +1031,7 @@ bool small_qr_fits(int64_t m, int64_t n) {
 void small_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t lda, double* Q,
                   double* R) {
   const size_t smem = sizeof(double) * size_t(m * n + std::min(m, n));
-  ensure_smem_attr(reinterpret_cast<const void*>(k_house_qr), c->device, int(SMEM_LIMIT + 1024));
+  ensure_smem_attr(k_house_qr.fn(), c->device, int(SMEM_LIMIT + 1024));
   launch(c, k_house_qr, 1, SD_THREADS, smem, int(m), int(n), A, int(lda), Q, R, c->skip);
   TTG_CHECK_LAUNCH();
 }
@@ -925,7 +1046,7 @@ void svd_tall_small_f64(Context* c, int64_t m, int64_t n, const double* A, int64
   TTG_REQUIRE(svd_tall_small_fits(m, n), "svd_tall_small: %lld x %lld out of range",
               (long long)m, (long long)n);
   const size_t smem = sizeof(double) * size_t(m * n);
-  ensure_smem_attr(reinterpret_cast<const void*>(k_svd_tall_small), c->device,
+  ensure_smem_attr(k_svd_tall_small.fn(), c->device,
                    int(128 * 1024 + 1024));
   launch(c, k_svd_tall_small, 1, TS_THREADS, smem, int(m), int(n), A, int(lda), U, S, VT,
          c->d_err + 3, c->jacobi_max_sweeps);
@@ -956,61 +1077,42 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
   if (mode == 0 && jacobi_block_fits(n)) {
     // Block-cyclic grid-wide rounds: one CTA per block pair.
     const size_t bsm = sizeof(double) * 4 * JB_W * size_t(n);
-    ensure_smem_attr(reinterpret_cast<const void*>(k_jacobi_block), c->device, int(bsm));
+    ensure_smem_attr(k_jacobi_block.fn(), c->device, int(bsm));
     int occ = 0;
-    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_block, JB_THREADS,
-                                                           bsm));
+    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_block.plain(),
+                                                           JB_THREADS, bsm));
     const int64_t bpairs = ((n + JB_W - 1) / JB_W + 1) / 2;
     const int blocks = int(std::max<int64_t>(
         1, std::min<int64_t>(bpairs, int64_t(c->num_sms) * std::max(occ, 1))));
     DBuf<unsigned> bar(c, 2);
     DBuf<unsigned long long> offmax(c, 3);
-    TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 2 * sizeof(unsigned), c->stream));
-    int ni = int(n), ldi = int(lda);
-    double* Aw = work.p();
-    double* Vp = V.p();
-    unsigned* barp = bar.p();
-    unsigned long long* offp = offmax.p();
-    int* errp = c->d_err + 0;
-    int* swp = c->d_err + 3;
-    int msw = c->jacobi_max_sweeps;
-    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp, &trans, &msw};
-    TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_jacobi_block, dim3(blocks),
-                                         dim3(JB_THREADS), args, bsm, c->stream));
+    memset_async(c, bar.p(), 0, 2 * sizeof(unsigned));
+    launch(c, k_jacobi_block, blocks, JB_THREADS, bsm, int(n), A, int(lda), work.p(), V.p(),
+           bar.p(), offmax.p(), c->d_err + 0, c->d_err + 3, trans, c->jacobi_max_sweeps);
     launch(c, k_jacobi_finish, 1, SD_THREADS, 0, int(n), work.p(), V.p(), U, S, VT,
            work.p() + int64_t(n) * n, trans);
-    c->launches += 1;  // the cooperative sweep kernel
     TTG_CHECK_LAUNCH();
     return;
   }
   if (mode != 2) {
     // Grid-wide rounds: one CTA per column pair (up to what fits at once).
     int occ = 0;
-    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_coop, JC_THREADS, 0));
+    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_coop.plain(),
+                                                           JC_THREADS, 0));
     const int64_t pairs = (n + 1) / 2;
     const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(pairs,
                                                                   int64_t(c->num_sms) * occ)));
     DBuf<unsigned> bar(c, 2);
     DBuf<unsigned long long> offmax(c, 3);
-    TTG_CUDA(cudaMemsetAsync(bar.p(), 0, 2 * sizeof(unsigned), c->stream));
-    int ni = int(n), ldi = int(lda);
-    double* Aw = work.p();
-    double* Vp = V.p();
-    unsigned* barp = bar.p();
-    unsigned long long* offp = offmax.p();
-    int* errp = c->d_err + 0;
-    int* swp = c->d_err + 3;
-    int msw = c->jacobi_max_sweeps;
-    void* args[] = {&ni, &A, &ldi, &Aw, &Vp, &barp, &offp, &errp, &swp, &trans, &msw};
-    TTG_CUDA(cudaLaunchCooperativeKernel((const void*)k_jacobi_coop, dim3(blocks),
-                                         dim3(JC_THREADS), args, 0, c->stream));
+    memset_async(c, bar.p(), 0, 2 * sizeof(unsigned));
+    launch(c, k_jacobi_coop, blocks, JC_THREADS, 0, int(n), A, int(lda), work.p(), V.p(),
+           bar.p(), offmax.p(), c->d_err + 0, c->d_err + 3, trans, c->jacobi_max_sweeps);
     launch(c, k_jacobi_finish, 1, SD_THREADS, 0, int(n), work.p(), V.p(), U, S, VT,
            work.p() + int64_t(n) * n, trans);
-    c->launches += 1;  // the cooperative sweep kernel
     TTG_CHECK_LAUNCH();
     return;
   }
-  ensure_smem_attr(reinterpret_cast<const void*>(k_jacobi_svd), c->device,
+  ensure_smem_attr(k_jacobi_svd.fn(), c->device,
                    int(SMEM_LIMIT + 1024));
   const size_t smem = size_t(mode) * mat;
   launch(c, k_jacobi_svd, 1, SD_THREADS, smem, int(n), A, int(lda), U, S, VT, V.p(), work.p(),
@@ -1021,7 +1123,7 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
 namespace {
 __global__ void k_selftest_jc_barrier(unsigned* bar, int* flag, long long limit) {
   if (blockIdx.x != 0) return;
-  jc_barrier(bar, flag, limit);
+  jc_barrier(blockIdx, gridDim, bar, flag, limit);
 }
 }  // namespace
 

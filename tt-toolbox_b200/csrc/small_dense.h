@@ -19,6 +19,10 @@ void skinny_qr_f64(Context* c, int64_t m, int64_t n, const double* A, int64_t ld
 // R' R = G + shift_factor * trace(G) * I, Rinv = R^{-1} (n x n, ld n, upper).
 // A non-positive pivot sets *flag (nullptr: the context's factorization
 // error slot).
+// X <- B^{-1} X (n x n B, n x nrhs X, column-major) by one-CTA LU with
+// partial pivoting; an exactly zero pivot sets error slot 4.
+bool lu_small_fits(int64_t n, int64_t nrhs);
+void lu_small_f64(Context* c, int64_t n, const double* B, double* X, int64_t nrhs);
 bool chol_inv_fits(int64_t n);
 void chol_inv_f64(Context* c, int64_t n, const double* G, int64_t ldg, double shift_factor,
                   double* R, double* Rinv, int* flag = nullptr);

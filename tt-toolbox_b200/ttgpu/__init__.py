@@ -84,6 +84,16 @@ class AmenStats(C.Structure):
                     trace_len=int(self.trace_len), gbyte_lp=float(self.gbyte_lp))
 
 
+class GroupStats(C.Structure):
+    _fields_ = [("flushes", _i64), ("launches", _i64), ("records", _i64),
+                ("grouped_records", _i64), ("ms_plan", C.c_double),
+                ("ms_issue_wait", C.c_double), ("ms_total", C.c_double)]
+
+    def to_dict(self):
+        return {k: (float(getattr(self, k)) if k.startswith("ms") else int(getattr(self, k)))
+                for k, _ in self._fields_}
+
+
 class AmenMvOpts(C.Structure):
     _fields_ = [("nswp", _i64), ("kickrank", _i64), ("init_qr", C.c_int32),
                 ("verb", C.c_int32), ("seed", C.c_uint64), ("reserved", _i64 * 4)]
@@ -156,6 +166,10 @@ def lib():
                                     C.POINTER(AmenOpts), C.POINTER(_vp), C.POINTER(_vp),
                                     C.c_int32, C.POINTER(_vp), C.POINTER(AmenStats),
                                     C.POINTER(C.c_int32)]
+    sigs["ttg_amen_solve_grouped"] = [_vp, _i64, C.POINTER(_vp), C.POINTER(_vp), _pd,
+                                      C.POINTER(AmenOpts), C.POINTER(_vp), C.POINTER(_vp),
+                                      C.c_int32, C.POINTER(_vp), C.POINTER(AmenStats),
+                                      C.POINTER(C.c_int32), C.POINTER(GroupStats)]
     sigs["ttg_grad_xb"] = [_vp, _vp, _vp, _pd]
     sigs["ttg_grad_sampled"] = [_vp, _i64, _vp, _vp, _vp, _pd]
     sigs["ttg_context_set_option"] = [_vp, C.c_int32, _i64]
@@ -283,6 +297,7 @@ class Context:
 
     # ttg_context_set_option keys
     OPT_JACOBI_MAX_SWEEPS = 1
+    OPT_GROUP_SMS = 2
 
     def set_option(self, key, value):
         """``ttg_context_set_option`` (e.g. the Jacobi SVD sweep limit)."""
@@ -547,9 +562,13 @@ def amen_solve2(A, y, tol, ctx=None, stats=None, trace=None, **opts):
 
 
 def amen_solve2_batch(As, ys, tol, x0s=None, z0s=None, workers=0, ctx=None, stats=None,
-                      per_system=None, **opts):
+                      per_system=None, grouped=False, group_stats=None, **opts):
     """Batched ``amen_solve2`` (``ttg_amen_solve_batch``): solves
     ``As[i] x = ys[i]`` for every i, concurrently on one device.
+
+    ``grouped=True`` runs the grouped batch (``ttg_amen_solve_grouped``):
+    ``workers`` is then the number of systems in flight (0: all), and
+    ``group_stats`` (optional dict) receives the executor's counters.
 
     ``tol``: scalar or one per system; ``opts``: options shared by all
     systems; ``per_system``: optional list of option dicts merged over
@@ -595,10 +614,20 @@ def amen_solve2_batch(As, ys, tol, x0s=None, z0s=None, workers=0, ctx=None, stat
     st = (AmenStats * max(count, 1))()
     status = (C.c_int32 * max(count, 1))()
     try:
-        code = lib().ttg_amen_solve_batch(ctx.h, count, HA, HY, _ptrd(tols), olist,
-                                          HX0 if x0s is not None else None,
-                                          HZ0 if z0s is not None else None, int(workers), out,
-                                          st, status)
+        if grouped:
+            gs = GroupStats()
+            code = lib().ttg_amen_solve_grouped(ctx.h, count, HA, HY, _ptrd(tols), olist,
+                                                HX0 if x0s is not None else None,
+                                                HZ0 if z0s is not None else None, int(workers),
+                                                out, st, status, C.byref(gs))
+            if group_stats is not None:
+                group_stats.clear()
+                group_stats.update(gs.to_dict())
+        else:
+            code = lib().ttg_amen_solve_batch(ctx.h, count, HA, HY, _ptrd(tols), olist,
+                                              HX0 if x0s is not None else None,
+                                              HZ0 if z0s is not None else None, int(workers),
+                                              out, st, status)
         msg = lib().ttg_last_error().decode(errors="replace") if code else ""
         res = []
         for i in range(count):

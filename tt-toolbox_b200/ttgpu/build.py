@@ -18,7 +18,12 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+# -fmad=false: no contraction of separate multiplies and adds into FMAs, so
+# a kernel body computes bit-identical results in every instantiation (its
+# plain launch and the grouped launch of a grouped batch); FMAs the code
+# wants are written as fma().
+CFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
+          "--expt-relaxed-constexpr",
           "-Xcompiler", "-Wall", "-Xcompiler", "-Wno-unused-function"]
 LIBS = ["-lcusolver", "-lcublas", "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")]
 
@@ -48,9 +53,26 @@ def _compile(src, extra, verbose):
     return obj
 
 
+def _flags_changed(extra):
+    """True (and the stamp rewritten) when the compile flags differ from the
+    ones the objects in _build/ were made with."""
+    stamp = os.path.join(BUILD, "flags.txt")
+    now = " ".join(ARCH + CFLAGS + list(extra))
+    old = open(stamp).read() if os.path.exists(stamp) else None
+    if old != now:
+        with open(stamp, "w") as f:
+            f.write(now)
+        return True
+    return False
+
+
 def build(verbose=False, extra=()):
     """Compile every ``csrc/*.cu`` for sm_100a and link ``libttgpu.so``."""
     os.makedirs(BUILD, exist_ok=True)
+    if _flags_changed(extra):
+        for f in os.listdir(BUILD):
+            if f.endswith(".o"):
+                os.remove(os.path.join(BUILD, f))
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, list(extra), verbose), srcs))
