@@ -33,8 +33,14 @@ def test_every_pdl_launched_kernel_waits_first():
         m = re.search(r"__global__ void[^;{]*?\b%s\s*\([^{]*\{\n(.*)\n" % re.escape(name), allsrc)
         if m is None:  # a TTG_BODY kernel (group.cuh)
             m = re.search(r"TTG_BODY\(%s\)\s*\([^{]*\{\n(.*)\n" % re.escape(name), allsrc)
-        if m is None or m.group(1).strip() != "pdl_begin();":
-            bad.append((name, None if m is None else m.group(1).strip()))
+        first = None if m is None else m.group(1).strip()
+        call = re.match(r"(\w+)(?:<[^>]*>)?\(", first or "")
+        if call and first != "pdl_begin();":  # a wrapper: the callee must wait first
+            d = re.search(r"__device__[^;{]*?\b%s\s*\([^{]*\{\n(.*)\n" % re.escape(call.group(1)),
+                          allsrc)
+            first = None if d is None else d.group(1).strip()
+        if first != "pdl_begin();":
+            bad.append((name, first))
     assert not bad, "kernels launched with launch() that do not start with pdl_begin(): %r" % bad
 
 
