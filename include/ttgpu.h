@@ -362,6 +362,11 @@ typedef struct {
   double ms_plan;           /* host time merging records and writing argument packs */
   double ms_issue_wait;     /* host time issuing and waiting for the device */
   double ms_total;          /* wall time of the call */
+  int64_t lanes_max;        /* most streams one flush issued on */
+  double ms_record;         /* wall time the solves spent recording between flushes */
+  int64_t allocs;           /* device blocks the solves took from the shared allocator */
+  int64_t device_mallocs;   /* of which new cudaMalloc blocks */
+  double ms_alloc;          /* thread time in the shared allocator (lock waits included) */
 } ttg_group_stats;
 
 /* Grouped batch: the same solves as ttg_amen_solve_batch (same arguments,

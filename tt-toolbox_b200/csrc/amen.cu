@@ -172,7 +172,7 @@ void dense_residual_dev(Context* c, int64_t N, const double* B, const double* x,
 // Free a TT handle whose core the context's recorded work may still use.
 void release_tt(Context* c, ttg_tt_s* t) {
   if (c->rec) {
-    rec_free(c->rec, t->core);
+    rec_free(c->rec, t->core, sizeof(double) * size_t(t->numel));
     delete t;
   } else {
     ttg_tt_free(t);

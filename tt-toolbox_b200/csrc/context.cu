@@ -1,8 +1,11 @@
 // Context, caching allocator, error reporting and TT handles of libttgpu.
+#include <atomic>
+#include <chrono>
 #include <cstdlib>
 #include <cstdarg>
 #include <cstring>
 #include <mutex>
+#include <tuple>
 
 #include "internal.h"
 
@@ -42,8 +45,18 @@ size_t Allocator::size_class(size_t bytes) {
 }
 
 void* Allocator::get(size_t bytes) {
+  const auto t0 = std::chrono::steady_clock::now();
+  struct Clock {  // time spent here, lock wait included
+    std::atomic<uint64_t>& ns;
+    std::chrono::steady_clock::time_point t0;
+    ~Clock() {
+      ns += uint64_t(std::chrono::duration_cast<std::chrono::nanoseconds>(
+                         std::chrono::steady_clock::now() - t0).count());
+    }
+  } clock{ns_get_, t0};
   std::lock_guard<std::mutex> lock(mu_);
   size_t cls = size_class(bytes);
+  ++n_get_;
   auto it = free_.find(cls);
   void* p = nullptr;
   if (it != free_.end() && !it->second.empty()) {
@@ -51,6 +64,7 @@ void* Allocator::get(size_t bytes) {
     it->second.pop_back();
     cached_ -= cls;
   } else {
+    ++n_malloc_;
     cudaError_t e = cudaMalloc(&p, cls);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -136,13 +150,34 @@ void context_release(Context& c) {
 }
 
 void ensure_smem_attr(const void* func, int device, int bytes) {
-  static std::mutex mu;
-  static std::map<std::pair<const void*, int>, int> done;
-  std::lock_guard<std::mutex> lock(mu);
-  auto it = done.find({func, device});
-  if (it != done.end() && it->second >= bytes) return;
-  TTG_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  done[{func, device}] = bytes;
+  // Per-thread memo in front of the shared one: the grouped batch calls this
+  // from many fibers on a few threads.
+  thread_local std::map<std::pair<const void*, int>, int> seen;
+  auto it = seen.find({func, device});
+  if (it != seen.end() && it->second >= bytes) return;
+  {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    auto d = done.find({func, device});
+    if (d == done.end() || d->second < bytes) {
+      TTG_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      done[{func, device}] = bytes;
+    }
+  }
+  seen[{func, device}] = bytes;
+}
+
+int max_active_blocks(const void* func, int threads, size_t smem) {
+  using Key = std::tuple<const void*, int, size_t>;
+  thread_local std::map<Key, int> seen;
+  const Key k{func, threads, smem};
+  auto it = seen.find(k);
+  if (it != seen.end()) return it->second;
+  int occ = 0;
+  TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, func, threads, smem));
+  seen[k] = occ;
+  return occ;
 }
 
 void read_device(Context* c, void* h, const void* d, size_t bytes) {

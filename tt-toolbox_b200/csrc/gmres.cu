@@ -278,7 +278,7 @@ TTG_COOP_KERNEL(k_hh_correct, HH_THREADS);
 
 int coop_blocks(Context* c, const void* kernel, size_t smem, int64_t sz) {
   int occ = 0;
-  TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, HH_THREADS, smem));
+  occ = max_active_blocks(kernel, HH_THREADS, smem);
   if (occ < 1) occ = 1;
   int64_t want = (sz + HH_THREADS * 4 - 1) / (HH_THREADS * 4);
   int64_t cap = int64_t(c->num_sms) * std::min(occ, 2);

@@ -1,11 +1,12 @@
 // Executor of grouped batches: many independent solves advance together on
 // one stream, and launches of the same kernel are merged into one launch.
 //
-// Each solve runs the ordinary host code on a host thread of its own with a
-// recording context (Context::rec): launches, memsets, copies and library
+// Each solve runs the ordinary host code on a fiber of its own (a few host
+// worker threads resume the fibers in turn) with a recording context
+// (Context::rec): launches, memsets, copies and library
 // calls are appended to the solve's record instead of being issued, and
-// device blocks it frees go back to the allocator only after the records
-// that may use them are issued.  A solve that needs a device result (a host
+// device blocks it frees are kept for its own later allocations (reused in
+// its own record order), going back to the allocator when the batch ends.  A solve that needs a device result (a host
 // read or a synchronisation) blocks.  Once every running solve is blocked,
 // the executor "flushes": it merges the records of all solves, issues them
 // on the stream and waits for the device, then wakes the solves, which go on
@@ -29,8 +30,13 @@
 #include <map>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <tuple>
 #include <vector>
+
+#include <sys/mman.h>
+#include <ucontext.h>
+#include <unistd.h>
 
 #include "group.cuh"
 
@@ -47,6 +53,24 @@ struct RecOp {
 };
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Member {  // one recorded launch of a grouped step
+  Recorder* r;
+  uint32_t op;
+};
+struct Step {
+  bool group;       // false: a stream operation (r, op)
+  Recorder* r;
+  uint32_t op;
+  size_t first, n;  // grouped step: members[first, first + n)
+};
+struct Launch {  // one grouped launch (a cooperative step may need several)
+  size_t lane, step;
+  size_t first, n;
+  uint32_t ctas, smem;
+  size_t map_off, hdr_off, pack_off;
+  uint32_t stride;
+};
 
 // TTG_GROUP=0 issues every recorded launch on its own (plain kernels, in the
 // merged order): the grouped launches can then be compared with it.
@@ -89,13 +113,120 @@ TTG_KERNEL(k_read_host, 0);
 
 class Executor;
 
+// A solve of a grouped batch runs on a fiber: its own stack and machine
+// context, resumed by one host worker thread until it waits for the device
+// (then it switches back to the worker) or its solves are done.  Many
+// fibers share a worker, so a flush wakes a few threads, not one per solve.
+struct Fiber {
+  ucontext_t ctx;
+  char* stack = nullptr;
+  size_t stack_size = 0;
+  Executor* ex = nullptr;
+  int worker = 0;
+  int slot = 0;  // recorder and context of this fiber
+  bool done = false;
+};
+
 struct Recorder {
   Executor* ex = nullptr;
+  Fiber* fiber = nullptr;
   std::vector<RecOp> ops;
   std::vector<StreamOp> closures;
   std::vector<char> arena;
-  std::vector<void*> frees;
+  // Device blocks this solve freed, by size class, for its own reuse.
+  std::unordered_map<size_t, std::vector<void*>> cache;
 };
+
+// Plan of one lane: the lane's records in issue order.  Stream operations at
+// the head of a solve go first, one by one; then the kernel (and block
+// shape) at the head of the most solves becomes one grouped step over all
+// of them; repeat.
+namespace {
+
+void plan_lane(const std::vector<Recorder*>& R, std::vector<Step>& steps,
+               std::vector<Member>& members) {
+  size_t remaining = 0;
+  for (Recorder* r : R) remaining += r->ops.size();
+  std::vector<size_t> head(R.size(), 0);
+  struct Key {
+    const GroupInfo* info;
+    dim3 block;
+    int count;
+  };
+  auto same = [](const RecOp& o, const GroupInfo* info, dim3 block) {
+    return o.info == info && o.block.x == block.x && o.block.y == block.y &&
+           o.block.z == block.z;
+  };
+  std::vector<Key> keys;
+  while (remaining) {
+    for (size_t q = 0; q < R.size(); ++q) {
+      auto& ops = R[q]->ops;
+      while (head[q] < ops.size() && !ops[head[q]].info) {
+        steps.push_back(Step{false, R[q], uint32_t(head[q]), 0, 0});
+        ++head[q];
+        --remaining;
+      }
+    }
+    if (!remaining) break;
+    keys.clear();
+    for (size_t q = 0; q < R.size(); ++q) {
+      if (head[q] >= R[q]->ops.size()) continue;
+      const RecOp& o = R[q]->ops[head[q]];
+      bool found = false;
+      for (auto& k : keys)
+        if (same(o, k.info, k.block)) {
+          ++k.count;
+          found = true;
+          break;
+        }
+      if (!found) keys.push_back(Key{o.info, o.block, 1});
+    }
+    const Key* best = &keys[0];
+    for (auto& k : keys)
+      if (k.count > best->count) best = &k;
+    const Key kb = *best;
+    Step g{true, nullptr, 0, members.size(), 0};
+    for (size_t q = 0; q < R.size(); ++q) {
+      if (head[q] >= R[q]->ops.size()) continue;
+      if (same(R[q]->ops[head[q]], kb.info, kb.block)) {
+        members.push_back(Member{R[q], uint32_t(head[q])});
+        ++head[q];
+        --remaining;
+      }
+    }
+    g.n = members.size() - g.first;
+    steps.push_back(g);
+  }
+}
+
+// Lanes: solves whose records are the same sequence of kernels (the same
+// phase of the sweep) share a lane, so that their launches merge step by
+// step; the largest clusters get lanes of their own, the others are dealt
+// round-robin.  Each lane is issued on its own stream.
+std::vector<std::vector<Recorder*>> make_lanes(const std::vector<Recorder*>& R, size_t max_lanes) {
+  std::map<uint64_t, std::vector<Recorder*>> clusters;
+  for (Recorder* r : R) {
+    uint64_t h = 1469598103934665603ull;
+    for (const RecOp& o : r->ops) {
+      h = (h ^ uint64_t(reinterpret_cast<uintptr_t>(o.info))) * 1099511628211ull;
+      h = (h ^ uint64_t(o.block.x)) * 1099511628211ull;
+    }
+    clusters[h].push_back(r);
+  }
+  std::vector<std::vector<Recorder*>*> cl;
+  for (auto& kv : clusters) cl.push_back(&kv.second);
+  std::stable_sort(cl.begin(), cl.end(),
+                   [](const std::vector<Recorder*>* a, const std::vector<Recorder*>* b) {
+                     return a->size() > b->size();
+                   });
+  const size_t nl = std::max<size_t>(1, std::min(max_lanes, cl.size()));
+  std::vector<std::vector<Recorder*>> lanes(nl);
+  for (size_t c = 0; c < cl.size(); ++c)
+    lanes[c % nl].insert(lanes[c % nl].end(), cl[c]->begin(), cl[c]->end());
+  return lanes;
+}
+
+}  // namespace
 
 class Executor {
  public:
@@ -103,9 +234,11 @@ class Executor {
   ~Executor();
   void run(int64_t count, const std::function<void(int64_t, Context*)>& body);
   void wait(Recorder* r);
+  void fiber_main(Fiber* f);
   ttg_group_stats st{};
 
  private:
+  void worker_loop(int w);
   void flush();
   int coop_capacity(const GroupInfo* info, dim3 block, size_t smem);
   void ensure_stage(size_t bytes);
@@ -119,6 +252,10 @@ class Executor {
   unsigned* d_tile_slab_ = nullptr;
   char* h_stage_ = nullptr;
   char* d_stage_ = nullptr;
+  // Streams of the lanes (lanes_[0] is the owner's stream) and the event that
+  // orders every lane after the copy of the argument packs.
+  std::vector<cudaStream_t> lanes_;
+  cudaEvent_t stage_ev_ = nullptr;
   size_t stage_cap_ = 0;
   std::map<std::tuple<const void*, unsigned, size_t>, int> occ_;
   const bool group_on_ = env_on("TTG_GROUP");
@@ -145,9 +282,20 @@ class Executor {
     return ok;
   }
 
+  // Fibers, the worker threads' own contexts, and the batch being run.
+  std::vector<std::unique_ptr<Fiber>> fibers_;
+  std::vector<std::unique_ptr<ucontext_t>> worker_ctx_;
+  int nworkers_ = 0;
+  std::atomic<int64_t> next_{0};
+  int64_t count_ = 0;
+  uint64_t gets0_ = 0, mallocs0_ = 0;
+  double ms_get0_ = 0.0;
+  const std::function<void(int64_t, Context*)>* body_ = nullptr;
+
   std::mutex mu_;
   std::condition_variable cv_main_, cv_sys_;
-  int live_ = 0, blocked_ = 0;
+  int idle_ = 0;      // workers whose fibers are all waiting or done
+  bool stop_ = false;
   uint64_t epoch_ = 0;
   bool failed_ = false;
   int fail_code_ = TTG_OK;
@@ -163,6 +311,16 @@ Executor::Executor(Context* owner, int width) : owner_(owner), width_(width) {
   TTG_CUDA(cudaMalloc(&d_tile_slab_, sizeof(unsigned) * GEMM_TILE_COUNTERS * size_t(width)));
   TTG_CUDA(cudaMemset(d_tile_slab_, 0, sizeof(unsigned) * GEMM_TILE_COUNTERS * size_t(width)));
   TTG_CUDA(cudaDeviceSynchronize());
+  // TTG_GROUP_LANES (default 16): streams the phase clusters are issued on.
+  int nlanes = 16;
+  if (const char* e = getenv("TTG_GROUP_LANES")) nlanes = std::max(1, std::min(64, atoi(e)));
+  lanes_.push_back(owner->stream);
+  for (int l = 1; l < nlanes; ++l) {
+    cudaStream_t st = nullptr;
+    TTG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    lanes_.push_back(st);
+  }
+  TTG_CUDA(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming));
   for (int k = 0; k < width; ++k) {
     recs_.emplace_back(new Recorder());
     recs_.back()->ex = this;
@@ -184,7 +342,9 @@ Executor::Executor(Context* owner, int width) : owner_(owner), width_(width) {
 }
 
 Executor::~Executor() {
-  cudaStreamSynchronize(owner_->stream);
+  for (cudaStream_t st : lanes_) cudaStreamSynchronize(st);
+  for (size_t l = 1; l < lanes_.size(); ++l) cudaStreamDestroy(lanes_[l]);
+  if (stage_ev_) cudaEventDestroy(stage_ev_);
   if (h_slab_) cudaFreeHost(h_slab_);
   if (d_err_slab_) cudaFree(d_err_slab_);
   if (d_tile_slab_) cudaFree(d_tile_slab_);
@@ -219,61 +379,119 @@ int Executor::coop_capacity(const GroupInfo* info, dim3 block, size_t smem) {
 }
 
 void Executor::wait(Recorder* r) {
-  (void)r;
-  std::unique_lock<std::mutex> lk(mu_);
-  const uint64_t e = epoch_;
-  ++blocked_;
-  if (blocked_ == live_) cv_main_.notify_one();
-  cv_sys_.wait(lk, [&] { return epoch_ != e; });
+  Fiber* f = r->fiber;
+  // Back to the worker; resumed after the flush that issued this record.
+  swapcontext(&f->ctx, worker_ctx_[f->worker].get());
   if (failed_) throw Error{fail_code_, fail_msg_};
 }
 
-void Executor::run(int64_t count, const std::function<void(int64_t, Context*)>& body) {
-  const int nthreads = int(std::min<int64_t>(width_, count));
-  std::atomic<int64_t> next{0};
-  {
-    std::lock_guard<std::mutex> lk(mu_);
-    live_ = nthreads;
-    blocked_ = 0;
+namespace {
+// makecontext passes int arguments: the fiber's address in two halves.
+void fiber_entry(unsigned lo, unsigned hi) {
+  Fiber* f = reinterpret_cast<Fiber*>((uintptr_t(hi) << 32) | uintptr_t(lo));
+  f->ex->fiber_main(f);
+}
+}  // namespace
+
+void Executor::fiber_main(Fiber* f) {
+  Context* c = ctxs_[f->slot].get();
+  for (;;) {
+    const int64_t i = next_.fetch_add(1);
+    if (i >= count_) break;
+    try {
+      (*body_)(i, c);
+    } catch (...) {  // the body reports its own failures
+    }
   }
+  f->done = true;
+  // A fiber never returns (its context has no successor): the worker does
+  // not resume a finished fiber.
+  swapcontext(&f->ctx, worker_ctx_[f->worker].get());
+}
+
+void Executor::worker_loop(int w) {
+  cudaSetDevice(owner_->device);
+  uint64_t seen = 0;
+  for (;;) {
+    for (auto& f : fibers_)
+      if (f->worker == w && !f->done) swapcontext(worker_ctx_[w].get(), &f->ctx);
+    std::unique_lock<std::mutex> lk(mu_);
+    if (++idle_ == nworkers_) cv_main_.notify_one();
+    cv_sys_.wait(lk, [&] { return epoch_ != seen || stop_; });
+    seen = epoch_;
+    if (stop_) return;
+  }
+}
+
+void Executor::run(int64_t count, const std::function<void(int64_t, Context*)>& body) {
+  const int nfib = int(std::min<int64_t>(width_, count));
+  const int hw = std::max(1, int(std::thread::hardware_concurrency()));
+  nworkers_ = std::max(1, std::min(nfib, hw));
+  count_ = count;
+  body_ = &body;
+  gets0_ = owner_->alloc->gets();
+  mallocs0_ = owner_->alloc->mallocs();
+  ms_get0_ = owner_->alloc->ms_get();
+  next_ = 0;
+  const size_t page = size_t(sysconf(_SC_PAGESIZE));
+  const size_t stack_size = size_t(2) << 20;
+  for (int k = 0; k < nfib; ++k) {
+    std::unique_ptr<Fiber> f(new Fiber());
+    void* mem = mmap(nullptr, stack_size, PROT_READ | PROT_WRITE,
+                     MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE | MAP_STACK, -1, 0);
+    if (mem == MAP_FAILED) fail(TTG_ERR_ALLOC, "grouped batch: no memory for a fiber stack");
+    mprotect(mem, page, PROT_NONE);  // guard page below the stack
+    f->stack = static_cast<char*>(mem);
+    f->stack_size = stack_size;
+    f->ex = this;
+    f->slot = k;
+    f->worker = k % nworkers_;
+    getcontext(&f->ctx);
+    f->ctx.uc_stack.ss_sp = f->stack + page;
+    f->ctx.uc_stack.ss_size = stack_size - page;
+    f->ctx.uc_link = nullptr;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(f.get());
+    makecontext(&f->ctx, reinterpret_cast<void (*)()>(fiber_entry), 2, unsigned(a & 0xffffffffu),
+                unsigned(a >> 32));
+    recs_[k]->fiber = f.get();
+    fibers_.push_back(std::move(f));
+  }
+  for (int w = 0; w < nworkers_; ++w) worker_ctx_.emplace_back(new ucontext_t());
   {
     const int share = owner_->group_sms > 0
                           ? std::min(owner_->group_sms, owner_->num_sms)
-                          : std::max(1, 2 * owner_->num_sms / std::max(1, nthreads));
+                          : std::max(1, 2 * owner_->num_sms / std::max(1, nfib));
     for (auto& c : ctxs_) c->num_sms = share;
   }
-  auto worker = [&](int k) {
-    cudaSetDevice(owner_->device);
-    Context* c = ctxs_[k].get();
-    for (;;) {
-      const int64_t i = next.fetch_add(1);
-      if (i >= count) break;
-      body(i, c);
-    }
-    std::lock_guard<std::mutex> lk(mu_);
-    --live_;
-    if (blocked_ == live_) cv_main_.notify_one();
-  };
   std::vector<std::thread> th;
-  th.reserve(nthreads);
-  for (int k = 0; k < nthreads; ++k) th.emplace_back(worker, k);
+  th.reserve(nworkers_);
+  for (int w = 0; w < nworkers_; ++w) th.emplace_back(&Executor::worker_loop, this, w);
   {
     std::unique_lock<std::mutex> lk(mu_);
+    auto t_wake = std::chrono::steady_clock::now();
     for (;;) {
-      cv_main_.wait(lk, [&] { return blocked_ == live_; });
-      const bool last = live_ == 0;
+      cv_main_.wait(lk, [&] { return idle_ == nworkers_; });
+      st.ms_record += std::chrono::duration<double, std::milli>(
+                          std::chrono::steady_clock::now() - t_wake).count();
+      int live = 0;
+      for (auto& f : fibers_) live += f->done ? 0 : 1;
       // Per-solve share of the SMs for the grids the solves size themselves
       // (cooperative Krylov grids, split-K slices, grid-stride loops): the
       // grouped launches fill the device across solves.
       const int share =
           owner_->group_sms > 0
               ? std::min(owner_->group_sms, owner_->num_sms)
-              : std::max(1, std::min(owner_->num_sms, 2 * owner_->num_sms / std::max(1, live_)));
+              : std::max(1, std::min(owner_->num_sms, 2 * owner_->num_sms / std::max(1, live)));
       for (auto& c : ctxs_) c->num_sms = share;
       lk.unlock();
       try {
         flush();
       } catch (const Error& e) {
+        for (auto& r : recs_) {  // nothing recorded so far is issued again
+          r->ops.clear();
+          r->closures.clear();
+          r->arena.clear();
+        }
         lk.lock();
         if (!failed_) {
           failed_ = true;
@@ -283,142 +501,90 @@ void Executor::run(int64_t count, const std::function<void(int64_t, Context*)>& 
         lk.unlock();
       }
       lk.lock();
-      blocked_ = 0;
+      idle_ = 0;
       ++epoch_;
+      t_wake = std::chrono::steady_clock::now();
+      if (live == 0) stop_ = true;
       cv_sys_.notify_all();
-      if (last) break;
+      if (live == 0) break;
     }
   }
   for (auto& t : th) t.join();
+  for (auto& f : fibers_) munmap(f->stack, f->stack_size);
+  st.allocs = int64_t(owner_->alloc->gets() - gets0_);
+  st.device_mallocs = int64_t(owner_->alloc->mallocs() - mallocs0_);
+  st.ms_alloc = owner_->alloc->ms_get() - ms_get0_;
+  for (auto& r : recs_) {  // every record is issued and complete
+    for (auto& kv : r->cache)
+      for (void* p : kv.second) owner_->alloc->put(p);
+    r->cache.clear();
+  }
   if (failed_) fail(fail_code_, "grouped batch: %s", fail_msg_.c_str());
 }
 
 void Executor::flush() {
   const auto t0 = std::chrono::steady_clock::now();
   st.flushes += 1;
-  cudaStream_t s = owner_->stream;
   std::vector<Recorder*> R;
-  size_t remaining = 0;
   for (auto& r : recs_)
     if (!r->ops.empty()) {
       R.push_back(r.get());
-      remaining += r->ops.size();
+      st.records += int64_t(r->ops.size());
     }
-  st.records += int64_t(remaining);
-
-  // ---- plan: steps in issue order
-  struct Member {
-    Recorder* r;
-    uint32_t op;
-  };
-  struct Step {
-    bool group;
-    Recorder* r;        // stream operation
-    uint32_t op;
-    size_t first, n;    // group members
-  };
-  std::vector<Step> steps;
+  const std::vector<std::vector<Recorder*>> laneR = make_lanes(R, lanes_.size());
+  const size_t nl = laneR.size();
+  std::vector<std::vector<Step>> steps(nl);
   std::vector<Member> members;
-  std::vector<size_t> head(R.size(), 0);
-  struct Key {
-    const GroupInfo* info;
-    dim3 block;
-    int count;
-  };
-  std::vector<Key> keys;
-  while (remaining) {
-    for (size_t q = 0; q < R.size(); ++q) {
-      auto& ops = R[q]->ops;
-      while (head[q] < ops.size() && !ops[head[q]].info) {
-        steps.push_back(Step{false, R[q], uint32_t(head[q]), 0, 0});
-        ++head[q];
-        --remaining;
-      }
-    }
-    if (!remaining) break;
-    keys.clear();
-    for (size_t q = 0; q < R.size(); ++q) {
-      if (head[q] >= R[q]->ops.size()) continue;
-      const RecOp& o = R[q]->ops[head[q]];
-      bool found = false;
-      for (auto& k : keys)
-        if (k.info == o.info && k.block.x == o.block.x && k.block.y == o.block.y &&
-            k.block.z == o.block.z) {
-          ++k.count;
-          found = true;
-          break;
-        }
-      if (!found) keys.push_back(Key{o.info, o.block, 1});
-    }
-    const Key* best = &keys[0];
-    for (auto& k : keys)
-      if (k.count > best->count) best = &k;
-    const Key kb = *best;
-    Step g{true, nullptr, 0, members.size(), 0};
-    for (size_t q = 0; q < R.size(); ++q) {
-      if (head[q] >= R[q]->ops.size()) continue;
-      const RecOp& o = R[q]->ops[head[q]];
-      if (o.info == kb.info && o.block.x == kb.block.x && o.block.y == kb.block.y &&
-          o.block.z == kb.block.z) {
-        members.push_back(Member{R[q], uint32_t(head[q])});
-        ++head[q];
-        --remaining;
-      }
-    }
-    g.n = members.size() - g.first;
-    steps.push_back(g);
-  }
+  for (size_t l = 0; l < nl; ++l) plan_lane(laneR[l], steps[l], members);
 
   // ---- launches: split cooperative groups by residency, lay out staging
-  struct Launch {
-    size_t step;        // index in steps
-    size_t first, n;    // members
-    uint32_t ctas;
-    uint32_t smem;
-    size_t map_off, hdr_off, pack_off;
-    uint32_t stride;
-  };
   std::vector<Launch> launches;
-  std::vector<size_t> launch_of_step(steps.size(), SIZE_MAX);
+  std::vector<std::vector<size_t>> launch_of_step(nl);
   size_t bytes = 0;
   auto ctas_of = [](const RecOp& o) -> uint64_t {
     return uint64_t(o.grid.x) * o.grid.y * o.grid.z;
   };
-  for (size_t si = 0; si < steps.size(); ++si) {
-    const Step& sp = steps[si];
-    if (!sp.group) continue;
-    const GroupInfo* info = members[sp.first].r->ops[members[sp.first].op].info;
-    const dim3 block = members[sp.first].r->ops[members[sp.first].op].block;
-    if (sp.n == 1 || !groupable(info)) continue;  // plain launches
-    uint32_t smem = 0;
-    for (size_t m = sp.first; m < sp.first + sp.n; ++m)
-      smem = std::max(smem, members[m].r->ops[members[m].op].smem);
-    uint64_t cap = UINT32_MAX / 2;
-    if (info->coop) cap = uint64_t(std::max(1, coop_capacity(info, block, smem)));
-    const uint32_t stride = uint32_t(align_up(info->pack_size, std::max<uint32_t>(16, info->pack_align)));
-    size_t m = sp.first;
-    launch_of_step[si] = launches.size();
-    while (m < sp.first + sp.n) {
-      Launch L{si, m, 0, 0, smem, 0, 0, 0, stride};
-      uint64_t ctas = 0;
+  for (size_t l = 0; l < nl; ++l) {
+    launch_of_step[l].assign(steps[l].size(), SIZE_MAX);
+    for (size_t si = 0; si < steps[l].size(); ++si) {
+      const Step& sp = steps[l][si];
+      if (!sp.group) continue;
+      const RecOp& o0 = members[sp.first].r->ops[members[sp.first].op];
+      if (sp.n == 1 || !groupable(o0.info)) continue;  // plain launches
+      uint32_t smem = 0;
+      for (size_t m = sp.first; m < sp.first + sp.n; ++m)
+        smem = std::max(smem, members[m].r->ops[members[m].op].smem);
+      uint64_t cap = UINT32_MAX / 2;
+      // Cooperative grids of all lanes may run at once: each lane keeps to
+      // its share of the resident CTAs.
+      if (o0.info->coop)
+        cap = uint64_t(std::max<int64_t>(1, coop_capacity(o0.info, o0.block, smem) / int64_t(nl)));
+      const uint32_t stride =
+          uint32_t(align_up(o0.info->pack_size, std::max<uint32_t>(16, o0.info->pack_align)));
+      size_t m = sp.first;
+      launch_of_step[l][si] = launches.size();
       while (m < sp.first + sp.n) {
-        const uint64_t k = ctas_of(members[m].r->ops[members[m].op]);
-        if (L.n > 0 && ctas + k > cap) break;
-        ctas += k;
-        ++L.n;
-        ++m;
+        Launch L{l, si, m, 0, 0, smem, 0, 0, 0, stride};
+        uint64_t ctas = 0;
+        while (m < sp.first + sp.n) {
+          const uint64_t k = ctas_of(members[m].r->ops[members[m].op]);
+          if (L.n > 0 && ctas + k > cap) break;
+          ctas += k;
+          ++L.n;
+          ++m;
+        }
+        L.ctas = uint32_t(ctas);
+        bytes = align_up(bytes, 256);
+        L.map_off = bytes;
+        bytes += sizeof(uint32_t) * ctas;
+        bytes = align_up(bytes, 256);
+        L.hdr_off = bytes;
+        bytes += sizeof(uint4) * L.n;
+        bytes = align_up(bytes, 256);
+        L.pack_off = bytes;
+        bytes += size_t(stride) * L.n;
+        launches.push_back(L);
       }
-      L.ctas = uint32_t(ctas);
-      bytes = align_up(bytes, 256);
-      L.map_off = bytes;
-      bytes += sizeof(uint32_t) * ctas;
-      bytes = align_up(bytes, 256);
-      L.hdr_off = bytes;
-      bytes += sizeof(uint4) * L.n;
-      bytes = align_up(bytes, 256);
-      L.pack_off = bytes;
-      bytes += size_t(stride) * L.n;
-      launches.push_back(L);
     }
   }
   ensure_stage(bytes + 256);
@@ -440,17 +606,27 @@ void Executor::flush() {
   const auto t1 = std::chrono::steady_clock::now();
   st.ms_plan += std::chrono::duration<double, std::milli>(t1 - t0).count();
 
-  // ---- issue
-  if (bytes) TTG_CUDA(cudaMemcpyAsync(d_stage_, h_stage_, bytes, cudaMemcpyHostToDevice, s));
-  for (size_t si = 0; si < steps.size(); ++si) {
-    const Step& sp = steps[si];
+  // ---- issue: one copy of the packs, then the lanes' steps interleaved
+  // across their streams (each lane in its own order).
+  cudaStream_t s0 = lanes_[0];
+  if (bytes) TTG_CUDA(cudaMemcpyAsync(d_stage_, h_stage_, bytes, cudaMemcpyHostToDevice, s0));
+  TTG_CUDA(cudaEventRecord(stage_ev_, s0));
+  for (size_t l = 1; l < nl; ++l) TTG_CUDA(cudaStreamWaitEvent(lanes_[l], stage_ev_, 0));
+  cudaStream_t solver_stream = owner_->stream;
+  auto issue_step = [&](size_t l, size_t si) {
+    cudaStream_t s = lanes_[l];
+    const Step& sp = steps[l][si];
     if (!sp.group) {
+      if (owner_->solver && solver_stream != s) {  // library calls go on the lane's stream
+        TTG_SOLVER(cusolverDnSetStream(owner_->solver, s));
+        solver_stream = s;
+      }
       sp.r->closures[sp.r->ops[sp.op].closure](s, owner_->solver);
       st.launches += 1;
-      continue;
+      return;
     }
-    const GroupInfo* info = members[sp.first].r->ops[members[sp.first].op].info;
-    const dim3 block = members[sp.first].r->ops[members[sp.first].op].block;
+    const RecOp& o0 = members[sp.first].r->ops[members[sp.first].op];
+    const GroupInfo* info = o0.info;
     auto plain_one = [&](const Member& mb) {
       const RecOp& o = mb.r->ops[mb.op];
       info->issue(mb.r->arena.data() + o.pack_off, o.grid, o.block, o.smem, s, owner_->pdl);
@@ -458,12 +634,13 @@ void Executor::flush() {
     };
     if (sp.n == 1 || !groupable(info)) {
       for (size_t m = sp.first; m < sp.first + sp.n; ++m) plain_one(members[m]);
-      continue;
+      return;
     }
     st.grouped_records += int64_t(sp.n);
-    for (size_t li = launch_of_step[si]; li < launches.size() && launches[li].step == si; ++li) {
+    for (size_t li = launch_of_step[l][si];
+         li < launches.size() && launches[li].lane == l && launches[li].step == si; ++li) {
       const Launch& L = launches[li];
-      if (L.n == 1) {  // one launch alone (a cooperative grid at its residency limit)
+      if (L.n == 1) {  // one launch alone (a cooperative grid at its residency share)
         plain_one(members[L.first]);
         continue;
       }
@@ -473,11 +650,12 @@ void Executor::flush() {
                    L.stride};
       void* kargs[] = {&ga};
       if (info->coop) {
-        TTG_CUDA(cudaLaunchCooperativeKernel(info->group, dim3(L.ctas), block, kargs, L.smem, s));
+        TTG_CUDA(cudaLaunchCooperativeKernel(info->group, dim3(L.ctas), o0.block, kargs, L.smem,
+                                             s));
       } else {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(L.ctas);
-        cfg.blockDim = block;
+        cfg.blockDim = o0.block;
         cfg.dynamicSmemBytes = L.smem;
         cfg.stream = s;
         cudaLaunchAttribute attr[1];
@@ -489,8 +667,25 @@ void Executor::flush() {
       }
       st.launches += 1;
     }
+  };
+  size_t longest = 0;
+  for (size_t l = 0; l < nl; ++l) longest = std::max(longest, steps[l].size());
+  cudaError_t e = cudaSuccess;
+  std::string issue_err;
+  try {
+    for (size_t k = 0; k < longest; ++k)
+      for (size_t l = 0; l < nl; ++l)
+        if (k < steps[l].size()) issue_step(l, k);
+  } catch (const Error& err) {
+    issue_err = err.msg;
   }
-  const cudaError_t e = cudaStreamSynchronize(s);
+  if (solver_stream != owner_->stream && owner_->solver)
+    cusolverDnSetStream(owner_->solver, owner_->stream);
+  for (size_t l = 0; l < nl; ++l) {
+    const cudaError_t el = cudaStreamSynchronize(lanes_[l]);
+    if (e == cudaSuccess) e = el;
+  }
+  st.lanes_max = std::max<int64_t>(st.lanes_max, int64_t(nl));
   const auto t2 = std::chrono::steady_clock::now();
   st.ms_issue_wait += std::chrono::duration<double, std::milli>(t2 - t1).count();
   for (Recorder* r : R) {
@@ -498,10 +693,14 @@ void Executor::flush() {
     r->closures.clear();
     r->arena.clear();
   }
-  for (auto& r : recs_) {
-    for (void* p : r->frees) owner_->alloc->put(p);
-    r->frees.clear();
+  // Blocks the solves freed during this flush's segments may now serve any
+  // solve: everything recorded so far is complete.
+  for (Recorder* r : R) {
+    for (auto& kv : r->cache)
+      for (void* p : kv.second) owner_->alloc->put(p);
+    r->cache.clear();
   }
+  if (!issue_err.empty()) fail(TTG_ERR_CUDA, "grouped launch: %s", issue_err.c_str());
   if (e != cudaSuccess) fail(TTG_ERR_CUDA, "grouped launch: %s", cudaGetErrorString(e));
 }
 
@@ -543,7 +742,19 @@ void rec_read(Context* c, size_t off, const void* src, size_t bytes) {
          reinterpret_cast<unsigned char*>(c->h_scal_dev) + off, int64_t(bytes));
 }
 
-void rec_free(Recorder* r, void* p) { r->frees.push_back(p); }
+void* rec_alloc(Recorder* r, Allocator* shared, size_t bytes) {
+  auto it = r->cache.find(Allocator::size_class(bytes));
+  if (it != r->cache.end() && !it->second.empty()) {
+    void* p = it->second.back();
+    it->second.pop_back();
+    return p;
+  }
+  return shared->get(bytes);
+}
+
+void rec_free(Recorder* r, void* p, size_t bytes) {
+  r->cache[Allocator::size_class(bytes)].push_back(p);
+}
 
 void run_grouped(Context* owner, int width, int64_t count,
                  const std::function<void(int64_t, Context*)>& body, ttg_group_stats* gs) {

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <functional>
@@ -71,15 +72,20 @@ class Allocator {
   void* get(size_t bytes);
   void put(void* p);
   size_t bytes_in_use() const { return in_use_; }
+  uint64_t gets() const { return n_get_; }
+  uint64_t mallocs() const { return n_malloc_; }
+  double ms_get() const { return double(ns_get_.load()) * 1e-6; }
   size_t bytes_cached() const { return cached_; }
+  static size_t size_class(size_t bytes);
 
  private:
-  static size_t size_class(size_t bytes);
   int device_;
   std::mutex mu_;
   std::map<size_t, std::vector<void*>> free_;
   std::map<void*, size_t> live_;
   size_t in_use_ = 0, cached_ = 0;
+  uint64_t n_get_ = 0, n_malloc_ = 0;
+  std::atomic<uint64_t> ns_get_{0};
 };
 
 struct Context;
@@ -95,9 +101,13 @@ using StreamOp = std::function<void(cudaStream_t, cusolverDnHandle_t)>;
 void rec_op(Recorder* r, StreamOp op);
 // Block until the executor has issued and completed everything recorded.
 void rec_wait(Recorder* r);
-// Return a device block to the allocator once the recorded work that may
-// use it has been issued.
-void rec_free(Recorder* r, void* p);
+class Allocator;
+// Device blocks of a recording context: each solve keeps the blocks it frees
+// for its own later allocations (its records are issued in its own order,
+// so a block is reused only after the records that used it); blocks go back
+// to the shared allocator when the batch ends.
+void* rec_alloc(Recorder* r, Allocator* shared, size_t bytes);
+void rec_free(Recorder* r, void* p, size_t bytes);
 struct Context;
 // Recorded memset and device-to-host read (into the context's pinned,
 // device-mapped scalar buffer at byte offset `off`) as grouped kernels.
@@ -260,13 +270,15 @@ void DBuf<T>::reset(Context* c, size_t n) {
   release();
   c_ = c;
   n_ = n;
-  p_ = n ? static_cast<T*>(c->alloc->get(n * sizeof(T))) : nullptr;
+  p_ = n ? static_cast<T*>(c->rec ? rec_alloc(c->rec, c->alloc, n * sizeof(T))
+                                 : c->alloc->get(n * sizeof(T)))
+         : nullptr;
 }
 template <typename T>
 void DBuf<T>::release() {
   if (p_ && c_) {
     if (c_->rec)
-      rec_free(c_->rec, p_);
+      rec_free(c_->rec, p_, n_ * sizeof(T));
     else
       c_->alloc->put(p_);
   }
@@ -364,6 +376,9 @@ void context_release(Context& c);
 // Raise a kernel's dynamic shared-memory limit to `bytes` on `device`, once
 // per (kernel, device); thread-safe (contexts on several host threads).
 void ensure_smem_attr(const void* func, int device, int bytes);
+// cudaOccupancyMaxActiveBlocksPerMultiprocessor, remembered per (kernel,
+// block size, shared memory); thread-safe.
+int max_active_blocks(const void* func, int threads, size_t smem);
 
 }  // namespace ttg
 

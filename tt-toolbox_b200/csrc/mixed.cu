@@ -328,8 +328,7 @@ struct Gmres32 {
     r.reset(c, sz);
     small.reset(c, size_t(m + 1) * m + 2 * m + (m + 1) + 8);
     int occ = 0;
-    TTG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_arnoldi.plain(), AR_THREADS,
-                                                           arnoldi_smem()));
+    occ = max_active_blocks(k_arnoldi.fn(), AR_THREADS, arnoldi_smem());
     if (occ < 1) occ = 1;
     int64_t want = (sz + AR_THREADS * 4 - 1) / (AR_THREADS * 4);
     const int64_t cap = int64_t(c->num_sms) * std::min(occ, 2);
