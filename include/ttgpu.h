@@ -367,6 +367,7 @@ typedef struct {
   int64_t allocs;           /* device blocks the solves took from the shared allocator */
   int64_t device_mallocs;   /* of which new cudaMalloc blocks */
   double ms_alloc;          /* thread time in the shared allocator (lock waits included) */
+  double ms_issue;          /* host time issuing (part of ms_issue_wait) */
 } ttg_group_stats;
 
 /* Grouped batch: the same solves as ttg_amen_solve_batch (same arguments,

@@ -28,20 +28,50 @@ Allocator::~Allocator() {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device_);
+  for (void* p : slabs_) cudaFree(p);
   for (auto& kv : free_)
-    for (void* p : kv.second) cudaFree(p);
-  for (auto& kv : live_) cudaFree(kv.first);
+    for (void* p : kv.second)
+      if (kv.first > SLAB_CLASS_MAX) cudaFree(p);
+  for (auto& kv : live_)
+    if (kv.second > SLAB_CLASS_MAX) cudaFree(kv.first);
   cudaSetDevice(prev);
 }
 
 size_t Allocator::size_class(size_t bytes) {
-  // 256-byte granularity below 1 MiB, then 1/8-octave classes.
+  // 256-byte granularity up to 4 KiB, then four classes per octave (at most
+  // 25% over the request): few distinct sizes, so blocks freed by one solve
+  // serve the next even when the shapes of the local problems vary.
   if (bytes < 256) return 256;
-  if (bytes <= (1u << 20)) return (bytes + 255) & ~size_t(255);
+  if (bytes <= 4096) return (bytes + 255) & ~size_t(255);
   size_t p = 1;
   while (p < bytes) p <<= 1;
-  size_t step = p >> 3;
+  size_t step = p >> 3;  // classes 5p/8, 6p/8, 7p/8, p of the octave (p/2, p]
   return ((bytes + step - 1) / step) * step;
+}
+
+// Blocks of at most SLAB_CLASS_MAX bytes are carved from slabs of 32 blocks
+// (2 MiB to 64 MiB), one cudaMalloc per slab: a batch of solves that grows
+// its pool by tens of thousands of blocks makes a few hundred driver calls.
+// Larger blocks are allocated one by one.
+void* Allocator::carve(size_t cls) {
+  auto& c = carve_[cls];
+  if (c.left < cls) {
+    const size_t slab = std::min<size_t>(std::max<size_t>(32 * cls, size_t(2) << 20),
+                                         size_t(64) << 20) / cls * cls;
+    void* base = nullptr;
+    ++n_malloc_;
+    if (cudaMalloc(&base, slab) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    slabs_.push_back(base);
+    c.next = static_cast<char*>(base);
+    c.left = slab;
+  }
+  void* p = c.next;
+  c.next += cls;
+  c.left -= cls;
+  return p;
 }
 
 void* Allocator::get(size_t bytes) {
@@ -64,22 +94,27 @@ void* Allocator::get(size_t bytes) {
     it->second.pop_back();
     cached_ -= cls;
   } else {
-    ++n_malloc_;
-    cudaError_t e = cudaMalloc(&p, cls);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      // Give cached blocks back and retry once.
-      for (auto& kv : free_) {
-        for (void* q : kv.second) cudaFree(q);
-        kv.second.clear();
+    for (int attempt = 0; attempt < 2 && !p; ++attempt) {
+      if (cls <= SLAB_CLASS_MAX) {
+        p = carve(cls);
+      } else {
+        ++n_malloc_;
+        if (cudaMalloc(&p, cls) != cudaSuccess) {
+          cudaGetLastError();
+          p = nullptr;
+        }
       }
-      cached_ = 0;
-      e = cudaMalloc(&p, cls);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        fail(TTG_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", cls, cudaGetErrorString(e));
+      if (!p && attempt == 0) {
+        // Give the cached large blocks back and retry once.
+        for (auto& kv : free_) {
+          if (kv.first <= SLAB_CLASS_MAX) continue;
+          for (void* q : kv.second) cudaFree(q);
+          cached_ -= kv.first * kv.second.size();
+          kv.second.clear();
+        }
       }
     }
+    if (!p) fail(TTG_ERR_ALLOC, "device allocation of %zu bytes failed", cls);
   }
   live_[p] = cls;
   in_use_ += cls;

@@ -226,6 +226,81 @@ std::vector<std::vector<Recorder*>> make_lanes(const std::vector<Recorder*>& R, 
   return lanes;
 }
 
+// Host threads that issue the lanes of a flush in parallel (each lane on its
+// own stream, so their launches need no order between them).
+class IssuePool {
+ public:
+  IssuePool(int nthreads, int device) : device_(device) {
+    for (int t = 0; t < nthreads; ++t) th_.emplace_back(&IssuePool::loop, this);
+  }
+  ~IssuePool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  // fn(j) for every j < jobs, on the pool and the calling thread; returns
+  // the first error message ("" when none).
+  std::string run(size_t jobs, const std::function<void(size_t)>& fn) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fn_ = &fn;
+      jobs_ = jobs;
+      next_ = 0;
+      active_ = int(th_.size());
+      err_.clear();
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_done_.wait(lk, [&] { return active_ == 0; });
+    return err_;
+  }
+
+ private:
+  void work() {
+    for (;;) {
+      const size_t j = next_.fetch_add(1);
+      if (j >= jobs_) return;
+      try {
+        (*fn_)(j);
+      } catch (const Error& e) {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (err_.empty()) err_ = e.msg;
+      }
+    }
+  }
+  void loop() {
+    cudaSetDevice(device_);
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen || stop_; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      work();
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--active_ == 0) cv_done_.notify_one();
+    }
+  }
+  int device_;
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, cv_done_;
+  const std::function<void(size_t)>* fn_ = nullptr;
+  size_t jobs_ = 0;
+  std::atomic<size_t> next_{0};
+  int active_ = 0;
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+  std::string err_;
+};
+
 }  // namespace
 
 class Executor {
@@ -235,6 +310,9 @@ class Executor {
   void run(int64_t count, const std::function<void(int64_t, Context*)>& body);
   void wait(Recorder* r);
   void fiber_main(Fiber* f);
+  // Device blocks of the fibers of one worker thread (no lock: touched by
+  // that thread while recording and by the executor while the workers wait).
+  std::unordered_map<size_t, std::vector<void*>>& pool(int w) { return pools_[w]; }
   ttg_group_stats st{};
 
  private:
@@ -256,6 +334,8 @@ class Executor {
   // orders every lane after the copy of the argument packs.
   std::vector<cudaStream_t> lanes_;
   cudaEvent_t stage_ev_ = nullptr;
+  std::unique_ptr<IssuePool> pool_;
+  std::mutex closure_mu_;  // stream operations (library calls share one handle)
   size_t stage_cap_ = 0;
   std::map<std::tuple<const void*, unsigned, size_t>, int> occ_;
   const bool group_on_ = env_on("TTG_GROUP");
@@ -285,6 +365,7 @@ class Executor {
   // Fibers, the worker threads' own contexts, and the batch being run.
   std::vector<std::unique_ptr<Fiber>> fibers_;
   std::vector<std::unique_ptr<ucontext_t>> worker_ctx_;
+  std::vector<std::unordered_map<size_t, std::vector<void*>>> pools_;
   int nworkers_ = 0;
   std::atomic<int64_t> next_{0};
   int64_t count_ = 0;
@@ -321,6 +402,10 @@ Executor::Executor(Context* owner, int width) : owner_(owner), width_(width) {
     lanes_.push_back(st);
   }
   TTG_CUDA(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming));
+  {
+    const int hw = std::max(2, int(std::thread::hardware_concurrency()));
+    pool_.reset(new IssuePool(std::min(nlanes - 1, std::min(7, hw / 2 - 1)), owner->device));
+  }
   for (int k = 0; k < width; ++k) {
     recs_.emplace_back(new Recorder());
     recs_.back()->ex = this;
@@ -457,6 +542,7 @@ void Executor::run(int64_t count, const std::function<void(int64_t, Context*)>& 
     fibers_.push_back(std::move(f));
   }
   for (int w = 0; w < nworkers_; ++w) worker_ctx_.emplace_back(new ucontext_t());
+  pools_.resize(nworkers_);
   {
     const int share = owner_->group_sms > 0
                           ? std::min(owner_->group_sms, owner_->num_sms)
@@ -519,6 +605,10 @@ void Executor::run(int64_t count, const std::function<void(int64_t, Context*)>& 
       for (void* p : kv.second) owner_->alloc->put(p);
     r->cache.clear();
   }
+  for (auto& pl : pools_)
+    for (auto& kv : pl)
+      for (void* p : kv.second) owner_->alloc->put(p);
+  pools_.clear();
   if (failed_) fail(fail_code_, "grouped batch: %s", fail_msg_.c_str());
 }
 
@@ -540,17 +630,20 @@ void Executor::flush() {
   // ---- launches: split cooperative groups by residency, lay out staging
   std::vector<Launch> launches;
   std::vector<std::vector<size_t>> launch_of_step(nl);
+  std::vector<std::vector<char>> grouped(nl);  // step issued as grouped launches
   size_t bytes = 0;
   auto ctas_of = [](const RecOp& o) -> uint64_t {
     return uint64_t(o.grid.x) * o.grid.y * o.grid.z;
   };
   for (size_t l = 0; l < nl; ++l) {
     launch_of_step[l].assign(steps[l].size(), SIZE_MAX);
+    grouped[l].assign(steps[l].size(), 0);
     for (size_t si = 0; si < steps[l].size(); ++si) {
       const Step& sp = steps[l][si];
       if (!sp.group) continue;
       const RecOp& o0 = members[sp.first].r->ops[members[sp.first].op];
       if (sp.n == 1 || !groupable(o0.info)) continue;  // plain launches
+      grouped[l][si] = 1;
       uint32_t smem = 0;
       for (size_t m = sp.first; m < sp.first + sp.n; ++m)
         smem = std::max(smem, members[m].r->ops[members[m].op].smem);
@@ -612,17 +705,16 @@ void Executor::flush() {
   if (bytes) TTG_CUDA(cudaMemcpyAsync(d_stage_, h_stage_, bytes, cudaMemcpyHostToDevice, s0));
   TTG_CUDA(cudaEventRecord(stage_ev_, s0));
   for (size_t l = 1; l < nl; ++l) TTG_CUDA(cudaStreamWaitEvent(lanes_[l], stage_ev_, 0));
-  cudaStream_t solver_stream = owner_->stream;
+  std::vector<int64_t> lane_launches(nl, 0), lane_grouped(nl, 0);
   auto issue_step = [&](size_t l, size_t si) {
     cudaStream_t s = lanes_[l];
     const Step& sp = steps[l][si];
-    if (!sp.group) {
-      if (owner_->solver && solver_stream != s) {  // library calls go on the lane's stream
-        TTG_SOLVER(cusolverDnSetStream(owner_->solver, s));
-        solver_stream = s;
-      }
+    if (!sp.group) {  // library calls go on the lane's stream
+      std::lock_guard<std::mutex> lk(closure_mu_);
+      if (owner_->solver) TTG_SOLVER(cusolverDnSetStream(owner_->solver, s));
       sp.r->closures[sp.r->ops[sp.op].closure](s, owner_->solver);
-      st.launches += 1;
+      if (owner_->solver) TTG_SOLVER(cusolverDnSetStream(owner_->solver, owner_->stream));
+      lane_launches[l] += 1;
       return;
     }
     const RecOp& o0 = members[sp.first].r->ops[members[sp.first].op];
@@ -630,13 +722,13 @@ void Executor::flush() {
     auto plain_one = [&](const Member& mb) {
       const RecOp& o = mb.r->ops[mb.op];
       info->issue(mb.r->arena.data() + o.pack_off, o.grid, o.block, o.smem, s, owner_->pdl);
-      st.launches += 1;
+      lane_launches[l] += 1;
     };
-    if (sp.n == 1 || !groupable(info)) {
+    if (!grouped[l][si]) {
       for (size_t m = sp.first; m < sp.first + sp.n; ++m) plain_one(members[m]);
       return;
     }
-    st.grouped_records += int64_t(sp.n);
+    lane_grouped[l] += int64_t(sp.n);
     for (size_t li = launch_of_step[l][si];
          li < launches.size() && launches[li].lane == l && launches[li].step == si; ++li) {
       const Launch& L = launches[li];
@@ -665,22 +757,20 @@ void Executor::flush() {
         cfg.numAttrs = owner_->pdl ? 1 : 0;
         TTG_CUDA(cudaLaunchKernelExC(&cfg, info->group, kargs));
       }
-      st.launches += 1;
+      lane_launches[l] += 1;
     }
   };
-  size_t longest = 0;
-  for (size_t l = 0; l < nl; ++l) longest = std::max(longest, steps[l].size());
+  // Lanes are issued by several host threads at once, each lane in order.
   cudaError_t e = cudaSuccess;
-  std::string issue_err;
-  try {
-    for (size_t k = 0; k < longest; ++k)
-      for (size_t l = 0; l < nl; ++l)
-        if (k < steps[l].size()) issue_step(l, k);
-  } catch (const Error& err) {
-    issue_err = err.msg;
+  const std::string issue_err = pool_->run(nl, [&](size_t l) {
+    for (size_t si = 0; si < steps[l].size(); ++si) issue_step(l, si);
+  });
+  for (size_t l = 0; l < nl; ++l) {
+    st.launches += lane_launches[l];
+    st.grouped_records += lane_grouped[l];
   }
-  if (solver_stream != owner_->stream && owner_->solver)
-    cusolverDnSetStream(owner_->solver, owner_->stream);
+  const auto t_issued = std::chrono::steady_clock::now();
+  st.ms_issue += std::chrono::duration<double, std::milli>(t_issued - t1).count();
   for (size_t l = 0; l < nl; ++l) {
     const cudaError_t el = cudaStreamSynchronize(lanes_[l]);
     if (e == cudaSuccess) e = el;
@@ -694,10 +784,13 @@ void Executor::flush() {
     r->arena.clear();
   }
   // Blocks the solves freed during this flush's segments may now serve any
-  // solve: everything recorded so far is complete.
+  // solve of the same worker: everything recorded so far is complete.
   for (Recorder* r : R) {
-    for (auto& kv : r->cache)
-      for (void* p : kv.second) owner_->alloc->put(p);
+    auto& pl = pools_[r->fiber->worker];
+    for (auto& kv : r->cache) {
+      auto& dst = pl[kv.first];
+      dst.insert(dst.end(), kv.second.begin(), kv.second.end());
+    }
     r->cache.clear();
   }
   if (!issue_err.empty()) fail(TTG_ERR_CUDA, "grouped launch: %s", issue_err.c_str());
@@ -743,10 +836,18 @@ void rec_read(Context* c, size_t off, const void* src, size_t bytes) {
 }
 
 void* rec_alloc(Recorder* r, Allocator* shared, size_t bytes) {
-  auto it = r->cache.find(Allocator::size_class(bytes));
+  const size_t cls = Allocator::size_class(bytes);
+  auto it = r->cache.find(cls);
   if (it != r->cache.end() && !it->second.empty()) {
     void* p = it->second.back();
     it->second.pop_back();
+    return p;
+  }
+  auto& pl = r->ex->pool(r->fiber->worker);
+  auto jt = pl.find(cls);
+  if (jt != pl.end() && !jt->second.empty()) {
+    void* p = jt->second.back();
+    jt->second.pop_back();
     return p;
   }
   return shared->get(bytes);

@@ -81,8 +81,16 @@ class Allocator {
  private:
   int device_;
   std::mutex mu_;
+  static constexpr size_t SLAB_CLASS_MAX = size_t(4) << 20;
+  struct Carve {
+    char* next = nullptr;
+    size_t left = 0;
+  };
+  void* carve(size_t cls);  // mu_ held
   std::map<size_t, std::vector<void*>> free_;
   std::map<void*, size_t> live_;
+  std::map<size_t, Carve> carve_;
+  std::vector<void*> slabs_;
   size_t in_use_ = 0, cached_ = 0;
   uint64_t n_get_ = 0, n_malloc_ = 0;
   std::atomic<uint64_t> ns_get_{0};

@@ -89,7 +89,8 @@ class GroupStats(C.Structure):
                 ("grouped_records", _i64), ("ms_plan", C.c_double),
                 ("ms_issue_wait", C.c_double), ("ms_total", C.c_double),
                 ("lanes_max", _i64), ("ms_record", C.c_double), ("allocs", _i64),
-                ("device_mallocs", _i64), ("ms_alloc", C.c_double)]
+                ("device_mallocs", _i64), ("ms_alloc", C.c_double),
+                ("ms_issue", C.c_double)]
 
     def to_dict(self):
         return {k: (float(getattr(self, k)) if k.startswith("ms") else int(getattr(self, k)))
