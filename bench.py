@@ -49,6 +49,7 @@ def parse():
                         "(one timed batch; --steps/--warmup do not apply)")
     p.add_argument("--batch-count", type=int, default=512)
     p.add_argument("--batch-workers", type=int, default=8)
+    p.add_argument("--batch-form", default="grouped", choices=["grouped", "streams"])
     p.add_argument("--batch-sample", type=int, default=32,
                    help="systems solved one by one (GPU FP64) and by the CPU oracle")
     return p.parse_args()
@@ -395,6 +396,7 @@ def run_ours(args, dist):
         if not args.no_batch:
             bargs = argparse.Namespace(batch_count=args.batch_count,
                                        batch_workers=args.batch_workers,
+                                       batch_form=args.batch_form,
                                        batch_sample=min(args.batch_sample, 16),
                                        no_cpu_baseline=args.no_cpu_baseline or dist.world > 1)
             line["configs"]["batch"] = run_batch(bargs, dist)
@@ -515,10 +517,13 @@ BATCH_METRIC = "batched AMEn: independent Laplacian systems to tol 1e-8, total t
 def run_batch(args, dist):
     """Config 4: ``count`` independent seeded Laplacian systems (d U{6..14},
     n in {8,16,32,64}, rmax U{8..64}, all-ones right-hand sides, tol 1e-8)
-    through ``ttg_amen_solve_batch`` (worker streams), mixed precision,
-    against the same systems solved one after another in FP64 on the GPU and
-    by the CPU oracle (both on the first ``batch_sample`` systems, scaled to
-    the whole batch by count)."""
+    through the grouped batch ``ttg_amen_solve_grouped`` (every system's
+    launches merged kernel by kernel into grouped launches), mixed precision
+    (the value) and FP64, against the same systems solved one after another
+    in FP64 on the GPU and by the CPU oracle (both on the first
+    ``batch_sample`` systems, scaled to the whole batch by count).
+    ``--batch-form streams`` times ``ttg_amen_solve_batch`` (worker host
+    threads, one stream each) instead."""
     if dist.rank != 0:
         return None
     import numpy as np
@@ -530,26 +535,80 @@ def run_batch(args, dist):
     dys = [ttgpu.DeviceTT.upload(ctx, y) for y in ys]
     per = [dict(rmax=r) for r in rmaxs]
     k = min(args.batch_sample, args.batch_count)
-    # warm-up: kernels loaded and tile widths tuned on a small batch
-    for x in ttgpu.amen_solve2_batch(dAs[:16], dys[:16], 1e-8, workers=args.batch_workers,
-                                     ctx=ctx, per_system=per[:16], precision="mixed"):
-        x.free()
+    grouped = args.batch_form == "grouped"
+    width = 0 if grouped else args.batch_workers
+
+    def run(prec, lo=0, hi=None, stats=None, gs=None):
+        hi = len(dAs) if hi is None else hi
+        return ttgpu.amen_solve2_batch(dAs[lo:hi], dys[lo:hi], 1e-8, workers=width, ctx=ctx,
+                                       stats=stats, per_system=per[lo:hi], precision=prec,
+                                       grouped=grouped, group_stats=gs)
+
+    # warm-up: kernels loaded, tile widths tuned and allocator slabs grown
+    for prec in ("mixed", "fp64"):
+        for x in run(prec, 0, 32):
+            x.free()
     ctx.sync()
-    clocks = Clocks(0)
-    clocks.start()
-    st = []
-    t0 = time.perf_counter()
-    xs = ttgpu.amen_solve2_batch(dAs, dys, 1e-8, workers=args.batch_workers, ctx=ctx,
-                                 stats=st, per_system=per, precision="mixed")
-    ctx.sync()
-    wall = time.perf_counter() - t0
-    clk = clocks.stop()
-    conv = sum(1 for q in st if q["sweeps"] and q["max_res"][q["sweeps"] - 1] < 1e-8)
-    res = [ttgpu.true_residual(dAs[i], xs[i], dys[i], ctx=ctx) for i in range(k)]
-    for x in xs:
-        x.free()
-    gflop = sum(q["matvec_gflop"] for q in st)
-    launches = sum(q["launches"] for q in st)
+    forms = {}
+    clk = None
+    res, conv, st_mixed = [], 0, None
+    for prec in ("mixed", "fp64"):
+        if prec == "mixed":
+            clocks = Clocks(0)
+            clocks.start()
+        st, gs = [], {}
+        t0 = time.perf_counter()
+        xs = run(prec, stats=st, gs=gs)
+        ctx.sync()
+        wall = time.perf_counter() - t0
+        # grouped: launches the executor issued; streams: each solve's own
+        launches = gs["launches"] if grouped else sum(q["launches"] for q in st)
+        if prec == "mixed":
+            clk = clocks.stop()
+            st_mixed = st
+        c = sum(1 for q in st if q["sweeps"] and q["max_res"][q["sweeps"] - 1] < 1e-8)
+        gflop = sum(q["matvec_gflop"] for q in st)
+        rs = [ttgpu.true_residual(dAs[i], xs[i], dys[i], ctx=ctx) for i in range(k)]
+        for x in xs:
+            x.free()
+        forms[prec] = {"value": wall, "unit": "s", "converged": c,
+                       "true_residual_max_of_sample": max(rs), "gpu_launches": launches,
+                       "recorded_launches": gs.get("records"),
+                       "matvec_gflop": gflop, "matvec_tflops": gflop / wall * 1e-3}
+        if prec == "mixed":
+            res, conv = rs, c
+    wall = forms["mixed"]["value"]
+    roof = None
+    if grouped:
+        # Instrumented pass (outside the timed region): CUDA events around
+        # every grouped launch of the BF16 tcgen05 GEMM (the local matvec
+        # stages), each launch carrying the GEMMs of many systems.
+        os.environ["TTG_GROUP_TIME"] = "1"
+        try:
+            gs = {}
+            for x in run("mixed", gs=gs):
+                x.free()
+        finally:
+            os.environ.pop("TTG_GROUP_TIME", None)
+        if gs.get("tc_ms", 0) > 0 and gs.get("tc_launches", 0) > 0:
+            peaks, peaks_kind = load_peaks()
+            peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1590.0))
+            achieved = gs["tc_gflop"] / gs["tc_ms"]  # GFLOP/ms = TFLOP/s
+            roof = {"kernel": "grouped BF16 tcgen05 GEMM launches (k_umma_group: the local "
+                              "matvec stages of many systems per launch)",
+                    "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_kind": "bf16 sustained, %s" % peaks_kind,
+                    "launches": gs["tc_launches"], "gemms": gs["tc_records"],
+                    "gemms_per_launch": gs["tc_records"] / gs["tc_launches"],
+                    "gflop_per_launch": gs["tc_gflop"] / gs["tc_launches"],
+                    "launch_ms": gs["tc_ms"] / gs["tc_launches"],
+                    "note": "event-timed launches on concurrent lanes (contention included); "
+                            "algorithmic FLOPs of the GEMMs that ran (skipped Krylov steps "
+                            "taken out)"}
+    # systems that stop short of 1e-8: at their rank cap or the sweep limit
+    capped = [i for i, q in enumerate(st_mixed)
+              if not (q["sweeps"] and q["max_res"][q["sweeps"] - 1] < 1e-8)]
     t0 = time.perf_counter()
     for i in range(k):
         ttgpu.amen_solve2(dAs[i], dys[i], 1e-8, ctx=ctx, rmax=rmaxs[i], precision="fp64").free()
@@ -562,11 +621,18 @@ def run_batch(args, dist):
         "data": "synthetic (seeded PCG64)",
         "config": {"workload": "%d Laplacian systems, d U{6..14}, n in {8,16,32,64}, rmax "
                                "U{8..64}, ones rhs, tol 1e-8" % args.batch_count,
-                   "workers": args.batch_workers, "converged": conv,
+                   "form": ("grouped launches (ttg_amen_solve_grouped)" if grouped else
+                            "worker streams (ttg_amen_solve_batch, %d workers)"
+                            % args.batch_workers),
+                   "converged": conv, "stopped_short": len(capped),
                    "true_residual_max_of_sample": max(res)},
-        "gpu_launches": launches, "matvec_tflops": gflop / wall * 1e-3, "clocks": clk,
+        "gpu_launches": forms["mixed"]["gpu_launches"],
+        "matvec_tflops": forms["mixed"]["matvec_tflops"], "clocks": clk,
+        "roofline": roof,
+        "forms": forms,
         "compare": {"serial_fp64_gpu_s": serial,
                     "speedup_vs_serial_fp64_gpu": serial / wall,
+                    "speedup_vs_same_form_fp64": forms["fp64"]["value"] / wall,
                     "sample": "first %d systems one by one, scaled by count" % k},
     }
     if not args.no_cpu_baseline:
@@ -583,7 +649,7 @@ def run_batch(args, dist):
             x0 = tt_randn([int(v) for v in A.n], A.d, 2, rng)
             ref_solve(Ao, yo, 1e-8, x0, None, rmax=rmaxs[i], nswp=20)
         cpu = (time.perf_counter() - t0) / kc * args.batch_count
-        line["cpu_baseline"] = {"value": cpu, "unit": "s", "cores": os.cpu_count(),
+        line["cpu_baseline"] = {"value": cpu, "unit": "s", "cores": blas_threads(),
                                 "kind": "port",
                                 "sample": "FP64 oracle on the first %d systems, scaled by count"
                                           % kc}

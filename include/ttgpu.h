@@ -368,6 +368,14 @@ typedef struct {
   int64_t device_mallocs;   /* of which new cudaMalloc blocks */
   double ms_alloc;          /* thread time in the shared allocator (lock waits included) */
   double ms_issue;          /* host time issuing (part of ms_issue_wait) */
+  /* BF16 tensor-core GEMM launches (the local matvec stages), counted and,
+   * with TTG_GROUP_TIME=1 in the environment, timed by CUDA events around
+   * each launch on its stream (the events cost the launches their
+   * programmatic overlap: use it in a separate, instrumented run). */
+  int64_t tc_launches;      /* issued launches of the BF16 GEMM kernel */
+  int64_t tc_records;       /* recorded GEMMs inside those launches */
+  double tc_gflop;          /* algorithmic GFLOP of those GEMMs (2 M N K) */
+  double tc_ms;             /* summed event time of those launches (0 untimed) */
 } ttg_group_stats;
 
 /* Grouped batch: the same solves as ttg_amen_solve_batch (same arguments,

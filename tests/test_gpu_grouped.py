@@ -79,6 +79,30 @@ def test_grouped_config4_sample(ctx):
             assert true_residual(Ao, xo, yo) < 1e-7
     assert gs["launches"] < gs["records"], gs
     assert gs["grouped_records"] > gs["records"] / 3, gs
+    # The executor's count of BF16 GEMM work (recorded GEMMs less the skipped
+    # Krylov steps) is the solves' own count of BF16 matvec FLOPs.
+    lp = sum(q["gflop_lp"] for q in stats)
+    assert lp > 0
+    assert abs(gs["tc_gflop"] - lp) <= 1e-9 * lp, (gs["tc_gflop"], lp)
+    assert gs["tc_records"] == 3 * sum(q["matvecs_lp"] for q in stats), gs
+    assert gs["tc_launches"] > 0
+    assert gs["tc_ms"] == 0.0  # untimed unless TTG_GROUP_TIME=1
+
+
+def test_grouped_gemm_timing(ctx, monkeypatch):
+    """TTG_GROUP_TIME=1 brackets every BF16 GEMM launch with CUDA events:
+    the summed launch time is positive and the results are unchanged."""
+    As, ys, rmaxs, _ = workloads.batch_systems(count=8, seed=9)
+    per = [dict(rmax=r) for r in rmaxs]
+    ref = ttgpu.amen_solve2_batch(As, ys, 1e-8, ctx=ctx, grouped=True, precision="mixed",
+                                  per_system=per)
+    monkeypatch.setenv("TTG_GROUP_TIME", "1")
+    gs = {}
+    got = ttgpu.amen_solve2_batch(As, ys, 1e-8, ctx=ctx, grouped=True, group_stats=gs,
+                                  precision="mixed", per_system=per)
+    assert gs["tc_ms"] > 0 and gs["tc_launches"] > 0 and gs["tc_gflop"] > 0, gs
+    for a, b in zip(ref, got):
+        assert list(a.r) == list(b.r) and np.array_equal(a.core, b.core)
 
 
 def test_grouped_reports_failing_systems(ctx):

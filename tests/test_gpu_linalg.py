@@ -21,10 +21,15 @@ def test_dense_svd_matches_lapack(ctx, m, n):
     # backward error of a one-sided Jacobi SVD grows like k * eps: 1e-13 up
     # to k = 256, 2.4e-13 at k = 600
     tol = max(1e-13, 4e-16 * k)
+    # V is a product of some sweeps * k^2 / 2 plane rotations: each entry
+    # takes a rounding error from each of the S k rotations that touch its
+    # row, so the k^2 entries of V^T V - I grow like eps sqrt(S k) each and
+    # the Frobenius norm like eps k^1.5 (3.7e-12 measured at k = 600)
+    orth = max(1e-12, 4e-16 * k ** 1.5)
     assert np.allclose(s, s_ref, rtol=0, atol=tol * s_ref[0])
     assert np.linalg.norm(U * s @ VT - A) / np.linalg.norm(A) < tol
-    assert np.linalg.norm(U.T @ U - np.eye(k)) < 10 * tol
-    assert np.linalg.norm(VT @ VT.T - np.eye(k)) < 10 * tol
+    assert np.linalg.norm(U.T @ U - np.eye(k)) < orth
+    assert np.linalg.norm(VT @ VT.T - np.eye(k)) < orth
     assert np.all(np.diff(s) <= 0)
 
 

@@ -50,6 +50,7 @@ struct RecOp {
   uint32_t smem;
   uint32_t pack_off;      // argument pack in Recorder::arena
   uint32_t closure;
+  double flop;            // > 0: a tensor-core GEMM of that many FLOPs
 };
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -135,6 +136,9 @@ struct Recorder {
   std::vector<char> arena;
   // Device blocks this solve freed, by size class, for its own reuse.
   std::unordered_map<size_t, std::vector<void*>> cache;
+  // Tensor-core GEMMs recorded (less those the solve later found skipped).
+  double tc_flop = 0.0;
+  int64_t tc_records = 0;
 };
 
 // Plan of one lane: the lane's records in issue order.  Stream operations at
@@ -339,6 +343,12 @@ class Executor {
   size_t stage_cap_ = 0;
   std::map<std::tuple<const void*, unsigned, size_t>, int> occ_;
   const bool group_on_ = env_on("TTG_GROUP");
+  // TTG_GROUP_TIME=1: CUDA events around every tensor-core GEMM launch.
+  const bool time_tc_ = [] {
+    const char* e = getenv("TTG_GROUP_TIME");
+    return e && e[0] == '1';
+  }();
+  std::vector<std::vector<cudaEvent_t>> tc_ev_;  // per lane: pairs, reused
   const bool group_coop_ = env_on("TTG_GROUP_COOP");
   std::string group_skip_ = getenv("TTG_GROUP_SKIP") ? getenv("TTG_GROUP_SKIP") : "";
   std::map<const GroupInfo*, bool> groupable_;
@@ -428,6 +438,8 @@ Executor::Executor(Context* owner, int width) : owner_(owner), width_(width) {
 
 Executor::~Executor() {
   for (cudaStream_t st : lanes_) cudaStreamSynchronize(st);
+  for (auto& v : tc_ev_)
+    for (cudaEvent_t e : v) cudaEventDestroy(e);
   for (size_t l = 1; l < lanes_.size(); ++l) cudaStreamDestroy(lanes_[l]);
   if (stage_ev_) cudaEventDestroy(stage_ev_);
   if (h_slab_) cudaFreeHost(h_slab_);
@@ -597,6 +609,10 @@ void Executor::run(int64_t count, const std::function<void(int64_t, Context*)>& 
   }
   for (auto& t : th) t.join();
   for (auto& f : fibers_) munmap(f->stack, f->stack_size);
+  for (auto& r : recs_) {
+    st.tc_gflop += r->tc_flop * 1e-9;
+    st.tc_records += r->tc_records;
+  }
   st.allocs = int64_t(owner_->alloc->gets() - gets0_);
   st.device_mallocs = int64_t(owner_->alloc->mallocs() - mallocs0_);
   st.ms_alloc = owner_->alloc->ms_get() - ms_get0_;
@@ -705,7 +721,25 @@ void Executor::flush() {
   if (bytes) TTG_CUDA(cudaMemcpyAsync(d_stage_, h_stage_, bytes, cudaMemcpyHostToDevice, s0));
   TTG_CUDA(cudaEventRecord(stage_ev_, s0));
   for (size_t l = 1; l < nl; ++l) TTG_CUDA(cudaStreamWaitEvent(lanes_[l], stage_ev_, 0));
-  std::vector<int64_t> lane_launches(nl, 0), lane_grouped(nl, 0);
+  std::vector<int64_t> lane_launches(nl, 0), lane_grouped(nl, 0), lane_tc(nl, 0);
+  if (time_tc_ && tc_ev_.size() < nl) tc_ev_.resize(nl);
+  // tc_begin / tc_end bracket a tensor-core GEMM launch on lane l (events
+  // only when timing is on; lane_tc counts the pairs used this flush).
+  auto tc_begin = [&](size_t l, cudaStream_t s) {
+    if (!time_tc_) return;
+    auto& v = tc_ev_[l];
+    const size_t k = size_t(lane_tc[l]) * 2;
+    while (v.size() < k + 2) {
+      cudaEvent_t e = nullptr;
+      TTG_CUDA(cudaEventCreate(&e));
+      v.push_back(e);
+    }
+    TTG_CUDA(cudaEventRecord(v[k], s));
+  };
+  auto tc_end = [&](size_t l, cudaStream_t s) {
+    if (time_tc_) TTG_CUDA(cudaEventRecord(tc_ev_[l][size_t(lane_tc[l]) * 2 + 1], s));
+    lane_tc[l] += 1;
+  };
   auto issue_step = [&](size_t l, size_t si) {
     cudaStream_t s = lanes_[l];
     const Step& sp = steps[l][si];
@@ -721,7 +755,9 @@ void Executor::flush() {
     const GroupInfo* info = o0.info;
     auto plain_one = [&](const Member& mb) {
       const RecOp& o = mb.r->ops[mb.op];
+      if (o.flop > 0) tc_begin(l, s);
       info->issue(mb.r->arena.data() + o.pack_off, o.grid, o.block, o.smem, s, owner_->pdl);
+      if (o.flop > 0) tc_end(l, s);
       lane_launches[l] += 1;
     };
     if (!grouped[l][si]) {
@@ -736,11 +772,16 @@ void Executor::flush() {
         plain_one(members[L.first]);
         continue;
       }
-      if (L.smem > 48 * 1024) ensure_smem_attr(info->group, owner_->device, int(L.smem));
+      // The limit without opt-in is 48 KB of static plus dynamic shared
+      // memory: a body with static arrays needs the attribute below 48 KB
+      // of dynamic memory already (memoised, so set once per size).
+      if (L.smem > 0) ensure_smem_attr(info->group, owner_->device, int(L.smem));
       GroupArgs ga{reinterpret_cast<const uint32_t*>(d_stage_ + L.map_off),
                    reinterpret_cast<const uint4*>(d_stage_ + L.hdr_off), d_stage_ + L.pack_off,
                    L.stride};
       void* kargs[] = {&ga};
+      const bool tc = o0.flop > 0;
+      if (tc) tc_begin(l, s);
       if (info->coop) {
         TTG_CUDA(cudaLaunchCooperativeKernel(info->group, dim3(L.ctas), o0.block, kargs, L.smem,
                                              s));
@@ -755,8 +796,16 @@ void Executor::flush() {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = owner_->pdl ? 1 : 0;
-        TTG_CUDA(cudaLaunchKernelExC(&cfg, info->group, kargs));
+        const cudaError_t le = cudaLaunchKernelExC(&cfg, info->group, kargs);
+        if (le != cudaSuccess) {
+          const char* name = "?";
+          cudaFuncGetName(&name, info->plain);
+          fail(TTG_ERR_CUDA, "grouped launch of %s (%zu launches, %u CTAs of %u threads, "
+               "%u B dynamic shared memory): %s", name ? name : "?", L.n, L.ctas,
+               o0.block.x * o0.block.y * o0.block.z, L.smem, cudaGetErrorString(le));
+        }
       }
+      if (tc) tc_end(l, s);
       lane_launches[l] += 1;
     }
   };
@@ -768,6 +817,7 @@ void Executor::flush() {
   for (size_t l = 0; l < nl; ++l) {
     st.launches += lane_launches[l];
     st.grouped_records += lane_grouped[l];
+    st.tc_launches += lane_tc[l];
   }
   const auto t_issued = std::chrono::steady_clock::now();
   st.ms_issue += std::chrono::duration<double, std::milli>(t_issued - t1).count();
@@ -776,6 +826,14 @@ void Executor::flush() {
     if (e == cudaSuccess) e = el;
   }
   st.lanes_max = std::max<int64_t>(st.lanes_max, int64_t(nl));
+  if (time_tc_ && e == cudaSuccess && issue_err.empty()) {
+    for (size_t l = 0; l < nl; ++l)
+      for (int64_t k = 0; k < lane_tc[l]; ++k) {
+        float ms = 0.0f;
+        TTG_CUDA(cudaEventElapsedTime(&ms, tc_ev_[l][2 * k], tc_ev_[l][2 * k + 1]));
+        st.tc_ms += ms;
+      }
+  }
   const auto t2 = std::chrono::steady_clock::now();
   st.ms_issue_wait += std::chrono::duration<double, std::milli>(t2 - t1).count();
   for (Recorder* r : R) {
@@ -817,6 +875,17 @@ void rec_group(Recorder* r, const GroupInfo* info, dim3 grid, dim3 block, size_t
   o.smem = uint32_t(smem);
   o.pack_off = uint32_t(off);
   r->ops.push_back(o);
+}
+
+void rec_note_flop(Recorder* r, double flop) {
+  r->ops.back().flop = flop;
+  r->tc_flop += flop;
+  r->tc_records += 1;
+}
+
+void rec_retract_flop(Recorder* r, double flop, int64_t records) {
+  r->tc_flop -= flop;
+  r->tc_records -= records;
 }
 
 void rec_wait(Recorder* r) { r->ex->wait(r); }

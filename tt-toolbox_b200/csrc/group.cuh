@@ -141,6 +141,9 @@ struct Recorder;
 // Record one launch of a grouped kernel (argument pack copied).
 void rec_group(Recorder* r, const GroupInfo* info, dim3 grid, dim3 block, size_t smem,
                const void* pack);
+// Marks the launch recorded last as a tensor-core GEMM of `flop` algorithmic
+// FLOPs (counted, and timed on request, by the executor).
+void rec_note_flop(Recorder* r, double flop);
 
 template <auto Body, int LB, bool COOP, class... A>
 struct Kern {

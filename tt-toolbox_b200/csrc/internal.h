@@ -109,6 +109,9 @@ using StreamOp = std::function<void(cudaStream_t, cusolverDnHandle_t)>;
 void rec_op(Recorder* r, StreamOp op);
 // Block until the executor has issued and completed everything recorded.
 void rec_wait(Recorder* r);
+// Takes back the FLOPs of recorded tensor-core GEMMs that the solve found
+// skipped on the device (Krylov steps queued past convergence).
+void rec_retract_flop(Recorder* r, double flop, int64_t records);
 class Allocator;
 // Device blocks of a recording context: each solve keeps the blocks it frees
 // for its own later allocations (its records are issued in its own order,

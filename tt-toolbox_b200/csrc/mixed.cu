@@ -440,6 +440,8 @@ struct Gmres32 {
           c->mv_count[1] -= skipped;
           c->mv_flops[1] -= fl * skipped;
           c->mv_bytes_lp -= op.bytes_per_matvec() * skipped;
+          // three recorded GEMMs per queued matvec (grouped: three-launch form)
+          if (c->rec) rec_retract_flop(c->rec, fl * skipped, 3 * int64_t(skipped));
           if (c->time_matvec) c->ev_void(seqs[done], c->ev_seq);
         }
       }

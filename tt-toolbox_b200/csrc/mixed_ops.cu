@@ -613,6 +613,7 @@ void launch_bn(Context* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t
                                          const int*>{},
               ta, tb, int(K), int(a_rows_pb), int(b_rows_pb), om, c->d_err + 1, c->skip);
     rec_group(c->rec, umma_info<BN, OB>(), grid, 128, smem, &p);
+    rec_note_flop(c->rec, 2.0 * double(M) * double(N) * double(K) * double(batch));
     c->launches += 1;
     return;
   }

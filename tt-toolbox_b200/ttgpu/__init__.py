@@ -90,11 +90,12 @@ class GroupStats(C.Structure):
                 ("ms_issue_wait", C.c_double), ("ms_total", C.c_double),
                 ("lanes_max", _i64), ("ms_record", C.c_double), ("allocs", _i64),
                 ("device_mallocs", _i64), ("ms_alloc", C.c_double),
-                ("ms_issue", C.c_double)]
+                ("ms_issue", C.c_double), ("tc_launches", _i64), ("tc_records", _i64),
+                ("tc_gflop", C.c_double), ("tc_ms", C.c_double)]
 
     def to_dict(self):
-        return {k: (float(getattr(self, k)) if k.startswith("ms") else int(getattr(self, k)))
-                for k, _ in self._fields_}
+        return {k: (float(getattr(self, k)) if t is C.c_double else int(getattr(self, k)))
+                for k, t in self._fields_}
 
 
 class AmenMvOpts(C.Structure):

@@ -174,8 +174,10 @@ def batch_bench(args):
         st = []
         ctx.sync()
         t = time.perf_counter()
+        gs = {}
         xs = amen_solve2_batch(dAs, dys, args.tol, workers=args.workers, ctx=ctx, stats=st,
-                               per_system=per, precision=prec)
+                               per_system=per, precision=prec, grouped=args.grouped,
+                               group_stats=gs)
         ctx.sync()
         wall = time.perf_counter() - t
         conv = sum(1 for s in st if s["sweeps"] and s["max_res"][s["sweeps"] - 1] < args.tol)
@@ -190,6 +192,10 @@ def batch_bench(args):
         ser = time.perf_counter() - t
         out[prec] = {"batch_s": wall, "converged": conv, "matvec_gflop": fl,
                      "matvec_tflops": fl / wall * 1e-3}
+        if args.grouped:
+            out[prec]["group"] = gs
+            if gs.get("tc_ms"):
+                out[prec]["tc_tflops_per_launch"] = gs["tc_gflop"] / gs["tc_ms"]
         if k:
             out[prec].update(serial_first_k_s=ser, serial_k=k,
                              batch_speedup_est=(ser / k * args.count) / wall)
@@ -376,6 +382,8 @@ def main():
     b = sub.add_parser("batch")
     b.add_argument("--count", type=int, default=512)
     b.add_argument("--workers", type=int, default=8)
+    b.add_argument("--grouped", action="store_true",
+                   help="grouped batch (workers = systems in flight, 0: all)")
     b.add_argument("--serial", type=int, default=64)
     b.add_argument("--tol", type=float, default=1e-8)
     b.add_argument("--precision", default="fp64,mixed")
