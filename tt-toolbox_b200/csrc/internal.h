@@ -35,9 +35,11 @@ struct Error {
 #define TTG_CUDA(call)                                                              \
   do {                                                                              \
     cudaError_t e_ = (call);                                                        \
-    if (e_ != cudaSuccess)                                                          \
+    if (e_ != cudaSuccess) {                                                        \
+      cudaGetLastError(); /* a refused call must not fail the next check */         \
       ::ttg::fail(TTG_ERR_CUDA, "%s:%d: %s: %s", __FILE__, __LINE__, #call,         \
                   cudaGetErrorString(e_));                                          \
+    }                                                                               \
   } while (0)
 
 #define TTG_SOLVER(call)                                                            \

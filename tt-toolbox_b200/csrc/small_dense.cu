@@ -14,6 +14,11 @@
 #include <cmath>
 #include <cstdlib>
 
+#include <map>
+#include <mutex>
+
+#include <cooperative_groups.h>
+
 #include "group.cuh"
 #include "small_dense.h"
 
@@ -316,6 +321,192 @@ TTG_BODY(k_jacobi_coop)(TTG_BLOCK, int n, const double* __restrict__ Ain,
   if (blockIdx.x == 0 && tid == 0 && sweep >= max_sweeps) atomicExch(sweep_err, 5);
 }
 TTG_COOP_KERNEL(k_jacobi_coop, JC_THREADS);
+
+// ---------------------------------------------------------------------------
+// Cluster Jacobi SVD for 160 < n <= 256 (the 256 x 256 R factors of the
+// rounding sweeps): one thread-block cluster of JK_CS CTAs holds A and V in
+// distributed shared memory, JK cols = ceil(n / JK_CS) columns per CTA, one
+// warp per column.  Columns never move: in each round of the round-robin
+// tournament the owners of a pair (P, Q) both read the two columns (one
+// local, one remote over DSMEM), compute the same rotation from the same
+// values in the same order, and each writes its own rotated column into the
+// other of two buffers.  One hardware cluster barrier per round replaces the
+// software grid barrier of k_jacobi_coop (the SVD is bound by the latency of
+// its ~2300 rounds, not by arithmetic).  Same rotation formula and stopping
+// rule as k_jacobi_svd; the rotated A and V go to global memory for
+// k_jacobi_finish.  All CTAs of a cluster are co-resident by construction,
+// and every CTA takes the same number of rounds (the stopping decision is
+// read by all from the same published values): the barriers cannot wait
+// for a CTA that is not running.
+// ---------------------------------------------------------------------------
+
+constexpr int JK_CS = 16;
+constexpr int JK_MAX_N = 256;
+constexpr int JK_MAX_COLS = JK_MAX_N / JK_CS;
+constexpr int JK_THREADS = 32 * JK_MAX_COLS;
+constexpr int JK_MAXR = JK_MAX_N / 32;  // column entries per lane
+
+// Partner of player p in round r of a circle-method tournament on ne (even)
+// players: player ne - 1 is fixed and meets r; the others pair as
+// p + q = 2 r (mod ne - 1).  Every pair meets once in ne - 1 rounds.
+__device__ __forceinline__ int jk_partner(int p, int r, int ne) {
+  const int m = ne - 1;
+  if (p == m) return r;
+  if (p == r) return m;
+  int q = 2 * r - p;
+  if (q < 0)
+    q += m;
+  else if (q >= m)
+    q -= m;
+  return q;
+}
+
+// Load of a double from the shared memory of a CTA of the cluster (address
+// from mapa: the partner's column, which may sit in this CTA too).
+__device__ __forceinline__ double ld_dsmem(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+  return v;
+}
+
+__global__ void __launch_bounds__(JK_THREADS, 1)
+    k_jacobi_cluster(int n, const double* __restrict__ Ain, int lda, int trans,
+                     double* __restrict__ Aout, double* __restrict__ Vout, int* err,
+                     int max_sweeps) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ double sm[];  // A[2][cpc][n], then V[2][cpc][n]
+  __shared__ double s_off[2][JK_CS];  // rank 0: per-CTA sweep maxima, by sweep parity
+  __shared__ double s_woff[JK_MAX_COLS];
+  const int rank = int(cl.block_rank());
+  const int ne = (n + 1) & ~1, cpc = (ne + JK_CS - 1) / JK_CS;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int64_t cn = int64_t(cpc) * n;
+  for (int64_t e = tid; e < cn; e += blockDim.x) {
+    const int j = int(e / n), i = int(e % n), p = rank * cpc + j;
+    if (p < n) {
+      sm[e] = trans ? Ain[p + int64_t(i) * lda] : Ain[i + int64_t(p) * lda];
+      sm[2 * cn + e] = (i == p) ? 1.0 : 0.0;
+    }
+  }
+  cl.sync();
+  const double tol = 4.0 * 2.220446049250313e-16, tol2 = tol * tol;
+  const int p = rank * cpc + w;
+  const bool own = w < cpc && p < n;
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
+  int cur = 0, sweep = 0;
+  for (sweep = 0; sweep < max_sweeps; ++sweep) {
+    double off = 0.0;
+    for (int r = 0; r < ne - 1; ++r) {
+      if (own) {
+        const int q = jk_partner(p, r, ne);
+        const double* ap = sm + cur * cn + int64_t(w) * n;
+        const double* vp = ap + 2 * cn;
+        double* na = sm + (cur ^ 1) * cn + int64_t(w) * n;
+        double* nv = na + 2 * cn;
+        if (q >= n) {  // dummy partner (odd n): the column stays
+          for (int i = lane; i < n; i += 32) {
+            na[i] = ap[i];
+            nv[i] = vp[i];
+          }
+        } else {
+          const int rq = q / cpc, jq = q - rq * cpc;
+          uint32_t rb;
+          asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(sbase), "r"(rq));
+          const uint32_t aq = rb + uint32_t(8 * (cur * cn + int64_t(jq) * n));
+          const uint32_t vq = aq + uint32_t(16 * cn);
+          // own column o (local), partner column t (over DSMEM)
+          double o[JK_MAXR], t[JK_MAXR], vo[JK_MAXR], vt[JK_MAXR];
+#pragma unroll
+          for (int k = 0; k < JK_MAXR; ++k) {
+            const int i = lane + 32 * k;
+            const bool in = i < n;
+            t[k] = in ? ld_dsmem(aq + 8 * i) : 0.0;
+            vt[k] = in ? ld_dsmem(vq + 8 * i) : 0.0;
+            o[k] = in ? ap[i] : 0.0;
+            vo[k] = in ? vp[i] : 0.0;
+          }
+          // al = |a_P|^2, be = |a_Q|^2, ga = <a_P, a_Q> for P < Q: both
+          // owners of the pair form the same sums in the same order.
+          const bool low = p < q;
+          double sp = 0.0, sq = 0.0, ga = 0.0;
+#pragma unroll
+          for (int k = 0; k < JK_MAXR; ++k) {
+            sp = fma(o[k], o[k], sp);
+            sq = fma(t[k], t[k], sq);
+            ga = low ? fma(o[k], t[k], ga) : fma(t[k], o[k], ga);
+          }
+          sp = wsum(sp);
+          sq = wsum(sq);
+          ga = wsum(ga);
+          const double al = low ? sp : sq, be = low ? sq : sp;
+          const double ab = al * be, g2 = ga * ga;
+          if (ab == 0.0 || g2 <= tol2 * ab) {
+#pragma unroll
+            for (int k = 0; k < JK_MAXR; ++k) {
+              const int i = lane + 32 * k;
+              if (i < n) {
+                na[i] = o[k];
+                nv[i] = vo[k];
+              }
+            }
+          } else {
+            off = fmax(off, g2 / ab);
+            const double dd = be - al, gg = 2.0 * ga;
+            const double sg = ((dd >= 0.0) == (gg > 0.0) || dd == 0.0) ? 1.0 : -1.0;
+            const double tt = sg * fabs(gg) / (fabs(dd) + sqrt(fma(dd, dd, gg * gg)));
+            const double c = rsqrt(fma(tt, tt, 1.0)), sn = c * tt;
+            // P' = c P - s Q, Q' = s P + c Q
+            if (low) {
+#pragma unroll
+              for (int k = 0; k < JK_MAXR; ++k) {
+                const int i = lane + 32 * k;
+                if (i < n) {
+                  na[i] = fma(c, o[k], -(sn * t[k]));
+                  nv[i] = fma(c, vo[k], -(sn * vt[k]));
+                }
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < JK_MAXR; ++k) {
+                const int i = lane + 32 * k;
+                if (i < n) {
+                  na[i] = fma(sn, t[k], c * o[k]);
+                  nv[i] = fma(sn, vt[k], c * vo[k]);
+                }
+              }
+            }
+          }
+        }
+      }
+      if (r == ne - 2) {  // last round of the sweep: publish this CTA's maximum
+        if (lane == 0 && w < JK_MAX_COLS) s_woff[w] = own ? off : 0.0;
+        __syncthreads();
+        if (tid == 0) {
+          double m = 0.0;
+          for (int j = 0; j < cpc; ++j) m = fmax(m, s_woff[j]);
+          double* so = cl.map_shared_rank(&s_off[sweep & 1][0], 0);
+          so[rank] = m;
+        }
+      }
+      cl.sync();
+      cur ^= 1;
+    }
+    const double* so = cl.map_shared_rank(&s_off[sweep & 1][0], 0);
+    double m = 0.0;
+    for (int k = 0; k < JK_CS; ++k) m = fmax(m, so[k]);
+    if (m <= tol2) break;
+  }
+  if (rank == 0 && tid == 0 && sweep >= max_sweeps) atomicExch(err, 5);
+  for (int64_t e = tid; e < cn; e += blockDim.x) {
+    const int j = int(e / n), i = int(e % n), pc = rank * cpc + j;
+    if (pc < n) {
+      Aout[i + int64_t(pc) * n] = sm[cur * cn + e];
+      Vout[i + int64_t(pc) * n] = sm[(2 + cur) * cn + e];
+    }
+  }
+  cl.sync();  // rank 0's published maxima are read until here
+}
 
 // ---------------------------------------------------------------------------
 // Block-cyclic form of the grid-wide Jacobi SVD: the n columns fall into
@@ -1067,6 +1258,55 @@ static bool jacobi_block_fits(int64_t n) {
          getenv_flag_on("TTG_JACOBI_BLOCK");
 }
 
+size_t jacobi_cluster_smem(int64_t n) {
+  const int64_t cpc = (((n + 1) & ~int64_t(1)) + JK_CS - 1) / JK_CS;
+  return sizeof(double) * 4 * size_t(cpc) * size_t(n);
+}
+
+// The cluster form runs where one CTA's shared memory is too small
+// (n > 160) up to JK_MAX_N, unless TTG_JACOBI_CLUSTER=0, when the device
+// can place a 16-CTA cluster with that shared memory (checked once per
+// device and size class: attributes set, cudaOccupancyMaxActiveClusters).
+bool jacobi_cluster_ok(Context* c, int64_t n) {
+  static const bool on = [] {
+    const char* e = getenv("TTG_JACOBI_CLUSTER");
+    return !(e && e[0] == '0');
+  }();
+  if (!on || n > JK_MAX_N || n < 2) return false;
+  const size_t smem = jacobi_cluster_smem(n);
+  static std::mutex mu;
+  static std::map<std::pair<int, size_t>, bool> seen;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair(c->device, smem);
+  auto it = seen.find(key);
+  if (it != seen.end()) return it->second;
+  // The attribute is set once to the largest size any n takes (setting it
+  // per size would lower it below a size already admitted).
+  bool ok = cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                 1) == cudaSuccess &&
+            cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(jacobi_cluster_smem(JK_MAX_N))) == cudaSuccess;
+  if (ok) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(JK_CS);
+    cfg.blockDim = dim3(JK_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = JK_CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    ok = cudaOccupancyMaxActiveClusters(&clusters, k_jacobi_cluster, &cfg) == cudaSuccess &&
+         clusters >= 1;
+  }
+  cudaGetLastError();  // a refused attribute or query leaves no sticky state
+  seen[key] = ok;
+  return ok;
+}
+
 void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double* U, double* S,
                     double* VT, bool via_transpose) {
   int trans = via_transpose ? 1 : 0;
@@ -1089,6 +1329,40 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
     memset_async(c, bar.p(), 0, 2 * sizeof(unsigned));
     launch(c, k_jacobi_block, blocks, JB_THREADS, bsm, int(n), A, int(lda), work.p(), V.p(),
            bar.p(), offmax.p(), c->d_err + 0, c->d_err + 3, trans, c->jacobi_max_sweeps);
+    launch(c, k_jacobi_finish, 1, SD_THREADS, 0, int(n), work.p(), V.p(), U, S, VT,
+           work.p() + int64_t(n) * n, trans);
+    TTG_CHECK_LAUNCH();
+    return;
+  }
+  if (mode == 0 && jacobi_cluster_ok(c, n)) {
+    // One 16-CTA cluster, A and V in distributed shared memory.
+    const size_t jsm = jacobi_cluster_smem(n);
+    const int ns = int(n), ilda = int(lda), sweeps = c->jacobi_max_sweeps;
+    double* Aw = work.p();
+    double* Vw = V.p();
+    int* err = c->d_err + 3;
+    auto issue = [=](cudaStream_t s) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(JK_CS);
+      cfg.blockDim = dim3(JK_THREADS);
+      cfg.dynamicSmemBytes = jsm;
+      cfg.stream = s;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = JK_CS;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      TTG_CUDA(cudaLaunchKernelEx(&cfg, k_jacobi_cluster, ns, A, ilda, trans, Aw, Vw, err,
+                                  sweeps));
+    };
+    if (c->rec) {
+      rec_op(c->rec, [issue](cudaStream_t s, cusolverDnHandle_t) { issue(s); });
+    } else {
+      issue(c->stream);
+    }
+    c->launches += 1;
     launch(c, k_jacobi_finish, 1, SD_THREADS, 0, int(n), work.p(), V.p(), U, S, VT,
            work.p() + int64_t(n) * n, trans);
     TTG_CHECK_LAUNCH();

@@ -31,6 +31,12 @@
     device time in that warm solve, the idle gaps between consecutive
     kernels, and the top launch shapes (grid, block, shared memory).
 
+``python -m ttgpu.kernel_bench svd --n 256,160,64``
+    the device SVD (``ttg_dense_svd``; square inputs go straight to the
+    Jacobi kernels) of seeded n x n Gaussian matrices: time per SVD, and the
+    time of one sweep alone (sweep limit 1, the call then reports its
+    non-convergence), so that time / sweep time estimates the sweeps run.
+
 ``python -m ttgpu.kernel_bench dgemm``
     cuBLAS FP64 GEMM throughput (torch.matmul, 8192^3) as the measured FP64
     tensor-core reference for the FP64 kernels.
@@ -304,6 +310,39 @@ def _kernel_table(run, top=30, top_shapes=25):
     return "\n".join(lines)
 
 
+def svd_bench(args):
+    from . import TTGError, dense_svd
+    ctx = Context(args.device)
+    rng = np.random.default_rng(args.seed)
+    out = {"workload": "device SVD of seeded n x n Gaussian matrices"}
+    for n in [int(v) for v in args.n.split(",")]:
+        A = rng.standard_normal((n, n))
+        dense_svd(A, ctx=ctx)
+        ts = []
+        for _ in range(args.reps):
+            t0 = time.perf_counter()
+            dense_svd(A, ctx=ctx)
+            ts.append(time.perf_counter() - t0)
+        ctx.set_option(Context.OPT_JACOBI_MAX_SWEEPS, 1)
+        t1 = []
+        try:
+            for _ in range(args.reps):
+                t0 = time.perf_counter()
+                try:
+                    dense_svd(A, ctx=ctx)
+                except TTGError:
+                    pass
+                t1.append(time.perf_counter() - t0)
+        finally:
+            ctx.set_option(Context.OPT_JACOBI_MAX_SWEEPS, 40)
+        med, med1 = float(np.median(ts)), float(np.median(t1))
+        out[str(n)] = {"ms": med * 1e3, "ms_one_sweep": med1 * 1e3,
+                       "sweeps_est": med / med1 if med1 > 0 else None,
+                       "us_per_round_est": med1 * 1e6 / max(1, n - 1 + n % 2)}
+    print(json.dumps(out))
+    ctx.close()
+
+
 def dgemm_bench(args):
     import torch
     n = args.size
@@ -400,12 +439,15 @@ def main():
     dg = sub.add_parser("dgemm")
     dg.add_argument("--size", type=int, default=8192)
     dg.add_argument("--reps", type=int, default=10)
-    for s in (m, r, g, b, am, dg):
+    sv = sub.add_parser("svd")
+    sv.add_argument("--n", default="256,200,160,128,96,64")
+    sv.add_argument("--reps", type=int, default=5)
+    for s in (m, r, g, b, am, dg, sv):
         s.add_argument("--device", type=int, default=0)
         s.add_argument("--seed", type=int, default=5)
     args = p.parse_args()
     {"matvec": matvec, "round": round_bench, "grad": grad_bench, "batch": batch_bench,
-     "amen": amen_bench, "dgemm": dgemm_bench}[args.what](args)
+     "amen": amen_bench, "dgemm": dgemm_bench, "svd": svd_bench}[args.what](args)
 
 
 if __name__ == "__main__":
