@@ -323,7 +323,7 @@ TTG_BODY(k_jacobi_coop)(TTG_BLOCK, int n, const double* __restrict__ Ain,
 TTG_COOP_KERNEL(k_jacobi_coop, JC_THREADS);
 
 // ---------------------------------------------------------------------------
-// Cluster Jacobi SVD for 160 < n <= 256 (the 256 x 256 R factors of the
+// Cluster Jacobi SVD for 113 < n <= 256 (the 256 x 256 R factors of the
 // rounding sweeps): one thread-block cluster of JK_CS CTAs holds A and V in
 // distributed shared memory, JK cols = ceil(n / JK_CS) columns per CTA, one
 // warp per column.  Columns never move: in each round of the round-robin
@@ -332,7 +332,11 @@ TTG_COOP_KERNEL(k_jacobi_coop, JC_THREADS);
 // values in the same order, and each writes its own rotated column into the
 // other of two buffers.  One hardware cluster barrier per round replaces the
 // software grid barrier of k_jacobi_coop (the SVD is bound by the latency of
-// its ~2300 rounds, not by arithmetic).  Same rotation formula and stopping
+// its ~2300 rounds, not by arithmetic): 0.27 us per cluster barrier against
+// several us per grid barrier, while reading the partner's two 256-entry
+// columns over DSMEM costs about 2.4 us per round (measured: per-thread
+// ld.shared::cluster; bulk shared::cta -> shared::cluster pushes of the
+// column blocks completing on the partner's mbarrier measured slower still).  Same rotation formula and stopping
 // rule as k_jacobi_svd; the rotated A and V go to global memory for
 // k_jacobi_finish.  All CTAs of a cluster are co-resident by construction,
 // and every CTA takes the same number of rounds (the stopping decision is
@@ -1263,8 +1267,9 @@ size_t jacobi_cluster_smem(int64_t n) {
   return sizeof(double) * 4 * size_t(cpc) * size_t(n);
 }
 
-// The cluster form runs where one CTA's shared memory is too small
-// (n > 160) up to JK_MAX_N, unless TTG_JACOBI_CLUSTER=0, when the device
+// The cluster form runs where one CTA's shared memory cannot hold both A
+// and V (n > 113) up to JK_MAX_N (measured 2.1x the grid-wide form's speed
+// at n = 120 and 144, 1.2x at 256), unless TTG_JACOBI_CLUSTER=0, when the device
 // can place a 16-CTA cluster with that shared memory (checked once per
 // device and size class: attributes set, cudaOccupancyMaxActiveClusters).
 bool jacobi_cluster_ok(Context* c, int64_t n) {
@@ -1334,7 +1339,7 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
     TTG_CHECK_LAUNCH();
     return;
   }
-  if (mode == 0 && jacobi_cluster_ok(c, n)) {
+  if ((mode == 0 || mode == 1) && jacobi_cluster_ok(c, n)) {
     // One 16-CTA cluster, A and V in distributed shared memory.
     const size_t jsm = jacobi_cluster_smem(n);
     const int ns = int(n), ilda = int(lda), sweeps = c->jacobi_max_sweeps;
