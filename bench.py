@@ -575,6 +575,10 @@ def run_batch(args, dist):
                        "true_residual_max_of_sample": max(rs), "gpu_launches": launches,
                        "recorded_launches": gs.get("records"),
                        "matvec_gflop": gflop, "matvec_tflops": gflop / wall * 1e-3}
+        if grouped:  # where the executor's time went (host ms, summed over threads)
+            forms[prec]["executor"] = {k: gs[k] for k in (
+                "flushes", "grouped_records", "ms_record", "ms_plan", "ms_issue",
+                "ms_issue_wait", "ms_alloc", "lanes_max", "tc_launches", "tc_records")}
         if prec == "mixed":
             res, conv = rs, c
     wall = forms["mixed"]["value"]

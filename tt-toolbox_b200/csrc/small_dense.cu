@@ -336,7 +336,10 @@ TTG_COOP_KERNEL(k_jacobi_coop, JC_THREADS);
 // several us per grid barrier, while reading the partner's two 256-entry
 // columns over DSMEM costs about 2.4 us per round (measured: per-thread
 // ld.shared::cluster; bulk shared::cta -> shared::cluster pushes of the
-// column blocks completing on the partner's mbarrier measured slower still).  Same rotation formula and stopping
+// column blocks completing on the partner's mbarrier measured slower still,
+// and so did a row-partitioned form that sends only the partial inner
+// products and the rotations across the cluster, with two barriers per
+// round: 235 against 195 ms for the config-2 SVD sweep).  Same rotation formula and stopping
 // rule as k_jacobi_svd; the rotated A and V go to global memory for
 // k_jacobi_finish.  All CTAs of a cluster are co-resident by construction,
 // and every CTA takes the same number of rounds (the stopping decision is
