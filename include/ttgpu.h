@@ -196,6 +196,25 @@ void ttg_amen_opts_default(ttg_amen_opts* opts);
 int ttg_amen_solve(ttg_tt A, ttg_tt y, double tol, const ttg_amen_opts* opts,
                    ttg_tt x0, ttg_tt z0, ttg_tt* x_out, ttg_amen_stats* stats);
 
+/* ---- ALS(t+z) solve ---------------------------------------------------------
+ * Replaces [x,testdata] = alstpz_solve(A, y, tol, 'name', value, ...)
+ * (solve/alstpz_solve.m:1) on its default path, kicktype 'svd': each of
+ * nswp sweeps rounds x to tol (:140), rounds the exact residual y - A x to
+ * rank kickrank (:189-195), appends it to x with weight zero (:199-201) and
+ * runs one ALS sweep of local solves (als_solve, :217-428: QR
+ * orthogonalisation, dense local solve below max_full_size, else the MEX
+ * local solver).  Every sweep runs (the reference has no stopping test).
+ * The options are ttg_amen_opts: nswp, max_full_size, local_restart,
+ * local_iters, kickrank, resid_damp, local_prec, precision, verb, seed are
+ * read; opts = NULL takes ttg_alstpz_opts_default (nswp 10, max_full_size
+ * 50, kickrank 4, :56-67).  x0 may be NULL: a right-orthogonal random TT of
+ * rank 2 is drawn on the device (tt_rand, :116-118).  stats (nullable):
+ * sweeps, per-sweep max_res / max_dx of the ALS sweeps (:371-373), local
+ * solves, Krylov steps, max rank, launches; ms_total is host-clock time. */
+void ttg_alstpz_opts_default(ttg_amen_opts* opts);
+int ttg_alstpz_solve(ttg_tt A, ttg_tt y, double tol, const ttg_amen_opts* opts, ttg_tt x0,
+                     ttg_tt* x_out, ttg_amen_stats* stats);
+
 /* ---- kernel-level entries (device pointers) --------------------------------
  * Local matvec y = (Phi1 x A x Phi2) x, the reference's bfun3
  * (solve/amen_solve2.m:924-951; twin fmex/solve3d.c:141-195).

@@ -23,6 +23,10 @@ Pinning status
   Jacobi): pinned against the reference's own C (``fmex/solve3d.c``) built
   by ``oracle/build_ref.py`` into ``oracle/_ref/`` and called through ctypes
   (``tests/test_oracle_ref.py``).
+* ``alstpz_solve``: the reference has no tests or golden vectors for it;
+  pinned by convergence of the true residual, the zero-weight enrichment
+  leaving the tensor unchanged, and the dense and GMRES local branches
+  agreeing (``tests/test_oracle_alstpz.py``).
 * ``amen_sum``: the reference has no tests or golden vectors for it; pinned
   by the exact linear combination at tight tolerance (full tensors at small
   d), rank bounds and tolerance-following errors (``tests/test_oracle_amen_sum.py``).

@@ -29,6 +29,15 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* A, ttg_tt_s* y, double tol, const ttg
                      ttg_tt_s* x0, ttg_tt_s* z0, ttg_amen_stats* stats,
                      Context* out_ctx = nullptr);
 
+// ALS(t+z) solve of solve/alstpz_solve.m (kicktype 'svd'): nswp sweeps of
+// rounding, residual enrichment of rank kickrank and one ALS sweep.  Uses
+// the fields nswp, max_full_size, local_restart, local_iters, kickrank,
+// resid_damp, local_prec, precision, verb and seed of o.  Stats: sweeps,
+// per-sweep max_res / max_dx, local solves, Krylov steps, max rank,
+// launches, host-clock time.
+ttg_tt_s* alstpz_solve(Context* c, ttg_tt_s* A, ttg_tt_s* y, double tol, const ttg_amen_opts& o,
+                       ttg_tt_s* x0, ttg_amen_stats* stats);
+
 // Right-orthogonal random TT of rank r (tt_rand(n,d,r,-1), core/tt_rand.m:40-62)
 // with entries from the device hash generator.
 ttg_tt_s* tt_rand_device(Context* c, const std::vector<int64_t>& n, int64_t r, uint64_t seed);

@@ -155,6 +155,31 @@ int ttg_amen_solve(ttg_tt A, ttg_tt y, double tol, const ttg_amen_opts* opts, tt
   TTG_API_END
 }
 
+void ttg_alstpz_opts_default(ttg_amen_opts* o) {
+  if (!o) return;
+  ttg_amen_opts_default(o);
+  o->nswp = 10;           // alstpz_solve.m:61
+  o->max_full_size = 50;  // :56
+  o->kickrank = 4;        // :67
+}
+
+int ttg_alstpz_solve(ttg_tt A, ttg_tt y, double tol, const ttg_amen_opts* opts, ttg_tt x0,
+                     ttg_tt* x_out, ttg_amen_stats* stats) {
+  TTG_API_BEGIN
+  TTG_REQUIRE(A && y && x_out, "NULL argument");
+  TTG_REQUIRE(std::isfinite(tol) && tol > 0, "tol must be > 0");
+  ttg_amen_opts o;
+  if (opts)
+    o = *opts;
+  else
+    ttg_alstpz_opts_default(&o);
+  if (stats) *stats = ttg_amen_stats{};
+  TTG_CUDA(cudaSetDevice(A->ctx->device));
+  if (x0) TTG_REQUIRE(x0->ctx == A->ctx, "x0 belongs to another context");
+  *x_out = alstpz_solve(A->ctx, A, y, tol, o, x0, stats);
+  TTG_API_END
+}
+
 int ttg_local_matvec(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2, int64_t ra1,
                      int64_t ra2, const double* Phi1, const double* A, const double* Phi2,
                      const double* x, double* y, int32_t precision) {

@@ -181,6 +181,8 @@ def lib():
                             C.POINTER(AmenSumOpts), _vp, _vp, C.POINTER(_vp), C.POINTER(_vp),
                             _p64]
     sigs["ttg_selftest_wait"] = [_vp, C.c_int32]
+    sigs["ttg_alstpz_solve"] = [_vp, _vp, C.c_double, C.POINTER(AmenOpts), _vp, C.POINTER(_vp),
+                                C.POINTER(AmenStats)]
     for name, args in sigs.items():
         f = getattr(L, name)
         f.argtypes = args
@@ -191,6 +193,8 @@ def lib():
     L.ttg_amen_mv_opts_default.restype = C.c_int
     L.ttg_amen_opts_default.argtypes = [C.POINTER(AmenOpts)]
     L.ttg_amen_opts_default.restype = None
+    L.ttg_alstpz_opts_default.argtypes = [C.POINTER(AmenOpts)]
+    L.ttg_alstpz_opts_default.restype = None
     _lib = L
     return L
 
@@ -563,6 +567,77 @@ def amen_solve2(A, y, tol, ctx=None, stats=None, trace=None, **opts):
     for h in owned:
         h.free()
     return host
+
+
+_ALSTPZ_KEYS = {"x0", "nswp", "max_full_size", "local_prec", "local_iters", "local_restart",
+                "kickrank", "kicktype", "ismex", "resid_damp", "symm", "verb", "precision",
+                "seed"}
+
+
+def alstpz_solve(A, y, tol, ctx=None, stats=None, **opts):
+    """``[x] = alstpz_solve(A, y, tol, 'name', value, ...)``
+    (``solve/alstpz_solve.m:1``, ALS(t+z), kicktype ``'svd'``).
+
+    Options follow ``alstpz_solve.m:55-104`` (defaults nswp 10,
+    max_full_size 50, kickrank 4, local_restart 40, local_iters 2,
+    resid_damp 2); ``kicktype 'als'`` and ``symm`` are not implemented and
+    raise ``TTGError``; ``ismex`` is accepted (the device local solver is
+    the MEX one).  ``precision`` 'fp64' or 'mixed' for the local solves.
+    ``stats`` (dict, optional) receives sweeps, per-sweep ``max_res`` and
+    ``max_dx``, local solves, Krylov steps, max rank."""
+    for k in opts:
+        if k.lower() not in _ALSTPZ_KEYS:
+            raise ValueError("Unrecognized option: %s" % k)
+    opts = {k.lower(): v for k, v in opts.items()}
+    if opts.get("kicktype", "svd") != "svd":
+        raise TTGError(7, "kicktype %r is not implemented (only 'svd')" % opts["kicktype"])
+    if opts.get("symm", False):
+        raise TTGError(7, "symm is not implemented")
+    lp = opts.get("local_prec", "")
+    if lp not in _LOCAL_PREC:
+        raise TTGError(7, "local_prec %r is unknown ('', 'cjacobi', 'ljacobi', 'rjacobi')"
+                       % (lp,))
+    ctx = ctx or (A.ctx if isinstance(A, DeviceTT) else default_context())
+    o = AmenOpts()
+    lib().ttg_alstpz_opts_default(C.byref(o))
+    for k in ("nswp", "max_full_size", "local_restart", "local_iters", "kickrank"):
+        if k in opts:
+            setattr(o, k, int(opts[k]))
+    if "resid_damp" in opts:
+        o.resid_damp = float(opts["resid_damp"])
+    if "verb" in opts:
+        o.verb = int(opts["verb"])
+    if "seed" in opts:
+        o.seed = int(opts["seed"])
+    o.local_prec = _LOCAL_PREC[lp]
+    o.precision = _PREC[opts.get("precision", "fp64")]
+    owned = []
+
+    def dev(t):
+        if t is None or isinstance(t, DeviceTT):
+            return t
+        h = DeviceTT.upload(ctx, t)
+        owned.append(h)
+        return h
+
+    try:
+        dA, dy, dx0 = dev(A), dev(y), dev(opts.get("x0"))
+        out = _vp()
+        st = AmenStats()
+        _check(lib().ttg_alstpz_solve(dA.h, dy.h, float(tol), C.byref(o),
+                                      dx0.h if dx0 is not None else None, C.byref(out),
+                                      C.byref(st)))
+        if stats is not None:
+            stats.update(st.to_dict())
+        res = DeviceTT(ctx, out)
+        if isinstance(y, DeviceTT):
+            return res
+        host = res.download()
+        res.free()
+        return host
+    finally:
+        for h in owned:
+            h.free()
 
 
 def amen_solve2_batch(As, ys, tol, x0s=None, z0s=None, workers=0, ctx=None, stats=None,
