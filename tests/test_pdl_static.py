@@ -19,29 +19,6 @@ def _sources():
     return {p.name: p.read_text() for p in sorted(CSRC.glob("*.cu"))}
 
 
-# Bodies that run set-up touching no global memory before the wait (so that
-# it overlaps the preceding grid's tail), with the tokens of their first
-# global accesses: pdl_begin() must come before every one of them.
-PRE_WAIT_SETUP = {
-    # TMEM allocation, mbarrier initialisation, prefetch of the tensor maps
-    # held in kernel parameters; then the skip flag, the TMA loads and the
-    # epilogue stores read or write global memory.
-    "umma_body": ("*skip", "tma_load_2d(", "om.base"),
-}
-
-
-def _pre_wait_ok(allsrc, fn):
-    m = re.search(r"__device__[^;{]*?\b%s\s*\([^{]*\{\n" % re.escape(fn), allsrc)
-    if m is None:
-        return False
-    rest = allsrc[m.end():]
-    end = rest.find("\n}\n")
-    body = rest[:end if end >= 0 else len(rest)]
-    w = body.find("pdl_begin();")
-    return w >= 0 and all(body.find(tok) < 0 or w < body.find(tok)
-                          for tok in PRE_WAIT_SETUP[fn])
-
-
 def test_every_pdl_launched_kernel_waits_first():
     src = _sources()
     names = set()
@@ -62,8 +39,6 @@ def test_every_pdl_launched_kernel_waits_first():
             d = re.search(r"__device__[^;{]*?\b%s\s*\([^{]*\{\n(.*)\n" % re.escape(call.group(1)),
                           allsrc)
             first = None if d is None else d.group(1).strip()
-            if call.group(1) in PRE_WAIT_SETUP and _pre_wait_ok(allsrc, call.group(1)):
-                continue
         if first != "pdl_begin();":
             bad.append((name, first))
     assert not bad, "kernels launched with launch() that do not start with pdl_begin(): %r" % bad

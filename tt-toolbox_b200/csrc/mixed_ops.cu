@@ -65,8 +65,10 @@ template <int BN, bool OUT_BF16>
 __device__ __forceinline__ void umma_body(TTG_BLOCK, const CUtensorMap* tmA,
                                           const CUtensorMap* tmB, int K, int a_rows_pb,
                                           int b_rows_pb, const OutMap& om, int* err,
-                                          const int* skip, bool prefetch_maps) {
+                                          const int* skip) {
+  pdl_begin();
   using namespace umma;
+  if (skip && *skip) return;  // queued Krylov step after convergence
   constexpr int B_BYTES = BN * UM_BK * 2;
   constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
   extern __shared__ uint8_t smem_raw[];
@@ -84,9 +86,6 @@ __device__ __forceinline__ void umma_body(TTG_BLOCK, const CUtensorMap* tmA,
   const int m0 = blockIdx.x * UM_BM, n0 = blockIdx.y * BN, bz = blockIdx.z;
   const int nk = (K + UM_BK - 1) / UM_BK;
 
-  // Set-up that touches no global memory runs before the wait on the
-  // preceding grid (programmatic dependent launch), overlapping its tail:
-  // TMEM allocation, barrier initialisation, descriptor prefetch.
   if (warp == 0) {
     tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
     tmem_relinquish();
@@ -100,19 +99,10 @@ __device__ __forceinline__ void umma_body(TTG_BLOCK, const CUtensorMap* tmA,
     fence_barrier_init();
     fence_proxy_async();
   }
-  if (prefetch_maps && threadIdx.x == 64) {
-    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmA)) : "memory");
-    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmB)) : "memory");
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  pdl_begin();
-  if (skip && *skip) {  // queued Krylov step after convergence: nothing was issued
-    if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
-    return;
-  }
 
   if (warp == 0 && lane == 0) {
     // TMA producer.
@@ -194,7 +184,7 @@ __global__ void __launch_bounds__(128, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 int K, int a_rows_pb, int b_rows_pb, OutMap om, int* err, const int* skip) {
   umma_body<BN, OUT_BF16>(blockIdx, gridDim, &tmA, &tmB, K, a_rows_pb, b_rows_pb, om, err,
-                          skip, true);
+                          skip);
 }
 
 // Grouped form: the argument packs (tensor maps first, 64-byte aligned) sit
@@ -214,7 +204,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_group(GroupArgs g) {
   asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&pk<1>(p))
                : "memory");
   umma_body<BN, OUT_BF16>(b, gd, &pk<0>(p), &pk<1>(p), pk<2>(p), pk<3>(p), pk<4>(p), pk<5>(p),
-                          pk<6>(p), pk<7>(p), false);
+                          pk<6>(p), pk<7>(p));
 }
 
 template <int BN, bool OUT_BF16>
