@@ -106,14 +106,31 @@ __device__ void ar_barrier(TTG_BLOCK, unsigned* bar, int* err, long long limit =
        idx += int64_t(gridDim.x) * blockDim.x)
 
 // part[c*nb + block] = block partial of V(:,c)'w, c < ncol.  red: AR_WARPS*(m+1) floats.
+// Columns go in groups of AR_COLS per pass over w, so that each thread has
+// AR_COLS independent loads in flight instead of one memory latency per
+// column; every column's sum is formed in the same order as one column per
+// pass would form it.
+constexpr int AR_COLS = 8;
 __device__ void partial_dots(TTG_BLOCK, const ArArgs& a, int ncol, double* part, float* red) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = 0; c < ncol; ++c) {
-    const float* Vc = a.V + int64_t(c) * a.sz;
-    float s = 0.f;
-    AR_LOOP(i, a.sz) s += Vc[i] * a.w[i];
-    s = warp_sumf(s);
-    if (lane == 0) red[warp * (a.m + 1) + c] = s;
+  for (int c0 = 0; c0 < ncol; c0 += AR_COLS) {
+    const int nc = ncol - c0 < AR_COLS ? ncol - c0 : AR_COLS;
+    float s[AR_COLS];
+#pragma unroll
+    for (int k = 0; k < AR_COLS; ++k) s[k] = 0.f;
+    AR_LOOP(i, a.sz) {
+      const float wi = a.w[i];
+#pragma unroll
+      for (int k = 0; k < AR_COLS; ++k)
+        if (k < nc) s[k] += a.V[int64_t(c0 + k) * a.sz + i] * wi;
+    }
+#pragma unroll
+    for (int k = 0; k < AR_COLS; ++k) {
+      if (k < nc) {
+        const float t = warp_sumf(s[k]);
+        if (lane == 0) red[warp * (a.m + 1) + c0 + k] = t;
+      }
+    }
   }
   __syncthreads();
   for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
