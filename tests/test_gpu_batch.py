@@ -106,4 +106,5 @@ def test_batch_config4_sample(ctx):
         if converged:
             Ao = TTMatrix.from_flat(A.n, A.m, A.r, A.core)
             yo = TT.from_flat(y.n, y.r, y.core)
-            assert true_residual(Ao, back(x), yo) < 1e-6
+            # the FP64 oracle on the same systems: at most 6.4e-9
+            assert true_residual(Ao, back(x), yo) <= 1e-8

@@ -76,7 +76,7 @@ def test_grouped_config4_sample(ctx):
             Ao = TTMatrix.from_flat(A.n, A.m, A.r, A.core)
             yo = TT.from_flat(y.n, y.r, y.core)
             xo = TT.from_flat(x.n, x.r, x.core)
-            assert true_residual(Ao, xo, yo) < 1e-7
+            assert true_residual(Ao, xo, yo) <= 1e-8  # the FP64 oracle: at most 6.4e-9
     assert gs["launches"] < gs["records"], gs
     assert gs["grouped_records"] > gs["records"] / 3, gs
     # The executor's count of BF16 GEMM work (recorded GEMMs less the skipped

@@ -90,7 +90,10 @@ def test_mixed_amen_laplace(ctx):
     A, y, x0, z0 = laplace_config(d=6, n=32)
     x, st = _solve(ctx, A, y, x0, z0, 1e-8, "mixed", rmax=30)
     assert st["max_res"][-1] < 1e-8
-    assert true_residual(A, x, y) < 1e-7
+    # the stated residual of the mixed form (the FP64 oracle: 2.8e-9)
+    res = true_residual(A, x, y)
+    print("mixed laplace d=6 n=32 true residual %.3e" % res)
+    assert res <= 1e-8
 
 
 def test_mixed_amen_aniso_matches_fp64_residual(ctx):
@@ -98,5 +101,7 @@ def test_mixed_amen_aniso_matches_fp64_residual(ctx):
     xm, stm = _solve(ctx, A, y, x0, z0, 1e-8, "mixed", rmax=64)
     xd, std = _solve(ctx, A, y, x0, z0, 1e-8, "fp64", rmax=64)
     rm, rd = true_residual(A, xm, y), true_residual(A, xd, y)
+    print("aniso d=6 n=32 true residual mixed %.3e fp64 %.3e" % (rm, rd))
     assert stm["max_res"][-1] < 1e-8
-    assert rm < 5e-8 and rm < 10 * rd
+    # the stated residual of the mixed form (the FP64 oracle: 9.0e-9)
+    assert rm <= 1e-8
