@@ -199,6 +199,8 @@ ttg_tt_s* alstpz_solve(Context* c, ttg_tt_s* A, ttg_tt_s* y, double tol, const t
                   o.local_iters >= 1 && o.kickrank >= 0 && o.resid_damp > 0,
               "invalid options");
   TTG_REQUIRE(o.local_prec >= 0 && o.local_prec <= 3, "local_prec %d is unknown", o.local_prec);
+  TTG_REQUIRE(3 * d <= 4096, "alstpz_solve: d = %lld cores is more than the per-sweep "
+              "residual read holds (1365)", (long long)d);
   TTG_REQUIRE(o.precision == TTG_FP64 || o.precision == TTG_MIXED, "unknown precision %d",
               o.precision);
   TTG_REQUIRE(o.local_prec <= 1 || o.precision == TTG_FP64,
