@@ -89,7 +89,7 @@ def test_batch_reports_failing_system(ctx):
     assert stats[2]["status"] == 0
 
 
-def test_batch_config4_sample(ctx):
+def test_batch_uneven_systems_sample(ctx):
     """A seeded sample of the batched workload (uneven d, n, rmax; tol 1e-8):
     every system either meets the stopping criterion or ran all sweeps at its
     rank cap, and the converged solutions have small true residuals."""

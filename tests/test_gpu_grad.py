@@ -217,7 +217,7 @@ def test_torch_autograd_harness(ctx):
                                     eps=FD_H, atol=1e-7, rtol=1e-6)
 
 
-def test_grad_config5_full_size(ctx):
+def test_grad_d12_n32_r64_full_size(ctx):
     """The differentiation workload at its full size (d=12, n=32, rank-64 x,
     rank-3 operator, rank-4 b, 1e6 samples from a hidden rank-8 TT plus
     N(0, 1e-3^2) noise) against the FP64 oracle."""

@@ -57,7 +57,7 @@ def test_grouped_matches_sequential_bitwise(ctx, precision):
         h.free()
 
 
-def test_grouped_config4_sample(ctx):
+def test_grouped_uneven_systems_sample(ctx):
     """A seeded sample of the batched workload with the default SM shares:
     every system meets the stopping criterion or stops at its rank cap or
     sweep limit, converged solutions have small true residuals, and the

@@ -145,7 +145,7 @@ def _round_strict(ctx, x, eps, rmax=None):
     return got, ref, info, st
 
 
-def test_round_parity_config2(ctx):
+def test_round_parity_d20_n16_r256(ctx):
     """Full size: d=20, n=16, the sum of four rank-64 Gaussian TTs (internal
     ranks 256 by concatenation) rounded at eps 1e-8."""
     x = round_config(d=20, n=16, r=64, terms=4, seed=2)
@@ -276,7 +276,7 @@ def _strict_parity(ctx, A, y, x0, z0, tol, **opts):
                 min_rank_margin=min(margins) if margins else None)
 
 
-def test_amen_parity_config1(ctx):
+def test_amen_parity_laplace_d8_n32(ctx):
     """The reference's CPU-runnable workload exactly as specified: d=8, n=32
     Laplacian, tol 1e-6, rmax 20, x0 a rank-2 TT with N(0,1) cores.  That
     x0 leaves a local residual 4.5e10 times the right-hand side at the
@@ -310,7 +310,7 @@ def test_amen_parity_aniso_rank3(ctx):
     _strict_parity(ctx, A, y, x0, z0, 1e-8, rmax=64, nswp=20)
 
 
-def test_amen_parity_config3(ctx):
+def test_amen_parity_aniso_d10_n64(ctx):
     """The headline workload at full size, FP64 form: d=10, n=64
     anisotropic diffusion + reaction (operator rank 3), rank-4 right-hand
     side, rmax 128, tol 1e-8."""

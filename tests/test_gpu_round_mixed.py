@@ -42,8 +42,8 @@ def test_round_mixed_decaying_spectrum(ctx):
     assert max(abs(int(a) - int(b)) for a, b in zip(got.r, ref.r)) <= 2
 
 
-def test_round_mixed_config2_shape(ctx):
-    """The config-2 input (sum of four rank-64 TTs, d=20, n=16) at eps 1e-8:
+def test_round_mixed_full_size(ctx):
+    """The full-size rounding input (sum of four rank-64 TTs, d=20, n=16) at eps 1e-8:
     all ranks stay 256 and the error is the BF16 operand rounding of the 38
     contractions (1.4e-2 when the same operand rounding is emulated in FP64
     on the host)."""

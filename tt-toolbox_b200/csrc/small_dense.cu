@@ -339,7 +339,8 @@ TTG_COOP_KERNEL(k_jacobi_coop, JC_THREADS);
 // column blocks completing on the partner's mbarrier measured slower still,
 // and so did a row-partitioned form that sends only the partial inner
 // products and the rotations across the cluster, with two barriers per
-// round: 235 against 195 ms for the config-2 SVD sweep).  Same rotation formula and stopping
+// round: 235 against 195 ms for the SVD sweep of rounding a d = 20, n = 16
+// sum of four rank-64 TTs).  Same rotation formula and stopping
 // rule as k_jacobi_svd; the rotated A and V go to global memory for
 // k_jacobi_finish.  All CTAs of a cluster are co-resident by construction,
 // and every CTA takes the same number of rounds (the stopping decision is
