@@ -265,11 +265,11 @@ int ttg_local_solve(ttg_context ctx, int64_t rx1, int64_t n, int64_t rx2,
  * Sizes whose intermediates (rx1*n*ra2*rx2 + rx1*ra1*n*rx2 doubles) exceed
  * it are rejected with TTG_ERR_INVALID.  stream: a cudaStream_t (NULL = the
  * legacy default stream) of the current device; the call returns after the
- * stream has finished (it synchronises the stream, so it cannot be recorded
- * into a CUDA graph).  The first call on a device looks up the array's
- * device address and caches it for the life of the process; after a
- * cudaDeviceReset the cached address is stale, so do not call it again in
- * that process.  All calls on a device share the array: calls whose GPU
+ * stream has finished.  The first call on a device looks up the array's
+ * device address and caches it for the life of the process, so make that
+ * first call before any stream capture; after a cudaDeviceReset the cached
+ * address is stale, so do not call it again in that process.  All calls on
+ * a device share the array: calls whose GPU
  * work overlaps (other streams, other host threads) race on it and must be
  * serialised by the caller. */
 int ttg_local_matvec_noalloc(void* stream, int64_t rx1, int64_t n, int64_t rx2,
