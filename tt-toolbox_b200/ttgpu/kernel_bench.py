@@ -176,15 +176,26 @@ def batch_bench(args):
     out = {"workload": "batch: %d Laplacian systems, d U{6..14}, n in {8,16,32,64}, "
                        "rmax U{8..64}, ones rhs, tol %g" % (args.count, args.tol),
            "workers": args.workers}
+    tables = {}
     for prec in args.precision.split(","):
         st = []
         ctx.sync()
         t = time.perf_counter()
         gs = {}
-        xs = amen_solve2_batch(dAs, dys, args.tol, workers=args.workers, ctx=ctx, stats=st,
-                               per_system=per, precision=prec, grouped=args.grouped,
-                               group_stats=gs)
-        ctx.sync()
+        res = {}
+
+        def run():
+            res["xs"] = amen_solve2_batch(dAs, dys, args.tol, workers=args.workers, ctx=ctx,
+                                          stats=st, per_system=per, precision=prec,
+                                          grouped=args.grouped, group_stats=gs)
+            ctx.sync()
+
+        table = None
+        if args.kernel_table:
+            table = _kernel_table(run)
+        else:
+            run()
+        xs = res["xs"]
         wall = time.perf_counter() - t
         conv = sum(1 for s in st if s["sweeps"] and s["max_res"][s["sweeps"] - 1] < args.tol)
         fl = sum(s["matvec_gflop"] for s in st)
@@ -198,6 +209,8 @@ def batch_bench(args):
         ser = time.perf_counter() - t
         out[prec] = {"batch_s": wall, "converged": conv, "matvec_gflop": fl,
                      "matvec_tflops": fl / wall * 1e-3}
+        if table is not None:
+            tables[prec] = table
         if args.grouped:
             out[prec]["group"] = gs
             if gs.get("tc_ms"):
@@ -206,6 +219,8 @@ def batch_bench(args):
             out[prec].update(serial_first_k_s=ser, serial_k=k,
                              batch_speedup_est=(ser / k * args.count) / wall)
     print(json.dumps(out))
+    for prec, tab in tables.items():
+        print("\n# kernels of the batch, precision %s\n%s" % (prec, tab))
     for h in dAs + dys:
         h.free()
     ctx.close()
@@ -274,7 +289,23 @@ def _kernel_table(run, top=30, top_shapes=25):
 
     def short(name):
         name = name.replace("(anonymous namespace)::", "").replace("ttg::", "")
-        return re.sub(r"^void ", "", name.split("(")[0])
+        name = re.sub(r"^void ", "", name)
+        # cut at the parameter list: the first '(' outside template brackets
+        depth = 0
+        for i, ch in enumerate(name):
+            if ch == "<":
+                depth += 1
+            elif ch == ">":
+                depth -= 1
+            elif ch == "(" and depth == 0:
+                name = name[:i]
+                break
+        # grouped / plain entries of a kernel body: name the body
+        m = re.match(r"k_(plain|group)_(?:no)?lb<&\(?(\w+?)_body(<[^>]*>)?", name)
+        if m:
+            return "%s%s%s" % (m.group(2), m.group(3) or "", " [grouped]" if m.group(1) == "group"
+                                else "")
+        return name
 
     tot, cnt = collections.defaultdict(float), collections.Counter()
     shp, shc = collections.defaultdict(float), collections.Counter()
@@ -423,6 +454,8 @@ def main():
     b.add_argument("--workers", type=int, default=8)
     b.add_argument("--grouped", action="store_true",
                    help="grouped batch (workers = systems in flight, 0: all)")
+    b.add_argument("--kernel-table", action="store_true",
+                   help="run under the CUDA activity tracer and summarise the kernels")
     b.add_argument("--serial", type=int, default=64)
     b.add_argument("--tol", type=float, default=1e-8)
     b.add_argument("--precision", default="fp64,mixed")
