@@ -152,6 +152,14 @@ __device__ void reduce_parts(TTG_BLOCK, const double* part, int ncol, double* ou
   __syncthreads();
 }
 
+// Shared memory of k_arnoldi: hp (m+1 doubles), ht (m+2), red (AR_WARPS
+// (m+1) floats), then 2 m doubles for the rotations of the Givens update,
+// 8-byte aligned.
+__device__ __forceinline__ double* red_d(double* shd, int m) {
+  const size_t off = sizeof(double) * 2 * (m + 2) + sizeof(float) * AR_WARPS * (m + 1);
+  return reinterpret_cast<double*>(reinterpret_cast<char*>(shd) + ((off + 7) & ~size_t(7)));
+}
+
 // One Arnoldi step for column j: w -= V h twice (CGS2), normalise into
 // V(:, j+1), Givens update of H(:, j) and g; scal[0] = |g_{j+1}|.
 TTG_BODY(k_arnoldi)(TTG_BLOCK, ArArgs a, int j) {
@@ -202,31 +210,45 @@ TTG_BODY(k_arnoldi)(TTG_BLOCK, ArArgs a, int j) {
     Vn[i] = v;
     put_x(a, i, v);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blockIdx.x == 0) {
+    // The Givens update runs on one thread over a shared-memory copy of the
+    // column (ht) and of the previous rotations: a chain of dependent
+    // shared-memory accesses instead of global ones.  Same operations in the
+    // same order as on the global arrays.
+    double* cl = red_d(shd, a.m);
+    double* sl = cl + a.m;
+    for (int i = threadIdx.x; i < j; i += blockDim.x) {
+      cl[i] = a.cs[i];
+      sl[i] = a.sn[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      ht[j + 1] = nrm;
+      for (int i = 0; i < j; ++i) {  // previous rotations
+        const double x = ht[i], y = ht[i + 1];
+        ht[i] = cl[i] * x + sl[i] * y;
+        ht[i + 1] = -sl[i] * x + cl[i] * y;
+      }
+      const double x = ht[j], y = ht[j + 1];
+      const double rho = sqrt(x * x + y * y);
+      const double c0 = rho > 0.0 ? x / rho : 1.0, s0 = rho > 0.0 ? y / rho : 0.0;
+      a.cs[j] = c0;
+      a.sn[j] = s0;
+      ht[j] = rho;
+      ht[j + 1] = 0.0;
+      a.g[j + 1] = -s0 * a.g[j];
+      a.g[j] = c0 * a.g[j];
+      a.scal[0] = fabs(a.g[j + 1]);
+      a.scal[1] = nrm;
+      if (a.scal[0] <= a.scal[4]) {
+        a.stop[1] = j;
+        __threadfence();
+        a.stop[0] = 1;
+      }
+    }
+    __syncthreads();
     double* Hj = a.H + int64_t(a.m + 1) * j;
-    for (int c = 0; c < ncol; ++c) Hj[c] = ht[c];
-    Hj[j + 1] = nrm;
-    for (int i = 0; i < j; ++i) {  // previous rotations
-      const double x = Hj[i], y = Hj[i + 1];
-      Hj[i] = a.cs[i] * x + a.sn[i] * y;
-      Hj[i + 1] = -a.sn[i] * x + a.cs[i] * y;
-    }
-    const double x = Hj[j], y = Hj[j + 1];
-    const double rho = sqrt(x * x + y * y);
-    const double c0 = rho > 0.0 ? x / rho : 1.0, s0 = rho > 0.0 ? y / rho : 0.0;
-    a.cs[j] = c0;
-    a.sn[j] = s0;
-    Hj[j] = rho;
-    Hj[j + 1] = 0.0;
-    a.g[j + 1] = -s0 * a.g[j];
-    a.g[j] = c0 * a.g[j];
-    a.scal[0] = fabs(a.g[j + 1]);
-    a.scal[1] = nrm;
-    if (a.scal[0] <= a.scal[4]) {
-      a.stop[1] = j;
-      __threadfence();
-      a.stop[0] = 1;
-    }
+    for (int c = threadIdx.x; c <= j + 1; c += blockDim.x) Hj[c] = ht[c];
   }
 }
 TTG_COOP_KERNEL(k_arnoldi, AR_THREADS);
@@ -279,12 +301,22 @@ TTG_COOP_KERNEL(k_ar_init, AR_THREADS);
 // x += V(:, 0:k) y with H(0:k,0:k) y = g(0:k) (upper triangular after Givens).
 TTG_BODY(k_ar_update)(TTG_BLOCK, ArArgs a, int k, float* x) {
   pdl_begin();
+  // y (m+1), then H's leading k x k block (ld k) and g (k), copied in
+  // parallel so that the back-substitution on one thread reads shared memory.
   extern __shared__ double y[];
+  double* Hs = y + (a.m + 1);
+  double* gs = Hs + int64_t(k) * k;
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+    const int row = e % k, col = e / k;
+    Hs[e] = a.H[row + int64_t(a.m + 1) * col];
+  }
+  for (int e = threadIdx.x; e < k; e += blockDim.x) gs[e] = a.g[e];
+  __syncthreads();
   if (threadIdx.x == 0) {
     for (int row = k - 1; row >= 0; --row) {
-      double v = a.g[row];
-      for (int col = row + 1; col < k; ++col) v -= a.H[row + int64_t(a.m + 1) * col] * y[col];
-      const double d = a.H[row + int64_t(a.m + 1) * row];
+      double v = gs[row];
+      for (int col = row + 1; col < k; ++col) v -= Hs[row + k * col] * y[col];
+      const double d = Hs[row + k * row];
       y[row] = d != 0.0 ? v / d : 0.0;
     }
   }
@@ -372,7 +404,8 @@ struct Gmres32 {
   }
 
   size_t arnoldi_smem() const {
-    return sizeof(double) * (2 * (m + 2)) + sizeof(float) * AR_WARPS * (m + 1) + 16;
+    return sizeof(double) * (2 * (m + 2)) + sizeof(float) * AR_WARPS * (m + 1) + 8 +
+           sizeof(double) * 2 * m + 16;
   }
 
 
@@ -466,7 +499,8 @@ struct Gmres32 {
       const int k = conv ? j + 1 : m;
       steps += k;
       c->krylov_hint = k;
-      launch(c, k_ar_update, blocks, AR_THREADS, sizeof(double) * (m + 1), a, k, x);
+      launch(c, k_ar_update, blocks, AR_THREADS,
+             sizeof(double) * (size_t(m + 1) + size_t(k) * k + size_t(k)), a, k, x);
       TTG_CHECK_LAUNCH();
       if (conv) break;
     }
