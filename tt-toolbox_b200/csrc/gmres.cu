@@ -25,6 +25,19 @@ namespace {
 constexpr int HH_THREADS = 256;
 constexpr long long BAR_SPIN_LIMIT = 1LL << 24;
 
+// Restart lengths up to which k_hh_tail / k_hh_correct stage their serial
+// sections in shared memory (3 nrestart + 1, nrestart^2 + 2 nrestart doubles).
+constexpr int64_t HH_STAGE_MAX = 1024;
+constexpr int64_t HH_CORRECT_STAGE_MAX = 64;
+
+size_t hh_tail_smem(int64_t nrestart) {
+  return nrestart <= HH_STAGE_MAX ? sizeof(double) * size_t(3 * nrestart + 1) : 0;
+}
+size_t hh_correct_smem(int64_t nrestart) {
+  return sizeof(double) * size_t(nrestart + (nrestart <= HH_CORRECT_STAGE_MAX
+                                                 ? nrestart * nrestart + nrestart : 0));
+}
+
 struct HhArgs {
   int64_t sz;
   int64_t nrestart;
@@ -214,32 +227,58 @@ TTG_BODY(k_hh_tail)(TTG_BLOCK, HhArgs a, int64_t j) {
     }
   }
   grid_barrier(blockIdx, gridDim, a.bar, a.err);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    // Givens rotations to the top of w (:445-449)
-    for (int64_t i = 0; i < j; ++i) {
-      const double b = __ldcg(w + i), b1 = __ldcg(w + i + 1);
-      const double c0 = a.J[2 * i], c1 = a.J[2 * i + 1];
-      w[i] = c0 * b + c1 * b1;
-      w[i + 1] = -c1 * b + c0 * b1;
+  if (blockIdx.x == 0) {
+    // Givens rotations to the top of w (:445-449) on one thread.  With
+    // staging (restart length up to HH_STAGE_MAX) the chain of dependent
+    // accesses runs on shared-memory copies of w's top entries and of the
+    // rotators, copied in and out by the block; the same operations in the
+    // same order as on the global arrays.
+    extern __shared__ double tsm[];
+    const bool staged = a.nrestart <= HH_STAGE_MAX;
+    const int64_t top = a.nrestart + 1 < sz ? a.nrestart + 1 : sz;
+    double* wl = staged ? tsm : w;
+    double* Jl = staged ? tsm + (a.nrestart + 1) : a.J;
+    if (staged) {
+      for (int64_t e = threadIdx.x; e < top; e += blockDim.x) wl[e] = __ldcg(w + e);
+      for (int64_t e = threadIdx.x; e < 2 * j; e += blockDim.x) Jl[e] = a.J[e];
+      __syncthreads();
     }
-    if (j < sz - 1) {  // new rotator (:454-465)
-      const double wj = __ldcg(w + j), wj1 = __ldcg(w + j + 1);
-      const double rho = sqrt(wj * wj + wj1 * wj1);
-      const double c0 = wj / rho, c1 = wj1 / rho;
-      a.J[2 * j] = c0;
-      a.J[2 * j + 1] = c1;
-      a.tau[j + 1] = -c1 * a.tau[j];
-      a.tau[j] = c0 * a.tau[j];
-      w[j] = rho;
-      w[j + 1] = 0.0;
+    if (threadIdx.x == 0) {
+      for (int64_t i = 0; i < j; ++i) {
+        const double b = staged ? wl[i] : __ldcg(w + i);
+        const double b1 = staged ? wl[i + 1] : __ldcg(w + i + 1);
+        const double c0 = Jl[2 * i], c1 = Jl[2 * i + 1];
+        wl[i] = c0 * b + c1 * b1;
+        wl[i + 1] = -c1 * b + c0 * b1;
+      }
+      if (j < sz - 1) {  // new rotator (:454-465)
+        const double wj = staged ? wl[j] : __ldcg(w + j);
+        const double wj1 = staged ? wl[j + 1] : __ldcg(w + j + 1);
+        const double rho = sqrt(wj * wj + wj1 * wj1);
+        const double c0 = wj / rho, c1 = wj1 / rho;
+        a.J[2 * j] = c0;
+        a.J[2 * j + 1] = c1;
+        a.tau[j + 1] = -c1 * a.tau[j];
+        a.tau[j] = c0 * a.tau[j];
+        wl[j] = rho;
+        wl[j + 1] = 0.0;
+      }
+      if (!staged)
+        for (int64_t k = 0; k < a.nrestart; ++k)
+          a.R[k + j * a.nrestart] = (k < sz) ? __ldcg(w + k) : 0.0;
+      const double curres = fabs(a.tau[j + 1]) / a.scal[0];
+      a.scal[1] = curres;
+      if (curres < a.tol) {  // (:476) later queued steps see the flag and return
+        a.stop[1] = int(j);
+        __threadfence();
+        a.stop[0] = 1;
+      }
     }
-    for (int64_t k = 0; k < a.nrestart; ++k) a.R[k + j * a.nrestart] = (k < sz) ? __ldcg(w + k) : 0.0;
-    const double curres = fabs(a.tau[j + 1]) / a.scal[0];
-    a.scal[1] = curres;
-    if (curres < a.tol) {  // (:476) later queued steps see the flag and return
-      a.stop[1] = int(j);
-      __threadfence();
-      a.stop[0] = 1;
+    if (staged) {
+      __syncthreads();
+      for (int64_t k = threadIdx.x; k < a.nrestart; k += blockDim.x)
+        a.R[k + j * a.nrestart] = (k < sz) ? wl[k] : 0.0;
+      for (int64_t e = threadIdx.x; e < top; e += blockDim.x) w[e] = wl[e];
     }
   }
 }
@@ -247,14 +286,27 @@ TTG_COOP_KERNEL(k_hh_tail, HH_THREADS);
 
 // Triangular solve + correction sol += P_0..P_j (sum y_i e_i)  (:487-507)
 TTG_BODY(k_hh_correct)(TTG_BLOCK, HhArgs a, int64_t j, int64_t ni) {
+  // y (nrestart); with staging also R's leading ni x ni block (ld ni) and
+  // tau, copied by the block so that the back-substitution on one thread
+  // reads shared memory (same operations, same order).
   extern __shared__ double y[];
   unsigned parity = 0;
   const int64_t sz = a.sz;
+  const bool staged = a.nrestart <= HH_CORRECT_STAGE_MAX;
+  double* Rs = y + a.nrestart;
+  double* ts = Rs + ni * ni;
+  if (staged) {
+    for (int64_t e = threadIdx.x; e < ni * ni; e += blockDim.x)
+      Rs[e] = a.R[(e % ni) + (e / ni) * a.nrestart];
+    for (int64_t e = threadIdx.x; e < ni; e += blockDim.x) ts[e] = a.tau[e];
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     for (int64_t row = ni - 1; row >= 0; --row) {
-      double v = a.tau[row];
-      for (int64_t col = row + 1; col < ni; ++col) v -= a.R[row + col * a.nrestart] * y[col];
-      y[row] = v / a.R[row + row * a.nrestart];
+      double v = staged ? ts[row] : a.tau[row];
+      for (int64_t col = row + 1; col < ni; ++col)
+        v -= (staged ? Rs[row + col * ni] : a.R[row + col * a.nrestart]) * y[col];
+      y[row] = v / (staged ? Rs[row + row * ni] : a.R[row + row * a.nrestart]);
     }
   }
   __syncthreads();
@@ -299,8 +351,8 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
   DBuf<double> small(c, (nrestart + 1) + 2 * nrestart + nrestart * nrestart + 8);
   const int blocks = std::min(
       std::min(coop_blocks(c, k_hh_init.fn(), 0, sz), coop_blocks(c, k_hh_build.fn(), 0, sz)),
-      std::min(coop_blocks(c, k_hh_tail.fn(), 0, sz),
-               coop_blocks(c, k_hh_correct.fn(), sizeof(double) * nrestart, sz)));
+      std::min(coop_blocks(c, k_hh_tail.fn(), hh_tail_smem(nrestart), sz),
+               coop_blocks(c, k_hh_correct.fn(), hh_correct_smem(nrestart), sz)));
   DBuf<double> part(c, 2 * blocks);
   DBuf<unsigned> bar(c, 4);
   DBuf<int> stop(c, 4);
@@ -372,7 +424,7 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
       for (int64_t jj = j; jj < jend; ++jj) {
         launch(c, k_hh_build, blocks, HH_THREADS, 0, a, jj);
         apply(w.p(), w2.p());
-        launch(c, k_hh_tail, blocks, HH_THREADS, 0, a, jj);
+        launch(c, k_hh_tail, blocks, HH_THREADS, hh_tail_smem(nrestart), a, jj);
       }
       Probe p;
       probe(p);
@@ -396,7 +448,7 @@ GmresResult gmres_hh_f64(Context* c, const ApplyFn& apply, const double* rhs, in
     } else {
       ni = j + 1;
     }
-    launch(c, k_hh_correct, blocks, HH_THREADS, sizeof(double) * nrestart, a, j, ni);
+    launch(c, k_hh_correct, blocks, HH_THREADS, hh_correct_smem(nrestart), a, j, ni);
     if (curres < tol) break;
   }
   res.relres = curres;
