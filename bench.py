@@ -515,7 +515,7 @@ BATCH_METRIC = "batched AMEn: independent Laplacian systems to tol 1e-8, total t
 
 
 def run_batch(args, dist):
-    """Config 4: ``count`` independent seeded Laplacian systems (d U{6..14},
+    """``count`` independent seeded Laplacian systems (d U{6..14},
     n in {8,16,32,64}, rmax U{8..64}, all-ones right-hand sides, tol 1e-8)
     through the grouped batch ``ttg_amen_solve_grouped`` (every system's
     launches merged kernel by kernel into grouped launches), mixed precision

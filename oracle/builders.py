@@ -67,7 +67,7 @@ def kron_sum_operator(mats, react=None):
 
 
 def laplace_config(d=8, n=32, x_rank=2, seed=1):
-    """Config 1: ``d``-dim Laplacian (rank 2), RHS ``tt_ones``, x0 seeded N(0,1) rank-``x_rank``."""
+    """``d``-dim Laplacian (rank 2), RHS ``tt_ones``, x0 seeded N(0,1) rank-``x_rank``."""
     rng = np.random.default_rng(seed)
     A = kron_sum_operator([lap1d(n)] * d)
     y = tt_ones(n, d)
@@ -77,7 +77,7 @@ def laplace_config(d=8, n=32, x_rank=2, seed=1):
 
 
 def aniso_config(d=10, n=64, rhs_rank=4, seed=3, react_scale=1.0):
-    """Config 3: anisotropic diffusion + separable reaction, operator rank 3.
+    """Anisotropic diffusion + separable reaction, operator rank 3.
 
     ``A = sum_k c_k (n+1)^2 tridiag(-1,2,-1)_k + sigma * (M x .. x M)`` with
     ``c_k ~ U[0.5, 2]`` seeded, ``M = tridiag(1,4,1)/6`` and
@@ -98,7 +98,7 @@ def aniso_config(d=10, n=64, rhs_rank=4, seed=3, react_scale=1.0):
 
 
 def round_config(d=20, n=16, r=64, terms=4, seed=2):
-    """Config 2: sum of ``terms`` independent rank-``r`` Gaussian TTs (true rank <= terms*r).
+    """Sum of ``terms`` independent rank-``r`` Gaussian TTs (true rank <= terms*r).
 
     Core entries are N(0, sigma^2) with ``sigma = 1/sqrt(r_k * n)`` (the
     left rank of the core), so every term has O(1) norm growth per core.

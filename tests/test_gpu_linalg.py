@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 
 SHAPES = [(64, 64), (132, 132), (4096, 64), (256, 4), (4, 256), (37, 53), (1, 5), (5, 1),
           (8448, 132), (160, 150), (256, 256), (1000, 201), (600, 600), (4096, 256),
-          (301, 301), (2000, 384)]
+          (301, 301), (2000, 384), (77, 77), (113, 113), (500, 90)]
 
 
 @pytest.mark.parametrize("m,n", SHAPES)

@@ -244,7 +244,7 @@ def _dump(trace, otrace, info, st, err=None):
 
 
 def _strict_parity(ctx, A, y, x0, z0, tol, **opts):
-    """The north-star bar for the FP64 form: the GPU solve records every
+    """The parity bar for the FP64 form: the GPU solve records every
     discrete decision (kept rank and Krylov step count of each local step,
     the per-sweep stopping test); the oracle replays the solve, checks each
     decision against its own, adopts the GPU's choice only at near ties and

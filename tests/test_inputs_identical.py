@@ -44,6 +44,6 @@ def test_aniso_workload_identical(d, n, seed):
 
 
 def test_round_workload_identical():
-    """Config 2 at full size: d=20, n=16, four rank-64 terms."""
+    """The rounding input at full size: d=20, n=16, four rank-64 terms."""
     _same_tt(workloads.round_input(d=20, n=16, r=64, terms=4, seed=2),
              builders.round_config(d=20, n=16, r=64, terms=4, seed=2))

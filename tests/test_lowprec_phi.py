@@ -1,6 +1,6 @@
 """Precision the interface (Phi) contractions need (CPU, oracle only).
 
-The north star asks for BF16/TF32 Phi/core contractions with FP64
+The mixed form wants BF16/TF32 Phi/core contractions with FP64
 refinement of the local residual.  This measures it on the oracle: the
 operands of every ``compute_next_Phi`` product (``solve/amen_solve2.m:834-920``)
 are rounded to BF16, TF32 or FP32 (FP64 accumulation, everything else FP64)

@@ -45,6 +45,61 @@ __device__ __forceinline__ int rr_player(int k, int r, int ne) {
   return k == 0 ? 0 : 1 + x;
 }
 
+// Sum over the G lanes of a warp (G = 32) or half-warp (G = 16); all 32
+// lanes take part in every shuffle.
+template <int G>
+__device__ __forceinline__ double gsum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One Jacobi rotation of the column pair p < q of A (n x n, ld n) and of V,
+// on the G lanes gl = 0..G-1 of a warp or half-warp.  live = false keeps the
+// group in the shuffles and touches nothing.  Returns max(off, ga^2/(al be))
+// when the pair is rotated, else off.
+template <int G>
+__device__ __forceinline__ double jacobi_pair(double* A, double* V, int n, int p, int q, int gl,
+                                              bool live, double tol2, double off) {
+  double* ap = A + int64_t(p) * n;
+  double* aq = A + int64_t(q) * n;
+  double al = 0.0, be = 0.0, ga = 0.0;
+  if (live) {
+    for (int i = gl; i < n; i += G) {
+      const double x = ap[i], y = aq[i];
+      al += x * x;
+      be += y * y;
+      ga += x * y;
+    }
+  }
+  al = gsum<G>(al);
+  be = gsum<G>(be);
+  ga = gsum<G>(ga);
+  // |ga| <= tol sqrt(al be), compared in squares (no square root on the
+  // path of a pair that needs no rotation)
+  const double ab = al * be, g2 = ga * ga;
+  if (!live || ab == 0.0 || g2 <= tol2 * ab) return off;
+  off = fmax(off, g2 / ab);
+  // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = (be - al) / (2 ga),
+  // written with one division: t = sign(zeta) |g| / (|dd| + hypot(dd, g))
+  // for dd = be - al, g = 2 ga (sign(zeta) = +1 when dd = 0).
+  const double dd = be - al, gg = 2.0 * ga;
+  const double sg = ((dd >= 0.0) == (gg > 0.0) || dd == 0.0) ? 1.0 : -1.0;
+  const double t = sg * fabs(gg) / (fabs(dd) + sqrt(dd * dd + gg * gg));
+  const double c = rsqrt(1.0 + t * t), s = c * t;
+  double* vp = V + int64_t(p) * n;
+  double* vq = V + int64_t(q) * n;
+  for (int i = gl; i < n; i += G) {
+    const double x = ap[i], y = aq[i];
+    ap[i] = c * x - s * y;
+    aq[i] = s * x + c * y;
+    const double vx = vp[i], vy = vq[i];
+    vp[i] = c * vx - s * vy;
+    vq[i] = s * vx + c * vy;
+  }
+  return off;
+}
+
 // Singular values = column norms of the rotated A, ranked descending
 // (stable on index); U = A diag(1/s), VT = V^T in that order.  With trans the
 // rotated matrix is the transpose of the input (X = In^T = Ux S Vx^T), so the
@@ -119,51 +174,39 @@ TTG_BODY(k_jacobi_svd)(TTG_BLOCK, int n, const double* __restrict__ Ain,
   for (sweep = 0; sweep < max_sweeps; ++sweep) {
     double off = 0.0;
     for (int r = 0; r < ne - 1; ++r) {
-      for (int pr = warp; pr < ne / 2; pr += SD_WARPS) {
-        int p = rr_player(pr, r, ne), q = rr_player(ne - 1 - pr, r, ne);
-        if (p > q) {
-          const int t = p;
-          p = q;
-          q = t;
+      if (ne / 2 > SD_WARPS && ne / 2 <= 2 * SD_WARPS) {
+        // 32 < pairs <= 64: one half-warp per pair, the whole round at once
+        // (a warp per pair would take two pairs in turn on most warps).
+        const int pr = tid >> 4;
+        int p = 0, q = 0;
+        bool live = false;
+        if (pr < ne / 2) {
+          p = rr_player(pr, r, ne);
+          q = rr_player(ne - 1 - pr, r, ne);
+          if (p > q) {
+            const int t = p;
+            p = q;
+            q = t;
+          }
+          live = q < n;  // else a dummy player
+          if (!live) p = q = 0;
         }
-        if (q >= n) continue;  // dummy player
-        double* ap = A + int64_t(p) * n;
-        double* aq = A + int64_t(q) * n;
-        double al = 0.0, be = 0.0, ga = 0.0;
-        for (int i = lane; i < n; i += 32) {
-          const double x = ap[i], y = aq[i];
-          al += x * x;
-          be += y * y;
-          ga += x * y;
-        }
-        al = wsum(al);
-        be = wsum(be);
-        ga = wsum(ga);
-        // |ga| <= tol sqrt(al be), compared in squares (no square root on
-        // the path of a pair that needs no rotation)
-        const double ab = al * be, g2 = ga * ga;
-        if (ab == 0.0 || g2 <= tol2 * ab) continue;
-        off = fmax(off, g2 / ab);
-        // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = (be - al) / (2 ga),
-        // written with one division: t = sign(zeta) |g| / (|dd| + hypot(dd, g))
-        // for dd = be - al, g = 2 ga (sign(zeta) = +1 when dd = 0).
-        const double dd = be - al, gg = 2.0 * ga;
-        const double sg = ((dd >= 0.0) == (gg > 0.0) || dd == 0.0) ? 1.0 : -1.0;
-        const double t = sg * fabs(gg) / (fabs(dd) + sqrt(dd * dd + gg * gg));
-        const double c = rsqrt(1.0 + t * t), s = c * t;
-        double* vp = V + int64_t(p) * n;
-        double* vq = V + int64_t(q) * n;
-        for (int i = lane; i < n; i += 32) {
-          const double x = ap[i], y = aq[i];
-          ap[i] = c * x - s * y;
-          aq[i] = s * x + c * y;
-          const double vx = vp[i], vy = vq[i];
-          vp[i] = c * vx - s * vy;
-          vq[i] = s * vx + c * vy;
+        off = jacobi_pair<16>(A, V, n, p, q, lane & 15, live, tol2, off);
+      } else {
+        for (int pr = warp; pr < ne / 2; pr += SD_WARPS) {
+          int p = rr_player(pr, r, ne), q = rr_player(ne - 1 - pr, r, ne);
+          if (p > q) {
+            const int t = p;
+            p = q;
+            q = t;
+          }
+          if (q >= n) continue;  // dummy player
+          off = jacobi_pair<32>(A, V, n, p, q, lane, true, tol2, off);
         }
       }
       __syncthreads();
     }
+    off = fmax(off, __shfl_xor_sync(0xffffffffu, off, 16));  // both half-warps
     if (lane == 0) s_off[warp] = off;
     __syncthreads();
     if (tid == 0) {
@@ -722,18 +765,19 @@ TTG_BODY(k_house_qr)(TTG_BLOCK, int m, int n, const double* __restrict__ Ain,
     const int i = e % k, c = e / k;
     R[i + int64_t(c) * ldr] = (i <= c) ? A[i + int64_t(c) * m] : 0.0;
   }
-  // Q = H_0 H_1 ... H_{k-1} I(:, 0:k), applied right to left into global Q.
-  for (int e = tid; e < m * k; e += SD_THREADS) {
-    const int i = e % m, c = e / m;
-    Q[e] = (i == c) ? 1.0 : 0.0;
-  }
   __syncthreads();
+  // Q = H_0 H_1 ... H_{k-1} I(:, 0:k), applied right to left in place of the
+  // reflectors (LAPACK dorg2r's scheme): when H_j is applied, columns c > j
+  // of A already hold Q's columns (zero in rows <= j, as I's are), so H_j
+  // updates them, and then column j becomes H_j e_j = e_j - tau_j v_j, with
+  // its rows above j cleared.  The arithmetic is that of applying H_j to I's
+  // column j (w = tau_j exactly), so Q matches a product formed on I.
   for (int j = k - 1; j >= 0; --j) {
     const double tj = tau[j];
-    const double* v = A + int64_t(j) * m;
+    double* v = A + int64_t(j) * m;
     if (tj != 0.0) {
-      for (int c = j + warp; c < k; c += SD_WARPS) {
-        double* qc = Q + int64_t(c) * m;
+      for (int c = j + 1 + warp; c < k; c += SD_WARPS) {
+        double* qc = A + int64_t(c) * m;
         double w = 0.0;
         for (int i = j + lane; i < m; i += 32) w += (i == j ? 1.0 : v[i]) * qc[i];
         w = wsum(w) * tj;
@@ -741,7 +785,11 @@ TTG_BODY(k_house_qr)(TTG_BLOCK, int m, int n, const double* __restrict__ Ain,
       }
     }
     __syncthreads();
+    for (int i = tid; i < m; i += SD_THREADS)
+      v[i] = i < j ? 0.0 : (i == j ? 1.0 - tj : 0.0 - tj * v[i]);
+    __syncthreads();
   }
+  for (int e = tid; e < m * k; e += SD_THREADS) Q[e] = A[e];
 }
 TTG_KERNEL(k_house_qr, SD_THREADS);
 
@@ -904,20 +952,30 @@ TTG_BODY(k_chol_inv)(TTG_BLOCK, int n, const double* __restrict__ G,
   // that step), removes column j from the trailing lower triangle and row j
   // from the rows of X below it (with the pivot's reciprocal squared), and
   // writes row j of R = L' and column j of Rinv = X' scaled: one barrier
-  // per column.
+  // per column.  The step's n columns -- trailing columns k of L (rows k..n)
+  // and columns cc <= j of X (rows j+1..n) -- go one per warp, lanes down
+  // the rows, so no thread divides an index or idles on the upper triangle;
+  // every element takes the same products in the same order as an
+  // element-per-thread loop.
+  const int lane = tid & 31, warp = tid >> 5;
   for (int j = 0; j < n; ++j) {
     const double d = L[j + n * j];
     const double dj = d > 0.0 ? sqrt(d) : 1.0;
     if (tid == 0 && !(d > 0.0)) s_bad = 1;
     const double inv = 1.0 / dj, inv2 = inv * inv;
     const int m = n - j - 1;
-    for (int e = tid; e < m * m; e += SD_THREADS) {
-      const int i = j + 1 + e % m, k = j + 1 + e / m;
-      if (k <= i) L[i + n * k] -= L[i + n * j] * L[k + n * j] * inv2;
-    }
-    for (int e = tid; e < m * (j + 1); e += SD_THREADS) {
-      const int i = j + 1 + e % m, cc = e / m;
-      X[i + n * cc] -= L[i + n * j] * X[j + n * cc] * inv2;
+    const double* lj = L + n * j;
+    for (int u = warp; u < n; u += SD_WARPS) {
+      if (u < m) {
+        const int k = j + 1 + u;
+        const double lk = lj[k];
+        double* col = L + n * k;
+        for (int i = k + lane; i < n; i += 32) col[i] -= lj[i] * lk * inv2;
+      } else {
+        double* col = X + n * (u - m);
+        const double xj = col[j];
+        for (int i = j + 1 + lane; i < n; i += 32) col[i] -= lj[i] * xj * inv2;
+      }
     }
     for (int i = j + tid; i < n; i += SD_THREADS)
       R[j + int64_t(n) * i] = (i == j) ? dj : L[i + n * j] * inv;
@@ -1276,6 +1334,21 @@ size_t jacobi_cluster_smem(int64_t n) {
 // at n = 120 and 144, 1.2x at 256), unless TTG_JACOBI_CLUSTER=0, when the device
 // can place a 16-CTA cluster with that shared memory (checked once per
 // device and size class: attributes set, cudaOccupancyMaxActiveClusters).
+// Outside a grouped batch it also takes the sizes from
+// TTG_JACOBI_CLUSTER_MIN_N (default 48) up, which the one-CTA kernel could
+// hold: a lone solve waits on each SVD (whole SVD of a Gaussian n x n matrix,
+// cluster against one CTA: 2.0 against 5.7 ms at n = 113, 0.89 against 1.39
+// at 64, 0.68 against 0.84 at 48, even at 32), while a grouped batch fills
+// the GPU with concurrent systems and wants the one-CTA kernel's single SM.
+int64_t jacobi_cluster_min_n() {
+  static const int64_t v = [] {
+    const char* e = getenv("TTG_JACOBI_CLUSTER_MIN_N");
+    const long long x = e ? atoll(e) : 0;
+    return int64_t(x >= 2 ? x : 48);
+  }();
+  return v;
+}
+
 bool jacobi_cluster_ok(Context* c, int64_t n) {
   static const bool on = [] {
     const char* e = getenv("TTG_JACOBI_CLUSTER");
@@ -1343,7 +1416,8 @@ void jacobi_svd_f64(Context* c, int64_t n, const double* A, int64_t lda, double*
     TTG_CHECK_LAUNCH();
     return;
   }
-  if ((mode == 0 || mode == 1) && jacobi_cluster_ok(c, n)) {
+  if ((mode == 0 || mode == 1 || (!c->rec && n >= jacobi_cluster_min_n())) &&
+      jacobi_cluster_ok(c, n)) {
     // One 16-CTA cluster, A and V in distributed shared memory.
     const size_t jsm = jacobi_cluster_smem(n);
     const int ns = int(n), ilda = int(lda), sweeps = c->jacobi_max_sweeps;
