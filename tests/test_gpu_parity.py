@@ -347,6 +347,18 @@ def test_amen_errors(ctx):
     assert e.value.code == 7
 
 
+def test_initial_guess_border_ranks_refused(ctx):
+    """Both solvers start their interfaces from 1 x 1 blocks: an initial
+    guess with a border rank other than 1 is refused, not solved."""
+    A, y, _, _ = laplace_config(d=3, n=4)
+    rng = np.random.default_rng(3)
+    bad = ttgpu.TensorTrain([4, 4, 4], [2, 2, 2, 1], rng.standard_normal(2 * 4 * 2 * 2 + 2 * 4))
+    with pytest.raises(ttgpu.TTGError, match="border ranks"):
+        ttgpu.amen_solve2(host_mat(A), host_tt(y), 1e-6, x0=bad, ctx=ctx)
+    with pytest.raises(ttgpu.TTGError, match="border ranks"):
+        ttgpu.alstpz_solve(host_mat(A), host_tt(y), 1e-6, x0=bad, ctx=ctx)
+
+
 def test_round_rank_deficient_concatenation(ctx):
     """x + x has exactly half the concatenated ranks: the QR sweep factors
     exactly rank-deficient tall cores (rows 1024, 32 columns, the shifted

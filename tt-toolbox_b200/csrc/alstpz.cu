@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <memory>
 #include <vector>
 
 #include "amen.h"
@@ -163,7 +164,7 @@ void als_sweep(Context* c, ttg_tt_s* A, ttg_tt_s* y, double tol, const ttg_amen_
 // A new tensor handle holding the cores crx (ranks rx).
 ttg_tt_s* assemble_tt(Context* c, const std::vector<int64_t>& n, const std::vector<int64_t>& rx,
                       const std::vector<DBuf<double>>& crx) {
-  auto* t = new ttg_tt_s();
+  std::unique_ptr<ttg_tt_s> t(new ttg_tt_s());
   t->ctx = c;
   t->d = int64_t(n.size());
   t->is_matrix = false;
@@ -173,9 +174,10 @@ ttg_tt_s* assemble_tt(Context* c, const std::vector<int64_t>& n, const std::vect
   for (int64_t k = 0; k < t->d; ++k) t->ps[k + 1] = t->ps[k] + rx[k] * n[k] * rx[k + 1];
   t->numel = t->ps[t->d];
   t->core = static_cast<double*>(c->alloc->get(sizeof(double) * std::max<int64_t>(t->numel, 1)));
-  for (int64_t k = 0; k < t->d; ++k)
-    copy_f64(c, t->ps[k + 1] - t->ps[k], crx[k].p(), t->core + t->ps[k]);
-  return t;
+  Owned guard(t.release());  // freed with its core if a copy launch fails
+  for (int64_t k = 0; k < guard.t->d; ++k)
+    copy_f64(c, guard.t->ps[k + 1] - guard.t->ps[k], crx[k].p(), guard.t->core + guard.t->ps[k]);
+  return guard.release();
 }
 
 }  // namespace
@@ -210,6 +212,7 @@ ttg_tt_s* alstpz_solve(Context* c, ttg_tt_s* A, ttg_tt_s* y, double tol, const t
   if (x0) {
     TTG_REQUIRE(!x0->is_matrix && x0->d == d && x0->ctx == c, "x0 shape mismatch");
     for (int64_t k = 0; k < d; ++k) TTG_REQUIRE(x0->n[k] == y->n[k], "x0 mode size mismatch");
+    TTG_REQUIRE(x0->r[0] == 1 && x0->r[d] == 1, "x0 border ranks must be 1");
     require_finite(x0, "x0");
   }
   const auto t0 = std::chrono::steady_clock::now();

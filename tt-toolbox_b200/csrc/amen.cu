@@ -284,16 +284,22 @@ ttg_tt_s* amen_solve(Context* c, ttg_tt_s* Ah, ttg_tt_s* yh, double tol, const t
   prof.start(c);
   prof.mark("init");
   // Initial guesses (:222-224, :250-252).
+  // Given guesses are checked before the random ones are drawn, so a
+  // rejected call holds no device tensor.
+  if (x0h) {
+    TTG_REQUIRE(x0h->d == d && !x0h->is_matrix, "x0 shape mismatch");
+    for (int64_t k = 0; k < d; ++k) TTG_REQUIRE(x0h->n[k] == n[k], "x0 mode size mismatch");
+    TTG_REQUIRE(x0h->r[0] == 1 && x0h->r[d] == 1, "x0 border ranks must be 1");
+  }
+  if (use_z && z0h) {
+    TTG_REQUIRE(z0h->d == d && !z0h->is_matrix, "z0 shape mismatch");
+    for (int64_t k = 0; k < d; ++k) TTG_REQUIRE(z0h->n[k] == n[k], "z0 mode size mismatch");
+    TTG_REQUIRE(z0h->r[0] == 1 && z0h->r[d] == 1, "z0 border ranks must be 1");
+  }
   ttg_tt_s* x0own = nullptr;
   ttg_tt_s* z0own = nullptr;
   if (!x0h) x0h = x0own = tt_rand_device(c, n, 2, o.seed);
   if (use_z && !z0h) z0h = z0own = tt_rand_device(c, n, kickrank, o.seed ^ 0x5bd1e995ull);
-  TTG_REQUIRE(x0h->d == d && !x0h->is_matrix, "x0 shape mismatch");
-  for (int64_t k = 0; k < d; ++k) TTG_REQUIRE(x0h->n[k] == n[k], "x0 mode size mismatch");
-  if (use_z) {
-    TTG_REQUIRE(z0h->d == d && !z0h->is_matrix, "z0 shape mismatch");
-    for (int64_t k = 0; k < d; ++k) TTG_REQUIRE(z0h->n[k] == n[k], "z0 mode size mismatch");
-  }
 
   std::vector<int64_t> rx = x0h->r, ry = yh->r, ra = Ah->r, rz;
   std::vector<Core> crx(d), crz(d);
